@@ -1,0 +1,265 @@
+/*
+ * midas_b200.h -- C ABI of the B200-native radial-integration ("caking") engine.
+ *
+ * This is the drop-in boundary for the MIDAS caking hot path.  Every entry point
+ * takes plain pointers and sizes; no PyTorch or CUDA C++ types cross it (a CUDA
+ * stream is passed as an opaque `void*`, NULL meaning the legacy default stream).
+ *
+ * Reference interfaces replaced (paths inside the MIDAS repository):
+ *   mi_plan_create       <- build_csr()                packages/midas_integrate/midas_integrate/kernels.py:242
+ *                           + ReadBins/PrecomputeOffsets FF_HEDM/src/IntegratorFitPeaksGPUStream.cu:742,901
+ *                           + initialize_PerFrameArr_Area_kernel  IntegratorFitPeaksGPUStream.cu:817
+ *   mi_plan_set_dark     <- dark upload (average of dark frames) IntegratorFitPeaksGPUStream.cu:2191-2238
+ *   mi_integrate_batch   <- integrate() + profile_1d()  kernels.py:416,567 (one frame per call there;
+ *                           here F frames per launch), and the submit path of the GPU stream,
+ *                           IntegratorFitPeaksGPUStream.cu:2806-2870
+ *   mi_integrate_plain   <- ProcessImageGPU + integrate_noMapMask + calculate_1D_profile_kernel(s),
+ *                           IntegratorFitPeaksGPUStream.cu:1633,975,1162,1256 (one frame per launch,
+ *                           thread per sorted bin: the reference's own GPU algorithm)
+ *   mi_cast_dark         <- process_direct_kernel<T>   IntegratorFitPeaksGPUStream.cu:1148
+ *   mi_fit_batch         <- fitPeaks()                 FF_HEDM/src/PeakFit.c:275 (called per frame at
+ *                           IntegratorFitPeaksGPUStream.cu:2630-2702) and fit_peaks()
+ *                           packages/midas_integrate/midas_integrate/peakfit.py:334
+ *   mi_map_build         <- mapper_build_map()         FF_HEDM/src/MapperCore.c:45 (DetectorMapper)
+ *   mi_last_error        <- (new) the reference aborts the process on any CUDA error
+ *                           (gpuAssert, IntegratorFitPeaksGPUStream.cu:299-308); this library
+ *                           returns a status code and keeps a thread-local message instead.
+ *
+ * Status codes: 0 = ok, negative = error (see MI_E_*).  No entry point ever calls exit().
+ */
+#ifndef MIDAS_B200_H
+#define MIDAS_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------- */
+#define MI_OK 0
+#define MI_E_ARG (-1)        /* bad argument (null pointer, size, unknown code)          */
+#define MI_E_MAP (-2)        /* malformed map: negative count, offset past end of Map.bin */
+#define MI_E_OOM (-3)        /* device or host allocation failed                         */
+#define MI_E_CUDA (-4)       /* CUDA runtime error (message has the CUDA error string)   */
+#define MI_E_TIMEOUT (-5)    /* a bounded device wait expired                            */
+#define MI_E_UNSUPPORTED (-6)/* valid request this build does not implement              */
+#define MI_E_RANGE (-7)      /* size beyond a documented maximum                         */
+
+/* ---- integration modes (MI/kernels.py module docstring) ----------------- */
+#define MI_MODE_FLOOR 0      /* truncated (y,z) lookup, 1 term per Map.bin record        */
+#define MI_MODE_BILINEAR 1   /* bilinear sample at (y,z), 4 corner terms, coalesced      */
+#define MI_MODE_GRADIENT 2   /* bilinear at (y,z) shifted by -deltaR along the radius    */
+
+/* ---- normalisation semantics (the reference has two) ----- */
+#define MI_SEM_PY 0          /* midas_integrate kernels.py: normaliser = sum of in-bounds
+                                areaWeight; invalid bins -> 0 when normalising, raw sum
+                                otherwise (kernels.py:311-318, 461-471)                  */
+#define MI_SEM_GPUSTREAM 1   /* IntegratorFitPeaksGPUStream.cu:1038-1049: normaliser = sum
+                                of ALL areaWeight of the bin; bins with area <= 1e-9 -> 0 */
+
+/* ---- frame dtype codes: the socket protocol's codes (MI/image.py:24-30) -- */
+#define MI_DT_U8 0
+#define MI_DT_U16 1
+#define MI_DT_U32 2
+#define MI_DT_I64 3
+#define MI_DT_F32 4
+#define MI_DT_F64 5
+/* code 6 (hybrid) is decoded on the host into u16 + overflow patch before upload */
+#define MI_DT_I32 7          /* extension: PILATUS-style signed 32-bit frames            */
+
+/* ---- maps ---------------------------------------------------------------- */
+/* One Map.bin record, 24 bytes, layout of struct data / MapPixelData
+ * (IntegratorFitPeaksGPUStream.cu:234-240, FF_HEDM/src/MapperCore.h:19-25). */
+typedef struct {
+  float y;           /* pixel column (+ sub-pixel centroid offset)            */
+  float z;           /* pixel row                                             */
+  double frac;       /* corrected weight = area / (solid angle x polarisation) */
+  float deltaR;      /* R(sub-pixel centre) - R(bin centre), px               */
+  float areaWeight;  /* geometric pixel-bin overlap area                      */
+} mi_map_record;
+
+typedef struct {
+  const mi_map_record *records; /* host pointer: Map.bin data (header skipped)          */
+  int64_t n_records;
+  const int32_t *nmap;          /* host pointer: nMap.bin {count, offset} pairs, n_bins */
+  int32_t n_r, n_eta;           /* bins are R-major: bin = r * n_eta + eta              */
+  int32_t ny, nz;               /* NrPixelsY, NrPixelsZ; flat pixel = z * ny + y        */
+  double bc_y, bc_z;            /* beam centre (px), used by MI_MODE_GRADIENT           */
+} mi_map_desc;
+
+typedef struct {
+  int32_t mode;            /* MI_MODE_*                                              */
+  int32_t normalize;       /* Normalize key (1 = divide by bin area)                  */
+  int32_t semantics;       /* MI_SEM_*                                               */
+  int32_t tile_rows;       /* rows (R bins) per tile strip; 0 = autotune              */
+  int32_t tile_pixels;     /* max staged pixels per tile; 0 = autotune                */
+  int32_t frames_per_lane; /* 1, 2 or 4 frames per thread; 0 = autotune               */
+} mi_plan_opts;
+
+typedef struct {
+  int64_t n_bins, n_r, n_eta;
+  int64_t nnz;             /* terms of the selected mode after coalescing             */
+  int64_t n_records;       /* Map.bin records read                                   */
+  int64_t n_tiles, n_items;/* staging tiles, scheduled work items                     */
+  int64_t staged_pixels;   /* sum over tiles of staged pixels (halo included)          */
+  int64_t ref_pixels;      /* distinct pixels the map references                       */
+  int64_t map_bytes;       /* device bytes of the tiled map read per batch             */
+  int64_t device_bytes;    /* all device memory the plan holds                        */
+  int64_t oob_records;     /* records whose truncated (y,z) is off the detector        */
+  int32_t tile_rows, tile_pixels, frames_per_lane;
+  int32_t run_len;         /* register-run length of the tile encoding                 */
+} mi_plan_info;
+
+typedef struct mi_plan mi_plan; /* opaque, immutable after creation except for the dark */
+
+/* Build a device-resident plan for one (map, binning, mode).  Validates the map
+ * (counts >= 0, offset + count <= n_records) like build_csr (kernels.py:288-301). */
+int mi_plan_create(const mi_map_desc *map, const mi_plan_opts *opts, int device,
+                   mi_plan **out);
+/* Set (or clear, dark == NULL) the per-pixel dark (ny*nz floats, host pointer).
+ * The reference subtracts (float)raw - dark[pixel] (IntegratorFitPeaksGPUStream.cu:1156). */
+int mi_plan_set_dark(mi_plan *plan, const float *dark_host);
+int mi_plan_get_info(const mi_plan *plan, mi_plan_info *info);
+int mi_plan_bytes(const mi_plan *plan, size_t *bytes);
+void mi_plan_destroy(mi_plan *plan);
+
+/* Cake F frames in one launch.
+ *   frames:      device pointer, F frames of ny*nz pixels, frame f at frames + f*frame_stride
+ *                elements (frame_stride >= ny*nz)
+ *   cake:        device [F][n_r][n_eta] float32, or NULL to skip the 2D output
+ *   lineout_aw:  device [F][n_r] float64, area-weighted eta average (calculate_1D_profile_kernel,
+ *                IntegratorFitPeaksGPUStream.cu:1162), or NULL
+ *   lineout_sm:  device [F][n_r] float64, simple mean over valid bins (…_simple_mean_kernel,
+ *                IntegratorFitPeaksGPUStream.cu:1256), or NULL
+ *   stream:      cudaStream_t or NULL
+ * Results for a frame do not depend on F or on the other frames in the batch. */
+int mi_integrate_batch(mi_plan *plan, const void *frames, int dtype, int n_frames,
+                       int64_t frame_stride, float *cake, double *lineout_aw,
+                       double *lineout_sm, void *stream);
+
+/* The reference's own GPU algorithm, one frame per launch: cast/dark kernel, one thread per
+ * bin in heaviest-first order with FP32 accumulation and on-the-fly bilinear sampling in
+ * gradient mode, FP64 cake, then the two profile kernels.  This is the plain baseline. */
+int mi_integrate_plain(mi_plan *plan, const void *frame, int dtype, double *cake,
+                       double *lineout_aw, double *lineout_sm, void *stream);
+
+/* Kernel (c) on a cake the caller already holds: area-weighted and simple-mean eta
+ * reductions of F frames of a [F][n_r][n_eta] cake (float32 with cake_dtype = MI_DT_F32,
+ * float64 with MI_DT_F64), with the plan's in-bounds bin areas (profile_1d,
+ * packages/midas_integrate/midas_integrate/kernels.py:567). */
+int mi_profile_batch(mi_plan *plan, const void *cake, int cake_dtype, int n_frames,
+                     double *lineout_aw, double *lineout_sm, void *stream);
+
+/* Kernel (a) on its own: out[f][p] = (float)frames[f][p] - dark[p] (dark may be NULL),
+ * 128-bit vector loads.  frames and out are device pointers. */
+int mi_cast_dark(const void *frames, int dtype, int64_t n_pixels, int n_frames,
+                 const float *dark, float *out, void *stream);
+
+/* ---- peak fitting ----------------------------------------------------------
+ * One warp per (frame, peak) window; Levenberg-Marquardt in FP32 with an FP64
+ * normal-equation Cholesky solve.  Models:
+ *   MI_FIT_PV  : I(x) = bg0 + bg1*xn + h*[eta*L(x) + (1-eta)*G(x)], FWHM shared, 6 params
+ *                (center, height, fwhm, eta, bg0, bg1); xn = 2(x-x_lo)/(x_hi-x_lo)-1
+ *   MI_FIT_TCH : area-normalised TCH pseudo-Voigt + 2-term Chebyshev background,
+ *                params (area, center, sig, gam, bg0, bg1) as pf_calculate_model
+ *                (FF_HEDM/src/PeakFit.c:50-92)
+ * Output per (frame, peak): MI_FIT_NOUT doubles
+ *   [area, center, sig, gam, fwhm, eta, chi2_dof, height, bg0, bg1, two_theta_deg]
+ * (first seven exactly the PF_PARAMS_PER_PEAK layout of PeakFit.h). */
+#define MI_FIT_PV 0
+#define MI_FIT_TCH 1
+#define MI_FIT_NOUT 11
+
+typedef struct {
+  int32_t model;        /* MI_FIT_*                                       */
+  int32_t half_window;  /* samples each side of the peak bin (FitROIPadding) */
+  int32_t max_iter;     /* LM iteration cap                                */
+  double x_bin;         /* x bin size (same units as x)                    */
+  double px_um;         /* pixel size (um) for the 2-theta conversion; 0 = skip */
+  double lsd_um;        /* sample-detector distance (um)                   */
+} mi_fit_opts;
+
+/* x: device [n_x] (R bin centres), lineouts: device [F][n_x], peaks: device [n_peaks]
+ * target x positions; out: device [F][n_peaks][MI_FIT_NOUT]; iters: device [F][n_peaks]
+ * int32 (negative = rejected window).  */
+int mi_fit_batch(const double *x, const double *lineouts, int n_frames, int n_x,
+                 const double *peaks, int n_peaks, const mi_fit_opts *opts,
+                 double *out, int32_t *iters, void *stream);
+
+/* ---- map building (DetectorMapper on the device) -------------------------- */
+typedef struct {
+  int32_t ny, nz;
+  double px_um;                 /* pixel size (um), square pixels              */
+  double lsd_um;                /* sample-detector distance (um)               */
+  double bc_y, bc_z;            /* beam centre (px)                            */
+  double tx, ty, tz;            /* tilts (deg)                                 */
+  double rho_d;                 /* distortion normalisation radius (um)        */
+  double p[15];                 /* p0..p14 distortion coefficients             */
+  double parallax_um;           /* Parallax key                                */
+  int32_t solid_angle;          /* SolidAngleCorrection                        */
+  int32_t polarization;         /* PolarizationCorrection                      */
+  double pol_fraction;          /* PolarizationFraction                        */
+  int32_t sub_pixel_level;      /* SubPixelLevel (1 = no splitting)            */
+  double sub_pixel_cardinal_width; /* SubPixelCardinalWidth (deg)              */
+  const uint8_t *mask_host;     /* optional ny*nz mask (1 = masked) or NULL    */
+} mi_geometry;
+
+typedef struct {
+  int32_t n_r, n_eta;
+  const double *r_lo, *r_hi;    /* host, n_r R-bin edges (px)                  */
+  const double *eta_lo, *eta_hi;/* host, n_eta eta-bin edges (deg)             */
+} mi_binning;
+
+typedef struct mi_map mi_map;   /* built map held on the host                  */
+
+/* device >= 0: build on that GPU; device == -1: build on the host cores (OpenMP),
+ * same code, used to cross-check the device build.  Entries of a bin are ordered by
+ * pixel (y outer, z inner), the serial loop order of mapper_build_map. */
+int mi_map_build(const mi_geometry *geom, const mi_binning *bins, int device,
+                 mi_map **out);
+int mi_map_sizes(const mi_map *map, int64_t *n_records, int64_t *n_bins);
+/* Copy out Map.bin records and nMap.bin pairs (host buffers sized by mi_map_sizes). */
+int mi_map_copy(const mi_map *map, mi_map_record *records, int32_t *nmap,
+                int32_t *bin_mask);
+void mi_map_destroy(mi_map *map);
+
+/* ---- synthetic detector frames (test and benchmark input) ------------------ */
+typedef struct {
+  int32_t ny, nz;
+  double bc_y, bc_z;            /* beam centre (px)                                */
+  double lsd_um, px_um;         /* geometry used for the ring radii                */
+  double ty, tz;                /* tilts (deg) applied to the ring model           */
+  int32_t n_rings;
+  double ring_r_px[32];         /* ring radii (px)                                 */
+  double ring_amp[32];          /* peak heights (counts)                           */
+  double fwhm_px, mix_eta;      /* radial pseudo-Voigt shape                       */
+  double texture;               /* cos(2 eta) modulation amplitude (0.3 = +-30 %)  */
+  double background;            /* flat background (counts)                        */
+  double amp_drift;             /* per-frame uniform amplitude drift (0.2 = +-20 %) */
+  int32_t n_spots;              /* Gaussian single-crystal spots per frame         */
+  double spot_sigma, spot_amp;
+  double dark_mean, dark_sigma; /* dark = dark_mean + N(0, dark_sigma)             */
+  uint64_t seed;
+  int32_t poisson;              /* 1 = Poisson counts, 0 = expected value rounded  */
+} mi_synth_desc;
+
+/* Frames first_frame .. first_frame+n_frames-1 of the seeded sweep, written as
+ * u16 (dtype MI_DT_U16) or i32 (MI_DT_I32) to a device buffer with frame_stride
+ * elements between frames.  Counts include the dark (raw = dark + signal). */
+int mi_synth_frames(const mi_synth_desc *desc, int64_t first_frame, int n_frames,
+                    int dtype, void *out, int64_t frame_stride, void *stream);
+/* The sweep's dark (float, ny*nz), device pointer. */
+int mi_synth_dark(const mi_synth_desc *desc, float *out, void *stream);
+
+/* ---- errors ---------------------------------------------------------------- */
+/* Message of the last failing call on this thread ("" if none). */
+const char *mi_last_error(void);
+/* Library version string. */
+const char *mi_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* MIDAS_B200_H */

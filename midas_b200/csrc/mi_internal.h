@@ -1,0 +1,161 @@
+// mi_internal.h -- shared internals of libmidas_b200 (not part of the C ABI).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+#include <vector>
+
+#include "../../include/midas_b200.h"
+
+namespace mi {
+
+// Bins whose normalising area is at or below this are invalid
+// (AREA_THRESHOLD, IntegratorFitPeaksGPUStream.cu and kernels.py:44).
+constexpr double kAreaThreshold = 1e-9;
+
+// Largest number of frames one launch of the batched kernel processes; larger
+// batches are split into several launches inside mi_integrate_batch.
+constexpr int kMaxFramesPerLaunch = 256;
+
+int set_error(int code, const char *fmt, ...);
+int cuda_error(cudaError_t e, const char *what, const char *file, int line);
+
+#define MI_CUDA(call)                                                         \
+  do {                                                                        \
+    cudaError_t mi_e_ = (call);                                               \
+    if (mi_e_ != cudaSuccess)                                                 \
+      return ::mi::cuda_error(mi_e_, #call, __FILE__, __LINE__);              \
+  } while (0)
+
+// ---------------------------------------------------------------------------
+// Tiled map encoding used by the batched caking kernel.
+//
+// Bins are R-major (bin = r * n_eta + e).  Rows are grouped into bands of
+// `tile_rows` R bins; a band is split along eta into work items (one CTA
+// each); an item is covered by staging tiles (rectangles of rows x eta
+// columns) whose union of referenced pixels fits in shared memory.
+// Each tile is one contiguous, 16-byte aligned blob in device memory that the
+// kernel copies to shared memory with one bulk (TMA) copy:
+//
+//   TileHdr                        32 B
+//   uint32 row_ptr[nb + 1]         term offsets per bin (bins row-major in tile)
+//   float  scale[nb]               result = sum * scale (1/area, 1 or 0)
+//   float  lw[nb]                  lineout weight: in-bounds area if > 1e-9 else 0
+//   uint32 upix[n_u]               staged pixels (flat detector index), ascending
+//   uint16 lcol[nnz]               term -> index into upix
+//   float  w[nnz]                  term weight (fp32)
+// every array starts on a 16-byte boundary; the blob size is a multiple of 16.
+struct TileHdr {
+  int32_t nb, nnz, n_u, n_rows, n_cols, r0, e0, row_in_band;
+};
+static_assert(sizeof(TileHdr) == 32, "TileHdr layout");
+
+struct TileRef {
+  uint64_t off;    // byte offset of the blob in the blob arena
+  uint32_t bytes;  // blob size (multiple of 16)
+  uint32_t pad;
+};
+
+struct WorkItem {
+  int32_t tile_begin, tile_end;  // tiles [begin, end) in the tile table
+  int32_t r0, n_rows;            // rows of the band this item covers
+  int32_t slot;                  // lineout partial slot (item index inside band)
+  int32_t nnz;                   // total terms (for scheduling)
+  int32_t pad0, pad1;
+};
+
+struct BlobLayout {
+  uint32_t o_rowptr, o_scale, o_lw, o_upix, o_lcol, o_w, bytes;
+};
+
+inline uint32_t align16(uint32_t x) { return (x + 15u) & ~15u; }
+
+__host__ __device__ inline void blob_layout(int nb, int nnz, int n_u, uint32_t *o_rowptr,
+                                            uint32_t *o_scale, uint32_t *o_lw,
+                                            uint32_t *o_upix, uint32_t *o_lcol,
+                                            uint32_t *o_w, uint32_t *bytes) {
+  auto a16 = [](uint32_t x) { return (x + 15u) & ~15u; };
+  uint32_t o = 32;
+  *o_rowptr = o; o = a16(o + 4u * (uint32_t)(nb + 1));
+  *o_scale = o;  o = a16(o + 4u * (uint32_t)nb);
+  *o_lw = o;     o = a16(o + 4u * (uint32_t)nb);
+  *o_upix = o;   o = a16(o + 4u * (uint32_t)n_u);
+  *o_lcol = o;   o = a16(o + 2u * (uint32_t)nnz);
+  *o_w = o;      o = a16(o + 4u * (uint32_t)nnz);
+  *bytes = o;
+}
+
+// Host-side CSR of one integration mode: rows = bins, cols = flat pixels.
+struct HostCSR {
+  std::vector<int64_t> row_ptr;  // n_bins + 1
+  std::vector<int32_t> col;
+  std::vector<double> w;
+  std::vector<double> area_norm;  // normaliser per bin (semantics dependent)
+  std::vector<double> area_in;    // in-bounds area per bin (profile weights)
+  int64_t oob = 0;
+};
+
+struct TileLimits {
+  int rows;      // rows per band
+  int max_u;     // max staged pixels per tile
+  int max_nb;    // max bins per tile
+  int max_nnz;   // max terms per tile
+  int item_cols; // eta columns per work item
+};
+
+struct Plan {
+  int device = 0;
+  int mode = 0, normalize = 1, semantics = 0;
+  int n_r = 0, n_eta = 0, ny = 0, nz = 0;
+  double bc_y = 0, bc_z = 0;
+  int64_t n_bins = 0, nnz = 0, n_records = 0, oob = 0;
+  int frames_per_lane = 1;
+  TileLimits lim{};
+  int64_t staged_pixels = 0, ref_pixels = 0;
+
+  // batched path
+  uint8_t *d_blobs = nullptr;
+  size_t blob_bytes = 0;
+  TileRef *d_tiles = nullptr;
+  int n_tiles = 0;
+  WorkItem *d_items = nullptr;   // in launch order (heaviest first)
+  int n_items = 0;
+  int n_slots = 0;               // work items per band
+  uint32_t max_blob = 0;         // largest blob (bytes)
+  int max_u = 0, max_nb = 0;     // realised maxima over tiles
+  double *d_den_aw = nullptr;    // per R row: sum of valid in-bounds area
+  double *d_cnt = nullptr;       // per R row: number of valid bins
+  double *d_partial = nullptr;   // [kMaxFramesPerLaunch][n_r][n_slots][2]
+  float *d_dark = nullptr;       // ny*nz (zeros when no dark is set)
+  int has_dark = 0;
+  int *d_err = nullptr;          // device error word (bounded waits)
+
+  // plain (reference-layout) path
+  int32_t *d_nmap = nullptr;     // {count, offset} per bin
+  int32_t *d_sorted = nullptr;   // bins, heaviest first
+  int32_t *d_off = nullptr;      // per record: flat pixel offset (floor mode)
+  float *d_w = nullptr, *d_aw = nullptr, *d_dr = nullptr, *d_py = nullptr, *d_pz = nullptr;
+  double *d_area_in = nullptr;   // per bin in-bounds area
+  double *d_area_all = nullptr;  // per bin sum of all areaWeight
+  float *d_plain_img = nullptr;  // one cast frame
+  size_t device_bytes = 0;
+};
+
+// Builders (mi_plan.cu)
+int build_host_csr(const mi_map_desc &m, int mode, int semantics, HostCSR *out);
+
+// Launchers (mi_cake.cu, mi_plain.cu)
+int launch_cake(Plan *p, const void *frames, int dtype, int n_frames, int64_t stride,
+                float *cake, double *lo_aw, double *lo_sm, cudaStream_t s);
+int launch_plain(Plan *p, const void *frame, int dtype, double *cake, double *lo_aw,
+                 double *lo_sm, cudaStream_t s);
+int launch_cast(const void *frames, int dtype, int64_t n_pixels, int n_frames,
+                const float *dark, float *out, cudaStream_t s);
+int launch_profile(Plan *p, const void *cake, int cake_dtype, int n_frames, double *lo_aw,
+                   double *lo_sm, cudaStream_t s);
+
+size_t dtype_size(int dtype);
+
+}  // namespace mi

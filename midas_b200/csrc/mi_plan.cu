@@ -1,0 +1,733 @@
+// mi_plan.cu -- plan creation: map validation, per-mode CSR, tiling, upload.
+//
+// Host side of the drop-in boundary.  The CSR construction restates
+// build_csr() of packages/midas_integrate/midas_integrate/kernels.py:242-375
+// (floor: one term per record, off-detector records dropped; bilinear and
+// gradient: four clamped corner terms per record, duplicates summed, exact
+// zeros removed), with the GPU-stream normaliser of
+// FF_HEDM/src/IntegratorFitPeaksGPUStream.cu:994-1049 as a selectable
+// semantic.  The tiled encoding is this library's own (see mi_internal.h).
+#include <omp.h>
+#include <stdarg.h>
+#include <stdio.h>
+#include <string.h>
+
+#include <algorithm>
+#include <cmath>
+#include <numeric>
+
+#include "mi_internal.h"
+
+namespace mi {
+
+static thread_local char g_err[1024] = "";
+
+int set_error(int code, const char *fmt, ...) {
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(g_err, sizeof(g_err), fmt, ap);
+  va_end(ap);
+  return code;
+}
+
+int cuda_error(cudaError_t e, const char *what, const char *file, int line) {
+  return set_error(e == cudaErrorMemoryAllocation ? MI_E_OOM : MI_E_CUDA,
+                   "CUDA error %s (%s) in %s at %s:%d", cudaGetErrorName(e),
+                   cudaGetErrorString(e), what, file, line);
+}
+
+size_t dtype_size(int dtype) {
+  switch (dtype) {
+    case MI_DT_U8: return 1;
+    case MI_DT_U16: return 2;
+    case MI_DT_U32: return 4;
+    case MI_DT_I64: return 8;
+    case MI_DT_F32: return 4;
+    case MI_DT_F64: return 8;
+    case MI_DT_I32: return 4;
+    default: return 0;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// CSR of one mode.  Per record (y, z, frac, deltaR, areaWeight):
+//  * in-bounds test on the truncated (y, z) (kernels.py:306-311) decides
+//    whether areaWeight enters area_in (the profile / Python normaliser);
+//  * MI_SEM_GPUSTREAM normalises by the sum of all areaWeight of the bin
+//    (IntegratorFitPeaksGPUStream.cu:1034-1040).
+// ---------------------------------------------------------------------------
+struct Term {
+  int32_t col;
+  double w;
+};
+
+static inline void add_bilinear(double sy, double sz, double frac, int ny, int nz,
+                                std::vector<Term> &t) {
+  // kernels.py:_build_bilinear_csr: floor, then clamp (over first, then under)
+  double fiy = std::floor(sy), fiz = std::floor(sz);
+  int64_t iy = (int64_t)fiy, iz = (int64_t)fiz;
+  double fy = sy - (double)iy, fz = sz - (double)iz;
+  bool over_y = iy >= (ny - 1), under_y = iy < 0;
+  bool over_z = iz >= (nz - 1), under_z = iz < 0;
+  if (over_y) { iy = ny - 2; fy = 1.0; }
+  if (under_y) { iy = 0; fy = 0.0; }
+  if (over_z) { iz = nz - 2; fz = 1.0; }
+  if (under_z) { iz = 0; fz = 0.0; }
+  int64_t base = iz * (int64_t)ny + iy;
+  double one_fy = 1.0 - fy, one_fz = 1.0 - fz;
+  t.push_back({(int32_t)base, one_fy * one_fz * frac});
+  t.push_back({(int32_t)(base + 1), fy * one_fz * frac});
+  t.push_back({(int32_t)(base + ny), one_fy * fz * frac});
+  t.push_back({(int32_t)(base + ny + 1), fy * fz * frac});
+}
+
+static void bin_terms(const mi_map_desc &m, int64_t b, int mode, int sem,
+                      std::vector<Term> &t, double *area_in, double *area_all,
+                      int64_t *oob) {
+  t.clear();
+  const int32_t cnt = m.nmap[2 * b], off = m.nmap[2 * b + 1];
+  double ain = 0.0, aall = 0.0;
+  const int ny = m.ny, nz = m.nz;
+  for (int32_t k = 0; k < cnt; ++k) {
+    const mi_map_record &r = m.records[(int64_t)off + k];
+    const double y = (double)r.y, z = (double)r.z;
+    // numpy astype(int64) truncates toward zero
+    const int64_t ty = (int64_t)y, tz = (int64_t)z;
+    const bool inb = ty >= 0 && ty < ny && tz >= 0 && tz < nz;
+    aall += (double)r.areaWeight;
+    if (inb) ain += (double)r.areaWeight;
+    else ++*oob;
+    if (mode == MI_MODE_FLOOR) {
+      if (sem == MI_SEM_GPUSTREAM) {
+        // PrecomputeOffsets_kernel: (long long)z * NY + y evaluated in float,
+        // then truncated (IntegratorFitPeaksGPUStream.cu:915-916)
+        long long zz = (long long)r.z;
+        float s = (float)(zz * (long long)ny) + r.y;
+        long long o = (long long)s;
+        if (o >= 0 && o < (long long)ny * nz) t.push_back({(int32_t)o, r.frac});
+      } else if (inb) {
+        t.push_back({(int32_t)(tz * ny + ty), r.frac});
+      }
+    } else {
+      double sy = y, sz = z;
+      if (mode == MI_MODE_GRADIENT) {
+        if (sem == MI_SEM_GPUSTREAM) {
+          // fp32 resampling of integrate_noMapMask (…Stream.cu:1007-1018)
+          float dy = r.y - (float)m.bc_y, dz = r.z - (float)m.bc_z;
+          float R = sqrtf(dy * dy + dz * dz);
+          float ry = r.y, rz = r.z;
+          if (R > 1.0f) {
+            ry -= r.deltaR * dy / R;
+            rz -= r.deltaR * dz / R;
+          }
+          sy = ry;
+          sz = rz;
+        } else {
+          // kernels.py:347-353 (fp64)
+          double dy = y - m.bc_y, dz = z - m.bc_z;
+          double R = std::sqrt(dy * dy + dz * dz);
+          double sc = R > 1.0 ? (double)r.deltaR / R : 0.0;
+          sy = y - sc * dy;
+          sz = z - sc * dz;
+        }
+      }
+      add_bilinear(sy, sz, r.frac, ny, nz, t);
+    }
+  }
+  *area_in = ain;
+  *area_all = aall;
+  // coalesce duplicates (sum), drop exact zeros (scipy sum_duplicates + eliminate_zeros)
+  std::stable_sort(t.begin(), t.end(), [](const Term &a, const Term &b) { return a.col < b.col; });
+  size_t o = 0;
+  for (size_t i = 0; i < t.size();) {
+    size_t j = i;
+    double s = 0.0;
+    while (j < t.size() && t[j].col == t[i].col) s += t[j++].w;
+    if (s != 0.0 || mode == MI_MODE_FLOOR) t[o++] = {t[i].col, s};
+    i = j;
+  }
+  t.resize(o);
+  if (mode == MI_MODE_FLOOR) {
+    // floor CSR keeps explicit zeros only if frac was zero; drop them too (no effect on sums)
+    size_t q = 0;
+    for (size_t i = 0; i < t.size(); ++i)
+      if (t[i].w != 0.0) t[q++] = t[i];
+    t.resize(q);
+  }
+}
+
+int build_host_csr(const mi_map_desc &m, int mode, int sem, HostCSR *out) {
+  const int64_t n_bins = (int64_t)m.n_r * m.n_eta;
+  // validation (kernels.py:288-301), plus negative offsets
+  for (int64_t b = 0; b < n_bins; ++b) {
+    const int64_t c = m.nmap[2 * b], o = m.nmap[2 * b + 1];
+    if (c < 0) return set_error(MI_E_MAP, "nMap.bin bin %lld has negative count %lld", (long long)b, (long long)c);
+    if (c > 0 && (o < 0 || o + c > m.n_records))
+      return set_error(MI_E_MAP, "bin %lld references past end of Map.bin (offset %lld, count %lld, n_records %lld)",
+                       (long long)b, (long long)o, (long long)c, (long long)m.n_records);
+  }
+  std::vector<int64_t> counts(n_bins + 1, 0);
+  out->area_in.assign(n_bins, 0.0);
+  out->area_norm.assign(n_bins, 0.0);
+  std::vector<double> area_all(n_bins, 0.0);
+  int64_t oob_total = 0;
+  // pass 1: term counts
+#pragma omp parallel reduction(+ : oob_total)
+  {
+    std::vector<Term> t;
+    t.reserve(1024);
+#pragma omp for schedule(dynamic, 256)
+    for (int64_t b = 0; b < n_bins; ++b) {
+      double ain, aall;
+      int64_t oob = 0;
+      bin_terms(m, b, mode, sem, t, &ain, &aall, &oob);
+      counts[b + 1] = (int64_t)t.size();
+      out->area_in[b] = ain;
+      area_all[b] = aall;
+      oob_total += oob;
+    }
+  }
+  out->row_ptr.assign(n_bins + 1, 0);
+  for (int64_t b = 0; b < n_bins; ++b) out->row_ptr[b + 1] = out->row_ptr[b] + counts[b + 1];
+  const int64_t nnz = out->row_ptr[n_bins];
+  out->col.resize(nnz);
+  out->w.resize(nnz);
+#pragma omp parallel
+  {
+    std::vector<Term> t;
+    t.reserve(1024);
+#pragma omp for schedule(dynamic, 256)
+    for (int64_t b = 0; b < n_bins; ++b) {
+      double ain, aall;
+      int64_t oob = 0;
+      bin_terms(m, b, mode, sem, t, &ain, &aall, &oob);
+      int64_t o = out->row_ptr[b];
+      for (const Term &x : t) {
+        out->col[o] = x.col;
+        out->w[o] = x.w;
+        ++o;
+      }
+    }
+  }
+  for (int64_t b = 0; b < n_bins; ++b)
+    out->area_norm[b] = (sem == MI_SEM_GPUSTREAM) ? area_all[b] : out->area_in[b];
+  out->oob = oob_total;
+  return MI_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Tiling
+// ---------------------------------------------------------------------------
+struct HostTile {
+  int r0, n_rows, e0, n_cols, nnz, n_u;
+};
+
+struct Builder {
+  const HostCSR &csr;
+  int n_r, n_eta;
+  int64_t n_pix;
+  TileLimits lim;
+  Builder(const HostCSR &c, int nr, int ne, int64_t np, TileLimits l)
+      : csr(c), n_r(nr), n_eta(ne), n_pix(np), lim(l) {}
+};
+
+// Greedily cover rows [r0, r0+nrows) x cols [e_begin, e_end) with tiles.
+static int tile_item(const Builder &B, int r0, int nrows, int e_begin, int e_end,
+                     std::vector<int32_t> &stamp, int32_t &stamp_id,
+                     std::vector<HostTile> &tiles) {
+  const TileLimits &L = B.lim;
+  auto col_terms = [&](int r, int e) {
+    int64_t b = (int64_t)r * B.n_eta + e;
+    return std::make_pair(B.csr.row_ptr[b], B.csr.row_ptr[b + 1]);
+  };
+  // unique pixels of a rectangle
+  std::vector<int32_t> added;
+  auto rect_fits = [&](int rc, int h, int e0, int ncols, int *nu_out, int *nnz_out) {
+    ++stamp_id;
+    int nu = 0, nnz = 0;
+    for (int e = e0; e < e0 + ncols; ++e)
+      for (int r = rc; r < rc + h; ++r) {
+        auto pr = col_terms(r, e);
+        nnz += (int)(pr.second - pr.first);
+        for (int64_t j = pr.first; j < pr.second; ++j) {
+          int32_t c = B.csr.col[j];
+          if (stamp[c] != stamp_id) { stamp[c] = stamp_id; ++nu; }
+        }
+      }
+    *nu_out = nu;
+    *nnz_out = nnz;
+    return nu <= L.max_u && nnz <= L.max_nnz && h * ncols <= L.max_nb;
+  };
+  // row-chunk height: largest h (halving) such that every single column fits
+  int h = nrows;
+  for (;;) {
+    bool ok = true;
+    for (int rc = r0; rc < r0 + nrows && ok; rc += h) {
+      int hh = std::min(h, r0 + nrows - rc);
+      for (int e = e_begin; e < e_end && ok; ++e) {
+        int nu, nnz;
+        if (!rect_fits(rc, hh, e, 1, &nu, &nnz)) ok = false;
+      }
+    }
+    if (ok) break;
+    if (h == 1)
+      return set_error(MI_E_RANGE,
+                       "a single bin (row %d) references more pixels or terms than one tile holds "
+                       "(max %d pixels, %d terms); raise tile_pixels",
+                       r0, L.max_u, L.max_nnz);
+    h = (h + 1) / 2;
+  }
+  for (int rc = r0; rc < r0 + nrows; rc += h) {
+    int hh = std::min(h, r0 + nrows - rc);
+    int e = e_begin;
+    while (e < e_end) {
+      int ncols = 1, nu = 0, nnz = 0;
+      rect_fits(rc, hh, e, 1, &nu, &nnz);
+      while (e + ncols < e_end) {
+        int nu2, nnz2;
+        if (!rect_fits(rc, hh, e, ncols + 1, &nu2, &nnz2)) break;
+        ++ncols;
+        nu = nu2;
+        nnz = nnz2;
+      }
+      tiles.push_back({rc, hh, e, ncols, nnz, nu});
+      e += ncols;
+    }
+  }
+  return MI_OK;
+}
+
+static int free_plan_mem(Plan *p) {
+  cudaSetDevice(p->device);
+  void *ptrs[] = {p->d_blobs, p->d_tiles, p->d_items, p->d_den_aw, p->d_cnt, p->d_partial,
+                  p->d_dark, p->d_err, p->d_nmap, p->d_sorted, p->d_off, p->d_w, p->d_aw,
+                  p->d_dr, p->d_py, p->d_pz, p->d_area_in, p->d_area_all, p->d_plain_img};
+  for (void *q : ptrs)
+    if (q) cudaFree(q);
+  return MI_OK;
+}
+
+template <typename T>
+static int upload(T **dst, const T *src, size_t n, size_t *acct) {
+  size_t bytes = std::max<size_t>(n, 1) * sizeof(T);
+  MI_CUDA(cudaMalloc((void **)dst, bytes));
+  *acct += bytes;
+  if (n) MI_CUDA(cudaMemcpy(*dst, src, n * sizeof(T), cudaMemcpyHostToDevice));
+  return MI_OK;
+}
+
+static int build_plan(const mi_map_desc &m, const mi_plan_opts &o, Plan *p) {
+  p->mode = o.mode;
+  p->normalize = o.normalize ? 1 : 0;
+  p->semantics = o.semantics;
+  p->n_r = m.n_r;
+  p->n_eta = m.n_eta;
+  p->ny = m.ny;
+  p->nz = m.nz;
+  p->bc_y = m.bc_y;
+  p->bc_z = m.bc_z;
+  p->n_bins = (int64_t)m.n_r * m.n_eta;
+  p->n_records = m.n_records;
+  const int64_t n_pix = (int64_t)m.ny * m.nz;
+
+  HostCSR csr;
+  int rc = build_host_csr(m, o.mode, o.semantics, &csr);
+  if (rc) return rc;
+  p->nnz = (int64_t)csr.col.size();
+  p->oob = csr.oob;
+
+  // ---- limits
+  int fpl = o.frames_per_lane > 0 ? o.frames_per_lane : 1;
+  if (fpl != 1 && fpl != 2 && fpl != 4) return set_error(MI_E_ARG, "frames_per_lane must be 1, 2 or 4");
+  p->frames_per_lane = fpl;
+  TileLimits L;
+  L.rows = o.tile_rows > 0 ? o.tile_rows : 16;
+  if (L.rows > 64) return set_error(MI_E_RANGE, "tile_rows %d > 64", L.rows);
+  L.max_u = o.tile_pixels > 0 ? o.tile_pixels : (fpl == 1 ? 768 : (fpl == 2 ? 384 : 192));
+  if (L.max_u > 65535) return set_error(MI_E_RANGE, "tile_pixels %d > 65535", L.max_u);
+  L.max_nb = 256;
+  L.max_nnz = 6144;
+  L.item_cols = std::max(1, (m.n_eta + 11) / 12);
+  p->lim = L;
+
+  // ---- items and tiles
+  const int n_bands = (m.n_r + L.rows - 1) / L.rows;
+  const int n_slots = (m.n_eta + L.item_cols - 1) / L.item_cols;
+  p->n_slots = n_slots;
+  const int n_items = n_bands * n_slots;
+  std::vector<std::vector<HostTile>> item_tiles(n_items);
+  int err = MI_OK;
+  {
+    int nthr = std::min(omp_get_max_threads(), 16);
+#pragma omp parallel num_threads(nthr)
+    {
+      std::vector<int32_t> stamp(n_pix, 0);
+      int32_t sid = 0;
+#pragma omp for schedule(dynamic, 1)
+      for (int it = 0; it < n_items; ++it) {
+        int band = it / n_slots, slot = it % n_slots;
+        int r0 = band * L.rows, nr = std::min(L.rows, m.n_r - r0);
+        int e0 = slot * L.item_cols, e1 = std::min(m.n_eta, e0 + L.item_cols);
+        int e = tile_item(Builder(csr, m.n_r, m.n_eta, n_pix, L), r0, nr, e0, e1, stamp, sid,
+                          item_tiles[it]);
+        if (e) {
+#pragma omp critical
+          err = e;
+        }
+      }
+    }
+  }
+  if (err) return err;
+
+  // ---- blob arena
+  std::vector<TileRef> tiles;
+  std::vector<WorkItem> items(n_items);
+  std::vector<uint64_t> tile_off;
+  uint64_t arena = 0;
+  uint32_t max_blob = 0;
+  int max_u = 0, max_nb = 0;
+  int64_t staged = 0;
+  for (int it = 0; it < n_items; ++it) {
+    int band = it / n_slots, slot = it % n_slots;
+    WorkItem &w = items[it];
+    w.tile_begin = (int)tiles.size();
+    w.r0 = band * L.rows;
+    w.n_rows = std::min(L.rows, m.n_r - w.r0);
+    w.slot = slot;
+    w.nnz = 0;
+    for (const HostTile &t : item_tiles[it]) {
+      uint32_t a, b, c, d, e, f, bytes;
+      blob_layout(t.n_rows * t.n_cols, t.nnz, t.n_u, &a, &b, &c, &d, &e, &f, &bytes);
+      tiles.push_back({arena, bytes, 0});
+      arena += bytes;
+      max_blob = std::max(max_blob, bytes);
+      max_u = std::max(max_u, t.n_u);
+      max_nb = std::max(max_nb, t.n_rows * t.n_cols);
+      staged += t.n_u;
+      w.nnz += t.nnz;
+    }
+    w.tile_end = (int)tiles.size();
+  }
+  p->n_tiles = (int)tiles.size();
+  p->max_blob = max_blob;
+  p->max_u = max_u;
+  p->max_nb = max_nb;
+  p->staged_pixels = staged;
+  std::vector<uint8_t> blobs(arena, 0);
+  {
+    std::vector<int64_t> first_tile(n_items);
+    for (int it = 0; it < n_items; ++it) first_tile[it] = items[it].tile_begin;
+    int nthr = std::min(omp_get_max_threads(), 16);
+#pragma omp parallel num_threads(nthr)
+    {
+      std::vector<int32_t> lut(n_pix, -1);
+#pragma omp for schedule(dynamic, 1)
+      for (int it = 0; it < n_items; ++it) {
+        int k = 0;
+        for (const HostTile &t : item_tiles[it]) {
+          const TileRef &ref = tiles[first_tile[it] + k++];
+          uint8_t *blob = blobs.data() + ref.off;
+          const int nb = t.n_rows * t.n_cols;
+          uint32_t o_rp, o_sc, o_lw, o_up, o_lc, o_w, bytes;
+          blob_layout(nb, t.nnz, t.n_u, &o_rp, &o_sc, &o_lw, &o_up, &o_lc, &o_w, &bytes);
+          TileHdr *h = (TileHdr *)blob;
+          h->nb = nb;
+          h->nnz = t.nnz;
+          h->n_u = t.n_u;
+          h->n_rows = t.n_rows;
+          h->n_cols = t.n_cols;
+          h->r0 = t.r0;
+          h->e0 = t.e0;
+          h->row_in_band = t.r0 - items[it].r0;
+          uint32_t *rowp = (uint32_t *)(blob + o_rp);
+          float *scale = (float *)(blob + o_sc);
+          float *lw = (float *)(blob + o_lw);
+          uint32_t *upix = (uint32_t *)(blob + o_up);
+          uint16_t *lcol = (uint16_t *)(blob + o_lc);
+          float *wt = (float *)(blob + o_w);
+          // staged pixel set, ascending
+          std::vector<int32_t> u;
+          u.reserve(t.n_u);
+          for (int r = t.r0; r < t.r0 + t.n_rows; ++r)
+            for (int e = t.e0; e < t.e0 + t.n_cols; ++e) {
+              int64_t b = (int64_t)r * m.n_eta + e;
+              for (int64_t j = csr.row_ptr[b]; j < csr.row_ptr[b + 1]; ++j) u.push_back(csr.col[j]);
+            }
+          std::sort(u.begin(), u.end());
+          u.erase(std::unique(u.begin(), u.end()), u.end());
+          for (size_t i = 0; i < u.size(); ++i) {
+            upix[i] = (uint32_t)u[i];
+            lut[u[i]] = (int32_t)i;
+          }
+          uint32_t nz_o = 0;
+          for (int r = t.r0; r < t.r0 + t.n_rows; ++r)
+            for (int e = t.e0; e < t.e0 + t.n_cols; ++e) {
+              int64_t b = (int64_t)r * m.n_eta + e;
+              int lb = (r - t.r0) * t.n_cols + (e - t.e0);
+              rowp[lb] = nz_o;
+              for (int64_t j = csr.row_ptr[b]; j < csr.row_ptr[b + 1]; ++j) {
+                lcol[nz_o] = (uint16_t)lut[csr.col[j]];
+                wt[nz_o] = (float)csr.w[j];
+                ++nz_o;
+              }
+              const double an = csr.area_norm[b], ai = csr.area_in[b];
+              double sc;
+              if (p->semantics == MI_SEM_GPUSTREAM)
+                sc = an > kAreaThreshold ? (p->normalize ? 1.0 / an : 1.0) : 0.0;
+              else
+                sc = p->normalize ? (ai > kAreaThreshold ? 1.0 / ai : 0.0) : 1.0;
+              scale[lb] = (float)sc;
+              lw[lb] = ai > kAreaThreshold ? (float)ai : 0.0f;
+            }
+          rowp[nb] = nz_o;
+          for (size_t i = 0; i < u.size(); ++i) lut[u[i]] = -1;
+        }
+      }
+    }
+  }
+  // distinct referenced pixels
+  {
+    std::vector<uint8_t> seen(n_pix, 0);
+    int64_t n = 0;
+    for (int32_t c : csr.col)
+      if (!seen[c]) { seen[c] = 1; ++n; }
+    p->ref_pixels = n;
+  }
+  // heaviest-first launch order
+  std::vector<int> order(n_items);
+  std::iota(order.begin(), order.end(), 0);
+  std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return items[a].nnz > items[b].nnz; });
+  std::vector<WorkItem> items_sorted(n_items);
+  for (int i = 0; i < n_items; ++i) items_sorted[i] = items[order[i]];
+  p->n_items = n_items;
+
+  // lineout denominators
+  std::vector<double> den(m.n_r, 0.0), cnt(m.n_r, 0.0);
+  for (int r = 0; r < m.n_r; ++r)
+    for (int e = 0; e < m.n_eta; ++e) {
+      double a = csr.area_in[(int64_t)r * m.n_eta + e];
+      if (a > kAreaThreshold) { den[r] += a; cnt[r] += 1.0; }
+    }
+
+  size_t acct = 0;
+  MI_CUDA(cudaSetDevice(p->device));
+  if ((rc = upload(&p->d_blobs, blobs.data(), blobs.size(), &acct))) return rc;
+  p->blob_bytes = blobs.size();
+  if ((rc = upload(&p->d_tiles, tiles.data(), tiles.size(), &acct))) return rc;
+  if ((rc = upload(&p->d_items, items_sorted.data(), items_sorted.size(), &acct))) return rc;
+  if ((rc = upload(&p->d_den_aw, den.data(), den.size(), &acct))) return rc;
+  if ((rc = upload(&p->d_cnt, cnt.data(), cnt.size(), &acct))) return rc;
+  {
+    size_t bytes = (size_t)kMaxFramesPerLaunch * m.n_r * n_slots * 2 * sizeof(double);
+    MI_CUDA(cudaMalloc((void **)&p->d_partial, bytes));
+    acct += bytes;
+  }
+  MI_CUDA(cudaMalloc((void **)&p->d_dark, n_pix * sizeof(float)));
+  MI_CUDA(cudaMemset(p->d_dark, 0, n_pix * sizeof(float)));
+  acct += n_pix * sizeof(float);
+  MI_CUDA(cudaMalloc((void **)&p->d_err, sizeof(int)));
+  MI_CUDA(cudaMemset(p->d_err, 0, sizeof(int)));
+
+  // ---- plain path: reference SoA layout (PrecomputeOffsets_kernel, …Stream.cu:901-924)
+  {
+    const int64_t nrec = m.n_records;
+    std::vector<int32_t> off(nrec);
+    std::vector<float> w(nrec), aw(nrec), dr(nrec), py(nrec), pz(nrec);
+#pragma omp parallel for schedule(static)
+    for (int64_t i = 0; i < nrec; ++i) {
+      const mi_map_record &r = m.records[i];
+      long long zz = (long long)r.z;
+      float s = (float)(zz * (long long)m.ny) + r.y;
+      long long o2 = (long long)s;
+      const int64_t ty = (int64_t)r.y, tz = (int64_t)r.z;
+      const bool inb = ty >= 0 && ty < m.ny && tz >= 0 && tz < m.nz;
+      if (p->semantics == MI_SEM_PY) o2 = inb ? (long long)(tz * m.ny + ty) : -1;
+      else if (o2 < 0 || o2 >= (long long)m.ny * m.nz) o2 = -1;
+      off[i] = (int32_t)o2;
+      w[i] = (float)r.frac;
+      aw[i] = r.areaWeight;
+      dr[i] = r.deltaR;
+      py[i] = r.y;
+      pz[i] = r.z;
+    }
+    std::vector<int32_t> sorted(p->n_bins);
+    std::iota(sorted.begin(), sorted.end(), 0);
+    std::stable_sort(sorted.begin(), sorted.end(),
+                     [&](int32_t a, int32_t b) { return m.nmap[2 * a] > m.nmap[2 * b]; });
+    std::vector<double> area_all(p->n_bins, 0.0);
+    for (int64_t b = 0; b < p->n_bins; ++b) {
+      double s = 0;
+      for (int32_t k = 0; k < m.nmap[2 * b]; ++k) s += m.records[(int64_t)m.nmap[2 * b + 1] + k].areaWeight;
+      area_all[b] = s;
+    }
+    if ((rc = upload(&p->d_nmap, m.nmap, (size_t)(2 * p->n_bins), &acct))) return rc;
+    if ((rc = upload(&p->d_sorted, sorted.data(), sorted.size(), &acct))) return rc;
+    if ((rc = upload(&p->d_off, off.data(), off.size(), &acct))) return rc;
+    if ((rc = upload(&p->d_w, w.data(), w.size(), &acct))) return rc;
+    if ((rc = upload(&p->d_aw, aw.data(), aw.size(), &acct))) return rc;
+    if ((rc = upload(&p->d_dr, dr.data(), dr.size(), &acct))) return rc;
+    if ((rc = upload(&p->d_py, py.data(), py.size(), &acct))) return rc;
+    if ((rc = upload(&p->d_pz, pz.data(), pz.size(), &acct))) return rc;
+    if ((rc = upload(&p->d_area_in, csr.area_in.data(), csr.area_in.size(), &acct))) return rc;
+    if ((rc = upload(&p->d_area_all, area_all.data(), area_all.size(), &acct))) return rc;
+    MI_CUDA(cudaMalloc((void **)&p->d_plain_img, n_pix * sizeof(float)));
+    acct += n_pix * sizeof(float);
+  }
+  p->device_bytes = acct;
+  return MI_OK;
+}
+
+}  // namespace mi
+
+using namespace mi;
+
+struct mi_plan : public mi::Plan {};
+
+extern "C" {
+
+const char *mi_last_error(void) { return mi::g_err; }
+const char *mi_version(void) { return "midas_b200 0.1.0 (sm_100a)"; }
+
+int mi_plan_create(const mi_map_desc *map, const mi_plan_opts *opts, int device, mi_plan **out) {
+  if (!map || !out) return set_error(MI_E_ARG, "mi_plan_create: null argument");
+  *out = nullptr;
+  if (map->n_r <= 0 || map->n_eta <= 0 || map->ny < 2 || map->nz < 2)
+    return set_error(MI_E_ARG, "mi_plan_create: bad shape n_r=%d n_eta=%d ny=%d nz=%d", map->n_r,
+                     map->n_eta, map->ny, map->nz);
+  if (!map->nmap || (map->n_records > 0 && !map->records))
+    return set_error(MI_E_ARG, "mi_plan_create: null map arrays");
+  if ((int64_t)map->ny * map->nz > (int64_t)INT32_MAX)
+    return set_error(MI_E_RANGE, "mi_plan_create: detector larger than 2^31 pixels");
+  mi_plan_opts o{};
+  if (opts) o = *opts;
+  else { o.mode = MI_MODE_FLOOR; o.normalize = 1; o.semantics = MI_SEM_PY; }
+  if (o.mode < 0 || o.mode > 2) return set_error(MI_E_ARG, "mi_plan_create: unknown mode %d", o.mode);
+  if (o.semantics < 0 || o.semantics > 1)
+    return set_error(MI_E_ARG, "mi_plan_create: unknown semantics %d", o.semantics);
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
+    return set_error(MI_E_CUDA, "mi_plan_create: no CUDA device available");
+  if (device < 0 || device >= ndev) return set_error(MI_E_ARG, "mi_plan_create: bad device %d", device);
+  mi_plan *p = new (std::nothrow) mi_plan();
+  if (!p) return set_error(MI_E_OOM, "mi_plan_create: host allocation failed");
+  p->device = device;
+  int prev = 0;
+  cudaGetDevice(&prev);
+  int rc = build_plan(*map, o, p);
+  cudaSetDevice(prev);
+  if (rc) {
+    free_plan_mem(p);
+    delete p;
+    return rc;
+  }
+  *out = p;
+  return MI_OK;
+}
+
+int mi_plan_set_dark(mi_plan *p, const float *dark) {
+  if (!p) return set_error(MI_E_ARG, "mi_plan_set_dark: null plan");
+  const size_t n = (size_t)p->ny * p->nz;
+  int prev = 0;
+  cudaGetDevice(&prev);
+  MI_CUDA(cudaSetDevice(p->device));
+  if (dark) MI_CUDA(cudaMemcpy(p->d_dark, dark, n * sizeof(float), cudaMemcpyHostToDevice));
+  else MI_CUDA(cudaMemset(p->d_dark, 0, n * sizeof(float)));
+  p->has_dark = dark ? 1 : 0;
+  cudaSetDevice(prev);
+  return MI_OK;
+}
+
+int mi_plan_get_info(const mi_plan *p, mi_plan_info *info) {
+  if (!p || !info) return set_error(MI_E_ARG, "mi_plan_get_info: null argument");
+  info->n_bins = p->n_bins;
+  info->n_r = p->n_r;
+  info->n_eta = p->n_eta;
+  info->nnz = p->nnz;
+  info->n_records = p->n_records;
+  info->n_tiles = p->n_tiles;
+  info->n_items = p->n_items;
+  info->staged_pixels = p->staged_pixels;
+  info->ref_pixels = p->ref_pixels;
+  info->map_bytes = (int64_t)p->blob_bytes;
+  info->device_bytes = (int64_t)p->device_bytes;
+  info->oob_records = p->oob;
+  info->tile_rows = p->lim.rows;
+  info->tile_pixels = p->lim.max_u;
+  info->frames_per_lane = p->frames_per_lane;
+  info->run_len = 0;
+  return MI_OK;
+}
+
+int mi_plan_bytes(const mi_plan *p, size_t *bytes) {
+  if (!p || !bytes) return set_error(MI_E_ARG, "mi_plan_bytes: null argument");
+  *bytes = p->device_bytes;
+  return MI_OK;
+}
+
+void mi_plan_destroy(mi_plan *p) {
+  if (!p) return;
+  int prev = 0;
+  cudaGetDevice(&prev);
+  free_plan_mem(p);
+  cudaSetDevice(prev);
+  delete p;
+}
+
+int mi_integrate_batch(mi_plan *p, const void *frames, int dtype, int n_frames, int64_t stride,
+                       float *cake, double *lo_aw, double *lo_sm, void *stream) {
+  if (!p || !frames) return set_error(MI_E_ARG, "mi_integrate_batch: null argument");
+  if (n_frames < 0) return set_error(MI_E_ARG, "mi_integrate_batch: n_frames < 0");
+  if (dtype_size(dtype) == 0) return set_error(MI_E_ARG, "mi_integrate_batch: unknown dtype code %d", dtype);
+  if (stride < (int64_t)p->ny * p->nz)
+    return set_error(MI_E_ARG, "mi_integrate_batch: frame_stride %lld < ny*nz", (long long)stride);
+  if (n_frames == 0) return MI_OK;
+  int prev = 0;
+  cudaGetDevice(&prev);
+  if (prev != p->device) MI_CUDA(cudaSetDevice(p->device));
+  int rc = MI_OK;
+  const size_t es = dtype_size(dtype);
+  for (int f0 = 0; f0 < n_frames && rc == MI_OK; f0 += kMaxFramesPerLaunch) {
+    int nf = std::min(kMaxFramesPerLaunch, n_frames - f0);
+    rc = launch_cake(p, (const uint8_t *)frames + (size_t)f0 * stride * es, dtype, nf, stride,
+                     cake ? cake + (size_t)f0 * p->n_bins : nullptr,
+                     lo_aw ? lo_aw + (size_t)f0 * p->n_r : nullptr,
+                     lo_sm ? lo_sm + (size_t)f0 * p->n_r : nullptr, (cudaStream_t)stream);
+  }
+  if (prev != p->device) cudaSetDevice(prev);
+  return rc;
+}
+
+int mi_integrate_plain(mi_plan *p, const void *frame, int dtype, double *cake, double *lo_aw,
+                       double *lo_sm, void *stream) {
+  if (!p || !frame) return set_error(MI_E_ARG, "mi_integrate_plain: null argument");
+  if (dtype_size(dtype) == 0) return set_error(MI_E_ARG, "mi_integrate_plain: unknown dtype code %d", dtype);
+  int prev = 0;
+  cudaGetDevice(&prev);
+  if (prev != p->device) MI_CUDA(cudaSetDevice(p->device));
+  int rc = launch_plain(p, frame, dtype, cake, lo_aw, lo_sm, (cudaStream_t)stream);
+  if (prev != p->device) cudaSetDevice(prev);
+  return rc;
+}
+
+int mi_profile_batch(mi_plan *p, const void *cake, int cake_dtype, int n_frames, double *lo_aw, double *lo_sm,
+                     void *stream) {
+  if (!p || !cake) return set_error(MI_E_ARG, "mi_profile_batch: null argument");
+  if (n_frames < 0) return set_error(MI_E_ARG, "mi_profile_batch: n_frames < 0");
+  int prev = 0;
+  cudaGetDevice(&prev);
+  if (prev != p->device) MI_CUDA(cudaSetDevice(p->device));
+  int rc = launch_profile(p, cake, cake_dtype, n_frames, lo_aw, lo_sm, (cudaStream_t)stream);
+  if (prev != p->device) cudaSetDevice(prev);
+  return rc;
+}
+
+int mi_cast_dark(const void *frames, int dtype, int64_t n_pixels, int n_frames, const float *dark,
+                 float *out, void *stream) {
+  if (!frames || !out) return set_error(MI_E_ARG, "mi_cast_dark: null argument");
+  if (dtype_size(dtype) == 0) return set_error(MI_E_ARG, "mi_cast_dark: unknown dtype code %d", dtype);
+  if (n_pixels < 0 || n_frames < 0) return set_error(MI_E_ARG, "mi_cast_dark: negative size");
+  if (n_pixels == 0 || n_frames == 0) return MI_OK;
+  return launch_cast(frames, dtype, n_pixels, n_frames, dark, out, (cudaStream_t)stream);
+}
+
+}  // extern "C"

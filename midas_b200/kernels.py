@@ -1,0 +1,311 @@
+"""Caking on the B200 through libmidas_b200 -- the midas_integrate kernels API.
+
+Mirrors packages/midas_integrate/midas_integrate/kernels.py (``build_csr``,
+``integrate``, ``profile_1d``, ``AREA_THRESHOLD``, ``r_axis``, ``eta_axis``) so
+a caller of the reference can switch imports; ``CakePlan`` is the native,
+batched interface underneath (F frames per launch, dark subtraction fused,
+lineouts reduced in the same launch).
+
+Every computation runs in the CUDA library; torch tensors are only buffers
+(device pointers and the current stream).  There is no CPU path: a plan needs a
+CUDA device and raises otherwise.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass, field
+from typing import Dict, Optional, Tuple
+
+import numpy as np
+import torch
+
+from . import _lib as L
+from .bin_io import PixelMap
+
+AREA_THRESHOLD = 1e-9
+
+_TORCH_DT = {
+    torch.uint8: L.DT_U8, torch.uint16: L.DT_U16, torch.uint32: L.DT_U32,
+    torch.int64: L.DT_I64, torch.float32: L.DT_F32, torch.float64: L.DT_F64,
+    torch.int32: L.DT_I32,
+}
+
+
+def dtype_code(t: torch.dtype) -> int:
+    if t not in _TORCH_DT:
+        raise TypeError(f"unsupported frame dtype {t}")
+    return _TORCH_DT[t]
+
+
+def _device_index(device) -> int:
+    d = torch.device(device)
+    if d.type != "cuda":
+        raise RuntimeError("midas_b200 runs on CUDA devices only (got device %r)" % (device,))
+    if not torch.cuda.is_available():
+        raise RuntimeError("midas_b200 needs a CUDA device; none is available")
+    return d.index if d.index is not None else torch.cuda.current_device()
+
+
+class CakePlan:
+    """Device-resident caking plan for one (map, binning, mode, normalisation).
+
+    Args:
+        pixmap: the Map.bin / nMap.bin pair (``bin_io.PixelMap``).
+        n_r, n_eta: bin grid; bins are R-major.
+        n_pixels_y, n_pixels_z: detector shape; flat pixel = z * NY + y.
+        mode: 'floor' | 'bilinear' | 'gradient'.
+        normalize: divide by the bin area (Normalize key).
+        semantics: 'py' (midas_integrate kernels.py) or 'gpustream'
+            (IntegratorFitPeaksGPUStream normaliser and fp32 resampling).
+        bc_y, bc_z: beam centre (px), used by gradient mode.
+        device: CUDA device.
+        tile_rows, tile_pixels, frames_per_lane: tiling knobs (0 = default).
+    """
+
+    def __init__(self, pixmap: PixelMap, *, n_r: int, n_eta: int, n_pixels_y: int,
+                 n_pixels_z: int, mode: str = "floor", normalize: bool = True,
+                 semantics: str = "py", bc_y: float = 0.0, bc_z: float = 0.0,
+                 device="cuda", tile_rows: int = 0, tile_pixels: int = 0,
+                 frames_per_lane: int = 0):
+        if pixmap.n_bins != n_r * n_eta:
+            raise ValueError(f"PixelMap has {pixmap.n_bins} bins; n_r * n_eta = {n_r * n_eta}")
+        if mode not in L.MODE:
+            raise ValueError(f"unknown integration mode {mode!r}; expected 'floor' | 'bilinear' | 'gradient'")
+        if semantics not in L.SEM:
+            raise ValueError(f"unknown semantics {semantics!r}")
+        self.device = torch.device("cuda", _device_index(device))
+        self.n_r, self.n_eta = int(n_r), int(n_eta)
+        self.ny, self.nz = int(n_pixels_y), int(n_pixels_z)
+        self.mode, self.normalize, self.semantics = mode, bool(normalize), semantics
+        self.bc_y, self.bc_z = float(bc_y), float(bc_z)
+        recs = np.ascontiguousarray(pixmap.pxList)
+        nmap = np.ascontiguousarray(pixmap.nmap_pairs())
+        desc = L.MiMapDesc(recs.ctypes.data if recs.size else None, recs.shape[0],
+                           nmap.ctypes.data, self.n_r, self.n_eta, self.ny, self.nz,
+                           self.bc_y, self.bc_z)
+        opts = L.MiPlanOpts(L.MODE[mode], int(self.normalize), L.SEM[semantics],
+                            int(tile_rows), int(tile_pixels), int(frames_per_lane))
+        h = C.c_void_p()
+        L.check(L.lib().mi_plan_create(C.byref(desc), C.byref(opts), self.device.index,
+                                       C.byref(h)), "mi_plan_create")
+        self._h = h
+        self._dark = None
+
+    # -- lifecycle --------------------------------------------------------
+    def close(self) -> None:
+        if getattr(self, "_h", None) and self._h.value:
+            L.lib().mi_plan_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def n_bins(self) -> int:
+        return self.n_r * self.n_eta
+
+    @property
+    def info(self) -> Dict[str, int]:
+        inf = L.MiPlanInfo()
+        L.check(L.lib().mi_plan_get_info(self._h, C.byref(inf)), "mi_plan_get_info")
+        return {k: getattr(inf, k) for k, _ in L.MiPlanInfo._fields_}
+
+    def set_dark(self, dark) -> None:
+        """Per-pixel dark (ny*nz floats; frames are cast and have it subtracted)."""
+        if dark is None:
+            L.check(L.lib().mi_plan_set_dark(self._h, None), "mi_plan_set_dark")
+            self._dark = None
+            return
+        d = np.ascontiguousarray(np.asarray(dark, dtype=np.float32).reshape(-1))
+        if d.size != self.ny * self.nz:
+            raise ValueError(f"dark has {d.size} pixels, expected {self.ny * self.nz}")
+        L.check(L.lib().mi_plan_set_dark(self._h, d.ctypes.data), "mi_plan_set_dark")
+        self._dark = d
+
+    # -- work ---------------------------------------------------------------
+    def _frames(self, frames: torch.Tensor) -> Tuple[torch.Tensor, int, int]:
+        if frames.device != self.device:
+            raise ValueError(f"frames on {frames.device}, plan on {self.device}")
+        if frames.dim() == 2:
+            frames = frames.unsqueeze(0)
+        if frames.dim() != 3 and frames.dim() != 2:
+            raise ValueError("frames must be (F, NZ, NY), (NZ, NY) or (F, NZ*NY)")
+        F = frames.shape[0]
+        per = frames[0].numel() if F else self.ny * self.nz
+        if per != self.ny * self.nz:
+            raise ValueError(f"frame has {per} pixels, expected {self.ny * self.nz}")
+        flat = frames.reshape(F, -1)
+        if flat.stride(1) != 1:
+            flat = flat.contiguous()
+        return flat, F, flat.stride(0) if F else per
+
+    def integrate(self, frames: torch.Tensor, *, cake: bool = True, lineouts: bool = True,
+                  out: Optional[Dict[str, torch.Tensor]] = None, stream=None):
+        """Cake a batch of frames (device tensor, any supported dtype).
+
+        Returns (cake [F, n_r, n_eta] float32 or None, lineout_aw [F, n_r] float64 or None,
+        lineout_sm [F, n_r] float64 or None)."""
+        flat, F, stride = self._frames(frames)
+        out = out or {}
+        ck = out.get("cake") if cake else None
+        if cake and ck is None:
+            ck = torch.empty((F, self.n_r, self.n_eta), dtype=torch.float32, device=self.device)
+        aw = sm = None
+        if lineouts:
+            aw = out.get("lineout_aw")
+            sm = out.get("lineout_sm")
+            if aw is None:
+                aw = torch.empty((F, self.n_r), dtype=torch.float64, device=self.device)
+            if sm is None:
+                sm = torch.empty((F, self.n_r), dtype=torch.float64, device=self.device)
+        if F:
+            L.check(L.lib().mi_integrate_batch(self._h, flat.data_ptr(), dtype_code(flat.dtype), F,
+                                               stride, L.ptr(ck), L.ptr(aw), L.ptr(sm),
+                                               L.stream_ptr(stream)), "mi_integrate_batch")
+        return ck, aw, sm
+
+    def integrate_plain(self, frame: torch.Tensor, stream=None):
+        """The reference algorithm, one frame per launch: (cake float64 [n_r, n_eta], aw, sm)."""
+        flat, F, _ = self._frames(frame)
+        if F != 1:
+            raise ValueError("integrate_plain takes exactly one frame")
+        ck = torch.empty((self.n_r, self.n_eta), dtype=torch.float64, device=self.device)
+        aw = torch.empty(self.n_r, dtype=torch.float64, device=self.device)
+        sm = torch.empty(self.n_r, dtype=torch.float64, device=self.device)
+        L.check(L.lib().mi_integrate_plain(self._h, flat.data_ptr(), dtype_code(flat.dtype),
+                                           ck.data_ptr(), aw.data_ptr(), sm.data_ptr(),
+                                           L.stream_ptr(stream)), "mi_integrate_plain")
+        return ck, aw, sm
+
+    def profile(self, cake: torch.Tensor, stream=None):
+        """Kernel (c) on a given cake [F, n_r, n_eta] (float32/float64) -> (aw, sm) [F, n_r]."""
+        if cake.dim() == 2:
+            cake = cake.unsqueeze(0)
+        if cake.dtype not in (torch.float32, torch.float64):
+            cake = cake.to(torch.float64)
+        cake = cake.contiguous()
+        F = cake.shape[0]
+        aw = torch.empty((F, self.n_r), dtype=torch.float64, device=self.device)
+        sm = torch.empty((F, self.n_r), dtype=torch.float64, device=self.device)
+        L.check(L.lib().mi_profile_batch(self._h, cake.data_ptr(), dtype_code(cake.dtype), F,
+                                         aw.data_ptr(), sm.data_ptr(), L.stream_ptr(stream)),
+                "mi_profile_batch")
+        return aw, sm
+
+
+# ---------------------------------------------------------------------------
+# midas_integrate-compatible surface
+# ---------------------------------------------------------------------------
+@dataclass
+class CSRGeometry:
+    """Geometry for a fixed detector + bin layout (kernels.py:CSRGeometry).
+
+    Holds one device plan per (mode, normalize) pair, created on first use."""
+    pixmap: PixelMap
+    area_per_bin: torch.Tensor
+    n_r: int
+    n_eta: int
+    n_pixels_y: int
+    n_pixels_z: int
+    bc_y: float = 0.0
+    bc_z: float = 0.0
+    semantics: str = "py"
+    build_modes: Tuple[str, ...] = ("floor", "bilinear", "gradient")
+    dtype: torch.dtype = torch.float32
+    plans: Dict[Tuple[str, bool], CakePlan] = field(default_factory=dict)
+
+    @property
+    def n_bins(self) -> int:
+        return self.n_r * self.n_eta
+
+    @property
+    def device(self) -> torch.device:
+        return self.area_per_bin.device
+
+    def plan(self, mode: str, normalize: bool = True) -> CakePlan:
+        if mode not in L.MODE:
+            raise ValueError(f"unknown integration mode {mode!r}; expected 'floor' | 'bilinear' | 'gradient'")
+        if mode not in self.build_modes:
+            raise RuntimeError(f"build_csr was called without {mode!r} in build_modes; "
+                               "rebuild with build_modes including this mode.")
+        key = (mode, bool(normalize))
+        if key not in self.plans:
+            self.plans[key] = CakePlan(self.pixmap, n_r=self.n_r, n_eta=self.n_eta,
+                                       n_pixels_y=self.n_pixels_y, n_pixels_z=self.n_pixels_z,
+                                       mode=mode, normalize=normalize, semantics=self.semantics,
+                                       bc_y=self.bc_y, bc_z=self.bc_z, device=self.device)
+        return self.plans[key]
+
+
+def _area_in(pixmap: PixelMap, ny: int, nz: int) -> np.ndarray:
+    """In-bounds areaWeight per bin (the bounds-checked area of kernels.py:306-311)."""
+    px = pixmap.pxList
+    counts = pixmap.counts.astype(np.int64)
+    if (counts < 0).any():
+        raise ValueError("nMap.bin contains negative pixel counts")
+    end = pixmap.offsets.astype(np.int64) + counts
+    if ((end > pixmap.n_entries) & (counts > 0)).any():
+        raise ValueError("bin(s) reference past end of pxList")
+    area = np.zeros(pixmap.n_bins, dtype=np.float64)
+    if counts.sum() == 0:
+        return area
+    idx = np.concatenate([np.arange(o, o + c) for o, c in zip(pixmap.offsets, counts) if c])
+    b = np.repeat(np.arange(pixmap.n_bins), counts)
+    rec = px[idx]
+    iy = rec["y"].astype(np.float64).astype(np.int64)
+    iz = rec["z"].astype(np.float64).astype(np.int64)
+    ok = (iy >= 0) & (iy < ny) & (iz >= 0) & (iz < nz)
+    np.add.at(area, b, np.where(ok, rec["areaWeight"].astype(np.float64), 0.0))
+    return area
+
+
+def build_csr(pixmap: PixelMap, *, n_r: int, n_eta: int, n_pixels_y: int, n_pixels_z: int,
+              device="cuda", dtype: torch.dtype = torch.float32, bc_y: float = 0.0,
+              bc_z: float = 0.0, build_modes: Tuple[str, ...] = ("floor", "bilinear", "gradient"),
+              semantics: str = "py") -> CSRGeometry:
+    """Prepare a map for integration (kernels.py:build_csr).  The per-mode device plans
+    are built lazily by the first ``integrate`` call of that mode."""
+    if pixmap.n_bins != n_r * n_eta:
+        raise ValueError(f"PixelMap has {pixmap.n_bins} bins; n_r * n_eta = {n_r * n_eta}")
+    dev = torch.device("cuda", _device_index(device))
+    area = _area_in(pixmap, n_pixels_y, n_pixels_z)
+    return CSRGeometry(pixmap=pixmap, area_per_bin=torch.from_numpy(area).to(dev, dtype),
+                       n_r=n_r, n_eta=n_eta, n_pixels_y=n_pixels_y, n_pixels_z=n_pixels_z,
+                       bc_y=bc_y, bc_z=bc_z, semantics=semantics,
+                       build_modes=tuple(build_modes), dtype=dtype)
+
+
+def integrate(image: torch.Tensor, geom: CSRGeometry, *, mode: str = "floor",
+              normalize: bool = True) -> torch.Tensor:
+    """Integrate one (dark-subtracted) image to the (n_r, n_eta) grid (kernels.py:integrate)."""
+    plan = geom.plan(mode, normalize)
+    flat = image.reshape(-1)
+    if flat.numel() != geom.n_pixels_y * geom.n_pixels_z:
+        raise ValueError(f"image numel {flat.numel()} != n_pixels {geom.n_pixels_y * geom.n_pixels_z}")
+    flat = flat.to(geom.device)
+    if flat.dtype not in _TORCH_DT:
+        flat = flat.to(torch.float32)
+    ck, _, _ = plan.integrate(flat.reshape(1, -1), cake=True, lineouts=False)
+    return ck[0].to(geom.dtype)
+
+
+def profile_1d(int2d: torch.Tensor, geom: CSRGeometry, *, mode: str = "area_weighted") -> torch.Tensor:
+    """Reduce (n_r, n_eta) -> (n_r,) over eta (kernels.py:profile_1d)."""
+    if mode not in ("area_weighted", "simple_mean"):
+        raise ValueError(f"unknown profile_1d mode {mode!r}")
+    plan = next(iter(geom.plans.values()), None) or geom.plan(geom.build_modes[0], True)
+    aw, sm = plan.profile(int2d.to(geom.device).reshape(1, geom.n_r, geom.n_eta))
+    return (aw[0] if mode == "area_weighted" else sm[0]).to(geom.dtype)
+
+
+def r_axis(*, n_r: int, RMin: float, RBinSize: float) -> np.ndarray:
+    """R at bin centres."""
+    return RMin + RBinSize * (np.arange(n_r, dtype=np.float64) + 0.5)
+
+
+def eta_axis(*, n_eta: int, EtaMin: float, EtaBinSize: float) -> np.ndarray:
+    """Eta at bin centres."""
+    return EtaMin + EtaBinSize * (np.arange(n_eta, dtype=np.float64) + 0.5)

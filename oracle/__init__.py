@@ -1,0 +1,162 @@
+"""FP64 CPU oracle of the MIDAS caking hot path -- TEST INFRASTRUCTURE ONLY.
+
+Python (ctypes) access to:
+  * liboracle.so: the FP64 C restatement in oracle.c (integrate in both reference
+    semantics, the two profiles, the LM fitter twin);
+  * _ref/libmidas_ref.so (when it was built from the reference sources):
+    the reference's own mapper_build_map and integration_apply_map.
+
+Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline / reference legs
+import this package; the library under test never does.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+LIB = HERE / "liboracle.so"
+REF_LIB = HERE / "_ref" / "libmidas_ref.so"
+
+REC_DTYPE = np.dtype([("y", "<f4"), ("z", "<f4"), ("frac", "<f8"), ("deltaR", "<f4"),
+                      ("areaWeight", "<f4")])
+MODES = {"floor": 0, "bilinear": 1, "gradient": 2}
+SEMS = {"py": 0, "gpustream": 1}
+
+_lib = None
+_ref = None
+
+
+def build() -> None:
+    """Compile liboracle.so (and _ref when the reference sources exist)."""
+    subprocess.run(["make", "-s", "-C", str(HERE)], check=True, capture_output=True)
+
+
+def lib() -> C.CDLL:
+    global _lib
+    if _lib is None:
+        if not LIB.exists():
+            build()
+        L = C.CDLL(str(LIB))
+        vp, i, d = C.c_void_p, C.c_int, C.c_double
+        L.or_integrate.argtypes = [vp, vp, C.c_int64, i, i, d, d, vp, i, i, i, vp, vp]
+        L.or_integrate.restype = i
+        L.or_area_in.argtypes = [vp, vp, C.c_int64, i, i, vp]
+        L.or_area_in.restype = None
+        L.or_profile.argtypes = [vp, vp, i, i, vp, vp]
+        L.or_profile.restype = None
+        L.or_fit.argtypes = [vp, vp, i, d, i, i, i, d, d, d, vp]
+        L.or_fit.restype = i
+        _lib = L
+    return _lib
+
+
+def ref_available() -> bool:
+    return REF_LIB.exists()
+
+
+def ref() -> C.CDLL:
+    global _ref
+    if _ref is None:
+        if not REF_LIB.exists():
+            raise RuntimeError("oracle/_ref/libmidas_ref.so was not built (reference sources absent)")
+        R = C.CDLL(str(REF_LIB))
+        vp, i, d = C.c_void_p, C.c_int, C.c_double
+        R.ref_build_map.argtypes = [i, i, d, d, d, d, d, d, d, d, vp, d, i, i, d, i, d, vp, vp, vp, vp, i, i, i,
+                                    C.POINTER(vp), C.POINTER(vp), C.POINTER(vp)]
+        R.ref_build_map.restype = C.c_longlong
+        R.ref_free.argtypes = [vp]
+        R.ref_integrate.argtypes = [vp, vp, i, i, vp, i, i, vp, d, d, i, i, i, vp, vp]
+        R.ref_integrate.restype = i
+        R.ref_max_threads.restype = i
+        _ref = R
+    return _ref
+
+
+def _c(a, dt):
+    return np.ascontiguousarray(a, dtype=dt)
+
+
+def integrate(records, nmap, n_bins, ny, nz, image, *, mode="floor", semantics="py", normalize=True,
+              bc_y=0.0, bc_z=0.0):
+    """FP64 cake (n_bins,) and normaliser (n_bins,) of one dark-subtracted image."""
+    rec = _c(records, REC_DTYPE)
+    nm = _c(nmap, np.int32).reshape(-1)
+    img = _c(image, np.float64).reshape(-1)
+    cake = np.zeros(n_bins)
+    area = np.zeros(n_bins)
+    rc = lib().or_integrate(rec.ctypes.data if rec.size else None, nm.ctypes.data, n_bins, ny, nz, bc_y, bc_z,
+                            img.ctypes.data, MODES[mode], SEMS[semantics], int(normalize), cake.ctypes.data,
+                            area.ctypes.data)
+    if rc:
+        raise ValueError(f"or_integrate failed ({rc})")
+    return cake, area
+
+
+def area_in(records, nmap, n_bins, ny, nz):
+    rec = _c(records, REC_DTYPE)
+    nm = _c(nmap, np.int32).reshape(-1)
+    out = np.zeros(n_bins)
+    lib().or_area_in(rec.ctypes.data if rec.size else None, nm.ctypes.data, n_bins, ny, nz, out.ctypes.data)
+    return out
+
+
+def profile(cake, area, n_r, n_eta):
+    ck = _c(cake, np.float64).reshape(-1)
+    ar = _c(area, np.float64).reshape(-1)
+    aw = np.zeros(n_r)
+    sm = np.zeros(n_r)
+    lib().or_profile(ck.ctypes.data, ar.ctypes.data, n_r, n_eta, aw.ctypes.data, sm.ctypes.data)
+    return aw, sm
+
+
+def fit(x, y, peak, *, half_window=15, model=0, max_iter=200, x_bin=1.0, px_um=0.0, lsd_um=0.0):
+    """FP64 LM fit of one window -> (11 outputs, iterations)."""
+    xs = _c(x, np.float64)
+    ys = _c(y, np.float64)
+    out = np.zeros(11)
+    it = lib().or_fit(xs.ctypes.data, ys.ctypes.data, xs.size, float(peak), int(half_window), int(model),
+                      int(max_iter), float(x_bin), float(px_um), float(lsd_um), out.ctypes.data)
+    return out, it
+
+
+def ref_build_map(*, ny, nz, px, lsd, bc_y, bc_z, tx=0.0, ty=0.0, tz=0.0, rho_d=0.0, p=None, parallax=0.0,
+                  solid_angle=0, polarization=0, pol_fraction=0.99, sub_pixel_level=1, sub_pixel_width=10.0,
+                  r_lo, r_hi, eta_lo, eta_hi, n_threads=0):
+    """The reference's mapper_build_map -> (records, nmap[n_bins, 2], bin_mask)."""
+    R = ref()
+    pp = _c(p if p is not None else np.zeros(15), np.float64)
+    rl, rh, el, eh = (_c(a, np.float64) for a in (r_lo, r_hi, eta_lo, eta_hi))
+    recs_p, nmap_p, mask_p = C.c_void_p(), C.c_void_p(), C.c_void_p()
+    tot = R.ref_build_map(ny, nz, px, lsd, bc_y, bc_z, tx, ty, tz, rho_d, pp.ctypes.data, parallax,
+                          int(solid_angle), int(polarization), pol_fraction, int(sub_pixel_level),
+                          sub_pixel_width, rl.ctypes.data, rh.ctypes.data, el.ctypes.data, eh.ctypes.data,
+                          rl.size, el.size, int(n_threads), C.byref(recs_p), C.byref(nmap_p), C.byref(mask_p))
+    nb = rl.size * el.size
+    recs = np.frombuffer((C.c_char * (24 * max(tot, 0))).from_address(recs_p.value), dtype=REC_DTYPE).copy() \
+        if tot > 0 else np.empty(0, REC_DTYPE)
+    nmap = np.frombuffer((C.c_int32 * (2 * nb)).from_address(nmap_p.value), dtype=np.int32).copy().reshape(nb, 2)
+    mask = np.frombuffer((C.c_int32 * nb).from_address(mask_p.value), dtype=np.int32).copy()
+    for q in (recs_p, nmap_p, mask_p):
+        R.ref_free(q)
+    return recs, nmap, mask
+
+
+def ref_integrate(records, nmap, n_r, n_eta, image, ny, nz, *, dark=None, bc_y=0.0, bc_z=0.0, gradient=0,
+                  n_threads=0, chunk_rows=8):
+    """The reference's integration_apply_map over R-row chunks -> (sums, norms) per bin."""
+    R = ref()
+    rec = _c(records, REC_DTYPE)
+    nm = _c(nmap, np.int32).reshape(-1)
+    img = _c(image, np.float64).reshape(-1)
+    dk = _c(dark, np.float64).reshape(-1) if dark is not None else None
+    prof = np.zeros(n_r * n_eta)
+    norm = np.zeros(n_r * n_eta)
+    R.ref_integrate(rec.ctypes.data, nm.ctypes.data, n_r, n_eta, img.ctypes.data, ny, nz,
+                    dk.ctypes.data if dk is not None else None, bc_y, bc_z, int(gradient), int(n_threads),
+                    int(chunk_rows), prof.ctypes.data, norm.ctypes.data)
+    return prof, norm

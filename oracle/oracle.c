@@ -1,0 +1,373 @@
+/*
+ * oracle.c -- FP64 CPU restatement of the MIDAS caking hot path (test infrastructure).
+ *
+ * or_integrate follows, per semantics:
+ *   0: integrate() of packages/midas_integrate/midas_integrate/kernels.py:416-473 with the
+ *      CSR of build_csr (kernels.py:242-375) written as the explicit per-record loops of
+ *      packages/midas_integrate/tests/test_kernels.py:55-114 (floor: truncated (y,z),
+ *      off-detector records skipped; bilinear: np.floor + clamp; gradient: sample point
+ *      shifted by -deltaR along the radius, kernels.py:343-353); normaliser = in-bounds
+ *      areaWeight sum (kernels.py:306-318).
+ *   1: integrate_noMapMask of FF_HEDM/src/IntegratorFitPeaksGPUStream.cu:975-1050
+ *      (floor offset (long long)z*NY + y evaluated in float, :915; fp32 gradient shift,
+ *      :1007-1018; normaliser = sum of all areaWeight, :1034-1040) with FP64 sums.
+ * or_profile follows profile_1d (kernels.py:567-601) = calculate_1D_profile_kernel and
+ * calculate_1D_profile_simple_mean_kernel (IntegratorFitPeaksGPUStream.cu:1162-1334).
+ * or_fit is the FP64 twin of the device Levenberg-Marquardt fitter (same window, same
+ * initial guess from pf_estimate_initial_params, FF_HEDM/src/PeakFit.c:218-250, same
+ * model definitions incl. pf_calculate_model / pf_tch_eta_fwhm, PeakFit.c:17-92).
+ */
+#include "oracle.h"
+
+#include <math.h>
+#include <string.h>
+
+#define AREA_THRESHOLD 1e-9
+
+static double bilinear(const double *img, int ny, int nz, double sy, double sz) {
+  double fiy = floor(sy), fiz = floor(sz);
+  long iy = (long)fiy, iz = (long)fiz;
+  double fy = sy - (double)iy, fz = sz - (double)iz;
+  int over_y = iy >= ny - 1, under_y = iy < 0, over_z = iz >= nz - 1, under_z = iz < 0;
+  if (over_y) { iy = ny - 2; fy = 1.0; }
+  if (under_y) { iy = 0; fy = 0.0; }
+  if (over_z) { iz = nz - 2; fz = 1.0; }
+  if (under_z) { iz = 0; fz = 0.0; }
+  const double *p = img + iz * (long)ny + iy;
+  return p[0] * (1 - fy) * (1 - fz) + p[1] * fy * (1 - fz) + p[ny] * (1 - fy) * fz + p[ny + 1] * fy * fz;
+}
+
+void or_area_in(const or_record *rec, const int32_t *nmap, int64_t n_bins, int ny, int nz, double *area) {
+  for (int64_t b = 0; b < n_bins; ++b) {
+    double A = 0;
+    for (int k = 0; k < nmap[2 * b]; ++k) {
+      const or_record *e = rec + nmap[2 * b + 1] + k;
+      long ty = (long)(double)e->y, tz = (long)(double)e->z;
+      if (ty >= 0 && ty < ny && tz >= 0 && tz < nz) A += e->areaWeight;
+    }
+    area[b] = A;
+  }
+}
+
+int or_integrate(const or_record *rec, const int32_t *nmap, int64_t n_bins, int ny, int nz, double bc_y,
+                 double bc_z, const double *image, int mode, int sem, int normalize, double *cake, double *area_out) {
+  const long npix = (long)ny * nz;
+  for (int64_t b = 0; b < n_bins; ++b) {
+    double I = 0.0, A_in = 0.0, A_all = 0.0;
+    const int cnt = nmap[2 * b], off = nmap[2 * b + 1];
+    if (cnt < 0) return -2;
+    for (int k = 0; k < cnt; ++k) {
+      const or_record *e = rec + off + k;
+      const double y = e->y, z = e->z;
+      const long ty = (long)y, tz = (long)z;
+      const int inb = ty >= 0 && ty < ny && tz >= 0 && tz < nz;
+      A_all += e->areaWeight;
+      if (inb) A_in += e->areaWeight;
+      if (mode == 0) {
+        if (sem == 1) {
+          long long zz = (long long)e->z;
+          float s = (float)(zz * (long long)ny) + e->y;
+          long long o = (long long)s;
+          if (o >= 0 && o < npix) I += image[o] * e->frac;
+        } else if (inb) {
+          I += image[tz * ny + ty] * e->frac;
+        }
+      } else {
+        double sy = y, sz = z;
+        if (mode == 2) {
+          if (sem == 1) {
+            float dy = e->y - (float)bc_y, dz = e->z - (float)bc_z;
+            float R = sqrtf(dy * dy + dz * dz);
+            float ry = e->y, rz = e->z;
+            if (R > 1.0f) {
+              ry -= e->deltaR * dy / R;
+              rz -= e->deltaR * dz / R;
+            }
+            sy = ry;
+            sz = rz;
+          } else {
+            double dy = y - bc_y, dz = z - bc_z;
+            double R = sqrt(dy * dy + dz * dz);
+            double sc = R > 1.0 ? (double)e->deltaR / R : 0.0;
+            sy = y - sc * dy;
+            sz = z - sc * dz;
+          }
+        }
+        I += bilinear(image, ny, nz, sy, sz) * e->frac;
+      }
+    }
+    double out;
+    if (sem == 1) {
+      out = A_all > AREA_THRESHOLD ? (normalize ? I / A_all : I) : 0.0;
+      if (area_out) area_out[b] = A_all;
+    } else {
+      out = normalize ? (A_in > AREA_THRESHOLD ? I / A_in : 0.0) : I;
+      if (area_out) area_out[b] = A_in;
+    }
+    cake[b] = out;
+  }
+  return 0;
+}
+
+void or_profile(const double *cake, const double *area_in, int n_r, int n_eta, double *lo_aw, double *lo_sm) {
+  for (int r = 0; r < n_r; ++r) {
+    double sia = 0, sa = 0, si = 0;
+    int n = 0;
+    for (int e = 0; e < n_eta; ++e) {
+      const long b = (long)r * n_eta + e;
+      const double A = area_in[b];
+      if (A > AREA_THRESHOLD) {
+        sia += cake[b] * A;
+        sa += A;
+        si += cake[b];
+        ++n;
+      }
+    }
+    if (lo_aw) lo_aw[r] = sa > AREA_THRESHOLD ? sia / sa : 0.0;
+    if (lo_sm) lo_sm[r] = n > 0 ? si / n : 0.0;
+  }
+}
+
+/* ------------------------------------------------------------------ fitter */
+#define NP 6
+
+static void tch(double sig, double gam, double *fw, double *eta, double *dfw_ds, double *dfw_dg, double *de_ds,
+                double *de_dg) {
+  const double ln2x8 = 5.545177444479562;
+  const double s = fmax(sig, 1e-12);
+  const double fg = sqrt(fmax(ln2x8 * s, 0.0)) / 100.0;
+  const double fl = fmax(gam, 1e-6) / 100.0;
+  const double dfg_ds = (sig > 1e-12) ? fg / (2.0 * s) : 0.0;
+  const double dfl_dg = (gam > 1e-6) ? 0.01 : 0.0;
+  const double g2 = fg * fg, g3 = g2 * fg, g4 = g3 * fg, g5 = g4 * fg;
+  const double l2 = fl * fl, l3 = l2 * fl, l4 = l3 * fl, l5 = l4 * fl;
+  const double P = g5 + 2.69269 * g4 * fl + 2.42843 * g3 * l2 + 4.47163 * g2 * l3 + 0.07842 * fg * l4 + l5;
+  double F = pow(fmax(P, 1e-300), 0.2);
+  const double dP_dg = 5 * g4 + 4 * 2.69269 * g3 * fl + 3 * 2.42843 * g2 * l2 + 2 * 4.47163 * fg * l3 + 0.07842 * l4;
+  const double dP_dl = 2.69269 * g4 + 2 * 2.42843 * g3 * fl + 3 * 4.47163 * g2 * l2 + 4 * 0.07842 * fg * l3 + 5 * l4;
+  const double dF_dP = (F > 1e-15) ? 0.2 * F / fmax(P, 1e-300) : 0.0;
+  if (F < 1e-15) F = 1e-15;
+  const double dF_dg = dF_dP * dP_dg, dF_dl = dF_dP * dP_dl;
+  const double r = fl / F;
+  double e = 1.36603 * r - 0.47719 * r * r + 0.11116 * r * r * r;
+  double de_dr = 1.36603 - 2 * 0.47719 * r + 3 * 0.11116 * r * r;
+  if (e < 0 || e > 1) de_dr = 0;
+  e = fmin(fmax(e, 0.0), 1.0);
+  const double dr_dl = 1.0 / F - fl * dF_dl / (F * F);
+  const double dr_dg = -fl * dF_dg / (F * F);
+  *fw = F;
+  *eta = e;
+  *dfw_ds = dF_dg * dfg_ds;
+  *dfw_dg = dF_dl * dfl_dg;
+  *de_ds = de_dr * dr_dg * dfg_ds;
+  *de_dg = de_dr * dr_dl * dfl_dg;
+}
+
+static double model(int kind, const double *p, double xl, double xn, double *g) {
+  if (kind == 0) {
+    const double c = p[0], h = p[1], w = fmax(p[2], 1e-6), et = p[3];
+    const double hw = 0.5 * w, u = (xl - c) / hw, u2 = u * u;
+    const double L = 1.0 / (1.0 + u2), G = exp(-0.6931471805599453 * u2);
+    const double P = et * L + (1.0 - et) * G;
+    const double dP_du2 = -et * L * L - (1.0 - et) * 0.6931471805599453 * G;
+    g[0] = h * dP_du2 * (-2.0 * u / hw);
+    g[1] = P;
+    g[2] = h * dP_du2 * (-u2 / hw);
+    g[3] = h * (L - G);
+    g[4] = 1.0;
+    g[5] = xn;
+    return p[4] + p[5] * xn + h * P;
+  }
+  const double A = p[0], c = p[1];
+  double F, et, dF_ds, dF_dg, de_ds, de_dg;
+  tch(p[2], p[3], &F, &et, &dF_ds, &dF_dg, &de_ds, &de_dg);
+  const double sg = F * 0.42466090014400953, Gn = 0.3989422804014327 / sg, hw = 0.5 * F;
+  const double dx = xl - c, dx2 = dx * dx;
+  const double G = Gn * exp(-0.5 * dx2 / (sg * sg));
+  const double den = dx2 + hw * hw;
+  const double L = 0.3183098861837907 * hw / den;
+  const double P = et * L + (1.0 - et) * G;
+  const double dG_dc = G * dx / (sg * sg), dL_dc = L * 2.0 * dx / den;
+  const double dG_dsg = G * (-1.0 / sg + dx2 / (sg * sg * sg));
+  const double dL_dhw = 0.3183098861837907 * (den - 2.0 * hw * hw) / (den * den);
+  const double dP_dF = et * dL_dhw * 0.5 + (1.0 - et) * dG_dsg * 0.42466090014400953;
+  const double dP_de = L - G;
+  g[0] = P;
+  g[1] = A * (et * dL_dc + (1.0 - et) * dG_dc);
+  g[2] = A * (dP_dF * dF_ds + dP_de * de_ds);
+  g[3] = A * (dP_dF * dF_dg + dP_de * de_dg);
+  g[4] = 1.0;
+  g[5] = xn;
+  return p[4] + p[5] * xn + A * P;
+}
+
+static int chol_solve(double A[NP][NP], const double *b, double *x) {
+  double L[NP][NP], y[NP];
+  memset(L, 0, sizeof(L));
+  for (int i = 0; i < NP; ++i)
+    for (int j = 0; j <= i; ++j) {
+      double s = A[i][j];
+      for (int k = 0; k < j; ++k) s -= L[i][k] * L[j][k];
+      if (i == j) {
+        if (!(s > 0.0)) return 0;
+        L[i][i] = sqrt(s);
+      } else {
+        L[i][j] = s / L[j][j];
+      }
+    }
+  for (int i = 0; i < NP; ++i) {
+    double s = b[i];
+    for (int k = 0; k < i; ++k) s -= L[i][k] * y[k];
+    y[i] = s / L[i][i];
+  }
+  for (int i = NP - 1; i >= 0; --i) {
+    double s = y[i];
+    for (int k = i + 1; k < NP; ++k) s -= L[k][i] * x[k];
+    x[i] = s / L[i][i];
+  }
+  return 1;
+}
+
+static void clamp_params(int kind, double *p, double half_span, double x_bin) {
+  if (kind == 0) {
+    p[0] = fmin(fmax(p[0], -half_span), half_span);
+    p[1] = fmax(p[1], 0.0);
+    p[2] = fmin(fmax(p[2], 0.05 * x_bin), 4.0 * half_span);
+    p[3] = fmin(fmax(p[3], 0.0), 1.0);
+  } else {
+    p[0] = fmax(p[0], 0.0);
+    p[1] = fmin(fmax(p[1], -half_span), half_span);
+    p[2] = fmax(p[2], 1e-6);
+    p[3] = fmax(p[3], 0.01);
+  }
+}
+
+static void eval(int kind, const double *p, const double *x, const double *y, int s0, int n, double xref, double xlo,
+                 double xr, double JtJ[NP][NP], double *Jtr, double *chi2) {
+  double jj[NP][NP], jr[NP], c2 = 0;
+  memset(jj, 0, sizeof(jj));
+  memset(jr, 0, sizeof(jr));
+  for (int i = 0; i < n; ++i) {
+    const double xi = x[s0 + i];
+    double g[NP];
+    const double m = model(kind, p, xi - xref, 2.0 * (xi - xlo) / xr - 1.0, g);
+    const double r = y[s0 + i] - m;
+    for (int u = 0; u < NP; ++u) {
+      for (int v = 0; v <= u; ++v) jj[u][v] += g[u] * g[v];
+      jr[u] += g[u] * r;
+    }
+    c2 += r * r;
+  }
+  if (JtJ)
+    for (int u = 0; u < NP; ++u)
+      for (int v = 0; v <= u; ++v) JtJ[u][v] = JtJ[v][u] = jj[u][v];
+  if (Jtr)
+    for (int u = 0; u < NP; ++u) Jtr[u] = jr[u];
+  *chi2 = c2;
+}
+
+int or_fit(const double *x, const double *y, int n_x, double loc, int half, int kind, int max_iter, double x_bin,
+           double px, double lsd, double *out) {
+  memset(out, 0, 11 * sizeof(double));
+  int best = -1;
+  double bd = 1e300;
+  for (int i = 0; i < n_x; ++i) {
+    const double d = fabs(x[i] - loc);
+    if (d < bd) { bd = d; best = i; }
+  }
+  if (best < 0 || !(bd < 2.0 * x_bin)) return -1;
+  const int s0 = best - half < 0 ? 0 : best - half;
+  const int s1 = best + half > n_x - 1 ? n_x - 1 : best + half;
+  const int n = s1 - s0 + 1;
+  if (n < NP + 1) return -2;
+  const double xref = x[best], xlo = x[s0], xhi = x[s1];
+  const double xr = fmax(xhi - xlo, 1e-12);
+  const double half_span = fmax(xhi - xref, xref - xlo);
+  int bgw = n / 4 < 5 ? n / 4 : 5;
+  if (bgw < 1) bgw = 1;
+  double bgs = 0;
+  for (int i = 0; i < bgw; ++i) bgs += y[s0 + i] + y[s1 - i];
+  const double bg = bgs / (2.0 * bgw);
+  double amp = y[best] - bg;
+  if (amp <= 0) amp = y[best];
+  const double hm = bg + 0.5 * amp;
+  int li = best - s0, ri = best - s0;
+  while (li > 0 && y[s0 + li] > hm) --li;
+  while (ri < n - 1 && y[s0 + ri] > hm) ++ri;
+  double fwb = (double)(ri - li);
+  if (!(fwb > 1.0)) fwb = 2.0;
+  const double fwx = fwb * x_bin;
+  double p[NP];
+  if (kind == 0) {
+    p[0] = 0; p[1] = amp; p[2] = fwx; p[3] = 0.5; p[4] = bg; p[5] = 0;
+  } else {
+    const double fg0 = 0.5 * fwx;
+    double sg = (fg0 * 100.0) * (fg0 * 100.0) / 5.545177444479562;
+    if (sg < 1e-6) sg = 1.0;
+    double gm = fwx * 0.5 * 100.0;
+    if (gm < 0.01) gm = 1.0;
+    double ar = amp * fwx * 1.5;
+    if (ar <= 0) ar = 1.0;
+    p[0] = ar; p[1] = 0; p[2] = sg; p[3] = gm; p[4] = bg; p[5] = 0;
+  }
+  clamp_params(kind, p, half_span, x_bin);
+  double JtJ[NP][NP], Jtr[NP], chi2;
+  eval(kind, p, x, y, s0, n, xref, xlo, xr, JtJ, Jtr, &chi2);
+  double lam = 1e-3;
+  int it = 0, stall = 0;
+  for (; it < max_iter; ++it) {
+    double A[NP][NP], d[NP], pn[NP];
+    for (int u = 0; u < NP; ++u)
+      for (int v = 0; v < NP; ++v) A[u][v] = JtJ[u][v] + (u == v ? lam * fmax(JtJ[u][u], 1e-30) : 0.0);
+    int ok = chol_solve(A, Jtr, d);
+    for (int u = 0; u < NP; ++u) pn[u] = ok ? p[u] + d[u] : p[u];
+    clamp_params(kind, pn, half_span, x_bin);
+    double c2n;
+    eval(kind, pn, x, y, s0, n, xref, xlo, xr, NULL, NULL, &c2n);
+    if (ok && c2n <= chi2) {
+      double rel = 0;
+      for (int u = 0; u < NP; ++u) rel = fmax(rel, fabs(pn[u] - p[u]) / fmax(fabs(p[u]), 1e-3));
+      const double dec = chi2 - c2n;
+      memcpy(p, pn, sizeof(p));
+      eval(kind, p, x, y, s0, n, xref, xlo, xr, JtJ, Jtr, &chi2);
+      lam = fmax(lam * 0.1, 1e-12);
+      if (rel < 1e-10 || dec <= 1e-14 * chi2) {
+        if (++stall >= 2) { ++it; break; }
+      } else {
+        stall = 0;
+      }
+    } else {
+      lam *= 10.0;
+      if (lam > 1e12) { ++it; break; }
+    }
+  }
+  double area, center, sig = 0, gam = 0, fw, et, height;
+  if (kind == 0) {
+    center = xref + p[0];
+    height = p[1];
+    fw = p[2];
+    et = p[3];
+    area = height * fw * (et * 1.5707963267948966 + (1.0 - et) * 1.0644670194312262);
+  } else {
+    double t0, t1, t2, t3;
+    tch(p[2], p[3], &fw, &et, &t0, &t1, &t2, &t3);
+    area = p[0];
+    center = xref + p[1];
+    sig = p[2];
+    gam = p[3];
+    const double sgm = fw * 0.42466090014400953;
+    height = area * (et * (2.0 / (3.141592653589793 * fw)) + (1.0 - et) * 0.3989422804014327 / sgm);
+  }
+  out[0] = area;
+  out[1] = center;
+  out[2] = sig;
+  out[3] = gam;
+  out[4] = fw;
+  out[5] = et;
+  out[6] = chi2 / fmax((double)(n - NP), 1.0);
+  out[7] = height;
+  out[8] = p[4];
+  out[9] = p[5];
+  out[10] = (px > 0 && lsd > 0) ? atan(center * px / lsd) * 57.29577951308232 : 0.0;
+  return it;
+}
