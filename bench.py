@@ -1,0 +1,454 @@
+#!/usr/bin/env python
+"""Benchmark of the B200 caking hot path (kernels (a)+(b)+(c)) on a synthetic sweep.
+
+One step = one batch of F frames of the seeded omega sweep, caked (2-D cake) and
+eta-reduced (two lineouts) in one launch of the batched kernel, with the frames
+already resident in HBM.  The sweep (1440 frames of 2880x2880 u16, 23.9 GB) is
+larger than L2, and consecutive steps walk through it, so no step re-reads a
+batch from L2.
+
+Prints ONE JSON line (rank 0).  Besides the contract keys it reports the HBM
+roofline of the batched kernel, the plain one-frame-per-launch kernel (the
+reference GPU algorithm) timed on the same frames, the FP64-oracle error of a
+sampled frame, the end-to-end rate through the public API with host frames,
+and the reference's own CPU integrator timed on this host.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import subprocess
+import sys
+import tempfile
+import time
+from pathlib import Path
+
+REPO = Path(__file__).resolve().parent
+sys.path.insert(0, str(REPO))
+
+METRIC = "caked_frames_per_s"
+UNIT = "frames/s"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="sweep_2880")
+    ap.add_argument("--batch", type=int, default=128, help="frames per launch (F)")
+    ap.add_argument("--sweep-frames", type=int, default=1440)
+    ap.add_argument("--tile-rows", type=int, default=0)
+    ap.add_argument("--tile-pixels", type=int, default=0)
+    ap.add_argument("--fpl", type=int, default=0)
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-plain", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-check", action="store_true")
+    ap.add_argument("--cpu-seconds", type=float, default=12.0)
+    return ap.parse_args()
+
+
+# ---------------------------------------------------------------------------
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled every 200 ms during the timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        self.p = None
+
+    def start(self):
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.Q}",
+                                       "--format=csv,noheader,nounits", "-lms", "200"],
+                                      stdout=self.f, stderr=subprocess.DEVNULL)
+        except OSError:
+            self.p = None
+
+    def stop(self):
+        if self.p is None:
+            return None
+        time.sleep(0.25)
+        self.p.terminate()
+        try:
+            self.p.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.p.kill()
+        self.f.flush()
+        rows = [r.split(",") for r in Path(self.f.name).read_text().splitlines() if r.strip()]
+        os.unlink(self.f.name)
+        sm, mx, reasons = [], 0.0, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            try:
+                sm.append(float(r[1]))
+                mx = max(mx, float(r[2]))
+                for k, n in enumerate(names):
+                    if r[5 + k].strip().lower() == "active":
+                        reasons.add(n)
+            except (ValueError, IndexError):
+                continue
+        if not sm:
+            return None
+        sm.sort()
+        return {"sm_mhz": sm[len(sm) // 2], "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def measured_peak():
+    p = REPO / "MEASURED_PEAKS.json"
+    if p.exists():
+        try:
+            return float(json.loads(p.read_text())["hbm_gbs"]), "measured"
+        except (KeyError, ValueError):
+            pass
+    return 6650.0, "fallback"
+
+
+# ---------------------------------------------------------------------------
+def dist_setup(args):
+    import torch
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+    return rank, world, local
+
+
+def dist_max(x: float, world: int) -> float:
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+# ---------------------------------------------------------------------------
+def cpu_reference_rate(pm, w, frame_u16, dark, seconds):
+    """The reference's own integrator (integration_apply_map, compiled from the MIDAS
+    sources into oracle/_ref; else the FP64 oracle port) on this host's cores:
+    (frames/s, cores, kind, sample)."""
+    import numpy as np
+    import oracle
+    ny, nz = w.mapper.NrPixelsY, w.mapper.NrPixelsZ
+    img = frame_u16.astype(np.float64)
+    dk = dark.astype(np.float64)
+    recs, nmap = pm.pxList, pm.nmap_pairs()
+    grad = 1 if w.mode == "gradient" else 0
+    if oracle.ref_available():
+        cores = oracle.ref().ref_max_threads()
+        run = lambda: oracle.ref_integrate(recs, nmap, w.n_r, w.n_eta, img, ny, nz, dark=dk, bc_y=w.mapper.BC_y,
+                                           bc_z=w.mapper.BC_z, gradient=grad, n_threads=cores, chunk_rows=8)
+        kind = "reference"
+    else:
+        cores = 1
+        sub = img - dk
+        run = lambda: oracle.integrate(recs, nmap, pm.n_bins, ny, nz, sub, mode=w.mode, bc_y=w.mapper.BC_y,
+                                       bc_z=w.mapper.BC_z)
+        kind = "port"
+    run()  # warm-up (page-in)
+    n, t0 = 0, time.perf_counter()
+    while True:
+        run()
+        n += 1
+        el = time.perf_counter() - t0
+        if el >= seconds or n >= 200:
+            break
+    return n / el, cores, kind, f"{n} full {w.mapper.NrPixelsZ}x{w.mapper.NrPixelsY} frame(s) in {el:.1f} s"
+
+
+def main_ours(args):
+    import numpy as np
+    import torch
+
+    from midas_b200 import _lib as L, synth
+    from midas_b200.kernels import CakePlan
+    from midas_b200.mapper import build_map
+
+    rank, world, local = dist_setup(args)
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    w = synth.WORKLOADS[args.workload]()
+    ny, nz = w.mapper.NrPixelsY, w.mapper.NrPixelsZ
+    F = args.batch
+    t_setup = time.time()
+    pm, _ = build_map(w.mapper, device=local)
+    t_map = time.time() - t_setup
+    t1 = time.time()
+    plan = CakePlan(pm, n_r=w.n_r, n_eta=w.n_eta, n_pixels_y=ny, n_pixels_z=nz, mode=w.mode,
+                    bc_y=w.mapper.BC_y, bc_z=w.mapper.BC_z, device=dev,
+                    tile_rows=args.tile_rows or w.tile_rows, tile_pixels=args.tile_pixels,
+                    frames_per_lane=args.fpl)
+    t_plan = time.time() - t1
+    info = plan.info
+    dark = w.dark(device=dev)
+    dark_np = dark.cpu().numpy()
+    plan.set_dark(dark_np)
+    sweep = max(F, (args.sweep_frames // F) * F)
+    frames = torch.empty((sweep, nz, ny), dtype=torch.uint16, device=dev)
+    for s in range(0, sweep, 256):
+        w.frames(rank * sweep + s, min(256, sweep - s), out=frames[s:s + 256])
+    torch.cuda.synchronize()
+    n_batches = sweep // F
+    cake = torch.empty((F, w.n_r, w.n_eta), dtype=torch.float32, device=dev)
+    aw = torch.empty((F, w.n_r), dtype=torch.float64, device=dev)
+    sm = torch.empty((F, w.n_r), dtype=torch.float64, device=dev)
+    bufs = {"cake": cake, "lineout_aw": aw, "lineout_sm": sm}
+
+    def step(i):
+        b = i % n_batches
+        plan.integrate(frames[b * F:(b + 1) * F], out=bufs)
+
+    # ---- accuracy of a sampled frame against the FP64 oracle (untimed)
+    err = None
+    if rank == 0 and not args.no_check:
+        import oracle
+        step(0)
+        torch.cuda.synchronize()
+        sub = frames[0].cpu().numpy().astype(np.float32) - dark_np
+        ref, _ = oracle.integrate(pm.pxList, pm.nmap_pairs(), pm.n_bins, ny, nz, sub.astype(np.float64),
+                                  mode=w.mode, bc_y=w.mapper.BC_y, bc_z=w.mapper.BC_z)
+        got = cake[0].reshape(-1).cpu().numpy().astype(np.float64)
+        tau = 1e-3 * np.median(np.abs(ref[ref != 0]))
+        r = np.abs(got - ref) / np.maximum(np.abs(ref), tau)
+        area = oracle.area_in(pm.pxList, pm.nmap_pairs(), pm.n_bins, ny, nz)
+        aw_ref, _ = oracle.profile(ref, area, w.n_r, w.n_eta)
+        ra = np.abs(aw[0].cpu().numpy() - aw_ref) / np.maximum(np.abs(aw_ref), 1e-3 * np.median(np.abs(aw_ref)))
+        err = {"cake_max_rel": float(r.max()), "cake_mean_rel": float(r.mean()),
+               "lineout_max_rel": float(ra.max()), "frames_checked": 1}
+
+    # ---- warm-up, then K timed steps
+    stream = torch.cuda.current_stream()
+    for i in range(args.warmup):
+        step(i)
+    torch.cuda.synchronize()
+    barrier(world)
+    torch.cuda.synchronize()
+    clocks = ClockSampler(dev.index)
+    clocks.start()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for i in range(args.steps):
+        ev[i][0].record(stream)
+        step(args.warmup + i)
+        ev[i][1].record(stream)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    barrier(world)
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    elapsed_ms = dist_max(e0.elapsed_time(e1), world)
+    step_ms = [a.elapsed_time(b) for a, b in ev]
+    value = world * args.steps * F / (elapsed_ms / 1e3)
+    launches = args.steps * 2 * math.ceil(F / 256)   # k_cake + k_lineout per launch group
+
+    # ---- roofline of the batched launch: A(F) = map bytes + F * frame bytes
+    peak, peak_kind = measured_peak()
+    frame_bytes = ny * nz * 2
+    map_bytes = info["map_bytes"]
+    alg = map_bytes + F * frame_bytes
+    mean_step_s = sum(step_ms) / len(step_ms) / 1e3
+    achieved = alg / mean_step_s / 1e9
+    ref_bytes = map_bytes + F * (info["ref_pixels"] * 2 + w.n_r * w.n_eta * 4)
+    roofline = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                "frac": round(achieved / peak, 4), "traffic": None, "peak_kind": peak_kind,
+                "alg_bytes_per_launch": alg,
+                "achieved_touched_bytes": round(ref_bytes / mean_step_s / 1e9, 1)}
+
+    out = {"metric": METRIC, "value": round(value, 1), "unit": UNIT, "n_gpus": world, "steps": args.steps,
+           "warmup": args.warmup, "ms_per_step": round(elapsed_ms / args.steps, 4), "higher_is_better": True,
+           "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+           "config": {"workload": w.name, "frames_per_step": F, "sweep_frames": sweep,
+                      "mode": w.mode, "n_bins": w.n_r * w.n_eta, "nnz": info["nnz"],
+                      "map_records": info["n_records"], "tiles": info["n_tiles"],
+                      "tile_rows": info["tile_rows"], "tile_pixels": info["tile_pixels"],
+                      "frames_per_lane": info["frames_per_lane"],
+                      "l2": "inputs larger than L2: each step reads a new %.1f GB batch" % (F * frame_bytes / 1e9),
+                      "parallelism": f"replicas{world}"},
+           "roofline": roofline, "gpu_launches": launches,
+           "setup_s": {"map_build_gpu": round(t_map, 2), "plan_build": round(t_plan, 2)}}
+    if clk:
+        out["clocks"] = clk
+    if err:
+        out["accuracy_vs_fp64_oracle"] = err
+
+    # ---- plain one-frame-per-launch kernel (reference GPU algorithm) on the same frames
+    if not args.no_plain:
+        P = 16
+        for k in range(2):
+            plan.integrate_plain(frames[k])
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        for k in range(P):
+            plan.integrate_plain(frames[(k * 37) % sweep])
+        b.record(stream)
+        torch.cuda.synchronize()
+        plain_fps = dist_max(0, world) if False else P / (a.elapsed_time(b) / 1e3)
+        out["plain"] = {"frames_per_s": round(plain_fps, 1), "frames": P,
+                        "speedup_batched_vs_plain": round(value / world / plain_fps, 2)}
+
+    # ---- end to end through the public API: pinned host frames -> cake + lineouts -> host lineouts
+    if not args.no_e2e:
+        out["e2e"] = e2e_rate(plan, frames, F, args, w, dev, world)
+
+    # ---- CPU baseline: the reference integrator on this host (rank 0, N = 1)
+    if rank == 0 and world == 1 and not args.no_cpu:
+        fps, cores, kind, sample = cpu_reference_rate(pm, w, frames[0].cpu().numpy(), dark_np, args.cpu_seconds)
+        out["cpu_baseline"] = {"value": round(fps, 3), "unit": UNIT, "cores": cores, "kind": kind,
+                               "sample": sample}
+    if rank == 0:
+        print(json.dumps(out), flush=True)
+    plan.close()
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+def e2e_rate(plan, frames, F, args, w, dev, world):
+    """Host (pinned) frames -> H2D -> batched caking -> D2H lineouts, double-buffered on two
+    streams so the copy of batch i+1 overlaps the caking of batch i."""
+    import torch
+    nz, ny = w.shape
+    pool = min(frames.shape[0], 2 * F)
+    host = torch.empty((pool, nz, ny), dtype=torch.uint16, pin_memory=True)
+    host.copy_(frames[:pool].cpu())
+    dbuf = [torch.empty((F, nz, ny), dtype=torch.uint16, device=dev) for _ in range(2)]
+    cake = torch.empty((F, w.n_r, w.n_eta), dtype=torch.float32, device=dev)
+    aw = torch.empty((F, w.n_r), dtype=torch.float64, device=dev)
+    sm = torch.empty((F, w.n_r), dtype=torch.float64, device=dev)
+    h_aw = torch.empty((2, F, w.n_r), dtype=torch.float64, pin_memory=True)
+    h_sm = torch.empty((2, F, w.n_r), dtype=torch.float64, pin_memory=True)
+    cs, ks = torch.cuda.Stream(dev), torch.cuda.Stream(dev)
+    copied = [torch.cuda.Event() for _ in range(2)]
+    done = [torch.cuda.Event() for _ in range(2)]
+    nb = pool // F
+
+    def run(n):
+        for i in range(n):
+            s = i % 2
+            with torch.cuda.stream(cs):
+                cs.wait_event(done[s])
+                dbuf[s].copy_(host[(i % nb) * F:(i % nb + 1) * F], non_blocking=True)
+                copied[s].record(cs)
+            with torch.cuda.stream(ks):
+                ks.wait_event(copied[s])
+                plan.integrate(dbuf[s], out={"cake": cake, "lineout_aw": aw, "lineout_sm": sm}, stream=ks)
+                h_aw[s].copy_(aw, non_blocking=True)
+                h_sm[s].copy_(sm, non_blocking=True)
+                done[s].record(ks)
+        torch.cuda.synchronize()
+
+    run(max(2, args.warmup))
+    barrier(world)
+    t0 = time.perf_counter()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record(cs)
+    run(args.steps)
+    b.record(ks)
+    torch.cuda.synchronize()
+    wall = time.perf_counter() - t0
+    dev_ms = dist_max(a.elapsed_time(b), world)
+    rate = world * args.steps * F / (dev_ms / 1e3)
+    return {"value": round(rate, 1), "unit": UNIT, "h2d_bytes_per_step": F * nz * ny * 2,
+            "d2h_bytes_per_step": 2 * F * w.n_r * 8, "wall_s": round(wall, 3),
+            "pipeline": "2 streams, double-buffered H2D"}
+
+
+# ---------------------------------------------------------------------------
+def main_reference(args):
+    """The reference's own CPU integrator (integration_apply_map from the MIDAS sources,
+    oracle/_ref) on this host's cores, same workload, metric and unit."""
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    import numpy as np
+
+    import oracle
+    from midas_b200 import synth
+    w = synth.WORKLOADS[args.workload]()
+    m = w.mapper
+    ny, nz = m.NrPixelsY, m.NrPixelsZ
+    if not oracle.ref_available():
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref was not built (MIDAS C sources absent)"}))
+        return
+    r_lo, r_hi, e_lo, e_hi = m.edges()
+    t0 = time.time()
+    recs, nmap, _ = oracle.ref_build_map(ny=ny, nz=nz, px=m.px, lsd=m.Lsd, bc_y=m.BC_y, bc_z=m.BC_z, tx=m.tx,
+                                         ty=m.ty, tz=m.tz, rho_d=m.RhoD, p=np.array(m.p, np.float64),
+                                         parallax=m.Parallax, solid_angle=m.SolidAngleCorrection,
+                                         polarization=m.PolarizationCorrection,
+                                         pol_fraction=m.PolarizationFraction, r_lo=r_lo, r_hi=r_hi,
+                                         eta_lo=e_lo, eta_hi=e_hi)
+    t_map = time.time() - t0
+    rng = np.random.default_rng(w.seed)
+    yy, zz = np.meshgrid(np.arange(ny, dtype=np.float64), np.arange(nz, dtype=np.float64))
+    R = np.hypot(yy - m.BC_y, zz - m.BC_z)
+    eta = np.arctan2(-(yy - m.BC_y), zz - m.BC_z)
+    tex = 1 + w.texture * np.cos(2 * eta)
+    mu = np.full((nz, ny), w.background)
+    for rr, aa in zip(w.ring_radii(), w.ring_amps()):
+        u2 = ((R - rr) / (w.fwhm_px / 2)) ** 2
+        mu += aa * tex * (w.mix_eta / (1 + u2) + (1 - w.mix_eta) * np.exp(-np.log(2) * u2))
+    dark = w.dark_mean + w.dark_sigma * rng.standard_normal((nz, ny))
+    frames = [np.clip(rng.poisson(mu) + np.rint(dark), 0, 65535).astype(np.float64) for _ in range(2)]
+    cores = oracle.ref().ref_max_threads()
+    grad = 1 if w.mode == "gradient" else 0
+
+    def step(i):
+        oracle.ref_integrate(recs, nmap, w.n_r, w.n_eta, frames[i % 2], ny, nz, dark=dark, bc_y=m.BC_y,
+                             bc_z=m.BC_z, gradient=grad, n_threads=cores)
+
+    for i in range(args.warmup):
+        step(i)
+    t0 = time.perf_counter()
+    for i in range(args.steps):
+        step(i)
+    el = time.perf_counter() - t0
+    fps = args.steps / el
+    print(json.dumps({"impl": "reference", "metric": METRIC, "value": round(fps, 3), "unit": UNIT,
+                      "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+                      "ms_per_step": round(el / args.steps * 1e3, 3), "higher_is_better": True,
+                      "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+                      "config": {"workload": w.name, "frames_per_step": 1, "mode": w.mode,
+                                 "map_records": int(recs.shape[0]), "map_build_s": round(t_map, 1)},
+                      "cpu_baseline": {"value": round(fps, 3), "unit": UNIT, "cores": cores, "kind": "reference",
+                                       "sample": f"{args.steps} full frames, integration_apply_map over "
+                                                 f"8-row chunks with OpenMP"},
+                      "e2e": {"value": round(fps, 3), "unit": UNIT, "h2d_bytes_per_step": 0,
+                              "d2h_bytes_per_step": 0}}), flush=True)
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        main_reference(args)
+    else:
+        main_ours(args)
+
+
+if __name__ == "__main__":
+    main()

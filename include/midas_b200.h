@@ -122,6 +122,10 @@ int mi_plan_create(const mi_map_desc *map, const mi_plan_opts *opts, int device,
  * The reference subtracts (float)raw - dark[pixel] (IntegratorFitPeaksGPUStream.cu:1156). */
 int mi_plan_set_dark(mi_plan *plan, const float *dark_host);
 int mi_plan_get_info(const mi_plan *plan, mi_plan_info *info);
+/* Device-side status of the plan's launches so far: the plan's error word (MI_E_TIMEOUT
+ * when a bounded in-kernel wait expired, else 0), which is then cleared.  Synchronises
+ * the plan's device. */
+int mi_plan_status(mi_plan *plan, int *device_status);
 int mi_plan_bytes(const mi_plan *plan, size_t *bytes);
 void mi_plan_destroy(mi_plan *plan);
 

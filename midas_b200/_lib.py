@@ -93,6 +93,7 @@ SIGNATURES = [
     ("mi_plan_set_dark", C.c_int, [C.c_void_p, C.c_void_p]),
     ("mi_plan_get_info", C.c_int, [C.c_void_p, C.POINTER(MiPlanInfo)]),
     ("mi_plan_bytes", C.c_int, [C.c_void_p, C.POINTER(C.c_size_t)]),
+    ("mi_plan_status", C.c_int, [C.c_void_p, C.POINTER(C.c_int)]),
     ("mi_plan_destroy", None, [C.c_void_p]),
     ("mi_integrate_batch", C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_int64,
                                      C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),

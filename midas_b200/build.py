@@ -46,12 +46,18 @@ def _newest_header() -> float:
     return max((h.stat().st_mtime for h in hs), default=0.0)
 
 
+# per-file extra flags: the map builder's polygon clipping solves ill-conditioned
+# quadratics near tangency; without FMA contraction the device build rounds like the
+# host build of the same source
+EXTRA = {"mi_mapper.cu": ["-fmad=false"]}
+
+
 def _compile(src: Path, force: bool, verbose: bool) -> Path:
     obj = OBJDIR / (src.stem + ".o")
     if (not force and obj.exists()
             and obj.stat().st_mtime > max(src.stat().st_mtime, _newest_header())):
         return obj
-    cmd = [nvcc(), *ARCH, *NVCC_FLAGS, "-c", str(src), "-o", str(obj)]
+    cmd = [nvcc(), *ARCH, *NVCC_FLAGS, *EXTRA.get(src.name, []), "-c", str(src), "-o", str(obj)]
     if verbose:
         print(" ".join(cmd), flush=True)
     r = subprocess.run(cmd, capture_output=True, text=True)

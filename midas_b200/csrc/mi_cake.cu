@@ -7,12 +7,16 @@
 // integrate() in packages/midas_integrate/midas_integrate/kernels.py:416-473
 // (and integrate_noMapMask, FF_HEDM/src/IntegratorFitPeaksGPUStream.cu:975-1050).
 //
-// One CTA runs one work item (a band of R rows x a range of eta columns).  Per
-// staging tile it bulk-copies the tile blob into shared memory, stages the
-// tile's referenced pixels of FG frames as (float)raw - dark into shared memory
-// (pixel-major, frames innermost, padded rows so both the staging writes and
-// the per-term reads are bank-conflict free), then one warp per bin walks the
-// bin's terms with lane = frame.  Bin results go through shared memory so the
+// One CTA runs one work item (a band of R rows x a range of eta columns).  The
+// item's staging tiles are streamed through shared memory: each tile blob is
+// brought in by one bulk (TMA) copy, double-buffered so tile k+1 is in flight
+// while tile k is computed; completion is tracked by an mbarrier whose waits
+// are bounded (a wait that runs out sets the plan's error word and the CTA
+// leaves).  Per tile and frame group the referenced pixels of FG frames are
+// gathered as (float)raw - dark into shared memory (pixel-major, frames
+// innermost, padded rows: bank-conflict-free writes and per-term reads), with
+// 32 independent loads in flight per thread; then one warp per bin walks the
+// bin's terms with lane = frame.  Bin results pass through shared memory so the
 // cake stores are coalesced along eta, and the eta partial sums of the two
 // lineouts are reduced inside the CTA: no global atomics anywhere.
 #include <stdint.h>
@@ -35,21 +39,14 @@ struct CakeArgs {
   int64_t n_bins;
   int want_cake, want_lo;
   int rows_max;
-  uint32_t off_val, off_out, off_lo;  // shared-memory section offsets (16-B aligned)
+  uint32_t blob_cap;                          // bytes per blob buffer (16-B multiple)
+  uint32_t off_val, off_out, off_lo, off_bar; // shared-memory section offsets
   int u_cap, nbp;
   int *err;
 };
 
-template <int FPL>
-__host__ __device__ inline void cake_smem(uint32_t blob_cap, int u_cap, int nbp, int rows,
-                                          uint32_t *off_val, uint32_t *off_out, uint32_t *off_lo,
-                                          uint32_t *total) {
-  auto a16 = [](uint32_t x) { return (x + 15u) & ~15u; };
-  *off_val = a16(blob_cap);
-  *off_out = a16(*off_val + (uint32_t)u_cap * 33u * FPL * 4u);
-  *off_lo = a16(*off_out + 32u * FPL * (uint32_t)nbp * 4u);
-  *total = *off_lo + 32u * FPL * (uint32_t)rows * 2u * 8u;
-}
+constexpr int kCakeThreads = 256;
+constexpr uint32_t kWaitLimit = 1u << 26;  // mbarrier polls before a wait is declared lost
 
 template <typename T>
 __device__ __forceinline__ float to_f(T v) {
@@ -69,9 +66,7 @@ struct FVec<2> {
     float2 t = *(const float2 *)p;
     v[0] = t.x; v[1] = t.y;
   }
-  __device__ static __forceinline__ void st(float *p, const float *v) {
-    *(float2 *)p = make_float2(v[0], v[1]);
-  }
+  __device__ static __forceinline__ void st(float *p, const float *v) { *(float2 *)p = make_float2(v[0], v[1]); }
 };
 template <>
 struct FVec<4> {
@@ -84,126 +79,192 @@ struct FVec<4> {
   }
 };
 
-constexpr int kCakeThreads = 256;
+// ---- mbarrier + bulk copy (sm_90+ PTX) -------------------------------------
+__device__ __forceinline__ uint32_t smem_u32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void fence_barrier_init() {
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+
+__device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+
+__device__ __forceinline__ void bulk_load(void *dst, const void *src, uint32_t bytes, uint64_t *bar) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+               : "memory");
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+          smem_u32(dst)),
+      "l"(src), "r"(bytes), "r"(smem_u32(bar))
+      : "memory");
+}
+
+// Bounded wait for phase `parity` of the barrier; false when the poll budget ran out.
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity) {
+  const uint32_t a = smem_u32(bar);
+  for (uint32_t it = 0; it < kWaitLimit; ++it) {
+    uint32_t done;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(done)
+        : "r"(a), "r"(parity)
+        : "memory");
+    if (done) return true;
+  }
+  return false;
+}
 
 template <typename T, int FPL>
 __global__ void __launch_bounds__(kCakeThreads) k_cake(CakeArgs a) {
   constexpr int FG = 32 * FPL;    // frames per group
-  constexpr int SROW = 33 * FPL;  // staged row pitch (floats): conflict-free writes & reads
+  constexpr int SROW = 33 * FPL;  // staged row pitch (floats)
   constexpr int NW = kCakeThreads / 32;
   extern __shared__ __align__(16) uint8_t smem[];
-  uint8_t *s_blob = smem;
   float *s_val = (float *)(smem + a.off_val);
   float *s_out = (float *)(smem + a.off_out);
   double *s_lo = (double *)(smem + a.off_lo);
+  uint64_t *bar = (uint64_t *)(smem + a.off_bar);
+  __shared__ int s_abort;
 
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const WorkItem it = a.items[blockIdx.x];
   const T *frames = (const T *)a.frames;
   const int nbp = a.nbp;
+  const int nt = it.tile_end - it.tile_begin;
+  const int n_groups = (a.F + FG - 1) / FG;
+  const int n_steps = nt * n_groups;  // (group, tile) pairs, group-major
 
-  for (int g0 = 0; g0 < a.F; g0 += FG) {
+  if (tid == 0) {
+    mbar_init(&bar[0], 1);
+    mbar_init(&bar[1], 1);
+    fence_barrier_init();
+    s_abort = 0;
+  }
+  __syncthreads();
+  if (n_steps == 0) return;
+  if (tid == 0) {
+    const TileRef r0 = a.tiles[it.tile_begin];
+    bulk_load(smem, a.blobs + r0.off, r0.bytes, &bar[0]);
+  }
+
+  for (int k = 0; k < n_steps; ++k) {
+    const int g = k / nt, t = k - g * nt;
+    const int g0 = g * FG;
     const int fg_n = min(FG, a.F - g0);
-    for (int i = tid; i < FG * a.rows_max * 2; i += kCakeThreads) s_lo[i] = 0.0;
-    for (int t = it.tile_begin; t < it.tile_end; ++t) {
-      __syncthreads();
-      const TileRef ref = a.tiles[t];
-      {
-        const uint4 *src = (const uint4 *)(a.blobs + ref.off);
-        uint4 *dst = (uint4 *)s_blob;
-        const int n16 = (int)(ref.bytes >> 4);
-        for (int i = tid; i < n16; i += kCakeThreads) dst[i] = __ldg(src + i);
-      }
-      __syncthreads();
-      const TileHdr h = *(const TileHdr *)s_blob;
-      uint32_t o_rp, o_sc, o_lw, o_up, o_lc, o_w, bytes;
-      blob_layout(h.nb, h.nnz, h.n_u, &o_rp, &o_sc, &o_lw, &o_up, &o_lc, &o_w, &bytes);
-      const uint32_t *rowp = (const uint32_t *)(s_blob + o_rp);
-      const float *scale = (const float *)(s_blob + o_sc);
-      const float *lw = (const float *)(s_blob + o_lw);
-      const uint32_t *upix = (const uint32_t *)(s_blob + o_up);
-      const uint16_t *lcol = (const uint16_t *)(s_blob + o_lc);
-      const float *wt = (const float *)(s_blob + o_w);
+    const int buf = k & 1;
+    uint8_t *s_blob = smem + buf * a.blob_cap;
+    if (t == 0)
+      for (int i = tid; i < FG * a.rows_max * 2; i += kCakeThreads) s_lo[i] = 0.0;
+    // prefetch the next (group, tile) blob into the other buffer (its readers finished
+    // at the barrier that ended step k-1)
+    if (tid == 0 && k + 1 < n_steps) {
+      const int t1 = (k + 1) % nt;
+      const TileRef r1 = a.tiles[it.tile_begin + t1];
+      fence_proxy_async();
+      bulk_load(smem + (buf ^ 1) * a.blob_cap, a.blobs + r1.off, r1.bytes, &bar[buf ^ 1]);
+    }
+    if (!mbar_wait(&bar[buf], (uint32_t)((k >> 1) & 1))) {
+      atomicExch(a.err, MI_E_TIMEOUT);
+      s_abort = 1;
+    }
+    __syncthreads();
+    if (s_abort) return;
+    const TileHdr h = *(const TileHdr *)s_blob;
+    uint32_t o_rp, o_sc, o_lw, o_up, o_lc, o_w, bytes;
+    blob_layout(h.nb, h.nnz, h.n_u, &o_rp, &o_sc, &o_lw, &o_up, &o_lc, &o_w, &bytes);
+    const uint32_t *rowp = (const uint32_t *)(s_blob + o_rp);
+    const float *scale = (const float *)(s_blob + o_sc);
+    const float *lw = (const float *)(s_blob + o_lw);
+    const uint32_t *upix = (const uint32_t *)(s_blob + o_up);
+    const uint16_t *lcol = (const uint16_t *)(s_blob + o_lc);
+    const float *wt = (const float *)(s_blob + o_w);
 
-      // ---- stage: s_val[u][q*FPL + k] = (float)frame[g0 + q*FPL + k][pix_u] - dark[pix_u]
-      const int n_u = h.n_u;
-      for (int i = tid; i < n_u * 32; i += kCakeThreads) {
-        const int u = i % n_u, q = i / n_u;
-        const uint32_t pix = upix[u];
-        const float d = __ldg(a.dark + pix);
-        float v[FPL];
+    // ---- stage: thread owns pixel u, gathers 32 frames at a time (32 loads in flight)
+    const int n_u = h.n_u;
+    for (int u = tid; u < n_u; u += kCakeThreads) {
+      const uint32_t pix = upix[u];
+      const float d = __ldg(a.dark + pix);
+      const T *src = frames + (int64_t)g0 * a.stride + pix;
+      float *dst = s_val + u * SROW;
 #pragma unroll
-        for (int k = 0; k < FPL; ++k) {
-          const int f = q * FPL + k;
-          v[k] = (f < fg_n) ? to_f(__ldg(frames + (int64_t)(g0 + f) * a.stride + pix)) - d : 0.0f;
-        }
-        FVec<FPL>::st(s_val + u * SROW + q * FPL, v);
-      }
-      __syncthreads();
-
-      // ---- compute: warp per bin, lane = frame(s)
-      for (int b = warp; b < h.nb; b += NW) {
-        const uint32_t j0 = rowp[b], j1 = rowp[b + 1];
-        float acc[FPL];
+      for (int c = 0; c < FG; c += 32) {
+        float v[32];
 #pragma unroll
-        for (int k = 0; k < FPL; ++k) acc[k] = 0.0f;
-        uint32_t j = j0;
-        for (; j + 4 <= j1; j += 4) {
-          uint32_t c[4];
-          float w[4], v[4][FPL];
+        for (int f = 0; f < 32; ++f)
+          v[f] = (c + f < fg_n) ? to_f(__ldg(src + (int64_t)(c + f) * a.stride)) : d;
 #pragma unroll
-          for (int q = 0; q < 4; ++q) {
-            c[q] = lcol[j + q];
-            w[q] = wt[j + q];
-          }
+        for (int f = 0; f < 32; ++f) v[f] -= d;
 #pragma unroll
-          for (int q = 0; q < 4; ++q) FVec<FPL>::ld(s_val + c[q] * SROW + lane * FPL, v[q]);
-#pragma unroll
-          for (int q = 0; q < 4; ++q)
-#pragma unroll
-            for (int k = 0; k < FPL; ++k) acc[k] = fmaf(w[q], v[q][k], acc[k]);
-        }
-        for (; j < j1; ++j) {
-          float v[FPL];
-          FVec<FPL>::ld(s_val + (uint32_t)lcol[j] * SROW + lane * FPL, v);
-          const float w = wt[j];
-#pragma unroll
-          for (int k = 0; k < FPL; ++k) acc[k] = fmaf(w, v[k], acc[k]);
-        }
-        const float sc = scale[b];
-#pragma unroll
-        for (int k = 0; k < FPL; ++k) s_out[(lane * FPL + k) * nbp + b] = acc[k] * sc;
-      }
-      __syncthreads();
-
-      // ---- cake store: runs of n_cols contiguous floats per (frame, row)
-      if (a.want_cake) {
-        for (int i = tid; i < fg_n * h.nb; i += kCakeThreads) {
-          const int f = i / h.nb, b = i - f * h.nb;
-          const int r = b / h.n_cols, e = b - r * h.n_cols;
-          a.cake[(int64_t)(g0 + f) * a.n_bins + (int64_t)(h.r0 + r) * a.n_eta + h.e0 + e] =
-              s_out[f * nbp + b];
-        }
-      }
-      // ---- lineout partials of this tile, accumulated per (frame, row of band)
-      if (a.want_lo) {
-        for (int i = tid; i < fg_n * h.n_rows; i += kCakeThreads) {
-          const int f = i / h.n_rows, r = i - f * h.n_rows;
-          double saw = 0.0, ssm = 0.0;
-          for (int e = 0; e < h.n_cols; ++e) {
-            const float v = s_out[f * nbp + r * h.n_cols + e];
-            const float l = lw[r * h.n_cols + e];
-            saw += (double)v * (double)l;
-            ssm += (l > 0.0f) ? (double)v : 0.0;
-          }
-          double *dst = s_lo + ((size_t)f * a.rows_max + h.row_in_band + r) * 2;
-          dst[0] += saw;
-          dst[1] += ssm;
-        }
+        for (int f = 0; f < 32; f += FPL) FVec<FPL>::st(dst + c + f, v + f);
       }
     }
     __syncthreads();
+
+    // ---- compute: warp per bin, lane = frame(s)
+    for (int b = warp; b < h.nb; b += NW) {
+      const uint32_t j0 = rowp[b], j1 = rowp[b + 1];
+      float acc[FPL];
+#pragma unroll
+      for (int q = 0; q < FPL; ++q) acc[q] = 0.0f;
+      uint32_t j = j0;
+      for (; j + 4 <= j1; j += 4) {
+        uint32_t c[4];
+        float w[4], v[4][FPL];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+          c[q] = lcol[j + q];
+          w[q] = wt[j + q];
+        }
+#pragma unroll
+        for (int q = 0; q < 4; ++q) FVec<FPL>::ld(s_val + c[q] * SROW + lane * FPL, v[q]);
+#pragma unroll
+        for (int q = 0; q < 4; ++q)
+#pragma unroll
+          for (int r = 0; r < FPL; ++r) acc[r] = fmaf(w[q], v[q][r], acc[r]);
+      }
+      for (; j < j1; ++j) {
+        float v[FPL];
+        FVec<FPL>::ld(s_val + (uint32_t)lcol[j] * SROW + lane * FPL, v);
+        const float w = wt[j];
+#pragma unroll
+        for (int r = 0; r < FPL; ++r) acc[r] = fmaf(w, v[r], acc[r]);
+      }
+      const float sc = scale[b];
+#pragma unroll
+      for (int r = 0; r < FPL; ++r) s_out[(lane * FPL + r) * nbp + b] = acc[r] * sc;
+    }
+    __syncthreads();
+
+    // ---- cake store: runs of n_cols contiguous floats per (frame, row)
+    if (a.want_cake) {
+      for (int i = tid; i < fg_n * h.nb; i += kCakeThreads) {
+        const int f = i / h.nb, b = i - f * h.nb;
+        const int r = b / h.n_cols, e = b - r * h.n_cols;
+        a.cake[(int64_t)(g0 + f) * a.n_bins + (int64_t)(h.r0 + r) * a.n_eta + h.e0 + e] = s_out[f * nbp + b];
+      }
+    }
+    // ---- lineout partials of this tile, accumulated per (frame, row of band)
     if (a.want_lo) {
+      for (int i = tid; i < fg_n * h.n_rows; i += kCakeThreads) {
+        const int f = i / h.n_rows, r = i - f * h.n_rows;
+        double saw = 0.0, ssm = 0.0;
+        for (int e = 0; e < h.n_cols; ++e) {
+          const float v = s_out[f * nbp + r * h.n_cols + e];
+          const float l = lw[r * h.n_cols + e];
+          saw += (double)v * (double)l;
+          ssm += (l > 0.0f) ? (double)v : 0.0;
+        }
+        double *dst = s_lo + ((size_t)f * a.rows_max + h.row_in_band + r) * 2;
+        dst[0] += saw;
+        dst[1] += ssm;
+      }
+    }
+    if (t == nt - 1 && a.want_lo) {
+      __syncthreads();
       for (int i = tid; i < fg_n * it.n_rows; i += kCakeThreads) {
         const int f = i / it.n_rows, r = i - f * it.n_rows;
         const double *src = s_lo + ((size_t)f * a.rows_max + r) * 2;
@@ -237,13 +298,11 @@ __global__ void k_lineout(const double *partial, int F, int n_r, int n_slots, co
 
 template <typename T, int FPL>
 static int launch_t(Plan *p, CakeArgs &a, cudaStream_t s) {
-  uint32_t total = 0;
-  cake_smem<FPL>((p->max_blob + 15u) & ~15u, a.u_cap, a.nbp, a.rows_max, &a.off_val, &a.off_out,
-                 &a.off_lo, &total);
-  const size_t smem = total;
+  const size_t smem =
+      cake_smem_layout(FPL, a.blob_cap, a.u_cap, a.nbp, a.rows_max, &a.off_val, &a.off_out, &a.off_lo, &a.off_bar);
   int dev_smem = 0;
   MI_CUDA(cudaDeviceGetAttribute(&dev_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, p->device));
-  if (smem > (size_t)dev_smem)
+  if (smem + 64 > (size_t)dev_smem)
     return set_error(MI_E_RANGE, "batched kernel needs %zu B shared memory (> %d); lower tile_pixels", smem,
                      dev_smem);
   MI_CUDA(cudaFuncSetAttribute(k_cake<T, FPL>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
@@ -273,7 +332,7 @@ int launch_cake(Plan *p, const void *frames, int dtype, int n_frames, int64_t st
   a.F = n_frames;
   a.dark = p->d_dark;
   a.cake = cake;
-  a.partial = (double *)p->d_partial;
+  a.partial = p->d_partial;
   a.n_slots = p->n_slots;
   a.n_r = p->n_r;
   a.n_eta = p->n_eta;
@@ -281,6 +340,7 @@ int launch_cake(Plan *p, const void *frames, int dtype, int n_frames, int64_t st
   a.want_cake = cake != nullptr;
   a.want_lo = (lo_aw != nullptr) || (lo_sm != nullptr);
   a.rows_max = p->lim.rows;
+  a.blob_cap = (p->max_blob + 15u) & ~15u;
   a.u_cap = std::max(p->max_u, 1);
   a.nbp = (p->max_nb | 1);  // odd pitch: conflict-free column writes
   a.err = p->d_err;
@@ -299,8 +359,8 @@ int launch_cake(Plan *p, const void *frames, int dtype, int n_frames, int64_t st
   if (rc) return rc;
   if (a.want_lo) {
     const int64_t n = (int64_t)n_frames * p->n_r;
-    k_lineout<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(a.partial, n_frames, p->n_r, p->n_slots,
-                                                          p->d_den_aw, p->d_cnt, lo_aw, lo_sm);
+    k_lineout<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(a.partial, n_frames, p->n_r, p->n_slots, p->d_den_aw,
+                                                          p->d_cnt, lo_aw, lo_sm);
     MI_CUDA(cudaGetLastError());
   }
   return MI_OK;

@@ -87,6 +87,24 @@ __host__ __device__ inline void blob_layout(int nb, int nnz, int n_u, uint32_t *
   *bytes = o;
 }
 
+// Shared-memory layout of the batched kernel for `fpl` frames per lane:
+// [2 blob buffers][staged values: u_cap x 33*fpl floats][bin results: 32*fpl x nbp floats]
+// [lineout partials: 32*fpl x rows x 2 doubles][2 mbarriers]; returns the total bytes.
+__host__ __device__ inline uint32_t cake_smem_layout(int fpl, uint32_t blob_cap, int u_cap, int nbp,
+                                                     int rows, uint32_t *off_val, uint32_t *off_out,
+                                                     uint32_t *off_lo, uint32_t *off_bar) {
+  auto a16 = [](uint32_t x) { return (x + 15u) & ~15u; };
+  const uint32_t ov = a16(2u * blob_cap);
+  const uint32_t oo = a16(ov + (uint32_t)u_cap * 33u * (uint32_t)fpl * 4u);
+  const uint32_t ol = a16(oo + 32u * (uint32_t)fpl * (uint32_t)nbp * 4u);
+  const uint32_t ob = a16(ol + 32u * (uint32_t)fpl * (uint32_t)rows * 2u * 8u);
+  if (off_val) *off_val = ov;
+  if (off_out) *off_out = oo;
+  if (off_lo) *off_lo = ol;
+  if (off_bar) *off_bar = ob;
+  return ob + 16u;
+}
+
 // Host-side CSR of one integration mode: rows = bins, cols = flat pixels.
 struct HostCSR {
   std::vector<int64_t> row_ptr;  // n_bins + 1

@@ -343,21 +343,23 @@ static int build_plan(const mi_map_desc &m, const mi_plan_opts &o, Plan *p) {
   TileLimits L;
   L.rows = o.tile_rows > 0 ? o.tile_rows : 16;
   if (L.rows > 64) return set_error(MI_E_RANGE, "tile_rows %d > 64", L.rows);
-  L.max_u = o.tile_pixels > 0 ? o.tile_pixels : (fpl == 1 ? 768 : (fpl == 2 ? 384 : 192));
+  L.max_u = o.tile_pixels > 0 ? o.tile_pixels : (fpl == 1 ? 640 : (fpl == 2 ? 320 : 160));
   if (L.max_u > 65535) return set_error(MI_E_RANGE, "tile_pixels %d > 65535", L.max_u);
   L.max_nb = 256;
-  L.max_nnz = 6144;
+  L.max_nnz = 4096;
   L.item_cols = std::max(1, (m.n_eta + 11) / 12);
-  p->lim = L;
+  int dev_smem = 0;
+  MI_CUDA(cudaDeviceGetAttribute(&dev_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, p->device));
 
-  // ---- items and tiles
+  // ---- items and tiles; shrink the tile limits until the kernel's shared memory fits
   const int n_bands = (m.n_r + L.rows - 1) / L.rows;
   const int n_slots = (m.n_eta + L.item_cols - 1) / L.item_cols;
   p->n_slots = n_slots;
   const int n_items = n_bands * n_slots;
   std::vector<std::vector<HostTile>> item_tiles(n_items);
-  int err = MI_OK;
-  {
+  for (int attempt = 0;; ++attempt) {
+    for (auto &v : item_tiles) v.clear();
+    int err = MI_OK;
     int nthr = std::min(omp_get_max_threads(), 16);
 #pragma omp parallel num_threads(nthr)
     {
@@ -376,8 +378,28 @@ static int build_plan(const mi_map_desc &m, const mi_plan_opts &o, Plan *p) {
         }
       }
     }
+    if (err) return err;
+    uint32_t mb = 0;
+    int mu = 1, mnb = 1;
+    for (const auto &v : item_tiles)
+      for (const HostTile &t : v) {
+        uint32_t a, b, c, d, e, f, bytes;
+        blob_layout(t.n_rows * t.n_cols, t.nnz, t.n_u, &a, &b, &c, &d, &e, &f, &bytes);
+        mb = std::max(mb, bytes);
+        mu = std::max(mu, t.n_u);
+        mnb = std::max(mnb, t.n_rows * t.n_cols);
+      }
+    const uint32_t need = cake_smem_layout(fpl, (mb + 15u) & ~15u, mu, mnb | 1, L.rows, nullptr, nullptr,
+                                           nullptr, nullptr);
+    if (need + 1024u <= (uint32_t)dev_smem) break;
+    if (attempt >= 10 || L.max_u <= 32)
+      return set_error(MI_E_RANGE, "tiles need %u B of shared memory (device allows %d); lower tile_rows",
+                       need, dev_smem);
+    L.max_u = std::max(32, L.max_u * 3 / 4);
+    L.max_nnz = std::max(256, L.max_nnz * 3 / 4);
+    L.max_nb = std::max(16, L.max_nb * 3 / 4);
   }
-  if (err) return err;
+  p->lim = L;
 
   // ---- blob arena
   std::vector<TileRef> tiles;
@@ -655,6 +677,18 @@ int mi_plan_get_info(const mi_plan *p, mi_plan_info *info) {
   info->tile_pixels = p->lim.max_u;
   info->frames_per_lane = p->frames_per_lane;
   info->run_len = 0;
+  return MI_OK;
+}
+
+int mi_plan_status(mi_plan *p, int *status) {
+  if (!p || !status) return set_error(MI_E_ARG, "mi_plan_status: null argument");
+  int prev = 0;
+  cudaGetDevice(&prev);
+  MI_CUDA(cudaSetDevice(p->device));
+  MI_CUDA(cudaDeviceSynchronize());
+  MI_CUDA(cudaMemcpy(status, p->d_err, sizeof(int), cudaMemcpyDeviceToHost));
+  MI_CUDA(cudaMemset(p->d_err, 0, sizeof(int)));
+  cudaSetDevice(prev);
   return MI_OK;
 }
 

@@ -113,6 +113,13 @@ class CakePlan:
         L.check(L.lib().mi_plan_get_info(self._h, C.byref(inf)), "mi_plan_get_info")
         return {k: getattr(inf, k) for k, _ in L.MiPlanInfo._fields_}
 
+    def status(self) -> int:
+        """Device status word of the plan's launches (0, or MI_E_TIMEOUT when a bounded
+        in-kernel wait expired); reading it synchronises the device and clears it."""
+        st = C.c_int(0)
+        L.check(L.lib().mi_plan_status(self._h, C.byref(st)), "mi_plan_status")
+        return st.value
+
     def set_dark(self, dark) -> None:
         """Per-pixel dark (ny*nz floats; frames are cast and have it subtracted)."""
         if dark is None:
@@ -137,8 +144,8 @@ class CakePlan:
         per = frames[0].numel() if F else self.ny * self.nz
         if per != self.ny * self.nz:
             raise ValueError(f"frame has {per} pixels, expected {self.ny * self.nz}")
-        flat = frames.reshape(F, -1)
-        if flat.stride(1) != 1:
+        flat = frames.reshape(F, per)
+        if F and flat.stride(1) != 1:
             flat = flat.contiguous()
         return flat, F, flat.stride(0) if F else per
 

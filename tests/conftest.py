@@ -1,0 +1,78 @@
+"""Shared pytest setup: the `gpu` marker, in-tree builds, golden-fixture loaders."""
+from __future__ import annotations
+
+import subprocess
+import sys
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+REPO = Path(__file__).resolve().parents[1]
+GOLDEN = Path(__file__).resolve().parent / "golden"
+if str(REPO) not in sys.path:
+    sys.path.insert(0, str(REPO))
+
+
+def pytest_configure(config):
+    config.addinivalue_line("markers", "gpu: needs a CUDA device (B200)")
+    config.addinivalue_line("markers", "slow: long-running")
+
+
+def _ensure_built():
+    lib = REPO / "midas_b200" / "libmidas_b200.so"
+    if not lib.exists():
+        from midas_b200 import build
+        build.build()
+    if not (REPO / "oracle" / "liboracle.so").exists():
+        subprocess.run(["make", "-s", "-C", str(REPO / "oracle")], check=True)
+
+
+_ensure_built()
+
+REC_DTYPE = np.dtype([("y", "<f4"), ("z", "<f4"), ("frac", "<f8"), ("deltaR", "<f4"),
+                      ("areaWeight", "<f4")])
+
+
+def load_kernels_case(tag):
+    g = dict(np.load(GOLDEN / f"kernels_{tag}.npz"))
+    g["records"] = g["records"].view(REC_DTYPE)
+    g["nmap"] = np.stack([g["counts"], g["offsets"]], 1).astype(np.int32)
+    for k in ("ny", "nz", "n_r", "n_eta"):
+        g[k] = int(g[k])
+    for k in ("bc_y", "bc_z"):
+        g[k] = float(g[k])
+    return g
+
+
+def load_mapper_case(tag):
+    g = dict(np.load(GOLDEN / f"mapper_{tag}.npz"))
+    g["records"] = g["records"].view(REC_DTYPE)
+    for k in ("ny", "nz", "sa", "pol"):
+        g[k] = int(g[k])
+    for k in ("px", "lsd", "bc_y", "bc_z", "ty", "tz", "parallax", "rho_d"):
+        g[k] = float(g[k])
+    return g
+
+
+KERNEL_CASES = ["a", "b", "c", "d"]
+MAPPER_CASES = ["m1", "m2", "m3"]
+
+
+def rel_err(x, ref, tau_frac=1e-3):
+    """max / mean of |x - ref| / max(|ref|, tau), tau = tau_frac * median |ref| over nonzero."""
+    x = np.asarray(x, np.float64).reshape(-1)
+    ref = np.asarray(ref, np.float64).reshape(-1)
+    nz = np.abs(ref[ref != 0])
+    tau = tau_frac * (np.median(nz) if nz.size else 1.0)
+    tau = max(tau, 1e-300)
+    r = np.abs(x - ref) / np.maximum(np.abs(ref), tau)
+    return float(r.max()) if r.size else 0.0, float(r.mean()) if r.size else 0.0
+
+
+@pytest.fixture(scope="session")
+def cuda():
+    import torch
+    if not torch.cuda.is_available():
+        pytest.skip("CUDA not available")
+    return torch.device("cuda", 0)

@@ -1,0 +1,65 @@
+"""The FP64 oracle is pinned to the reference: golden vectors from the reference's own
+midas_integrate kernels (build_csr/integrate/profile_1d in FP64) and from its compiled
+IntegrationCore.c (integration_apply_map)."""
+import numpy as np
+import pytest
+
+import oracle
+from conftest import KERNEL_CASES, MAPPER_CASES, load_kernels_case, load_mapper_case
+
+
+@pytest.mark.parametrize("tag", KERNEL_CASES)
+@pytest.mark.parametrize("mode", ["floor", "bilinear", "gradient"])
+@pytest.mark.parametrize("norm", [True, False])
+def test_oracle_matches_reference_python(tag, mode, norm):
+    g = load_kernels_case(tag)
+    nb = g["n_r"] * g["n_eta"]
+    ck, _ = oracle.integrate(g["records"], g["nmap"], nb, g["ny"], g["nz"], g["image"], mode=mode,
+                             normalize=norm, bc_y=g["bc_y"], bc_z=g["bc_z"])
+    key = f"{mode}_{'n' if norm else 'r'}"
+    np.testing.assert_allclose(ck, g["cake_" + key], rtol=1e-12, atol=1e-9)
+    area = oracle.area_in(g["records"], g["nmap"], nb, g["ny"], g["nz"])
+    np.testing.assert_allclose(area, g["area_per_bin"], rtol=1e-12, atol=0)
+    aw, sm = oracle.profile(ck, area, g["n_r"], g["n_eta"])
+    np.testing.assert_allclose(aw, g["aw_" + key], rtol=1e-12, atol=1e-9)
+    np.testing.assert_allclose(sm, g["sm_" + key], rtol=1e-12, atol=1e-9)
+
+
+@pytest.mark.parametrize("tag", MAPPER_CASES)
+@pytest.mark.parametrize("mode", ["bilinear", "gradient"])
+def test_oracle_matches_reference_integration_core(tag, mode):
+    """integration_apply_map (IntegrationCore.c) sums vs oracle raw sums of (image - dark).
+    IntegrationCore normalises by every record's areaWeight: identical to the in-bounds
+    area for DetectorMapper maps, whose records are all on the detector."""
+    g = load_mapper_case(tag)
+    nb = g["nmap"].shape[0]
+    img = g["image"] - g["dark"]
+    ck, area = oracle.integrate(g["records"], g["nmap"], nb, g["ny"], g["nz"], img, mode=mode,
+                                normalize=False, bc_y=g["bc_y"], bc_z=g["bc_z"])
+    # IntegrationCore floors the FP64 sample position through floorf(): a position a few
+    # 1e-8 px below an integer rounds up in float, giving a negative fraction.  The Python
+    # reference (np.floor) and the oracle do not, so a handful of bins differ at ~1e-8.
+    np.testing.assert_allclose(ck, g[f"ic_sums_{mode}"], rtol=1e-7, atol=1e-9)
+    exact = np.isclose(ck, g[f"ic_sums_{mode}"], rtol=1e-12, atol=1e-12)
+    assert exact.mean() > 0.999
+    np.testing.assert_allclose(area, g[f"ic_norms_{mode}"], rtol=1e-6, atol=1e-9)
+
+
+def test_oracle_gpustream_semantics_area_covers_all_records():
+    g = load_kernels_case("a")
+    nb = g["n_r"] * g["n_eta"]
+    _, a_py = oracle.integrate(g["records"], g["nmap"], nb, g["ny"], g["nz"], g["image"], semantics="py")
+    _, a_gs = oracle.integrate(g["records"], g["nmap"], nb, g["ny"], g["nz"], g["image"],
+                               semantics="gpustream")
+    assert np.all(a_gs >= a_py - 1e-12)
+    assert np.any(a_gs > a_py + 1e-6)          # the case has off-detector records
+
+
+@pytest.mark.skipif(not oracle.ref_available(), reason="reference C sources not compiled here")
+@pytest.mark.parametrize("tag", MAPPER_CASES)
+def test_reference_integrator_reproduces_fixture(tag):
+    g = load_mapper_case(tag)
+    n_r, n_eta = g["r_lo"].size, g["eta_lo"].size
+    sums, norms = oracle.ref_integrate(g["records"], g["nmap"], n_r, n_eta, g["image"], g["ny"], g["nz"],
+                                       dark=g["dark"], bc_y=g["bc_y"], bc_z=g["bc_z"], gradient=1, n_threads=2)
+    np.testing.assert_allclose(sums, g["ic_sums_gradient"], rtol=1e-12, atol=1e-12)
