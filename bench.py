@@ -46,6 +46,8 @@ def parse():
     ap.add_argument("--tile-rows", type=int, default=0)
     ap.add_argument("--tile-pixels", type=int, default=0)
     ap.add_argument("--fpl", type=int, default=0)
+    ap.add_argument("--encoding", default="auto", choices=["auto", "runs", "csr"])
+    ap.add_argument("--run-len", type=int, default=0)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
@@ -200,7 +202,7 @@ def main_ours(args):
     plan = CakePlan(pm, n_r=w.n_r, n_eta=w.n_eta, n_pixels_y=ny, n_pixels_z=nz, mode=w.mode,
                     bc_y=w.mapper.BC_y, bc_z=w.mapper.BC_z, device=dev,
                     tile_rows=args.tile_rows or w.tile_rows, tile_pixels=args.tile_pixels,
-                    frames_per_lane=args.fpl)
+                    frames_per_lane=args.fpl, encoding=args.encoding, run_len=args.run_len)
     t_plan = time.time() - t1
     info = plan.info
     dark = w.dark(device=dev)
@@ -286,6 +288,9 @@ def main_ours(args):
                       "map_records": info["n_records"], "tiles": info["n_tiles"],
                       "tile_rows": info["tile_rows"], "tile_pixels": info["tile_pixels"],
                       "frames_per_lane": info["frames_per_lane"],
+                      "encoding": args.encoding if args.encoding != "auto" else "runs",
+                      "run_len": info["run_len"], "staged_pixels_per_frame": info["staged_pixels"],
+                      "referenced_pixels": info["ref_pixels"], "map_bytes": info["map_bytes"],
                       "l2": "inputs larger than L2: each step reads a new %.1f GB batch" % (F * frame_bytes / 1e9),
                       "parallelism": f"replicas{world}"},
            "roofline": roofline, "gpu_launches": launches,

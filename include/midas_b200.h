@@ -95,8 +95,14 @@ typedef struct {
   int32_t semantics;       /* MI_SEM_*                                               */
   int32_t tile_rows;       /* rows (R bins) per tile strip; 0 = autotune              */
   int32_t tile_pixels;     /* max staged pixels per tile; 0 = autotune                */
-  int32_t frames_per_lane; /* 1, 2 or 4 frames per thread; 0 = autotune               */
+  int32_t frames_per_lane; /* CSR encoding only: 1, 2 or 4 frames per thread; 0 = auto */
+  int32_t encoding;        /* MI_ENC_*: tile encoding of the map                      */
+  int32_t run_len;         /* run encoding: rows per record (2, 4 or 8); 0 = auto      */
 } mi_plan_opts;
+
+#define MI_ENC_AUTO 0      /* runs                                                       */
+#define MI_ENC_CSR 1       /* per-bin term lists, one warp per bin, lane = frame         */
+#define MI_ENC_RUNS 2      /* per-pixel radial runs: one staged value feeds run_len bins */
 
 typedef struct {
   int64_t n_bins, n_r, n_eta;

@@ -346,7 +346,9 @@ int launch_cake(Plan *p, const void *frames, int dtype, int n_frames, int64_t st
   a.err = p->d_err;
   if (!a.want_cake && !a.want_lo) return MI_OK;
   int rc = MI_OK;
-  switch (dtype) {
+  if (p->encoding == MI_ENC_RUNS) {
+    rc = launch_runs(p, frames, dtype, n_frames, stride, cake, a.want_lo, s);
+  } else switch (dtype) {
     case MI_DT_U8: rc = launch_fpl<uint8_t>(p, a, s); break;
     case MI_DT_U16: rc = launch_fpl<uint16_t>(p, a, s); break;
     case MI_DT_U32: rc = launch_fpl<uint32_t>(p, a, s); break;

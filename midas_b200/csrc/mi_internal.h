@@ -87,6 +87,74 @@ __host__ __device__ inline void blob_layout(int nb, int nnz, int n_u, uint32_t *
   *bytes = o;
 }
 
+// ---------------------------------------------------------------------------
+// Run encoding (MI_ENC_RUNS).  A tile is split into strips, one per eta column,
+// each strip being the tile's G rows of that column.  Every staged pixel that
+// feeds a strip contributes one or more records: a record holds the pixel's
+// weights for L consecutive rows starting at row rs (zero where the pixel has no
+// term), so one staged value per frame feeds L accumulators held in registers.
+// Records of a strip are sorted by rs; rs_ptr[strip][q] is the first record with
+// rs >= q (q = 0 .. G-L+1, the last entry being the strip's end).
+//
+//   TileHdr                          32 B  (nnz field = number of records)
+//   uint16 rs_ptr[n_cols][G-L+2]
+//   float  scale[nb], lw[nb]         nb = n_rows * n_cols, row-major
+//   uint32 upix[n_u]
+//   uint16 lcol[n_rec]
+//   float  w[n_rec][L]
+// every array 16-byte aligned; the blob size is a multiple of 16.
+__host__ __device__ inline uint32_t runs_blob_layout(int nb, int n_cols, int n_rec, int n_u, int G, int L,
+                                                     uint32_t *o_rsp, uint32_t *o_sc, uint32_t *o_lw,
+                                                     uint32_t *o_up, uint32_t *o_lc, uint32_t *o_w) {
+  auto a16 = [](uint32_t x) { return (x + 15u) & ~15u; };
+  uint32_t o = 32;
+  *o_rsp = o; o = a16(o + 2u * (uint32_t)n_cols * (uint32_t)(G - L + 2));
+  *o_sc = o;  o = a16(o + 4u * (uint32_t)nb);
+  *o_lw = o;  o = a16(o + 4u * (uint32_t)nb);
+  *o_up = o;  o = a16(o + 4u * (uint32_t)n_u);
+  *o_lc = o;  o = a16(o + 2u * (uint32_t)n_rec);
+  *o_w = o;   o = a16(o + 4u * (uint32_t)n_rec * (uint32_t)L);
+  return o;
+}
+
+constexpr int kRunWarps = 8;         // consumer (compute) warps per CTA of the run kernel
+constexpr int kRunProducerWarps = 6; // producer (gather/staging) warps per CTA
+constexpr int kRunCtasPerSm = 1;
+constexpr int kRunPitch = 144;       // bytes per staged pixel: 64 x u16 or 32 x f32, + 16 pad
+
+// Frames per group of the run kernel: 8/16-bit frames are staged as u16 and, with G <= 16,
+// computed two frames per lane (64 per group); otherwise one frame per lane (32).
+__host__ __device__ constexpr int runs_frames_per_group(int sizeof_t, int G) {
+  return (sizeof_t <= 2 && G <= 16) ? 64 : 32;
+}
+
+// Shared memory of the run kernel (two pipeline slots b = 0, 1):
+//   [blob b: blob_cap][staging b: u_cap x kRunPitch, then u_cap darks; reused for the unit
+//    partials once consumed] x 2, [bin results: fg x nbp floats]
+//   [lineout partials: rows x fg x 2 doubles][2 mbarriers]
+// Offsets of slot 1 are those of slot 0 plus *slot_bytes.
+__host__ __device__ inline uint32_t runs_smem_layout(uint32_t blob_cap, int u_cap, int nbp, int rows, int G, int fg,
+                                                     uint32_t *off_val, uint32_t *off_dark, uint32_t *slot_bytes,
+                                                     uint32_t *off_out, uint32_t *off_lo, uint32_t *off_bar) {
+  auto a16 = [](uint32_t x) { return (x + 15u) & ~15u; };
+  const uint32_t ov = a16(blob_cap);                        // staging area of slot 0
+  const uint32_t od = a16(ov + (uint32_t)u_cap * (uint32_t)kRunPitch);
+  uint32_t end = a16(od + 4u * (uint32_t)u_cap);
+  const uint32_t parts = ov + (uint32_t)kRunWarps * (uint32_t)G * (uint32_t)fg * 4u;
+  if (parts > end) end = a16(parts);
+  const uint32_t slot = end;                                // [blob | staging] of one slot
+  const uint32_t oo = 2u * slot;
+  const uint32_t ol = a16(oo + (uint32_t)fg * (uint32_t)nbp * 4u);
+  const uint32_t ob = a16(ol + (uint32_t)fg * (uint32_t)rows * 2u * 8u);
+  if (off_val) *off_val = ov;
+  if (off_dark) *off_dark = od;
+  if (slot_bytes) *slot_bytes = slot;
+  if (off_out) *off_out = oo;
+  if (off_lo) *off_lo = ol;
+  if (off_bar) *off_bar = ob;
+  return ob + 16u;
+}
+
 // Shared-memory layout of the batched kernel for `fpl` frames per lane:
 // [2 blob buffers][staged values: u_cap x 33*fpl floats][bin results: 32*fpl x nbp floats]
 // [lineout partials: 32*fpl x rows x 2 doubles][2 mbarriers]; returns the total bytes.
@@ -120,6 +188,7 @@ struct TileLimits {
   int max_u;     // max staged pixels per tile
   int max_nb;    // max bins per tile
   int max_nnz;   // max terms per tile
+  int max_cols;  // max eta columns per tile
   int item_cols; // eta columns per work item
 };
 
@@ -130,6 +199,8 @@ struct Plan {
   double bc_y = 0, bc_z = 0;
   int64_t n_bins = 0, nnz = 0, n_records = 0, oob = 0;
   int frames_per_lane = 1;
+  int encoding = MI_ENC_RUNS;
+  int run_g = 0, run_l = 0;      // run encoding: rows per strip (8/16/32), rows per record
   TileLimits lim{};
   int64_t staged_pixels = 0, ref_pixels = 0;
 
@@ -167,6 +238,8 @@ int build_host_csr(const mi_map_desc &m, int mode, int semantics, HostCSR *out);
 // Launchers (mi_cake.cu, mi_plain.cu)
 int launch_cake(Plan *p, const void *frames, int dtype, int n_frames, int64_t stride,
                 float *cake, double *lo_aw, double *lo_sm, cudaStream_t s);
+int launch_runs(Plan *p, const void *frames, int dtype, int n_frames, int64_t stride, float *cake, bool want_lo,
+                cudaStream_t s);
 int launch_plain(Plan *p, const void *frame, int dtype, double *cake, double *lo_aw,
                  double *lo_sm, cudaStream_t s);
 int launch_cast(const void *frames, int dtype, int64_t n_pixels, int n_frames,

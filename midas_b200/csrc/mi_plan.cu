@@ -256,7 +256,7 @@ static int tile_item(const Builder &B, int r0, int nrows, int e_begin, int e_end
       }
     *nu_out = nu;
     *nnz_out = nnz;
-    return nu <= L.max_u && nnz <= L.max_nnz && h * ncols <= L.max_nb;
+    return nu <= L.max_u && nnz <= L.max_nnz && h * ncols <= L.max_nb && ncols <= L.max_cols;
   };
   // row-chunk height: largest h (halving) such that every single column fits
   int h = nrows;
@@ -295,6 +295,177 @@ static int tile_item(const Builder &B, int r0, int nrows, int e_begin, int e_end
     }
   }
   return MI_OK;
+}
+
+// normalisation factor and lineout weight of bin b (see mi_internal.h)
+static inline void bin_scale(const HostCSR &csr, const Plan *p, int64_t b, float *scale, float *lw) {
+  const double an = csr.area_norm[b], ai = csr.area_in[b];
+  double sc;
+  if (p->semantics == MI_SEM_GPUSTREAM)
+    sc = an > kAreaThreshold ? (p->normalize ? 1.0 / an : 1.0) : 0.0;
+  else
+    sc = p->normalize ? (ai > kAreaThreshold ? 1.0 / ai : 0.0) : 1.0;
+  *scale = (float)sc;
+  *lw = ai > kAreaThreshold ? (float)ai : 0.0f;
+}
+
+// staged pixel set of a tile (ascending), with lut[pixel] = local index
+static std::vector<int32_t> tile_pixels(const HostCSR &csr, const mi_map_desc &m, const HostTile &t,
+                                        std::vector<int32_t> &lut) {
+  std::vector<int32_t> u;
+  u.reserve(t.n_u);
+  for (int r = t.r0; r < t.r0 + t.n_rows; ++r)
+    for (int e = t.e0; e < t.e0 + t.n_cols; ++e) {
+      const int64_t b = (int64_t)r * m.n_eta + e;
+      for (int64_t j = csr.row_ptr[b]; j < csr.row_ptr[b + 1]; ++j) u.push_back(csr.col[j]);
+    }
+  std::sort(u.begin(), u.end());
+  u.erase(std::unique(u.begin(), u.end()), u.end());
+  for (size_t i = 0; i < u.size(); ++i) lut[u[i]] = (int32_t)i;
+  return u;
+}
+
+static void csr_blob(const HostCSR &csr, const mi_map_desc &m, const Plan *p, const HostTile &t, int row_in_band,
+                     std::vector<int32_t> &lut, std::vector<uint8_t> &out) {
+  const int nb = t.n_rows * t.n_cols;
+  uint32_t o_rp, o_sc, o_lw, o_up, o_lc, o_w, bytes;
+  blob_layout(nb, t.nnz, t.n_u, &o_rp, &o_sc, &o_lw, &o_up, &o_lc, &o_w, &bytes);
+  out.assign(bytes, 0);
+  uint8_t *blob = out.data();
+  TileHdr *h = (TileHdr *)blob;
+  *h = TileHdr{nb, t.nnz, t.n_u, t.n_rows, t.n_cols, t.r0, t.e0, row_in_band};
+  uint32_t *rowp = (uint32_t *)(blob + o_rp);
+  float *scale = (float *)(blob + o_sc);
+  float *lw = (float *)(blob + o_lw);
+  uint32_t *upix = (uint32_t *)(blob + o_up);
+  uint16_t *lcol = (uint16_t *)(blob + o_lc);
+  float *wt = (float *)(blob + o_w);
+  std::vector<int32_t> u = tile_pixels(csr, m, t, lut);
+  for (size_t i = 0; i < u.size(); ++i) upix[i] = (uint32_t)u[i];
+  uint32_t nz_o = 0;
+  for (int r = t.r0; r < t.r0 + t.n_rows; ++r)
+    for (int e = t.e0; e < t.e0 + t.n_cols; ++e) {
+      const int64_t b = (int64_t)r * m.n_eta + e;
+      const int lb = (r - t.r0) * t.n_cols + (e - t.e0);
+      rowp[lb] = nz_o;
+      for (int64_t j = csr.row_ptr[b]; j < csr.row_ptr[b + 1]; ++j) {
+        lcol[nz_o] = (uint16_t)lut[csr.col[j]];
+        wt[nz_o] = (float)csr.w[j];
+        ++nz_o;
+      }
+      bin_scale(csr, p, b, scale + lb, lw + lb);
+    }
+  rowp[nb] = nz_o;
+  for (int32_t v : u) lut[v] = -1;
+}
+
+struct RunRec {
+  int rs, u;
+  float w[8];
+};
+
+static void runs_blob(const HostCSR &csr, const mi_map_desc &m, const Plan *p, const HostTile &t, int row_in_band,
+                      int G, int L, std::vector<int32_t> &lut, std::vector<uint8_t> &out) {
+  const int nb = t.n_rows * t.n_cols, NRS = G - L + 2;
+  std::vector<int32_t> u = tile_pixels(csr, m, t, lut);
+  std::vector<uint16_t> rsp((size_t)t.n_cols * NRS, 0);
+  std::vector<RunRec> all;
+  struct Trip {
+    int u, row;
+    double w;
+  };
+  std::vector<Trip> trip;
+  std::vector<RunRec> recs;
+  for (int c = 0; c < t.n_cols; ++c) {
+    trip.clear();
+    for (int i = 0; i < t.n_rows; ++i) {
+      const int64_t b = (int64_t)(t.r0 + i) * m.n_eta + t.e0 + c;
+      for (int64_t j = csr.row_ptr[b]; j < csr.row_ptr[b + 1]; ++j) trip.push_back({lut[csr.col[j]], i, csr.w[j]});
+    }
+    std::sort(trip.begin(), trip.end(), [](const Trip &a, const Trip &b) {
+      return a.u != b.u ? a.u < b.u : a.row < b.row;
+    });
+    recs.clear();
+    for (size_t k = 0; k < trip.size();) {
+      const int uu = trip[k].u;
+      while (k < trip.size() && trip[k].u == uu) {
+        RunRec r;
+        r.rs = std::min(trip[k].row, G - L);
+        r.u = uu;
+        for (int q = 0; q < 8; ++q) r.w[q] = 0.0f;
+        while (k < trip.size() && trip[k].u == uu && trip[k].row < r.rs + L) {
+          r.w[trip[k].row - r.rs] = (float)trip[k].w;
+          ++k;
+        }
+        recs.push_back(r);
+      }
+    }
+    std::stable_sort(recs.begin(), recs.end(), [](const RunRec &a, const RunRec &b) { return a.rs < b.rs; });
+    const size_t base = all.size();
+    size_t k = 0;
+    for (int q = 0; q < NRS; ++q) {
+      while (k < recs.size() && recs[k].rs < q) ++k;
+      rsp[(size_t)c * NRS + q] = (uint16_t)(base + (q == NRS - 1 ? recs.size() : k));
+    }
+    all.insert(all.end(), recs.begin(), recs.end());
+  }
+  const int n_rec = (int)all.size();
+  uint32_t o_rsp, o_sc, o_lw, o_up, o_lc, o_w;
+  const uint32_t bytes = runs_blob_layout(nb, t.n_cols, n_rec, t.n_u, G, L, &o_rsp, &o_sc, &o_lw, &o_up, &o_lc, &o_w);
+  out.assign(bytes, 0);
+  uint8_t *blob = out.data();
+  *(TileHdr *)blob = TileHdr{nb, n_rec, t.n_u, t.n_rows, t.n_cols, t.r0, t.e0, row_in_band};
+  memcpy(blob + o_rsp, rsp.data(), rsp.size() * sizeof(uint16_t));
+  float *scale = (float *)(blob + o_sc);
+  float *lw = (float *)(blob + o_lw);
+  for (int r = 0; r < t.n_rows; ++r)
+    for (int c = 0; c < t.n_cols; ++c)
+      bin_scale(csr, p, (int64_t)(t.r0 + r) * m.n_eta + t.e0 + c, scale + r * t.n_cols + c, lw + r * t.n_cols + c);
+  uint32_t *upix = (uint32_t *)(blob + o_up);
+  for (size_t i = 0; i < u.size(); ++i) upix[i] = (uint32_t)u[i];
+  uint16_t *lcol = (uint16_t *)(blob + o_lc);
+  float *w = (float *)(blob + o_w);
+  for (int i = 0; i < n_rec; ++i) {
+    lcol[i] = (uint16_t)all[i].u;
+    for (int q = 0; q < L; ++q) w[(size_t)i * L + q] = all[i].w[q];
+  }
+  for (int32_t v : u) lut[v] = -1;
+}
+
+// Rows per record: the candidate (2, 4 or 8 <= G/2) with the least estimated work
+// (records x (L + 6) instructions) over a sample of strips.
+static int choose_run_len(const HostCSR &csr, const mi_map_desc &m, int rows, int G) {
+  const int cands[3] = {2, 4, 8};
+  double cost[3] = {0, 0, 0};
+  std::vector<std::pair<int32_t, int>> pr;
+  const int bands = (m.n_r + rows - 1) / rows;
+  for (int band = 0; band < bands; band += std::max(1, bands / 24))
+    for (int e = 0; e < m.n_eta; e += std::max(1, m.n_eta / 16)) {
+      pr.clear();
+      for (int i = 0; i < rows && band * rows + i < m.n_r; ++i) {
+        const int64_t b = (int64_t)(band * rows + i) * m.n_eta + e;
+        for (int64_t j = csr.row_ptr[b]; j < csr.row_ptr[b + 1]; ++j) pr.push_back({csr.col[j], i});
+      }
+      std::sort(pr.begin(), pr.end());
+      for (int ci = 0; ci < 3; ++ci) {
+        const int L = cands[ci];
+        if (L > G / 2 || (G >= 16 && L == 2)) { cost[ci] = 1e300; continue; }
+        int64_t nrec = 0;
+        for (size_t k = 0; k < pr.size();) {
+          const int32_t uu = pr[k].first;
+          while (k < pr.size() && pr[k].first == uu) {
+            const int rs = std::min(pr[k].second, G - L);
+            while (k < pr.size() && pr[k].first == uu && pr[k].second < rs + L) ++k;
+            ++nrec;
+          }
+        }
+        cost[ci] += (double)nrec * (L + 6);
+      }
+    }
+  int best = 1;
+  for (int ci = 0; ci < 3; ++ci)
+    if (cost[ci] < cost[best]) best = ci;
+  return cands[best];
 }
 
 static int free_plan_mem(Plan *p) {
@@ -336,20 +507,41 @@ static int build_plan(const mi_map_desc &m, const mi_plan_opts &o, Plan *p) {
   p->nnz = (int64_t)csr.col.size();
   p->oob = csr.oob;
 
-  // ---- limits
+  // ---- encoding and limits
+  const int enc = (o.encoding == MI_ENC_CSR) ? MI_ENC_CSR : MI_ENC_RUNS;
+  if (o.encoding < 0 || o.encoding > 2) return set_error(MI_E_ARG, "unknown encoding %d", o.encoding);
+  p->encoding = enc;
   int fpl = o.frames_per_lane > 0 ? o.frames_per_lane : 1;
   if (fpl != 1 && fpl != 2 && fpl != 4) return set_error(MI_E_ARG, "frames_per_lane must be 1, 2 or 4");
   p->frames_per_lane = fpl;
   TileLimits L;
   L.rows = o.tile_rows > 0 ? o.tile_rows : 16;
-  if (L.rows > 64) return set_error(MI_E_RANGE, "tile_rows %d > 64", L.rows);
-  L.max_u = o.tile_pixels > 0 ? o.tile_pixels : (fpl == 1 ? 640 : (fpl == 2 ? 320 : 160));
+  if (L.rows > (enc == MI_ENC_RUNS ? 32 : 64))
+    return set_error(MI_E_RANGE, "tile_rows %d > %d", L.rows, enc == MI_ENC_RUNS ? 32 : 64);
+  L.max_u = o.tile_pixels > 0 ? o.tile_pixels
+                              : (enc == MI_ENC_RUNS ? 1024 : (fpl == 1 ? 640 : (fpl == 2 ? 320 : 160)));
   if (L.max_u > 65535) return set_error(MI_E_RANGE, "tile_pixels %d > 65535", L.max_u);
   L.max_nb = 256;
-  L.max_nnz = 4096;
+  L.max_nnz = enc == MI_ENC_RUNS ? 12288 : 4096;
+  L.max_cols = enc == MI_ENC_RUNS ? kRunWarps : 1 << 30;
   L.item_cols = std::max(1, (m.n_eta + 11) / 12);
+  int G = 0, RL = 0;
+  if (enc == MI_ENC_RUNS) {
+    G = L.rows <= 8 ? 8 : (L.rows <= 16 ? 16 : 32);
+    RL = o.run_len > 0 ? o.run_len : choose_run_len(csr, m, L.rows, G);
+    if (!(RL == 2 || RL == 4 || RL == 8) || RL > G / 2 || (G == 32 && RL == 2) || (G == 16 && RL == 2))
+      return set_error(MI_E_ARG, "run_len %d not supported with %d rows per strip", RL, G);
+  }
+  p->run_g = G;
+  p->run_l = RL;
   int dev_smem = 0;
   MI_CUDA(cudaDeviceGetAttribute(&dev_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, p->device));
+  if (enc == MI_ENC_RUNS) {
+    // budget for kRunCtasPerSm resident CTAs per SM (1 KB per CTA is reserved by the runtime)
+    int sm_smem = 0;
+    MI_CUDA(cudaDeviceGetAttribute(&sm_smem, cudaDevAttrMaxSharedMemoryPerMultiprocessor, p->device));
+    dev_smem = std::min(dev_smem, sm_smem / kRunCtasPerSm - 1024);
+  }
 
   // ---- items and tiles; shrink the tile limits until the kernel's shared memory fits
   const int n_bands = (m.n_r + L.rows - 1) / L.rows;
@@ -357,16 +549,18 @@ static int build_plan(const mi_map_desc &m, const mi_plan_opts &o, Plan *p) {
   p->n_slots = n_slots;
   const int n_items = n_bands * n_slots;
   std::vector<std::vector<HostTile>> item_tiles(n_items);
+  std::vector<std::vector<std::vector<uint8_t>>> item_blobs(n_items);
   for (int attempt = 0;; ++attempt) {
-    for (auto &v : item_tiles) v.clear();
     int err = MI_OK;
     int nthr = std::min(omp_get_max_threads(), 16);
 #pragma omp parallel num_threads(nthr)
     {
-      std::vector<int32_t> stamp(n_pix, 0);
+      std::vector<int32_t> stamp(n_pix, 0), lut(n_pix, -1);
       int32_t sid = 0;
 #pragma omp for schedule(dynamic, 1)
       for (int it = 0; it < n_items; ++it) {
+        item_tiles[it].clear();
+        item_blobs[it].clear();
         int band = it / n_slots, slot = it % n_slots;
         int r0 = band * L.rows, nr = std::min(L.rows, m.n_r - r0);
         int e0 = slot * L.item_cols, e1 = std::min(m.n_eta, e0 + L.item_cols);
@@ -375,36 +569,44 @@ static int build_plan(const mi_map_desc &m, const mi_plan_opts &o, Plan *p) {
         if (e) {
 #pragma omp critical
           err = e;
+          continue;
+        }
+        for (const HostTile &t : item_tiles[it]) {
+          item_blobs[it].emplace_back();
+          if (enc == MI_ENC_RUNS)
+            runs_blob(csr, m, p, t, t.r0 - r0, G, RL, lut, item_blobs[it].back());
+          else
+            csr_blob(csr, m, p, t, t.r0 - r0, lut, item_blobs[it].back());
         }
       }
     }
     if (err) return err;
     uint32_t mb = 0;
     int mu = 1, mnb = 1;
-    for (const auto &v : item_tiles)
-      for (const HostTile &t : v) {
-        uint32_t a, b, c, d, e, f, bytes;
-        blob_layout(t.n_rows * t.n_cols, t.nnz, t.n_u, &a, &b, &c, &d, &e, &f, &bytes);
-        mb = std::max(mb, bytes);
-        mu = std::max(mu, t.n_u);
-        mnb = std::max(mnb, t.n_rows * t.n_cols);
+    for (int it = 0; it < n_items; ++it)
+      for (size_t k = 0; k < item_tiles[it].size(); ++k) {
+        mb = std::max(mb, (uint32_t)item_blobs[it][k].size());
+        mu = std::max(mu, item_tiles[it][k].n_u);
+        mnb = std::max(mnb, item_tiles[it][k].n_rows * item_tiles[it][k].n_cols);
       }
-    const uint32_t need = cake_smem_layout(fpl, (mb + 15u) & ~15u, mu, mnb | 1, L.rows, nullptr, nullptr,
-                                           nullptr, nullptr);
+    const uint32_t cap = (mb + 15u) & ~15u;
+    const uint32_t need = enc == MI_ENC_RUNS
+                              ? runs_smem_layout(cap, mu, mnb | 1, L.rows, G, runs_frames_per_group(2, G), nullptr,
+                                                 nullptr, nullptr, nullptr, nullptr, nullptr)
+                              : cake_smem_layout(fpl, cap, mu, mnb | 1, L.rows, nullptr, nullptr, nullptr, nullptr);
     if (need + 1024u <= (uint32_t)dev_smem) break;
-    if (attempt >= 10 || L.max_u <= 32)
+    if (attempt >= 12 || L.max_u <= 32)
       return set_error(MI_E_RANGE, "tiles need %u B of shared memory (device allows %d); lower tile_rows",
                        need, dev_smem);
-    L.max_u = std::max(32, L.max_u * 3 / 4);
-    L.max_nnz = std::max(256, L.max_nnz * 3 / 4);
-    L.max_nb = std::max(16, L.max_nb * 3 / 4);
+    L.max_u = std::max(32, L.max_u * 4 / 5);
+    L.max_nnz = std::max(256, L.max_nnz * 4 / 5);
+    L.max_nb = std::max(16, L.max_nb * 4 / 5);
   }
   p->lim = L;
 
   // ---- blob arena
   std::vector<TileRef> tiles;
   std::vector<WorkItem> items(n_items);
-  std::vector<uint64_t> tile_off;
   uint64_t arena = 0;
   uint32_t max_blob = 0;
   int max_u = 0, max_nb = 0;
@@ -417,9 +619,9 @@ static int build_plan(const mi_map_desc &m, const mi_plan_opts &o, Plan *p) {
     w.n_rows = std::min(L.rows, m.n_r - w.r0);
     w.slot = slot;
     w.nnz = 0;
-    for (const HostTile &t : item_tiles[it]) {
-      uint32_t a, b, c, d, e, f, bytes;
-      blob_layout(t.n_rows * t.n_cols, t.nnz, t.n_u, &a, &b, &c, &d, &e, &f, &bytes);
+    for (size_t k = 0; k < item_tiles[it].size(); ++k) {
+      const HostTile &t = item_tiles[it][k];
+      const uint32_t bytes = (uint32_t)item_blobs[it][k].size();
       tiles.push_back({arena, bytes, 0});
       arena += bytes;
       max_blob = std::max(max_blob, bytes);
@@ -436,77 +638,11 @@ static int build_plan(const mi_map_desc &m, const mi_plan_opts &o, Plan *p) {
   p->max_nb = max_nb;
   p->staged_pixels = staged;
   std::vector<uint8_t> blobs(arena, 0);
-  {
-    std::vector<int64_t> first_tile(n_items);
-    for (int it = 0; it < n_items; ++it) first_tile[it] = items[it].tile_begin;
-    int nthr = std::min(omp_get_max_threads(), 16);
-#pragma omp parallel num_threads(nthr)
-    {
-      std::vector<int32_t> lut(n_pix, -1);
-#pragma omp for schedule(dynamic, 1)
-      for (int it = 0; it < n_items; ++it) {
-        int k = 0;
-        for (const HostTile &t : item_tiles[it]) {
-          const TileRef &ref = tiles[first_tile[it] + k++];
-          uint8_t *blob = blobs.data() + ref.off;
-          const int nb = t.n_rows * t.n_cols;
-          uint32_t o_rp, o_sc, o_lw, o_up, o_lc, o_w, bytes;
-          blob_layout(nb, t.nnz, t.n_u, &o_rp, &o_sc, &o_lw, &o_up, &o_lc, &o_w, &bytes);
-          TileHdr *h = (TileHdr *)blob;
-          h->nb = nb;
-          h->nnz = t.nnz;
-          h->n_u = t.n_u;
-          h->n_rows = t.n_rows;
-          h->n_cols = t.n_cols;
-          h->r0 = t.r0;
-          h->e0 = t.e0;
-          h->row_in_band = t.r0 - items[it].r0;
-          uint32_t *rowp = (uint32_t *)(blob + o_rp);
-          float *scale = (float *)(blob + o_sc);
-          float *lw = (float *)(blob + o_lw);
-          uint32_t *upix = (uint32_t *)(blob + o_up);
-          uint16_t *lcol = (uint16_t *)(blob + o_lc);
-          float *wt = (float *)(blob + o_w);
-          // staged pixel set, ascending
-          std::vector<int32_t> u;
-          u.reserve(t.n_u);
-          for (int r = t.r0; r < t.r0 + t.n_rows; ++r)
-            for (int e = t.e0; e < t.e0 + t.n_cols; ++e) {
-              int64_t b = (int64_t)r * m.n_eta + e;
-              for (int64_t j = csr.row_ptr[b]; j < csr.row_ptr[b + 1]; ++j) u.push_back(csr.col[j]);
-            }
-          std::sort(u.begin(), u.end());
-          u.erase(std::unique(u.begin(), u.end()), u.end());
-          for (size_t i = 0; i < u.size(); ++i) {
-            upix[i] = (uint32_t)u[i];
-            lut[u[i]] = (int32_t)i;
-          }
-          uint32_t nz_o = 0;
-          for (int r = t.r0; r < t.r0 + t.n_rows; ++r)
-            for (int e = t.e0; e < t.e0 + t.n_cols; ++e) {
-              int64_t b = (int64_t)r * m.n_eta + e;
-              int lb = (r - t.r0) * t.n_cols + (e - t.e0);
-              rowp[lb] = nz_o;
-              for (int64_t j = csr.row_ptr[b]; j < csr.row_ptr[b + 1]; ++j) {
-                lcol[nz_o] = (uint16_t)lut[csr.col[j]];
-                wt[nz_o] = (float)csr.w[j];
-                ++nz_o;
-              }
-              const double an = csr.area_norm[b], ai = csr.area_in[b];
-              double sc;
-              if (p->semantics == MI_SEM_GPUSTREAM)
-                sc = an > kAreaThreshold ? (p->normalize ? 1.0 / an : 1.0) : 0.0;
-              else
-                sc = p->normalize ? (ai > kAreaThreshold ? 1.0 / ai : 0.0) : 1.0;
-              scale[lb] = (float)sc;
-              lw[lb] = ai > kAreaThreshold ? (float)ai : 0.0f;
-            }
-          rowp[nb] = nz_o;
-          for (size_t i = 0; i < u.size(); ++i) lut[u[i]] = -1;
-        }
-      }
+  for (int it = 0, ti = 0; it < n_items; ++it)
+    for (size_t k = 0; k < item_blobs[it].size(); ++k, ++ti) {
+      memcpy(blobs.data() + tiles[ti].off, item_blobs[it][k].data(), item_blobs[it][k].size());
+      std::vector<uint8_t>().swap(item_blobs[it][k]);
     }
-  }
   // distinct referenced pixels
   {
     std::vector<uint8_t> seen(n_pix, 0);
@@ -676,7 +812,7 @@ int mi_plan_get_info(const mi_plan *p, mi_plan_info *info) {
   info->tile_rows = p->lim.rows;
   info->tile_pixels = p->lim.max_u;
   info->frames_per_lane = p->frames_per_lane;
-  info->run_len = 0;
+  info->run_len = p->run_l;
   return MI_OK;
 }
 

@@ -60,13 +60,15 @@ class CakePlan:
         bc_y, bc_z: beam centre (px), used by gradient mode.
         device: CUDA device.
         tile_rows, tile_pixels, frames_per_lane: tiling knobs (0 = default).
+        encoding: 'auto' (= 'runs') | 'runs' (register-blocked radial runs) | 'csr'
+            (per-bin term lists); run_len: rows per run record (2, 4, 8; 0 = auto).
     """
 
     def __init__(self, pixmap: PixelMap, *, n_r: int, n_eta: int, n_pixels_y: int,
                  n_pixels_z: int, mode: str = "floor", normalize: bool = True,
                  semantics: str = "py", bc_y: float = 0.0, bc_z: float = 0.0,
                  device="cuda", tile_rows: int = 0, tile_pixels: int = 0,
-                 frames_per_lane: int = 0):
+                 frames_per_lane: int = 0, encoding: str = "auto", run_len: int = 0):
         if pixmap.n_bins != n_r * n_eta:
             raise ValueError(f"PixelMap has {pixmap.n_bins} bins; n_r * n_eta = {n_r * n_eta}")
         if mode not in L.MODE:
@@ -83,8 +85,11 @@ class CakePlan:
         desc = L.MiMapDesc(recs.ctypes.data if recs.size else None, recs.shape[0],
                            nmap.ctypes.data, self.n_r, self.n_eta, self.ny, self.nz,
                            self.bc_y, self.bc_z)
+        if encoding not in L.ENC:
+            raise ValueError(f"unknown encoding {encoding!r}; expected 'auto' | 'csr' | 'runs'")
         opts = L.MiPlanOpts(L.MODE[mode], int(self.normalize), L.SEM[semantics],
-                            int(tile_rows), int(tile_pixels), int(frames_per_lane))
+                            int(tile_rows), int(tile_pixels), int(frames_per_lane),
+                            L.ENC[encoding], int(run_len))
         h = C.c_void_p()
         L.check(L.lib().mi_plan_create(C.byref(desc), C.byref(opts), self.device.index,
                                        C.byref(h)), "mi_plan_create")

@@ -138,7 +138,7 @@ def sweep_2880() -> Workload:
                      EtaMin=-180.0, EtaMax=180.0, EtaBinSize=1.0, SolidAngleCorrection=1,
                      PolarizationCorrection=1, PolarizationFraction=0.99, Parallax=100.0)
     return Workload("sweep_2880x2880_u16_3960x360_gradient", m, "gradient", amp_drift=0.2,
-                    n_spots=50, n_frames=1440, tile_rows=32)
+                    n_spots=50, n_frames=1440, tile_rows=16)
 
 
 def scaled(w: Workload, factor: int, name: Optional[str] = None) -> Workload:

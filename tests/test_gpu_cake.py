@@ -44,11 +44,12 @@ def _oracle_batch(g, frames, mode, norm, sem, records=None, nmap=None):
 @pytest.mark.parametrize("mode", ["floor", "bilinear", "gradient"])
 @pytest.mark.parametrize("norm", [True, False])
 @pytest.mark.parametrize("sem", ["py", "gpustream"])
-def test_batched_matches_oracle(cuda, tag, mode, norm, sem):
+@pytest.mark.parametrize("enc", ["runs", "csr"])
+def test_batched_matches_oracle(cuda, tag, mode, norm, sem, enc):
     g = load_kernels_case(tag)
     pm = from_arrays(g["records"], g["nmap"])
     plan = CakePlan(pm, n_r=g["n_r"], n_eta=g["n_eta"], n_pixels_y=g["ny"], n_pixels_z=g["nz"], mode=mode,
-                    normalize=norm, semantics=sem, bc_y=g["bc_y"], bc_z=g["bc_z"], device=cuda)
+                    normalize=norm, semantics=sem, bc_y=g["bc_y"], bc_z=g["bc_z"], device=cuda, encoding=enc)
     frames = _frames_like(g["image"], 7, seed=1)
     ck, aw, sm = plan.integrate(torch.from_numpy(frames).to(cuda))
     rc, raw, rsm = _oracle_batch(g, frames, mode, norm, sem)
@@ -82,16 +83,23 @@ def test_midas_integrate_api_matches_reference_golden(cuda, tag, mode):
             assert rel_err(prof.cpu().numpy(), g[gk + key])[0] <= 1e-6
 
 
+ENCODINGS = [("csr", 1, 0, 8), ("csr", 2, 0, 8), ("csr", 4, 0, 8), ("runs", 0, 2, 8), ("runs", 0, 4, 8),
+             ("runs", 0, 4, 16), ("runs", 0, 8, 16), ("runs", 0, 4, 32), ("runs", 0, 8, 32), ("runs", 0, 0, 12)]
+
+
 @pytest.mark.parametrize("tag", MAPPER_CASES)
 @pytest.mark.parametrize("mode", ["floor", "gradient"])
-@pytest.mark.parametrize("fpl", [1, 2, 4])
-def test_detector_maps_u16_with_dark(cuda, tag, mode, fpl):
-    """DetectorMapper maps, raw u16 frames and a float dark (cast + dark fused into staging)."""
+@pytest.mark.parametrize("enc,fpl,rl,rows", ENCODINGS)
+def test_detector_maps_u16_with_dark(cuda, tag, mode, enc, fpl, rl, rows):
+    """DetectorMapper maps, raw u16 frames and a float dark (cast + dark fused into staging),
+    every tile encoding and register-run shape."""
     g = load_mapper_case(tag)
     n_r, n_eta = g["r_lo"].size, g["eta_lo"].size
     pm = from_arrays(g["records"], g["nmap"])
     plan = CakePlan(pm, n_r=n_r, n_eta=n_eta, n_pixels_y=g["ny"], n_pixels_z=g["nz"], mode=mode,
-                    bc_y=g["bc_y"], bc_z=g["bc_z"], device=cuda, frames_per_lane=fpl, tile_rows=8)
+                    bc_y=g["bc_y"], bc_z=g["bc_z"], device=cuda, frames_per_lane=fpl, tile_rows=rows,
+                    encoding=enc, run_len=rl)
+    fpl = max(fpl, 1)
     rng = np.random.default_rng(5)
     F = 33 * fpl + 3                      # crosses frame-group boundaries
     raw = rng.integers(90, 60000, size=(F, g["nz"], g["ny"])).astype(np.uint16)
@@ -125,11 +133,12 @@ def test_frame_result_independent_of_batch(cuda):
 
 @pytest.mark.parametrize("dt", [torch.uint8, torch.uint16, torch.int32, torch.int64, torch.float32,
                                 torch.float64])
-def test_dtypes_agree(cuda, dt):
+@pytest.mark.parametrize("enc", ["runs", "csr"])
+def test_dtypes_agree(cuda, dt, enc):
     g = load_mapper_case("m1")
     n_r, n_eta = g["r_lo"].size, g["eta_lo"].size
     plan = CakePlan(from_arrays(g["records"], g["nmap"]), n_r=n_r, n_eta=n_eta, n_pixels_y=g["ny"],
-                    n_pixels_z=g["nz"], mode="floor", device=cuda)
+                    n_pixels_z=g["nz"], mode="floor", device=cuda, encoding=enc)
     rng = np.random.default_rng(3)
     raw = torch.from_numpy(rng.integers(0, 250, size=(4, g["nz"], g["ny"])).astype(np.uint8)).to(cuda)
     ref, _, _ = plan.integrate(raw)
