@@ -149,6 +149,20 @@ int mi_integrate_batch(mi_plan *plan, const void *frames, int dtype, int n_frame
                        int64_t frame_stride, float *cake, double *lineout_aw,
                        double *lineout_sm, void *stream);
 
+/* mi_integrate_batch that allocates nothing (no counterpart in the reference).
+ * For callers that cannot have device memory allocated for them once running -- a
+ * detector front-end that owns the whole device memory budget, or a host recording its
+ * per-batch work into a CUDA graph -- the batched kernels keep their only scratch, the
+ * per-row lineout partial sums, in a fixed 8 MiB array inside the library (held on every
+ * GPU that loads it until exit).  Same arguments and results as mi_integrate_batch;
+ * frames are processed in chunks that fit the array; a plan needing more than the array
+ * for one frame (n_r x 12 x 2 doubles > 1,048,576) gets MI_E_RANGE.  The first call on a
+ * device looks up the array's address: make it before any stream capture.  Calls that
+ * overlap on the GPU share the array and race. */
+int mi_integrate_batch_static(mi_plan *plan, const void *frames, int dtype, int n_frames,
+                              int64_t frame_stride, float *cake, double *lineout_aw,
+                              double *lineout_sm, void *stream);
+
 /* The reference's own GPU algorithm, one frame per launch: cast/dark kernel, one thread per
  * bin in heaviest-first order with FP32 accumulation and on-the-fly bilinear sampling in
  * gradient mode, FP64 cake, then the two profile kernels.  This is the plain baseline. */

@@ -100,6 +100,8 @@ SIGNATURES = [
     ("mi_plan_destroy", None, [C.c_void_p]),
     ("mi_integrate_batch", C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_int64,
                                      C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
+    ("mi_integrate_batch_static", C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_int64,
+                                            C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     ("mi_integrate_plain", C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p,
                                      C.c_void_p, C.c_void_p]),
     ("mi_profile_batch", C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_void_p,
