@@ -53,6 +53,9 @@ def parse():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-check", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
+    ap.add_argument("--serve-seconds", type=float, default=8.0,
+                    help="duration of the 6-stream serving load (0 = skip)")
+    ap.add_argument("--serve-trace", default="", help="write per-frame serving timestamps to <prefix>_*.npz")
     return ap.parse_args()
 
 
@@ -170,7 +173,7 @@ def cpu_reference_rate(pm, w, frame_u16, dark, seconds):
         run = lambda: oracle.integrate(recs, nmap, pm.n_bins, ny, nz, sub, mode=w.mode, bc_y=w.mapper.BC_y,
                                        bc_z=w.mapper.BC_z)
         kind = "port"
-    run()  # warm-up (page-in)
+    out = run()  # warm-up (page-in)
     n, t0 = 0, time.perf_counter()
     while True:
         run()
@@ -178,7 +181,55 @@ def cpu_reference_rate(pm, w, frame_u16, dark, seconds):
         el = time.perf_counter() - t0
         if el >= seconds or n >= 200:
             break
-    return n / el, cores, kind, f"{n} full {w.mapper.NrPixelsZ}x{w.mapper.NrPixelsY} frame(s) in {el:.1f} s"
+    return (n / el, cores, kind, f"{n} full {w.mapper.NrPixelsZ}x{w.mapper.NrPixelsY} frame(s) in {el:.1f} s",
+            out)
+
+
+def _rel(got, ref):
+    import numpy as np
+    nz = ref[ref != 0]
+    tau = 1e-3 * np.median(np.abs(nz)) if nz.size else 1e-30
+    return np.abs(got - ref) / np.maximum(np.abs(ref), tau)
+
+
+def accuracy_check(pm, w, frame, dark, got, ref_out, kind):
+    """Frame 0 of the batched path against the FP64 oracle and, when the reference integrator
+    ran, against its own output (sums / norms of integration_apply_map)."""
+    import numpy as np
+    import oracle
+    ny, nz = w.mapper.NrPixelsY, w.mapper.NrPixelsZ
+    sub = (frame.astype(np.float32) - dark).astype(np.float64)
+    ref, _ = oracle.integrate(pm.pxList, pm.nmap_pairs(), pm.n_bins, ny, nz, sub, mode=w.mode,
+                              bc_y=w.mapper.BC_y, bc_z=w.mapper.BC_z)
+    area = oracle.area_in(pm.pxList, pm.nmap_pairs(), pm.n_bins, ny, nz)
+    aw_ref, _ = oracle.profile(ref, area, w.n_r, w.n_eta)
+    r, ra = _rel(got[0], ref), _rel(got[1], aw_ref)
+    acc = {"cake_max_rel": float(r.max()), "cake_mean_rel": float(r.mean()), "lineout_max_rel": float(ra.max()),
+           "frames_checked": 1}
+    ic = None
+    if kind == "reference" and w.mode in ("floor", "gradient"):
+        sums, norms = ref_out
+        ic_cake = np.where(norms > 0, sums / np.where(norms > 0, norms, 1.0), 0.0)
+        ri = _rel(got[0], ic_cake)
+        ic = {"cake_max_rel": float(ri.max()), "cake_mean_rel": float(ri.mean()), "frames_checked": 1,
+              "integrator": "integration_apply_map (IntegrationCore.c), sums / norms"}
+    return acc, ic
+
+
+def served_accuracy(served):
+    """Max relative error of each served stream's first lineout against the FP64 oracle."""
+    import numpy as np
+    import oracle
+    worst = 0.0
+    for c, frame, lineout in served:
+        pm = c.pixmap
+        ck, _ = oracle.integrate(pm.pxList, pm.nmap_pairs(), pm.n_bins, c.n_pixels_y, c.n_pixels_z,
+                                 (frame.astype(np.float32) - c.dark).astype(np.float64), mode=c.mode,
+                                 bc_y=c.bc_y, bc_z=c.bc_z)
+        area = oracle.area_in(pm.pxList, pm.nmap_pairs(), pm.n_bins, c.n_pixels_y, c.n_pixels_z)
+        ref, _ = oracle.profile(ck, area, c.n_r, c.n_eta)
+        worst = max(worst, float(_rel(lineout, ref).max()))
+    return worst
 
 
 def main_ours(args):
@@ -223,23 +274,12 @@ def main_ours(args):
         b = i % n_batches
         plan.integrate(frames[b * F:(b + 1) * F], out=bufs)
 
-    # ---- accuracy of a sampled frame against the FP64 oracle (untimed)
-    err = None
-    if rank == 0 and not args.no_check:
-        import oracle
-        step(0)
-        torch.cuda.synchronize()
-        sub = frames[0].cpu().numpy().astype(np.float32) - dark_np
-        ref, _ = oracle.integrate(pm.pxList, pm.nmap_pairs(), pm.n_bins, ny, nz, sub.astype(np.float64),
-                                  mode=w.mode, bc_y=w.mapper.BC_y, bc_z=w.mapper.BC_z)
-        got = cake[0].reshape(-1).cpu().numpy().astype(np.float64)
-        tau = 1e-3 * np.median(np.abs(ref[ref != 0]))
-        r = np.abs(got - ref) / np.maximum(np.abs(ref), tau)
-        area = oracle.area_in(pm.pxList, pm.nmap_pairs(), pm.n_bins, ny, nz)
-        aw_ref, _ = oracle.profile(ref, area, w.n_r, w.n_eta)
-        ra = np.abs(aw[0].cpu().numpy() - aw_ref) / np.maximum(np.abs(aw_ref), 1e-3 * np.median(np.abs(aw_ref)))
-        err = {"cake_max_rel": float(r.max()), "cake_mean_rel": float(r.mean()),
-               "lineout_max_rel": float(ra.max()), "frames_checked": 1}
+    # ---- frame 0 through the batched path, kept for the accuracy check of the CPU leg
+    # (a frame's result does not depend on the rest of its batch)
+    frame0 = frames[0].cpu().numpy()
+    c0, a0, _ = plan.integrate(frames[0:1])
+    got0 = (c0[0].reshape(-1).cpu().numpy().astype(np.float64), a0[0].cpu().numpy())
+    del c0, a0
 
     # ---- warm-up, then K timed steps
     stream = torch.cuda.current_stream()
@@ -297,8 +337,6 @@ def main_ours(args):
            "setup_s": {"map_build_gpu": round(t_map, 2), "plan_build": round(t_plan, 2)}}
     if clk:
         out["clocks"] = clk
-    if err:
-        out["accuracy_vs_fp64_oracle"] = err
 
     # ---- plain one-frame-per-launch kernel (reference GPU algorithm) on the same frames
     if not args.no_plain:
@@ -312,7 +350,7 @@ def main_ours(args):
             plan.integrate_plain(frames[(k * 37) % sweep])
         b.record(stream)
         torch.cuda.synchronize()
-        plain_fps = dist_max(0, world) if False else P / (a.elapsed_time(b) / 1e3)
+        plain_fps = P / (a.elapsed_time(b) / 1e3)
         out["plain"] = {"frames_per_s": round(plain_fps, 1), "frames": P,
                         "speedup_batched_vs_plain": round(value / world / plain_fps, 2)}
 
@@ -320,17 +358,159 @@ def main_ours(args):
     if not args.no_e2e:
         out["e2e"] = e2e_rate(plan, frames, F, args, w, dev, world)
 
-    # ---- CPU baseline: the reference integrator on this host (rank 0, N = 1)
+    # ---- serving load: six streams with different maps, Poisson arrivals (rank 0, N = 1)
+    served = []
+    if rank == 0 and world == 1 and args.serve_seconds > 0:
+        del frames
+        plan.close()
+        torch.cuda.empty_cache()
+        out["serving"], served = serving_load(args, dev, plain=False)
+        out["serving"]["plain_loop"], _ = serving_load(args, dev, plain=True)
+
+    # ---- CPU leg (rank 0, N = 1): the reference integrator timed on this host's cores, and
+    # the accuracy of frame 0 and of the served lineouts against it and the FP64 oracle
     if rank == 0 and world == 1 and not args.no_cpu:
-        fps, cores, kind, sample = cpu_reference_rate(pm, w, frames[0].cpu().numpy(), dark_np, args.cpu_seconds)
+        fps, cores, kind, sample, ref_out = cpu_reference_rate(pm, w, frame0, dark_np, args.cpu_seconds)
         out["cpu_baseline"] = {"value": round(fps, 3), "unit": UNIT, "cores": cores, "kind": kind,
                                "sample": sample}
+        if not args.no_check:
+            out["accuracy_vs_fp64_oracle"], ic = accuracy_check(pm, w, frame0, dark_np, got0, ref_out, kind)
+            if ic:
+                out["accuracy_vs_reference_integrator"] = ic
+            if served:
+                out["serving"]["lineout_max_rel_vs_fp64_oracle"] = served_accuracy(served)
     if rank == 0:
         print(json.dumps(out), flush=True)
     plan.close()
     if world > 1:
         import torch.distributed as dist
         dist.destroy_process_group()
+
+
+def serving_load(args, dev, plain=False, n_distinct=8):
+    """Six concurrent detector streams (synth.serving_mix) with Poisson frame arrivals served
+    by CakeServer for ``--serve-seconds``; a seventh stream with a fresh map is admitted
+    half way through.  Latency = scheduled arrival -> lineouts + fits on the host."""
+    import threading
+
+    import numpy as np
+    import torch
+
+    from midas_b200 import synth
+    from midas_b200.server import AdmissionError, CakeServer, DeviceBackend
+
+    T = args.serve_seconds
+    mix = synth.serving_mix()
+
+    def cfg_of(w, rate):
+        c = synth.serving_stream(w, device=dev.index)
+        c.max_batch = 16 if rate >= 100 else 4
+        return c
+
+    streams = [(cfg_of(w, rate), rate, synth.host_frames(w, 0, n_distinct, dev.index)) for w, rate in mix]
+    late_w, late_rate = synth.late_stream()
+    late_frames = synth.host_frames(late_w, 0, n_distinct, dev.index)
+    backend = DeviceBackend(device=dev.index, max_batch=16, max_inflight=2, plain=plain)
+    srv = CakeServer(backend=backend).start()
+    sids = [srv.admit(c) for c, _, _ in streams]
+    # warm-up: every stream once (plan upload, first launches), then clear the counters
+    warm = [srv.submit(sid, fr[0]) for sid, (_, _, fr) in zip(sids, streams)]
+    for f in warm:
+        f.result(timeout=300)
+    srv.latencies.clear()
+    srv.completed = srv.batches = 0
+    backend.alg_bytes = backend.launches = 0
+    per_stream = {}
+    offered = {}
+    stop_at = [0.0]
+    late_info = {}
+
+    def producer(name, sid, rate, frames, seed, t_end):
+        rng = np.random.default_rng(seed)
+        t = time.perf_counter()
+        futs = []
+        i = 0
+        while True:
+            t += rng.exponential(1.0 / rate)
+            if t >= t_end:
+                break
+            d = t - time.perf_counter()
+            if d > 0:
+                time.sleep(d)
+            futs.append(srv.submit(sid, frames[i % len(frames)], t_arrival=t))
+            i += 1
+        offered[name] = i
+        per_stream[name] = futs
+
+    def late():
+        time.sleep(T / 2)
+        t0 = time.perf_counter()
+        try:
+            c = cfg_of(late_w, late_rate)
+            sid = srv.admit(c)
+        except AdmissionError as e:
+            late_info.update(admitted=False, reason=str(e))
+            return
+        late_info.update(admitted=True, admit_s=round(time.perf_counter() - t0, 3), name=c.name,
+                         window=(t0, time.perf_counter()))
+        producer(c.name, sid, late_rate, late_frames, 99, stop_at[0])
+
+    # the host loop is Python: keep the cyclic garbage collector's pauses out of the window
+    import gc
+    gc.collect()
+    gc.freeze()
+    gc.disable()
+    t_start = time.perf_counter()
+    stop_at[0] = t_start + T
+    th = [threading.Thread(target=producer, args=(c.name, sid, rate, fr, k, stop_at[0]))
+          for k, (sid, (c, rate, fr)) in enumerate(zip(sids, streams))]
+    th.append(threading.Thread(target=late))
+    for t in th:
+        t.start()
+    for t in th:
+        t.join()
+    results = {name: [f.result(timeout=600) for f in futs] for name, futs in per_stream.items()}
+    t_done = time.perf_counter()
+    gc.enable()
+    gc.unfreeze()
+    srv.stop()
+    wall = t_done - t_start
+    lat = srv.latency_ms()
+    n_done = sum(len(v) for v in results.values())
+    streams_out = {}
+    for name, res in results.items():
+        a = np.sort(np.array([r.latency_s for r in res])) * 1e3
+        streams_out[name] = {"frames": len(res), "p50_ms": round(float(np.percentile(a, 50)), 3) if len(a) else None,
+                             "p99_ms": round(float(np.percentile(a, 99)), 3) if len(a) else None,
+                             "mean_batch": round(float(np.mean([r.batch_size for r in res])), 2) if res else None}
+    window = late_info.pop("window", None)
+    if args.serve_trace:
+        names = sorted(results)
+        rows = [(names.index(n), r.t_arrival - t_start, r.t_submit - t_start, r.t_dispatch - t_start,
+                 r.t_complete - t_start, r.batch_size) for n in names for r in results[n]]
+        np.savez(f"{args.serve_trace}_{'plain' if plain else 'batched'}.npz", rows=np.array(rows),
+                 names=np.array(names), window=np.array(window if window else (0.0, 0.0)) - t_start)
+    if window:
+        # frames that arrived while the late stream's map and plan were being built
+        lo, hi = window[0], window[1] + 0.05
+        steady = np.sort(np.array([r.latency_s for v in results.values() for r in v
+                                   if not lo <= r.t_arrival <= hi])) * 1e3
+        late_info["p99_ms_outside_admission"] = round(float(np.percentile(steady, 99)), 3)
+        late_info["frames_during_admission"] = int(sum(lo <= r.t_arrival <= hi for v in results.values()
+                                                       for r in v))
+    out = {"streams": len(streams) + (1 if late_info.get("admitted") else 0), "seconds": round(T, 2),
+           "offered_frames": sum(offered.values()), "completed_frames": n_done,
+           "frames_per_s": round(n_done / wall, 1), "p50_ms": round(lat["p50"], 3), "p99_ms": round(lat["p99"], 3),
+           "max_ms": round(lat["max"], 3), "hbm_alg_gb_s": round(backend.alg_bytes / wall / 1e9, 2),
+           "launch_calls": backend.launches, "batches": srv.batches,
+           "mode": "plain one-frame-per-launch" if plain else "continuous batching",
+           "late_stream": late_info, "per_stream": streams_out,
+           "latency": "scheduled Poisson arrival -> lineouts and ring fits in host memory"}
+    # each producer's first request carried frames[0] of its stream
+    served = [(c, fr[0], results[c.name][0].lineout_aw) for c, _, fr in streams if results.get(c.name)]
+    del streams
+    torch.cuda.empty_cache()
+    return out, served
 
 
 def e2e_rate(plan, frames, F, args, w, dev, world):

@@ -1,0 +1,501 @@
+"""Serving: continuous batching of frames from several detector streams on one GPU.
+
+Replaces the one-frame-at-a-time worker of the reference servers
+(packages/midas_integrate/midas_integrate/server.py:113-179; the stream loop of
+FF_HEDM/src/IntegratorFitPeaksGPUStream.cu:2571-2883, 4 CUDA streams round-robin,
+one frame per submit) with a scheduler that
+
+* keeps every admitted stream's map plan, dark and fit state resident on the device;
+* admits a stream only if its HBM footprint (plan + device buffers) fits the budget
+  left by the streams already admitted; a refused stream can be retried once others
+  leave;
+* on every scheduling tick, takes ALL frames that arrived for a stream since its last
+  dispatch (up to ``max_batch``) and launches them as one batch -- H2D copy, batched
+  caking with both lineouts, batched peak fits, D2H of lineouts and fits -- on that
+  stream's own CUDA stream, with up to ``max_inflight`` batches per stream in flight, so
+  work from different streams and successive batches overlaps on the device;
+* completes each request's future when its batch's event has fired, with the latency
+  arrival -> results on the host.
+
+A frame's results do not depend on which other frames share its batch (each frame is
+one lane of the batched kernels and is reduced in a fixed order), so a stream gets the
+same answer alone and in the mix.
+
+The device work goes through a backend; the default ``DeviceBackend`` runs
+libmidas_b200.  There is no CPU path in the product: a backend that computes on the
+host exists only in the tests, to exercise the scheduling logic without a GPU.
+"""
+from __future__ import annotations
+
+import collections
+import ctypes as C
+import itertools
+import threading
+import time
+from concurrent.futures import Future
+from dataclasses import dataclass, field
+from typing import Dict, List, Optional
+
+import numpy as np
+
+from . import _lib as L
+from .kernels import dtype_code
+from .peakfit import MODELS
+
+
+class AdmissionError(RuntimeError):
+    """The stream's device footprint does not fit the remaining HBM budget (or its host
+    staging does not fit the pinned pool)."""
+
+
+class PinnedPool:
+    """Page-locked host memory taken once, up front, and carved into staging buffers.
+
+    Page-locking memory (cudaHostAlloc) takes a driver lock for a time proportional to
+    the size, stalling the CUDA calls of every other thread; a stream admitted while
+    others run must not do that, so its staging comes from this pool (first fit,
+    256-byte aligned, coalescing free list)."""
+
+    ALIGN = 256
+
+    def __init__(self, nbytes: int, pin: bool = True):
+        import torch
+        self.torch = torch
+        self.nbytes = int(nbytes)
+        self.buf = torch.empty(self.nbytes, dtype=torch.uint8, pin_memory=pin)
+        self.free = [(0, self.nbytes)]
+        self._lock = threading.Lock()
+
+    def alloc(self, shape, dtype):
+        """(tensor view, token) or AdmissionError when no free range is large enough."""
+        n = int(np.prod(shape)) * self.torch.empty((), dtype=dtype).element_size()
+        n = max(self.ALIGN, (n + self.ALIGN - 1) // self.ALIGN * self.ALIGN)
+        with self._lock:
+            for i, (off, size) in enumerate(self.free):
+                if size >= n:
+                    self.free[i:i + 1] = [(off + n, size - n)] if size > n else []
+                    t = self.buf[off:off + n].view(dtype)[:int(np.prod(shape))].view(shape)
+                    return t, (off, n)
+        raise AdmissionError(f"pinned staging pool ({self.nbytes / 1e9:.2f} GB) has no free {n / 1e6:.1f} MB range")
+
+    def release(self, token) -> None:
+        off, n = token
+        with self._lock:
+            self.free.append((off, n))
+            self.free.sort()
+            merged = []
+            for o, s in self.free:
+                if merged and merged[-1][0] + merged[-1][1] == o:
+                    merged[-1] = (merged[-1][0], merged[-1][1] + s)
+                else:
+                    merged.append((o, s))
+            self.free = merged
+
+    def free_bytes(self) -> int:
+        with self._lock:
+            return sum(s for _, s in self.free)
+
+
+@dataclass
+class StreamConfig:
+    name: str
+    pixmap: object                 # bin_io.PixelMap
+    n_r: int
+    n_eta: int
+    n_pixels_y: int
+    n_pixels_z: int
+    mode: str = "floor"
+    bc_y: float = 0.0
+    bc_z: float = 0.0
+    dark: Optional[np.ndarray] = None
+    frame_dtype: str = "uint16"    # numpy dtype name of the raw frames
+    r_axis: Optional[np.ndarray] = None     # lineout x (R bin centres) for the fits
+    peaks: Optional[np.ndarray] = None      # ring positions to fit (x units)
+    fit_model: str = "pv"
+    fit_half_window: int = 12
+    x_bin: float = 1.0
+    want_cake: bool = False
+    tile_rows: int = 0
+    max_batch: int = 0             # frames per launch at most (0 = the backend's default)
+
+
+@dataclass
+class FrameResult:
+    stream: str
+    seq: int
+    lineout_aw: np.ndarray
+    lineout_sm: np.ndarray
+    fits: Optional[np.ndarray]     # [n_peaks, 11]
+    cake: Optional[np.ndarray]
+    latency_s: float
+    batch_size: int
+    t_arrival: float               # time.perf_counter() of the arrival,
+    t_submit: float                # of the submit() call,
+    t_dispatch: float              # of the launch of its batch,
+    t_complete: float              # and of its completion
+
+
+@dataclass
+class _Req:
+    seq: int
+    frame: np.ndarray
+    t_arrival: float
+    fut: Future
+    t_submit: float = 0.0
+    t_dispatch: float = 0.0
+
+
+@dataclass
+class _Stream:
+    sid: int
+    cfg: StreamConfig
+    state: object                  # backend-specific
+    footprint: int
+    pending: collections.deque = field(default_factory=collections.deque)
+    inflight: collections.deque = field(default_factory=collections.deque)   # (handle, reqs)
+    seq: itertools.count = field(default_factory=itertools.count)
+    closing: bool = False
+
+
+class DeviceBackend:
+    """Runs a stream's batches through libmidas_b200 on one CUDA device.
+
+    Each admitted stream gets its plan (map, dark), its own CUDA stream and
+    ``max_inflight`` slots of pinned host staging + device buffers sized for its batch
+    limit; a batch is H2D -> ``mi_integrate_batch`` -> ``mi_fit_batch`` -> D2H, all on the
+    stream's CUDA stream, and a slot is reused only after its event has fired.
+
+    ``plain=True`` serves the same requests with the reference's algorithm, one frame
+    per launch (``mi_integrate_plain`` and a one-frame fit per frame): the comparison
+    arm of the serving benchmark.
+    """
+
+    def __init__(self, device: int = 0, max_batch: int = 32, max_inflight: int = 2, plain: bool = False,
+                 pinned_bytes: int = 2 << 30):
+        import torch
+        self.torch = torch
+        self.device = torch.device("cuda", device)
+        self.max_batch = max_batch
+        self.max_inflight = max_inflight
+        self.plain = plain
+        self.pool = PinnedPool(pinned_bytes)
+        self.alg_bytes = 0          # map bytes per launch + frame bytes, summed over dispatches
+        self.launches = 0           # libmidas_b200 entry-point calls that launch kernels
+
+    def free_bytes(self) -> int:
+        free, _ = self.torch.cuda.mem_get_info(self.device)
+        return int(free)
+
+    def batch_limit(self, st) -> int:
+        return st["B"]
+
+    def open(self, cfg: StreamConfig):
+        torch = self.torch
+        from .kernels import CakePlan
+        fit = cfg.peaks is not None and len(cfg.peaks) > 0
+        if fit and (cfg.r_axis is None or len(cfg.r_axis) != cfg.n_r):
+            raise ValueError(f"stream {cfg.name!r}: fits need r_axis with n_r = {cfg.n_r} entries")
+        tdt = getattr(torch, cfg.frame_dtype)
+        B, nz, ny = cfg.max_batch or self.max_batch, cfg.n_pixels_z, cfg.n_pixels_y
+        ck_dt = torch.float64 if self.plain else torch.float32
+        tokens = []
+
+        def pinned(shape, dtype):
+            t, tok = self.pool.alloc(shape, dtype)
+            tokens.append(tok)
+            return t
+
+        try:
+            host = []
+            for _ in range(self.max_inflight):
+                h = {"h_frames": pinned((B, nz, ny), tdt), "h_aw": pinned((B, cfg.n_r), torch.float64),
+                     "h_sm": pinned((B, cfg.n_r), torch.float64)}
+                if cfg.want_cake:
+                    h["h_cake"] = pinned((B, cfg.n_r, cfg.n_eta), ck_dt)
+                if fit:
+                    h["h_fit"] = pinned((B, len(cfg.peaks), L.FIT_NOUT), torch.float64)
+                host.append(h)
+        except AdmissionError:
+            for tok in tokens:
+                self.pool.release(tok)
+            raise
+        plan = CakePlan(cfg.pixmap, n_r=cfg.n_r, n_eta=cfg.n_eta, n_pixels_y=cfg.n_pixels_y,
+                        n_pixels_z=cfg.n_pixels_z, mode=cfg.mode, bc_y=cfg.bc_y, bc_z=cfg.bc_z,
+                        device=self.device, tile_rows=cfg.tile_rows)
+        if cfg.dark is not None:
+            plan.set_dark(cfg.dark)
+        slots = []
+        for h in host:
+            s = dict(h)
+            s.update({
+                "d_frames": torch.empty((B, nz, ny), dtype=tdt, device=self.device),
+                "d_aw": torch.empty((B, cfg.n_r), dtype=torch.float64, device=self.device),
+                "d_sm": torch.empty((B, cfg.n_r), dtype=torch.float64, device=self.device),
+                "event": torch.cuda.Event(),
+            })
+            if cfg.want_cake or self.plain:
+                s["d_cake"] = torch.empty((B, cfg.n_r, cfg.n_eta), dtype=ck_dt, device=self.device)
+            if fit:
+                npk = len(cfg.peaks)
+                s["d_fit"] = torch.empty((B, npk, L.FIT_NOUT), dtype=torch.float64, device=self.device)
+                s["d_iters"] = torch.empty((B, npk), dtype=torch.int32, device=self.device)
+            slots.append(s)
+        st = {"plan": plan, "slots": slots, "free": list(range(self.max_inflight)), "B": B,
+              "stream": torch.cuda.Stream(self.device), "map_bytes": int(plan.info["map_bytes"]),
+              "frame_bytes": nz * ny * np.dtype(cfg.frame_dtype).itemsize, "tokens": tokens}
+        if fit:
+            st["x"] = torch.as_tensor(np.asarray(cfg.r_axis, np.float64), device=self.device)
+            st["peaks"] = torch.as_tensor(np.asarray(cfg.peaks, np.float64), device=self.device)
+            st["fit_opts"] = L.MiFitOpts(MODELS[cfg.fit_model], int(cfg.fit_half_window), 100,
+                                         float(cfg.x_bin), 0.0, 0.0)
+        fp = plan.info["device_bytes"]
+        for s in slots:
+            fp += sum(v.numel() * v.element_size() for k, v in s.items() if k.startswith("d_"))
+        return st, int(fp)
+
+    def footprint_estimate(self, cfg: StreamConfig) -> int:
+        """Upper estimate before building anything: map + staging + buffers."""
+        recs = cfg.pixmap.n_entries
+        B = cfg.max_batch or self.max_batch
+        item = np.dtype(cfg.frame_dtype).itemsize
+        ck = 8 if self.plain else (4 if cfg.want_cake else 0)
+        per_slot = B * (cfg.n_pixels_y * cfg.n_pixels_z * item + 16 * cfg.n_r + ck * cfg.n_r * cfg.n_eta)
+        plan = recs * 60 + 256 * cfg.n_r * 12 * 16 + cfg.n_pixels_y * cfg.n_pixels_z * 8
+        return int(plan + self.max_inflight * per_slot)
+
+    def can_dispatch(self, st) -> bool:
+        return bool(st["free"])
+
+    def _fit(self, st, cfg, s, first, n, strm):
+        L.check(L.lib().mi_fit_batch(st["x"].data_ptr(), s["d_aw"][first].data_ptr(), n, cfg.n_r,
+                                     st["peaks"].data_ptr(), st["peaks"].numel(), C.byref(st["fit_opts"]),
+                                     s["d_fit"][first].data_ptr(), s["d_iters"][first].data_ptr(),
+                                     L.stream_ptr(strm)), "mi_fit_batch")
+        self.launches += 1
+
+    def dispatch(self, st, cfg: StreamConfig, frames: List[np.ndarray]):
+        torch = self.torch
+        k = st["free"].pop()
+        s = st["slots"][k]
+        n = len(frames)
+        hf = s["h_frames"]
+        for i, f in enumerate(frames):
+            hf[i].numpy()[...] = f.reshape(cfg.n_pixels_z, cfg.n_pixels_y)
+        strm = st["stream"]
+        fit = "d_fit" in s
+        with torch.cuda.stream(strm):
+            s["d_frames"][:n].copy_(hf[:n], non_blocking=True)
+            if self.plain:
+                code = dtype_code(s["d_frames"].dtype)
+                for i in range(n):
+                    L.check(L.lib().mi_integrate_plain(st["plan"]._h, s["d_frames"][i].data_ptr(), code,
+                                                       s["d_cake"][i].data_ptr(), s["d_aw"][i].data_ptr(),
+                                                       s["d_sm"][i].data_ptr(), L.stream_ptr(strm)),
+                            "mi_integrate_plain")
+                    self.launches += 1
+                    if fit:
+                        self._fit(st, cfg, s, i, 1, strm)
+                self.alg_bytes += n * (st["map_bytes"] + st["frame_bytes"])
+            else:
+                out = {"lineout_aw": s["d_aw"][:n], "lineout_sm": s["d_sm"][:n]}
+                if cfg.want_cake:
+                    out["cake"] = s["d_cake"][:n]
+                st["plan"].integrate(s["d_frames"][:n], cake=cfg.want_cake, out=out, stream=strm)
+                self.launches += 1
+                self.alg_bytes += st["map_bytes"] + n * st["frame_bytes"]
+                if fit:
+                    self._fit(st, cfg, s, 0, n, strm)
+            if fit:
+                s["h_fit"][:n].copy_(s["d_fit"][:n], non_blocking=True)
+            s["h_aw"][:n].copy_(s["d_aw"][:n], non_blocking=True)
+            s["h_sm"][:n].copy_(s["d_sm"][:n], non_blocking=True)
+            if cfg.want_cake:
+                s["h_cake"][:n].copy_(s["d_cake"][:n], non_blocking=True)
+            s["event"].record(strm)
+        return (k, n)
+
+    def ready(self, st, handle) -> bool:
+        return st["slots"][handle[0]]["event"].query()
+
+    def collect(self, st, cfg: StreamConfig, handle):
+        k, n = handle
+        s = st["slots"][k]
+        res = []
+        for i in range(n):
+            res.append((s["h_aw"][i].numpy().copy(), s["h_sm"][i].numpy().copy(),
+                        s["h_fit"][i].numpy().copy() if "h_fit" in s else None,
+                        s["h_cake"][i].numpy().copy() if cfg.want_cake else None))
+        st["free"].append(k)
+        return res
+
+    def close(self, st):
+        st["stream"].synchronize()
+        st["plan"].close()
+        st["slots"].clear()
+        for tok in st["tokens"]:
+            self.pool.release(tok)
+
+
+class CakeServer:
+    """Continuous-batching scheduler over admitted detector streams.
+
+    Args:
+        backend: executes batches (default: DeviceBackend on cuda:0).
+        hbm_budget: bytes the admitted streams may hold on the device (default: 90 % of
+            the device memory free at construction).
+        tick_s: idle sleep between scheduling passes.
+    """
+
+    def __init__(self, backend=None, hbm_budget: Optional[int] = None, tick_s: float = 2e-4):
+        self.backend = backend or DeviceBackend()
+        self.budget = int(hbm_budget if hbm_budget is not None else 0.9 * self.backend.free_bytes())
+        self.used = 0
+        self.tick_s = tick_s
+        self.streams: Dict[int, _Stream] = {}
+        self._ids = itertools.count()
+        self._lock = threading.Lock()
+        self._wake = threading.Event()
+        self._thread: Optional[threading.Thread] = None
+        self._running = False
+        self.latencies: List[float] = []
+        self.completed = 0
+        self.batches = 0
+
+    # -- admission -----------------------------------------------------------
+    def admit(self, cfg: StreamConfig) -> int:
+        """Admit a stream if its footprint fits the remaining budget; AdmissionError otherwise."""
+        with self._lock:
+            est = self.backend.footprint_estimate(cfg)
+            if self.used + est > self.budget:
+                raise AdmissionError(f"stream {cfg.name!r} needs ~{est / 1e9:.2f} GB; "
+                                     f"{(self.budget - self.used) / 1e9:.2f} GB of the budget left")
+            self.used += est
+        try:
+            state, fp = self.backend.open(cfg)
+        except Exception:
+            with self._lock:
+                self.used -= est
+            raise
+        with self._lock:
+            self.used += fp - est
+            sid = next(self._ids)
+            self.streams[sid] = _Stream(sid, cfg, state, fp)
+        return sid
+
+    def remove(self, sid: int, *, drain: bool = True, timeout: float = 30.0) -> None:
+        """Stop a stream; with drain, its queued frames are processed first."""
+        with self._lock:
+            s = self.streams.get(sid)
+            if s is None:
+                return
+            s.closing = True
+            if not drain:
+                while s.pending:
+                    s.pending.popleft().fut.cancel()
+        t0 = time.time()
+        while True:
+            with self._lock:
+                busy = bool(s.pending or s.inflight)
+            if not busy or time.time() - t0 > timeout:
+                break
+            if self._running:
+                time.sleep(self.tick_s)
+            else:
+                self._pass()
+        with self._lock:
+            while s.pending:
+                s.pending.popleft().fut.cancel()
+            del self.streams[sid]
+            self.used -= s.footprint
+        self.backend.close(s.state)
+
+    # -- requests ---------------------------------------------------------------
+    def submit(self, sid: int, frame: np.ndarray, t_arrival: Optional[float] = None) -> Future:
+        fut: Future = Future()
+        with self._lock:
+            s = self.streams.get(sid)
+            if s is None or s.closing:
+                fut.set_exception(KeyError(f"stream {sid} is not admitted"))
+                return fut
+            cfg = s.cfg
+            if frame.size != cfg.n_pixels_y * cfg.n_pixels_z:
+                fut.set_exception(ValueError(f"frame has {frame.size} pixels, stream {cfg.name!r} expects "
+                                             f"{cfg.n_pixels_y * cfg.n_pixels_z}"))
+                return fut
+            now = time.perf_counter()
+            s.pending.append(_Req(next(s.seq), frame, t_arrival if t_arrival is not None else now, fut, now))
+        self._wake.set()
+        return fut
+
+    # -- scheduling ---------------------------------------------------------------
+    def _pass(self) -> bool:
+        """One scheduling pass: complete finished batches, dispatch pending frames."""
+        did = False
+        with self._lock:
+            streams = list(self.streams.values())
+        for s in streams:
+            while s.inflight and self.backend.ready(s.state, s.inflight[0][0]):
+                handle, reqs = s.inflight.popleft()
+                res = self.backend.collect(s.state, s.cfg, handle)
+                now = time.perf_counter()
+                for r, (aw, sm, fit, cake) in zip(reqs, res):
+                    lat = now - r.t_arrival
+                    self.latencies.append(lat)
+                    r.fut.set_result(FrameResult(s.cfg.name, r.seq, aw, sm, fit, cake, lat, len(reqs),
+                                                 r.t_arrival, r.t_submit, r.t_dispatch, now))
+                self.completed += len(reqs)
+                did = True
+            while s.pending and self.backend.can_dispatch(s.state):
+                with self._lock:
+                    n = min(len(s.pending), self.backend.batch_limit(s.state))
+                    reqs = [s.pending.popleft() for _ in range(n)]
+                t_disp = time.perf_counter()
+                for r in reqs:
+                    r.t_dispatch = t_disp
+                handle = self.backend.dispatch(s.state, s.cfg, [r.frame for r in reqs])
+                s.inflight.append((handle, reqs))
+                self.batches += 1
+                did = True
+        return did
+
+    def _loop(self):
+        while self._running:
+            if not self._pass():
+                self._wake.wait(self.tick_s)
+                self._wake.clear()
+
+    def start(self) -> "CakeServer":
+        if not self._running:
+            self._running = True
+            self._thread = threading.Thread(target=self._loop, name="cake-server", daemon=True)
+            self._thread.start()
+        return self
+
+    def stop(self, *, drain: bool = True, timeout: float = 30.0) -> None:
+        if drain:
+            t0 = time.time()
+            while time.time() - t0 < timeout:
+                with self._lock:
+                    busy = any(s.pending or s.inflight for s in self.streams.values())
+                if not busy:
+                    break
+                time.sleep(self.tick_s)
+        self._running = False
+        self._wake.set()
+        if self._thread:
+            self._thread.join(timeout)
+        for sid in list(self.streams):
+            self.remove(sid, drain=False)
+
+    def __enter__(self):
+        return self.start()
+
+    def __exit__(self, *exc):
+        self.stop()
+
+    def latency_ms(self) -> Dict[str, float]:
+        if not self.latencies:
+            return {"p50": float("nan"), "p99": float("nan"), "n": 0}
+        a = np.sort(np.asarray(self.latencies)) * 1e3
+        return {"p50": float(np.percentile(a, 50)), "p99": float(np.percentile(a, 99)),
+                "max": float(a[-1]), "n": int(a.size)}

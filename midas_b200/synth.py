@@ -11,6 +11,12 @@ the host.
                    Gaussian spots per frame, RBin 0.25 px, eta 1 deg (3960x360 bins),
                    gradient mode, solid-angle + polarisation (0.99) + parallax in the map
   sweep_2880_small the same model scaled down (for tests)
+  pilatus_1679     1475x1679 int32, 172 um pixels, module gaps masked (serving mix)
+  detector_1024    1024x1024 u16 panels (serving mix)
+  powder_2048_fine 2048x2048 u16, RBin 0.5 px, eta 2 deg, gradient (serving mix)
+
+``serving_mix`` lists the six concurrent streams of the serving load with their
+Poisson frame rates; ``serving_stream`` turns a workload into a server stream.
 """
 from __future__ import annotations
 
@@ -62,6 +68,8 @@ class Workload:
     lattice_A: float = 5.4116
     n_frames: int = 10
     tile_rows: int = 0
+    frame_dtype: str = "uint16"    # raw frame type: "uint16" or "int32"
+    module_gaps: Optional[tuple] = None   # (module_y, gap_y, module_z, gap_z) px, masked in the map
 
     @property
     def n_r(self) -> int:
@@ -74,6 +82,16 @@ class Workload:
     @property
     def shape(self):
         return self.mapper.NrPixelsZ, self.mapper.NrPixelsY
+
+    def mask(self) -> Optional[np.ndarray]:
+        """(NZ, NY) uint8 mask (1 = excluded) of the inter-module gaps, or None."""
+        if self.module_gaps is None:
+            return None
+        my, gy, mz, gz = self.module_gaps
+        nz, ny = self.shape
+        y = np.arange(ny) % (my + gy) >= my
+        z = np.arange(nz) % (mz + gz) >= mz
+        return (z[:, None] | y[None, :]).astype(np.uint8)
 
     def ring_radii(self) -> np.ndarray:
         return ring_radii_px(self.lattice_A, self.wavelength_A, self.mapper.Lsd, self.mapper.px)
@@ -141,14 +159,102 @@ def sweep_2880() -> Workload:
                     n_spots=50, n_frames=1440, tile_rows=16)
 
 
+def pilatus_1679() -> Workload:
+    """PILATUS-2M-like panel: 1475x1679 int32, 172 um pixels, 3x8 modules of 487x195 px
+    with 7 px (y) and 17 px (z) gaps masked in the map; RBin 1 px, eta 5 deg, floor."""
+    m = MapperParams(NrPixelsY=1475, NrPixelsZ=1679, px=172.0, Lsd=8.0e5, BC_y=737.6,
+                     BC_z=841.2, ty=0.2, tz=0.1, RMin=10.0, RMax=800.0, RBinSize=1.0,
+                     EtaMin=-180.0, EtaMax=180.0, EtaBinSize=5.0)
+    return Workload("pilatus_1475x1679_i32_790x72_floor", m, "floor", frame_dtype="int32",
+                    module_gaps=(487, 7, 195, 17), tile_rows=8)
+
+
+def detector_1024(variant: int = 0) -> Workload:
+    """1024x1024 u16 panels of the serving mix: variant 0 = RBin 1 px, eta 8 deg (495x45 bins,
+    floor); variant 1 = tilted, RBin 0.5 px, eta 5 deg (990x72 bins, bilinear)."""
+    if variant == 0:
+        m = MapperParams(NrPixelsY=1024, NrPixelsZ=1024, px=400.0, Lsd=1.0e6, BC_y=512.4,
+                         BC_z=511.8, RMin=5.0, RMax=500.0, RBinSize=1.0, EtaMin=-180.0,
+                         EtaMax=180.0, EtaBinSize=8.0)
+        return Workload("detector_1024_u16_495x45_floor", m, "floor", tile_rows=8)
+    m = MapperParams(NrPixelsY=1024, NrPixelsZ=1024, px=400.0, Lsd=1.1e6, BC_y=530.1,
+                     BC_z=498.3, ty=0.4, tz=-0.3, RMin=5.0, RMax=500.0, RBinSize=0.5,
+                     EtaMin=-180.0, EtaMax=180.0, EtaBinSize=5.0)
+    return Workload("detector_1024_u16_990x72_bilinear", m, "bilinear", seed=77, tile_rows=8)
+
+
+def powder_2048_fine() -> Workload:
+    """2048x2048 u16, shifted centre and tilts, RBin 0.5 px, eta 2 deg (1980x180 bins), gradient."""
+    m = MapperParams(NrPixelsY=2048, NrPixelsZ=2048, px=200.0, Lsd=1.05e6, BC_y=1010.7,
+                     BC_z=1040.2, ty=-0.3, tz=0.25, RMin=10.0, RMax=1000.0, RBinSize=0.5,
+                     EtaMin=-180.0, EtaMax=180.0, EtaBinSize=2.0)
+    return Workload("powder_2048x2048_u16_1980x180_gradient", m, "gradient", seed=91, tile_rows=16)
+
+
+def serving_mix() -> List[tuple]:
+    """The six concurrent streams of the serving load, as (workload, Poisson rate in Hz):
+    frame sizes 1024^2, 2048^2, 2880^2 and 1475x1679, 2.2e4 to 1.43e6 bins, 10-500 Hz."""
+    return [(sweep_2880(), 10.0), (powder_2048(), 100.0), (powder_2048_fine(), 50.0),
+            (pilatus_1679(), 200.0), (detector_1024(0), 500.0), (detector_1024(1), 200.0)]
+
+
+def late_stream() -> tuple:
+    """The stream with a fresh map admitted while the serving load runs."""
+    m = MapperParams(NrPixelsY=2048, NrPixelsZ=2048, px=200.0, Lsd=0.95e6, BC_y=1030.9,
+                     BC_z=1019.4, ty=0.15, tz=0.2, RMin=10.0, RMax=1000.0, RBinSize=1.0,
+                     EtaMin=-180.0, EtaMax=180.0, EtaBinSize=5.0)
+    return Workload("powder_2048x2048_u16_990x72_floor_late", m, "floor", seed=5, tile_rows=8), 30.0
+
+
 def scaled(w: Workload, factor: int, name: Optional[str] = None) -> Workload:
     """The same workload on a detector `factor` times smaller in each direction."""
     m = w.mapper
     m2 = replace(m, NrPixelsY=m.NrPixelsY // factor, NrPixelsZ=m.NrPixelsZ // factor,
                  BC_y=m.BC_y / factor, BC_z=m.BC_z / factor, px=m.px * factor,
                  RMin=m.RMin / factor, RMax=m.RMax / factor)
+    gaps = None
+    if w.module_gaps is not None:
+        my, gy, mz, gz = w.module_gaps
+        gaps = (max(1, my // factor), max(1, gy // factor), max(1, mz // factor), max(1, gz // factor))
     return replace(w, name=name or f"{w.name}_div{factor}", mapper=m2,
-                   fwhm_px=max(w.fwhm_px, 1.2), n_spots=min(w.n_spots, 8))
+                   fwhm_px=max(w.fwhm_px, 1.2), n_spots=min(w.n_spots, 8), module_gaps=gaps)
 
 
-WORKLOADS = {"powder_2048": powder_2048, "sweep_2880": sweep_2880}
+def ring_peaks(w: Workload, half_window: int = 15) -> np.ndarray:
+    """Ring radii (px) whose +-half_window-bin fit window lies inside the R range."""
+    m = w.mapper
+    rr = w.ring_radii()
+    lo, hi = m.RMin + (half_window + 1) * m.RBinSize, m.RMax - (half_window + 1) * m.RBinSize
+    return rr[(rr > lo) & (rr < hi)]
+
+
+def r_centres(w: Workload) -> np.ndarray:
+    m = w.mapper
+    return m.RMin + m.RBinSize * (np.arange(m.n_r, dtype=np.float64) + 0.5)
+
+
+def serving_stream(w: Workload, *, device: int = 0, fit: bool = True, want_cake: bool = False,
+                   half_window: int = 15):
+    """StreamConfig of a workload for ``server.CakeServer``: map built on the device, the
+    workload's dark, fits of its rings on the area-weighted lineout."""
+    from .mapper import build_map
+    from .server import StreamConfig
+    pm, _ = build_map(w.mapper, device=device, mask=w.mask())
+    dark = w.dark(device=torch.device("cuda", device)).cpu().numpy()
+    m = w.mapper
+    peaks = ring_peaks(w, half_window) if fit else None
+    return StreamConfig(name=w.name, pixmap=pm, n_r=w.n_r, n_eta=w.n_eta, n_pixels_y=m.NrPixelsY,
+                        n_pixels_z=m.NrPixelsZ, mode=w.mode, bc_y=m.BC_y, bc_z=m.BC_z, dark=dark,
+                        frame_dtype=w.frame_dtype, r_axis=r_centres(w) if fit else None, peaks=peaks,
+                        fit_half_window=half_window, x_bin=m.RBinSize, want_cake=want_cake,
+                        tile_rows=w.tile_rows)
+
+
+def host_frames(w: Workload, first: int, n: int, device: int = 0) -> np.ndarray:
+    """Frames first..first+n-1 generated on the device and copied to host memory."""
+    dt = {"uint16": torch.uint16, "int32": torch.int32}[w.frame_dtype]
+    return w.frames(first, n, device=torch.device("cuda", device), dtype=dt).cpu().numpy()
+
+
+WORKLOADS = {"powder_2048": powder_2048, "sweep_2880": sweep_2880, "pilatus_1679": pilatus_1679,
+             "detector_1024": detector_1024, "powder_2048_fine": powder_2048_fine}
