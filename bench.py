@@ -192,9 +192,10 @@ def _rel(got, ref):
     return np.abs(got - ref) / np.maximum(np.abs(ref), tau)
 
 
-def accuracy_check(pm, w, frame, dark, got, ref_out, kind):
+def accuracy_check(pm, w, frame, dark, got, ref_out, kind, got_ic=None):
     """Frame 0 of the batched path against the FP64 oracle and, when the reference integrator
-    ran, against its own output (sums / norms of integration_apply_map)."""
+    ran, the same frame through a plan with IntegrationCore semantics against that
+    integrator's own output (sums / norms of integration_apply_map)."""
     import numpy as np
     import oracle
     ny, nz = w.mapper.NrPixelsY, w.mapper.NrPixelsZ
@@ -207,12 +208,14 @@ def accuracy_check(pm, w, frame, dark, got, ref_out, kind):
     acc = {"cake_max_rel": float(r.max()), "cake_mean_rel": float(r.mean()), "lineout_max_rel": float(ra.max()),
            "frames_checked": 1}
     ic = None
-    if kind == "reference" and w.mode in ("floor", "gradient"):
+    if kind == "reference" and w.mode in ("bilinear", "gradient") and got_ic is not None:
         sums, norms = ref_out
-        ic_cake = np.where(norms > 0, sums / np.where(norms > 0, norms, 1.0), 0.0)
-        ri = _rel(got[0], ic_cake)
+        ic_cake = np.where(norms > 1e-9, sums / np.where(norms > 1e-9, norms, 1.0), 0.0)
+        ri, rp = _rel(got_ic, ic_cake), _rel(got[0], ic_cake)
         ic = {"cake_max_rel": float(ri.max()), "cake_mean_rel": float(ri.mean()), "frames_checked": 1,
-              "integrator": "integration_apply_map (IntegrationCore.c), sums / norms"}
+              "semantics": "ic (plan built with IntegrationCore's rounding and normaliser)",
+              "integrator": "integration_apply_map (IntegrationCore.c) compiled from the reference, sums / norms",
+              "py_semantics_cake_max_rel": float(rp.max())}
     return acc, ic
 
 
@@ -374,7 +377,17 @@ def main_ours(args):
         out["cpu_baseline"] = {"value": round(fps, 3), "unit": UNIT, "cores": cores, "kind": kind,
                                "sample": sample}
         if not args.no_check:
-            out["accuracy_vs_fp64_oracle"], ic = accuracy_check(pm, w, frame0, dark_np, got0, ref_out, kind)
+            got_ic = None
+            if kind == "reference" and w.mode in ("bilinear", "gradient"):
+                plan_ic = CakePlan(pm, n_r=w.n_r, n_eta=w.n_eta, n_pixels_y=ny, n_pixels_z=nz, mode=w.mode,
+                                   semantics="ic", bc_y=w.mapper.BC_y, bc_z=w.mapper.BC_z, device=dev,
+                                   tile_rows=args.tile_rows or w.tile_rows)
+                plan_ic.set_dark(dark_np)
+                c_ic, _, _ = plan_ic.integrate(torch.from_numpy(frame0[None]).to(dev), lineouts=False)
+                got_ic = c_ic[0].reshape(-1).cpu().numpy().astype(np.float64)
+                plan_ic.close()
+            out["accuracy_vs_fp64_oracle"], ic = accuracy_check(pm, w, frame0, dark_np, got0, ref_out, kind,
+                                                                got_ic)
             if ic:
                 out["accuracy_vs_reference_integrator"] = ic
             if served:

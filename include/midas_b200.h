@@ -52,12 +52,19 @@ extern "C" {
 #define MI_MODE_BILINEAR 1   /* bilinear sample at (y,z), 4 corner terms, coalesced      */
 #define MI_MODE_GRADIENT 2   /* bilinear at (y,z) shifted by -deltaR along the radius    */
 
-/* ---- normalisation semantics (the reference has two) ----- */
+/* ---- semantics: the reference's three integrators differ in rounding and normaliser -- */
 #define MI_SEM_PY 0          /* midas_integrate kernels.py: normaliser = sum of in-bounds
                                 areaWeight; invalid bins -> 0 when normalising, raw sum
                                 otherwise (kernels.py:311-318, 461-471)                  */
 #define MI_SEM_GPUSTREAM 1   /* IntegratorFitPeaksGPUStream.cu:1038-1049: normaliser = sum
                                 of ALL areaWeight of the bin; bins with area <= 1e-9 -> 0 */
+#define MI_SEM_IC 2          /* IntegrationCore.c:integration_apply_map (:14-82), the CPU
+                                integrator: bilinear at (y,z) (gradient: shifted by
+                                -deltaR*d/R in FP64 when deltaR != 0 and R > 1), base pixel
+                                = floorf() of the position rounded to float, clamp under
+                                then over; normaliser = sum of ALL areaWeight (<= 1e-9 ->
+                                0). It has no floor mode: MI_MODE_FLOOR is rejected, and
+                                mi_integrate_plain does not take this semantics.          */
 
 /* ---- frame dtype codes: the socket protocol's codes (MI/image.py:24-30) -- */
 #define MI_DT_U8 0

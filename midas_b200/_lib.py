@@ -23,7 +23,7 @@ MI_E_UNSUPPORTED = -6
 MI_E_RANGE = -7
 
 MODE = {"floor": 0, "bilinear": 1, "gradient": 2}
-SEM = {"py": 0, "gpustream": 1}
+SEM = {"py": 0, "gpustream": 1, "ic": 2}
 DT_U8, DT_U16, DT_U32, DT_I64, DT_F32, DT_F64, DT_I32 = 0, 1, 2, 3, 4, 5, 7
 FIT_PV, FIT_TCH = 0, 1
 FIT_NOUT = 11

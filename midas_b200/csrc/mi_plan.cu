@@ -81,6 +81,24 @@ static inline void add_bilinear(double sy, double sz, double frac, int ny, int n
   t.push_back({(int32_t)(base + ny + 1), fy * fz * frac});
 }
 
+// integration_apply_map (IntegrationCore.c:52-63): the base pixel is floorf() of the FP64
+// position (rounded to float on the way in), the fractions are taken from the FP64
+// position, and the clamps run under-then-over
+static inline void add_bilinear_ic(double sy, double sz, double frac, int ny, int nz,
+                                   std::vector<Term> &t) {
+  int iy = (int)floorf((float)sy), iz = (int)floorf((float)sz);
+  double fy = sy - iy, fz = sz - iz;
+  if (iy < 0) { iy = 0; fy = 0; }
+  if (iy >= ny - 1) { iy = ny - 2; fy = 1; }
+  if (iz < 0) { iz = 0; fz = 0; }
+  if (iz >= nz - 1) { iz = nz - 2; fz = 1; }
+  const int64_t base = (int64_t)iz * ny + iy;
+  t.push_back({(int32_t)base, (1 - fy) * (1 - fz) * frac});
+  t.push_back({(int32_t)(base + 1), fy * (1 - fz) * frac});
+  t.push_back({(int32_t)(base + ny), (1 - fy) * fz * frac});
+  t.push_back({(int32_t)(base + ny + 1), fy * fz * frac});
+}
+
 static void bin_terms(const mi_map_desc &m, int64_t b, int mode, int sem,
                       std::vector<Term> &t, double *area_in, double *area_all,
                       int64_t *oob) {
@@ -108,6 +126,18 @@ static void bin_terms(const mi_map_desc &m, int64_t b, int mode, int sem,
       } else if (inb) {
         t.push_back({(int32_t)(tz * ny + ty), r.frac});
       }
+    } else if (sem == MI_SEM_IC) {
+      // IntegrationCore.c:38-50: FP64 shift, only for records with deltaR != 0 and R > 1
+      double sy = y, sz = z;
+      if (mode == MI_MODE_GRADIENT && r.deltaR != 0.0f) {
+        const double dy = y - m.bc_y, dz = z - m.bc_z;
+        const double R = std::sqrt(dy * dy + dz * dz);
+        if (R > 1.0) {
+          sy -= r.deltaR * dy / R;
+          sz -= r.deltaR * dz / R;
+        }
+      }
+      add_bilinear_ic(sy, sz, r.frac, ny, nz, t);
     } else {
       double sy = y, sz = z;
       if (mode == MI_MODE_GRADIENT) {
@@ -210,7 +240,7 @@ int build_host_csr(const mi_map_desc &m, int mode, int sem, HostCSR *out) {
     }
   }
   for (int64_t b = 0; b < n_bins; ++b)
-    out->area_norm[b] = (sem == MI_SEM_GPUSTREAM) ? area_all[b] : out->area_in[b];
+    out->area_norm[b] = (sem == MI_SEM_PY) ? out->area_in[b] : area_all[b];
   out->oob = oob_total;
   return MI_OK;
 }
@@ -301,7 +331,7 @@ static int tile_item(const Builder &B, int r0, int nrows, int e_begin, int e_end
 static inline void bin_scale(const HostCSR &csr, const Plan *p, int64_t b, float *scale, float *lw) {
   const double an = csr.area_norm[b], ai = csr.area_in[b];
   double sc;
-  if (p->semantics == MI_SEM_GPUSTREAM)
+  if (p->semantics != MI_SEM_PY)
     sc = an > kAreaThreshold ? (p->normalize ? 1.0 / an : 1.0) : 0.0;
   else
     sc = p->normalize ? (ai > kAreaThreshold ? 1.0 / ai : 0.0) : 1.0;
@@ -760,8 +790,11 @@ int mi_plan_create(const mi_map_desc *map, const mi_plan_opts *opts, int device,
   if (opts) o = *opts;
   else { o.mode = MI_MODE_FLOOR; o.normalize = 1; o.semantics = MI_SEM_PY; }
   if (o.mode < 0 || o.mode > 2) return set_error(MI_E_ARG, "mi_plan_create: unknown mode %d", o.mode);
-  if (o.semantics < 0 || o.semantics > 1)
+  if (o.semantics < 0 || o.semantics > 2)
     return set_error(MI_E_ARG, "mi_plan_create: unknown semantics %d", o.semantics);
+  if (o.semantics == MI_SEM_IC && o.mode == MI_MODE_FLOOR)
+    return set_error(MI_E_ARG, "mi_plan_create: IntegrationCore semantics has no floor mode "
+                               "(integration_apply_map always interpolates)");
   int ndev = 0;
   if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
     return set_error(MI_E_CUDA, "mi_plan_create: no CUDA device available");
@@ -871,6 +904,9 @@ int mi_integrate_plain(mi_plan *p, const void *frame, int dtype, double *cake, d
                        double *lo_sm, void *stream) {
   if (!p || !frame) return set_error(MI_E_ARG, "mi_integrate_plain: null argument");
   if (dtype_size(dtype) == 0) return set_error(MI_E_ARG, "mi_integrate_plain: unknown dtype code %d", dtype);
+  if (p->semantics == MI_SEM_IC)
+    return set_error(MI_E_UNSUPPORTED, "mi_integrate_plain: the one-frame GPU kernel follows the GPU stream "
+                                       "or midas_integrate semantics, not IntegrationCore's");
   int prev = 0;
   cudaGetDevice(&prev);
   if (prev != p->device) MI_CUDA(cudaSetDevice(p->device));

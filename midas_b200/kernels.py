@@ -55,8 +55,9 @@ class CakePlan:
         n_pixels_y, n_pixels_z: detector shape; flat pixel = z * NY + y.
         mode: 'floor' | 'bilinear' | 'gradient'.
         normalize: divide by the bin area (Normalize key).
-        semantics: 'py' (midas_integrate kernels.py) or 'gpustream'
-            (IntegratorFitPeaksGPUStream normaliser and fp32 resampling).
+        semantics: 'py' (midas_integrate kernels.py), 'gpustream'
+            (IntegratorFitPeaksGPUStream normaliser and fp32 resampling) or 'ic'
+            (IntegrationCore.c integration_apply_map: bilinear/gradient only).
         bc_y, bc_z: beam centre (px), used by gradient mode.
         device: CUDA device.
         tile_rows, tile_pixels, frames_per_lane: tiling knobs (0 = default).

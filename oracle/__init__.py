@@ -25,7 +25,7 @@ REF_LIB = HERE / "_ref" / "libmidas_ref.so"
 REC_DTYPE = np.dtype([("y", "<f4"), ("z", "<f4"), ("frac", "<f8"), ("deltaR", "<f4"),
                       ("areaWeight", "<f4")])
 MODES = {"floor": 0, "bilinear": 1, "gradient": 2}
-SEMS = {"py": 0, "gpustream": 1}
+SEMS = {"py": 0, "gpustream": 1, "ic": 2}
 
 _lib = None
 _ref = None

@@ -11,6 +11,10 @@
  *   1: integrate_noMapMask of FF_HEDM/src/IntegratorFitPeaksGPUStream.cu:975-1050
  *      (floor offset (long long)z*NY + y evaluated in float, :915; fp32 gradient shift,
  *      :1007-1018; normaliser = sum of all areaWeight, :1034-1040) with FP64 sums.
+ *   2: integration_apply_map of FF_HEDM/src/IntegrationCore.c:14-82 (bilinear at the
+ *      record's position, gradient shift in FP64 only when deltaR != 0 and R > 1, base
+ *      pixel from floorf() of the float-rounded position, clamps under-then-over;
+ *      normaliser = sum of all areaWeight); no floor mode.
  * or_profile follows profile_1d (kernels.py:567-601) = calculate_1D_profile_kernel and
  * calculate_1D_profile_simple_mean_kernel (IntegratorFitPeaksGPUStream.cu:1162-1334).
  * or_fit is the FP64 twin of the device Levenberg-Marquardt fitter (same window, same
@@ -23,6 +27,18 @@
 #include <string.h>
 
 #define AREA_THRESHOLD 1e-9
+
+/* integration_apply_map, FF_HEDM/src/IntegrationCore.c:52-69 */
+static double bilinear_ic(const double *img, int ny, int nz, double sy, double sz) {
+  int iy = (int)floorf((float)sy), iz = (int)floorf((float)sz);
+  double fy = sy - iy, fz = sz - iz;
+  if (iy < 0) { iy = 0; fy = 0; }
+  if (iy >= ny - 1) { iy = ny - 2; fy = 1; }
+  if (iz < 0) { iz = 0; fz = 0; }
+  if (iz >= nz - 1) { iz = nz - 2; fz = 1; }
+  const double *p = img + (long)iz * ny + iy;
+  return p[0] * ((1 - fy) * (1 - fz)) + p[1] * (fy * (1 - fz)) + p[ny] * ((1 - fy) * fz) + p[ny + 1] * (fy * fz);
+}
 
 static double bilinear(const double *img, int ny, int nz, double sy, double sz) {
   double fiy = floor(sy), fiz = floor(sz);
@@ -52,6 +68,7 @@ void or_area_in(const or_record *rec, const int32_t *nmap, int64_t n_bins, int n
 int or_integrate(const or_record *rec, const int32_t *nmap, int64_t n_bins, int ny, int nz, double bc_y,
                  double bc_z, const double *image, int mode, int sem, int normalize, double *cake, double *area_out) {
   const long npix = (long)ny * nz;
+  if (sem == 2 && mode == 0) return -3; /* IntegrationCore has no floor mode */
   for (int64_t b = 0; b < n_bins; ++b) {
     double I = 0.0, A_in = 0.0, A_all = 0.0;
     const int cnt = nmap[2 * b], off = nmap[2 * b + 1];
@@ -72,6 +89,18 @@ int or_integrate(const or_record *rec, const int32_t *nmap, int64_t n_bins, int 
         } else if (inb) {
           I += image[tz * ny + ty] * e->frac;
         }
+      } else if (sem == 2) {
+        /* IntegrationCore.c:38-50 */
+        double sy = y, sz = z;
+        if (mode == 2 && e->deltaR != 0.0f) {
+          double dy = y - bc_y, dz = z - bc_z;
+          double R = sqrt(dy * dy + dz * dz);
+          if (R > 1.0) {
+            sy -= e->deltaR * dy / R;
+            sz -= e->deltaR * dz / R;
+          }
+        }
+        I += bilinear_ic(image, ny, nz, sy, sz) * e->frac;
       } else {
         double sy = y, sz = z;
         if (mode == 2) {
@@ -97,7 +126,7 @@ int or_integrate(const or_record *rec, const int32_t *nmap, int64_t n_bins, int 
       }
     }
     double out;
-    if (sem == 1) {
+    if (sem == 1 || sem == 2) {
       out = A_all > AREA_THRESHOLD ? (normalize ? I / A_all : I) : 0.0;
       if (area_out) area_out[b] = A_all;
     } else {

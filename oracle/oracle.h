@@ -20,7 +20,7 @@ typedef struct {
   float deltaR, areaWeight;
 } or_record;
 
-/* semantics: 0 = midas_integrate kernels.py, 1 = IntegratorFitPeaksGPUStream.cu
+/* semantics: 0 = midas_integrate kernels.py, 1 = IntegratorFitPeaksGPUStream.cu, 2 = IntegrationCore.c
  * mode: 0 floor, 1 bilinear, 2 gradient
  * image: dark-subtracted frame, double, nz*ny (flat index z*ny + y)
  * cake_out: n_bins, area_out (may be NULL): normaliser per bin */

@@ -43,11 +43,16 @@ def _oracle_batch(g, frames, mode, norm, sem, records=None, nmap=None):
 @pytest.mark.parametrize("tag", KERNEL_CASES)
 @pytest.mark.parametrize("mode", ["floor", "bilinear", "gradient"])
 @pytest.mark.parametrize("norm", [True, False])
-@pytest.mark.parametrize("sem", ["py", "gpustream"])
+@pytest.mark.parametrize("sem", ["py", "gpustream", "ic"])
 @pytest.mark.parametrize("enc", ["runs", "csr"])
 def test_batched_matches_oracle(cuda, tag, mode, norm, sem, enc):
     g = load_kernels_case(tag)
     pm = from_arrays(g["records"], g["nmap"])
+    if sem == "ic" and mode == "floor":
+        with pytest.raises(L.MidasError, match="no floor mode"):
+            CakePlan(pm, n_r=g["n_r"], n_eta=g["n_eta"], n_pixels_y=g["ny"], n_pixels_z=g["nz"], mode=mode,
+                     semantics=sem, device=cuda)
+        return
     plan = CakePlan(pm, n_r=g["n_r"], n_eta=g["n_eta"], n_pixels_y=g["ny"], n_pixels_z=g["nz"], mode=mode,
                     normalize=norm, semantics=sem, bc_y=g["bc_y"], bc_z=g["bc_z"], device=cuda, encoding=enc)
     frames = _frames_like(g["image"], 7, seed=1)
@@ -112,6 +117,32 @@ def test_detector_maps_u16_with_dark(cuda, tag, mode, enc, fpl, rl, rows):
     assert rel_err(ck.cpu().numpy(), rc)[0] <= TOL
     assert rel_err(aw.cpu().numpy(), raw_)[0] <= TOL
     assert rel_err(sm.cpu().numpy(), rsm)[0] <= TOL
+
+
+@pytest.mark.skipif(not oracle.ref_available(), reason="reference integrator not compiled")
+def test_ic_semantics_matches_reference_integrator_at_detector_scale(cuda):
+    """The batched path with IntegrationCore semantics against integration_apply_map itself
+    (compiled from the reference sources), on a 1440x1440 u16 detector with a dark,
+    gradient mode: cake within 1e-6 relative of the reference's own integrator."""
+    from midas_b200 import synth
+    from midas_b200.mapper import build_map
+    w = synth.scaled(synth.sweep_2880(), 2)
+    m = w.mapper
+    pm, _ = build_map(m, device=0)
+    plan = CakePlan(pm, n_r=w.n_r, n_eta=w.n_eta, n_pixels_y=m.NrPixelsY, n_pixels_z=m.NrPixelsZ,
+                    mode="gradient", semantics="ic", bc_y=m.BC_y, bc_z=m.BC_z, device=cuda)
+    dark = w.dark().cpu().numpy()
+    plan.set_dark(dark)
+    frames = w.frames(0, 3)
+    ck, _, _ = plan.integrate(frames)
+    ck = ck.cpu().numpy()
+    for f in range(3):
+        sums, norms = oracle.ref_integrate(pm.pxList, pm.nmap_pairs(), w.n_r, w.n_eta,
+                                           frames[f].cpu().numpy().astype(np.float64), m.NrPixelsY, m.NrPixelsZ,
+                                           dark=dark.astype(np.float64), bc_y=m.BC_y, bc_z=m.BC_z, gradient=1,
+                                           n_threads=8)
+        ref = np.where(norms > 1e-9, sums / np.where(norms > 1e-9, norms, 1.0), 0.0)
+        assert rel_err(ck[f].reshape(-1), ref)[0] <= TOL
 
 
 def test_frame_result_independent_of_batch(cuda):

@@ -63,3 +63,41 @@ def test_reference_integrator_reproduces_fixture(tag):
     sums, norms = oracle.ref_integrate(g["records"], g["nmap"], n_r, n_eta, g["image"], g["ny"], g["nz"],
                                        dark=g["dark"], bc_y=g["bc_y"], bc_z=g["bc_z"], gradient=1, n_threads=2)
     np.testing.assert_allclose(sums, g["ic_sums_gradient"], rtol=1e-12, atol=1e-12)
+
+
+@pytest.mark.parametrize("tag", MAPPER_CASES)
+@pytest.mark.parametrize("mode", ["bilinear", "gradient"])
+def test_oracle_ic_semantics_reproduces_integration_core(tag, mode):
+    """Semantics 'ic' restates integration_apply_map itself (float-rounded floorf base
+    pixel included): the fixture's IntegrationCore sums and norms to 1e-12."""
+    g = load_mapper_case(tag)
+    nb = g["nmap"].shape[0]
+    ck, area = oracle.integrate(g["records"], g["nmap"], nb, g["ny"], g["nz"], g["image"] - g["dark"],
+                                mode=mode, semantics="ic", normalize=False, bc_y=g["bc_y"], bc_z=g["bc_z"])
+    np.testing.assert_allclose(ck, g[f"ic_sums_{mode}"], rtol=1e-12, atol=1e-9)
+    np.testing.assert_allclose(area, g[f"ic_norms_{mode}"], rtol=1e-12, atol=1e-12)
+
+
+@pytest.mark.skipif(not oracle.ref_available(), reason="reference C sources not compiled here")
+def test_oracle_ic_semantics_matches_integration_core_at_detector_scale():
+    """On a 1440x1440 detector positions reach ~1440 px, where a float holds them to
+    ~1e-4 px: IntegrationCore's floorf() then picks the upper pixel for positions just
+    below an integer and extrapolates, moving some bins by ~1e-5 relative from the
+    midas_integrate result.  Semantics 'ic' reproduces that; 'py' does not."""
+    from midas_b200 import synth
+    from midas_b200.mapper import build_map
+    w = synth.scaled(synth.sweep_2880(), 2)
+    pm, _ = build_map(w.mapper, device=-1)
+    ny, nz = w.mapper.NrPixelsY, w.mapper.NrPixelsZ
+    rng = np.random.default_rng(5)
+    img = rng.poisson(300.0, size=(nz, ny)).astype(np.float64)
+    dark = np.round(100 + 5 * rng.standard_normal((nz, ny)), 3)
+    sums, norms = oracle.ref_integrate(pm.pxList, pm.nmap_pairs(), w.n_r, w.n_eta, img, ny, nz, dark=dark,
+                                       bc_y=w.mapper.BC_y, bc_z=w.mapper.BC_z, gradient=1, n_threads=8)
+    ck, area = oracle.integrate(pm.pxList, pm.nmap_pairs(), pm.n_bins, ny, nz, img - dark, mode="gradient",
+                                semantics="ic", normalize=False, bc_y=w.mapper.BC_y, bc_z=w.mapper.BC_z)
+    np.testing.assert_allclose(ck, sums, rtol=1e-10, atol=1e-8)
+    np.testing.assert_allclose(area, norms, rtol=1e-12, atol=1e-12)
+    py, _ = oracle.integrate(pm.pxList, pm.nmap_pairs(), pm.n_bins, ny, nz, img - dark, mode="gradient",
+                             semantics="py", normalize=False, bc_y=w.mapper.BC_y, bc_z=w.mapper.BC_z)
+    assert np.max(np.abs(py - sums) / np.maximum(np.abs(sums), 1.0)) > 1e-7
