@@ -308,7 +308,13 @@ def main_ours(args):
     elapsed_ms = dist_max(e0.elapsed_time(e1), world)
     step_ms = [a.elapsed_time(b) for a, b in ev]
     value = world * args.steps * F / (elapsed_ms / 1e3)
-    launches = args.steps * 2 * math.ceil(F / 256)   # k_cake + k_lineout per launch group
+    # kernels per step: per 256-frame launch group one k_lineout, plus either one caking
+    # kernel or (pixel-major staging) k_xc + k_runs per 128 frames
+    groups = [min(256, F - f0) for f0 in range(0, F, 256)]
+    if info["xc_pixels"] > 0:
+        launches = args.steps * sum(1 + 2 * math.ceil(g / 128) for g in groups)
+    else:
+        launches = args.steps * 2 * len(groups)
 
     # ---- roofline of the batched launch: A(F) = map bytes + F * frame bytes
     peak, peak_kind = measured_peak()

@@ -123,6 +123,8 @@ typedef struct {
   int64_t oob_records;     /* records whose truncated (y,z) is off the detector        */
   int32_t tile_rows, tile_pixels, frames_per_lane;
   int32_t run_len;         /* register-run length of the tile encoding                 */
+  int64_t xc_pixels;       /* pixels of the pixel-major staging spans (8/16-bit frames
+                              of the run encoding); 0: frames are gathered frame-major */
 } mi_plan_info;
 
 typedef struct mi_plan mi_plan; /* opaque, immutable after creation except for the dark */

@@ -87,6 +87,10 @@ __host__ __device__ inline void blob_layout(int nb, int nnz, int n_u, uint32_t *
   *bytes = o;
 }
 
+constexpr int kRunWarps = 8;          // consumer (compute) warps per CTA of the run kernel
+constexpr uint32_t kRunUnitsOff = 32;  // unit and strip tables follow the tile header
+constexpr uint32_t kRunUnitsBytes = kRunWarps * 8 + kRunWarps * 4;
+
 // ---------------------------------------------------------------------------
 // Run encoding (MI_ENC_RUNS).  A tile is split into strips, one per eta column,
 // each strip being the tile's G rows of that column.  Every staged pixel that
@@ -97,6 +101,10 @@ __host__ __device__ inline void blob_layout(int nb, int nnz, int n_u, uint32_t *
 // rs >= q (q = 0 .. G-L+1, the last entry being the strip's end).
 //
 //   TileHdr                          32 B  (nnz field = number of records)
+//   uint16 units[kRunWarps][4]       {strip, first record, end record, 0}: the record range
+//                                    of each consumer warp; units of a strip are consecutive
+//                                    and split the strip's records evenly
+//   uint16 strips[kRunWarps][2]      {first unit, number of units} of each strip
 //   uint16 rs_ptr[n_cols][G-L+2]
 //   float  scale[nb], lw[nb]         nb = n_rows * n_cols, row-major
 //   uint32 upix[n_u]
@@ -107,7 +115,7 @@ __host__ __device__ inline uint32_t runs_blob_layout(int nb, int n_cols, int n_r
                                                      uint32_t *o_rsp, uint32_t *o_sc, uint32_t *o_lw,
                                                      uint32_t *o_up, uint32_t *o_lc, uint32_t *o_w) {
   auto a16 = [](uint32_t x) { return (x + 15u) & ~15u; };
-  uint32_t o = 32;
+  uint32_t o = kRunUnitsOff + kRunUnitsBytes;
   *o_rsp = o; o = a16(o + 2u * (uint32_t)n_cols * (uint32_t)(G - L + 2));
   *o_sc = o;  o = a16(o + 4u * (uint32_t)nb);
   *o_lw = o;  o = a16(o + 4u * (uint32_t)nb);
@@ -117,10 +125,11 @@ __host__ __device__ inline uint32_t runs_blob_layout(int nb, int n_cols, int n_r
   return o;
 }
 
-constexpr int kRunWarps = 8;         // consumer (compute) warps per CTA of the run kernel
-constexpr int kRunProducerWarps = 6; // producer (gather/staging) warps per CTA
+constexpr int kRunProducerWarps = 6; // producer (gather) warps per CTA, frame-major staging
+constexpr int kRunProducersXc = 2;   // producer warps issuing the copies of pixel-major staging
 constexpr int kRunCtasPerSm = 1;
-constexpr int kRunPitch = 144;       // bytes per staged pixel: 64 x u16 or 32 x f32, + 16 pad
+constexpr int kRunPitch = 144;       // bytes per staged pixel: 64 x u16 or 32 x f32, then (u16
+                                     // staging) the pixel's dark as f32 at byte 128, pad
 
 // Frames per group of the run kernel: 8/16-bit frames are staged as u16 and, with G <= 16,
 // computed two frames per lane (64 per group); otherwise one frame per lane (32).
@@ -129,30 +138,31 @@ __host__ __device__ constexpr int runs_frames_per_group(int sizeof_t, int G) {
 }
 
 // Shared memory of the run kernel (two pipeline slots b = 0, 1):
-//   [blob b: blob_cap][staging b: u_cap x kRunPitch, then u_cap darks; reused for the unit
-//    partials once consumed] x 2, [bin results: fg x nbp floats]
-//   [lineout partials: rows x fg x 2 doubles][2 mbarriers]
+//   [blob b: blob_cap][staging b: u_cap x kRunPitch]  x 2
+//   [unit partials: kRunWarps x G x fg floats, then the bin results fg x nbp floats]
+//   [scale, lineout weight: 2 x nbp floats][lineout partials: rows x fg x 2 doubles]
+//   [4 mbarriers: blob b, staging b]
 // Offsets of slot 1 are those of slot 0 plus *slot_bytes.
 __host__ __device__ inline uint32_t runs_smem_layout(uint32_t blob_cap, int u_cap, int nbp, int rows, int G, int fg,
-                                                     uint32_t *off_val, uint32_t *off_dark, uint32_t *slot_bytes,
-                                                     uint32_t *off_out, uint32_t *off_lo, uint32_t *off_bar) {
+                                                     uint32_t *off_val, uint32_t *slot_bytes, uint32_t *off_part,
+                                                     uint32_t *off_sc, uint32_t *off_lo, uint32_t *off_bar) {
   auto a16 = [](uint32_t x) { return (x + 15u) & ~15u; };
   const uint32_t ov = a16(blob_cap);                        // staging area of slot 0
-  const uint32_t od = a16(ov + (uint32_t)u_cap * (uint32_t)kRunPitch);
-  uint32_t end = a16(od + 4u * (uint32_t)u_cap);
-  const uint32_t parts = ov + (uint32_t)kRunWarps * (uint32_t)G * (uint32_t)fg * 4u;
-  if (parts > end) end = a16(parts);
-  const uint32_t slot = end;                                // [blob | staging] of one slot
-  const uint32_t oo = 2u * slot;
-  const uint32_t ol = a16(oo + (uint32_t)fg * (uint32_t)nbp * 4u);
+  const uint32_t slot = a16(ov + (uint32_t)u_cap * (uint32_t)kRunPitch);   // [blob | staging]
+  const uint32_t op = 2u * slot;
+  uint32_t part = (uint32_t)kRunWarps * (uint32_t)G * (uint32_t)fg * 4u;
+  const uint32_t outb = (uint32_t)fg * (uint32_t)nbp * 4u;
+  if (outb > part) part = outb;
+  const uint32_t osc = a16(op + part);
+  const uint32_t ol = a16(osc + 8u * (uint32_t)nbp);
   const uint32_t ob = a16(ol + (uint32_t)fg * (uint32_t)rows * 2u * 8u);
   if (off_val) *off_val = ov;
-  if (off_dark) *off_dark = od;
   if (slot_bytes) *slot_bytes = slot;
-  if (off_out) *off_out = oo;
+  if (off_part) *off_part = op;
+  if (off_sc) *off_sc = osc;
   if (off_lo) *off_lo = ol;
   if (off_bar) *off_bar = ob;
-  return ob + 16u;
+  return ob + 32u;
 }
 
 // Shared-memory layout of the batched kernel for `fpl` frames per lane:
@@ -192,6 +202,20 @@ struct TileLimits {
   int item_cols; // eta columns per work item
 };
 
+// Pixel-major staging of 8/16-bit frames for the run kernel.  The referenced pixels
+// of each detector row are covered by one span [span_lo, span_lo + len) with both ends
+// on 8-pixel boundaries (len may end at ny when ny is not a multiple of 8); the spans,
+// concatenated row by row, give the compact pixel index c.  Kernel (a) writes
+// xc[c][f] (u16, kXcFrames * kXcGroups frames per compact pixel), so a tile stages each
+// of its pixels, one frame group at a time, with one 128-byte bulk copy.  Transpose work
+// is cut into chunks of <= kXcChunk pixels of one span.
+constexpr int kXcFrames = 64;   // frames of one group (one 128-byte staged row)
+constexpr int kXcGroups = 2;    // groups held per launch
+constexpr int kXcChunk = 256;
+struct XcChunk {
+  int32_t z, y0, n, c0;  // detector row, first column, pixels, compact index of the first
+};
+
 struct Plan {
   int device = 0;
   int mode = 0, normalize = 1, semantics = 0;
@@ -220,6 +244,16 @@ struct Plan {
   float *d_dark = nullptr;       // ny*nz (zeros when no dark is set)
   int has_dark = 0;
   int *d_err = nullptr;          // device error word (bounded waits)
+  int *d_ctr = nullptr;          // work-item counter of the persistent run kernel
+  int n_sms = 0;
+
+  // pixel-major staging (run encoding with 64-frame groups)
+  int64_t n_xc = 0;              // compact pixels (0: not built)
+  int32_t *d_span_lo = nullptr;  // per detector row: first column of its span
+  int32_t *d_row_off = nullptr;  // per detector row: compact index of the span start
+  XcChunk *d_xchunks = nullptr;
+  int n_xchunks = 0;
+  uint16_t *d_xc = nullptr;      // [n_xc][kXcFrames * kXcGroups]
 
   // plain (reference-layout) path
   int32_t *d_nmap = nullptr;     // {count, offset} per bin
@@ -240,6 +274,9 @@ int launch_cake(Plan *p, const void *frames, int dtype, int n_frames, int64_t st
                 float *cake, double *lo_aw, double *lo_sm, cudaStream_t s);
 int launch_runs(Plan *p, const void *frames, int dtype, int n_frames, int64_t stride, float *cake, bool want_lo,
                 cudaStream_t s);
+// true when launch_runs stages this dtype through the pixel-major buffer
+bool runs_uses_xc(const Plan *p, int dtype);
+int launch_xc(Plan *p, const void *frames, int dtype, int F, int64_t stride, cudaStream_t s);
 int launch_plain(Plan *p, const void *frame, int dtype, double *cake, double *lo_aw,
                  double *lo_sm, cudaStream_t s);
 int launch_cast(const void *frames, int dtype, int64_t n_pixels, int n_frames,

@@ -445,6 +445,32 @@ static void runs_blob(const HostCSR &csr, const mi_map_desc &m, const Plan *p, c
   out.assign(bytes, 0);
   uint8_t *blob = out.data();
   *(TileHdr *)blob = TileHdr{nb, n_rec, t.n_u, t.n_rows, t.n_cols, t.r0, t.e0, row_in_band};
+  // consumer units: every strip gets at least one; the rest go one by one to the strip with
+  // the most records per unit; a strip's records are split evenly between its units
+  {
+    std::vector<int> cnt(t.n_cols), K(t.n_cols, 1);
+    for (int c = 0; c < t.n_cols; ++c) cnt[c] = rsp[(size_t)c * NRS + NRS - 1] - rsp[(size_t)c * NRS];
+    for (int left = kRunWarps - t.n_cols; left > 0; --left) {
+      int best = 0;
+      for (int c = 1; c < t.n_cols; ++c)
+        if ((int64_t)cnt[c] * K[best] > (int64_t)cnt[best] * K[c]) best = c;
+      ++K[best];
+    }
+    uint16_t *ut = (uint16_t *)(blob + kRunUnitsOff);
+    uint16_t *st = ut + 4 * kRunWarps;
+    int w = 0;
+    for (int c = 0; c < t.n_cols; ++c) {
+      const int j0 = rsp[(size_t)c * NRS];
+      st[2 * c] = (uint16_t)w;
+      st[2 * c + 1] = (uint16_t)K[c];
+      for (int q = 0; q < K[c]; ++q, ++w) {
+        ut[4 * w] = (uint16_t)c;
+        ut[4 * w + 1] = (uint16_t)(j0 + (int)((int64_t)cnt[c] * q / K[c]));
+        ut[4 * w + 2] = (uint16_t)(j0 + (int)((int64_t)cnt[c] * (q + 1) / K[c]));
+        ut[4 * w + 3] = 0;
+      }
+    }
+  }
   memcpy(blob + o_rsp, rsp.data(), rsp.size() * sizeof(uint16_t));
   float *scale = (float *)(blob + o_sc);
   float *lw = (float *)(blob + o_lw);
@@ -502,7 +528,8 @@ static int free_plan_mem(Plan *p) {
   cudaSetDevice(p->device);
   void *ptrs[] = {p->d_blobs, p->d_tiles, p->d_items, p->d_den_aw, p->d_cnt, p->d_partial,
                   p->d_dark, p->d_err, p->d_nmap, p->d_sorted, p->d_off, p->d_w, p->d_aw,
-                  p->d_dr, p->d_py, p->d_pz, p->d_area_in, p->d_area_all, p->d_plain_img};
+                  p->d_dr, p->d_py, p->d_pz, p->d_area_in, p->d_area_all, p->d_plain_img,
+                  p->d_ctr, p->d_span_lo, p->d_row_off, p->d_xchunks, p->d_xc};
   for (void *q : ptrs)
     if (q) cudaFree(q);
   return MI_OK;
@@ -673,13 +700,32 @@ static int build_plan(const mi_map_desc &m, const mi_plan_opts &o, Plan *p) {
       memcpy(blobs.data() + tiles[ti].off, item_blobs[it][k].data(), item_blobs[it][k].size());
       std::vector<uint8_t>().swap(item_blobs[it][k]);
     }
-  // distinct referenced pixels
+  // distinct referenced pixels, and their row spans for pixel-major staging
+  std::vector<int32_t> span_lo(m.nz, 0), row_off(m.nz, 0);
+  std::vector<XcChunk> xchunks;
+  int64_t n_xc = 0;
   {
     std::vector<uint8_t> seen(n_pix, 0);
     int64_t n = 0;
     for (int32_t c : csr.col)
       if (!seen[c]) { seen[c] = 1; ++n; }
     p->ref_pixels = n;
+    if (p->encoding == MI_ENC_RUNS && runs_frames_per_group(2, p->run_g) == kXcFrames) {
+      for (int z = 0; z < m.nz; ++z) {
+        const uint8_t *row = seen.data() + (int64_t)z * m.ny;
+        int lo = 0, hi = m.ny;
+        while (lo < m.ny && !row[lo]) ++lo;
+        while (hi > lo && !row[hi - 1]) --hi;
+        lo &= ~7;
+        if (hi > lo) hi = std::min(m.ny, (hi + 7) & ~7);
+        else hi = lo;
+        span_lo[z] = lo;
+        row_off[z] = (int32_t)n_xc;
+        for (int y = lo; y < hi; y += kXcChunk)
+          xchunks.push_back({z, y, std::min(kXcChunk, hi - y), (int32_t)(n_xc + (y - lo))});
+        n_xc += hi - lo;
+      }
+    }
   }
   // heaviest-first launch order
   std::vector<int> order(n_items);
@@ -715,6 +761,18 @@ static int build_plan(const mi_map_desc &m, const mi_plan_opts &o, Plan *p) {
   acct += n_pix * sizeof(float);
   MI_CUDA(cudaMalloc((void **)&p->d_err, sizeof(int)));
   MI_CUDA(cudaMemset(p->d_err, 0, sizeof(int)));
+  MI_CUDA(cudaMalloc((void **)&p->d_ctr, sizeof(int)));
+  MI_CUDA(cudaDeviceGetAttribute(&p->n_sms, cudaDevAttrMultiProcessorCount, p->device));
+  if (n_xc > 0) {
+    if ((rc = upload(&p->d_span_lo, span_lo.data(), span_lo.size(), &acct))) return rc;
+    if ((rc = upload(&p->d_row_off, row_off.data(), row_off.size(), &acct))) return rc;
+    if ((rc = upload(&p->d_xchunks, xchunks.data(), xchunks.size(), &acct))) return rc;
+    const size_t bytes = (size_t)n_xc * kXcFrames * kXcGroups * sizeof(uint16_t);
+    MI_CUDA(cudaMalloc((void **)&p->d_xc, bytes));
+    acct += bytes;
+    p->n_xc = n_xc;
+    p->n_xchunks = (int)xchunks.size();
+  }
 
   // ---- plain path: reference SoA layout (PrecomputeOffsets_kernel, …Stream.cu:901-924)
   {
@@ -846,6 +904,7 @@ int mi_plan_get_info(const mi_plan *p, mi_plan_info *info) {
   info->tile_pixels = p->lim.max_u;
   info->frames_per_lane = p->frames_per_lane;
   info->run_len = p->run_l;
+  info->xc_pixels = p->n_xc;
   return MI_OK;
 }
 

@@ -3,27 +3,29 @@
 // Same contract and semantics as the CSR kernel of mi_cake.cu (integrate() of
 // packages/midas_integrate/midas_integrate/kernels.py:416-473): cake =
 // diag(scale) * W * (frames - dark) for a batch of frames, plus the eta
-// partial sums of both lineouts, with no global atomics.
+// partial sums of both lineouts, with no global atomics on the data.
 //
-// What changes is the inner loop.  A tile's bins are grouped into strips (one
-// eta column, G consecutive R rows).  A warp owns a strip (or a slice of its rs
-// range when the tile has fewer strips than warps) and keeps the strip's G bin
-// accumulators in registers for its frames.  The map arrives as records
-// {staged pixel, first row rs, weights for rows rs..rs+L-1}; records are sorted
-// by rs and the loop over rs is unrolled at compile time, so each record does
-// one shared-memory read of the pixel's frame values and L FMAs per frame into
-// statically indexed registers: a pixel's radial run (the R bins its
-// pixel-split or bilinear footprint reaches) costs one staged read, not one per
-// bin.
+// A tile's bins are grouped into strips (one eta column, G consecutive R rows).  The
+// map arrives as records {staged pixel, first row rs, weights for rows rs..rs+L-1};
+// records of a strip are sorted by rs, the loop over rs is unrolled at compile time,
+// and each record does one shared-memory read of the pixel's frame values and L FMAs
+// per frame into statically indexed registers: a pixel's radial run (the R bins its
+// pixel-split or bilinear footprint reaches) costs one staged read, not one per bin.
+// Each of the 8 consumer warps owns a unit: a contiguous record range of one strip,
+// chosen on the host so that the units of a tile carry equal numbers of records.
 //
-// Frames of 8/16-bit types are staged as u16 and, with G <= 16, each lane reads
-// one 32-bit word = two frames (64 frames per group); the dark is subtracted at
-// use, (float)raw - dark, the reference's arithmetic.  Wider types are staged as
-// (float)raw - dark, one frame per lane (32 per group).  After the record loop
-// the partial sums of the units of a strip are combined in a fixed order (the
-// result of a frame never depends on the batch), scaled, and eta-reduced for
-// the lineouts in the same warp-per-row pass.
+// The kernel is persistent (one CTA per SM) and warp-specialized: producer warps
+// claim work items from a counter (heaviest first), bring each tile's blob in with
+// one bulk copy (TMA) and stage its pixels into one of two slots; consumer warps run
+// the record loop, hand the slot back, then combine the unit partials in a fixed
+// order (a frame's result never depends on the rest of its batch), scale, reduce the
+// lineouts and store the cake.  Staging of 8/16-bit frames comes from the
+// pixel-major buffer written by kernel (a) (mi_stage.cu): one 128-byte bulk copy per
+// pixel per 64-frame group; other frame types are gathered from frame-major memory.
+// The dark is subtracted at use, (float)raw - dark, the reference's arithmetic.
 #include <stdint.h>
+
+#include <algorithm>
 
 #include "mi_internal.h"
 
@@ -44,18 +46,32 @@ struct RunArgs {
   int want_cake, want_lo;
   int rows_max;
   uint32_t blob_cap;
-  uint32_t off_val, off_dark, slot_bytes, off_out, off_lo, off_bar;
+  uint32_t off_val, slot_bytes, off_part, off_sc, off_lo, off_bar;
   int nbp;
   int *err;
+  int n_items;
+  int *counter;     // work-item claims of this launch (zero at launch)
+  // pixel-major staging (8/16-bit frames): xc[c * xc_pitch + f], c = row_off[z] + y - span_lo[z]
+  const uint16_t *xc;
+  int64_t xc_pitch;
+  const int32_t *span_lo, *row_off;
+  int ny;
 };
 
-constexpr int kRunThreads = (kRunWarps + kRunProducerWarps) * 32;
 constexpr uint32_t kRunWaitLimit = 1u << 26;
 
 __device__ __forceinline__ uint32_t r_smem(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
 
 __device__ __forceinline__ void r_bulk(void *dst, const void *src, uint32_t bytes, uint64_t *bar) {
   asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(r_smem(bar)), "r"(bytes) : "memory");
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(r_smem(dst)),
+      "l"(src), "r"(bytes), "r"(r_smem(bar))
+      : "memory");
+}
+
+// Bulk copy whose bytes count against an expect_tx made earlier on the same barrier.
+__device__ __forceinline__ void r_copy(void *dst, const void *src, uint32_t bytes, uint64_t *bar) {
   asm volatile(
       "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(r_smem(dst)),
       "l"(src), "r"(bytes), "r"(r_smem(bar))
@@ -101,57 +117,114 @@ __device__ __forceinline__ void load_weights(const float *wr, float *w) {
 }
 
 // Named barriers (bar.sync / bar.arrive with an id and a thread count) hand the two
-// pipeline slots back and forth between the producer warps (gather) and the consumer
-// warps (compute).  Id 1: consumers only.  Ids 2+b: slot b staged.  Ids 4+b: slot b free.
+// pipeline slots back and forth between the producer warps and the consumer warps.
+// Id 1: consumers only.  Ids 2+b: slot b staged.  Ids 4+b: slot b free.  Id 6: producers.
 __device__ __forceinline__ void nb_sync(int id, int n) { asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(n) : "memory"); }
 __device__ __forceinline__ void nb_arrive(int id, int n) {
   asm volatile("bar.arrive %0, %1;" ::"r"(id), "r"(n) : "memory");
 }
 
-template <typename T, int G, int L>
-__global__ void __launch_bounds__(kRunThreads, 1) k_runs(RunArgs a) {
+// u16 -> float exactly, on the FMA/ALU pipes: 2^23 + x has x in its low mantissa bits
+__device__ __forceinline__ float u16lo_to_f(uint32_t w) {
+  return __uint_as_float(__byte_perm(w, 0x4B000000u, 0x7610)) - 8388608.0f;
+}
+__device__ __forceinline__ float u16hi_to_f(uint32_t w) {
+  return __uint_as_float(__byte_perm(w, 0x4B000000u, 0x7632)) - 8388608.0f;
+}
+
+// The FPL frame values of one staged pixel for this lane, dark subtracted.
+template <bool kU16, int FPL, int FG>
+__device__ __forceinline__ void staged_values(const uint8_t *s_val, uint32_t u, int lane, float *v) {
+  const uint8_t *row = s_val + u * (uint32_t)kRunPitch;
+  if constexpr (kU16 && FPL == 2) {
+    const uint32_t w2 = *(const uint32_t *)(row + 4 * lane);
+    const float d = *(const float *)(row + FG * 2);
+    v[0] = u16lo_to_f(w2) - d;
+    v[1] = u16hi_to_f(w2) - d;
+  } else if constexpr (kU16) {
+    v[0] = (float)*(const uint16_t *)(row + 2 * lane) - *(const float *)(row + FG * 2);
+  } else {
+    v[0] = *(const float *)(row + 4 * lane);
+  }
+}
+
+// Per-slot schedule record written by the producers: which item, frame group and
+// tile the slot holds (item < 0: no more work for this CTA).
+struct SlotTag {
+  int32_t item, g, t, pad;
+};
+
+template <typename T, int G, int L, bool XC, int NP>
+__global__ void __launch_bounds__((kRunWarps + NP) * 32, 1) k_runs(RunArgs a) {
   constexpr bool kU16 = sizeof(T) <= 2;              // staged as u16
   constexpr int FG = runs_frames_per_group(sizeof(T), G);
   constexpr int FPL = FG / 32;                       // frames per lane
   constexpr int NRS = G - L + 2;
   constexpr int NC = kRunWarps;                      // consumer warps
   constexpr int NCT = NC * 32;
-  constexpr int NPT = kRunProducerWarps * 32;        // producer threads
+  constexpr int NPT = NP * 32;                       // producer threads
   constexpr int NALL = NCT + NPT;
+  constexpr int MAXR = (G + NC - 1) / NC;            // rows of a tile per consumer warp
+  static_assert(!XC || (kU16 && FG == kXcFrames), "pixel-major staging holds 64 u16 frames per group");
   extern __shared__ __align__(16) uint8_t smem[];
-  float *s_out = (float *)(smem + a.off_out);        // [FG][nbp]
+  float *s_part = (float *)(smem + a.off_part);      // [NC units][G][FG]; then the bin results [FG][nbp]
+  float *s_out = s_part;
+  float *s_sc = (float *)(smem + a.off_sc);          // [2][nbp]: scale, lineout weight of the tile's bins
   double *s_lo = (double *)(smem + a.off_lo);        // [rows][FG][2]
-  uint64_t *bar = (uint64_t *)(smem + a.off_bar);
-  __shared__ int s_abort;
+  uint64_t *bar = (uint64_t *)(smem + a.off_bar);    // [0,1]: blob of slot b; [2,3]: staging of slot b
+  __shared__ SlotTag s_tag[2];
+  __shared__ int s_abort, s_next;
 
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const WorkItem it = a.items[blockIdx.x];
   const int nbp = a.nbp;
-  const int nt = it.tile_end - it.tile_begin;
   const int n_groups = (a.F + FG - 1) / FG;
-  const int n_steps = nt * n_groups;
 
   if (tid == 0) {
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(r_smem(&bar[0])) : "memory");
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(r_smem(&bar[1])) : "memory");
+#pragma unroll
+    for (int q = 0; q < 4; ++q)
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(r_smem(&bar[q])) : "memory");
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     s_abort = 0;
   }
   __syncthreads();
-  if (n_steps == 0) return;
 
   if (warp >= NC) {
-    // ================= producers: bring tile blob k in (TMA), gather its pixels
+    // ================= producers: claim work items, bring tile blobs in (TMA), stage pixels
     const int ptid = tid - NCT;
     const T *frames = (const T *)a.frames;
-    for (int k = 0; k < n_steps; ++k) {
+    int k = 0, item = -1, nt = 0, g = 0, t = 0;
+    WorkItem it{};
+    for (;; ++k) {
       const int b = k & 1;
-      const int g0 = (k / nt) * FG;
+      // next (item, group, tile); items are claimed from the launch's counter
+      if (item >= 0 && ++t == nt) {
+        t = 0;
+        if (++g == n_groups) item = -1;
+      }
+      while (item < 0) {
+        if (ptid == 0) s_next = atomicAdd(a.counter, 1);
+        asm volatile("bar.sync 6, %0;" ::"r"(NPT) : "memory");
+        const int claimed = s_next;
+        asm volatile("bar.sync 6, %0;" ::"r"(NPT) : "memory");
+        if (claimed >= a.n_items) break;
+        it = a.items[claimed];
+        nt = it.tile_end - it.tile_begin;
+        g = 0;
+        t = 0;
+        if (nt > 0) item = claimed;
+      }
+      if (k >= 2) nb_sync(4 + b, NALL);              // consumers are done with slot b (step k-2)
+      if (item < 0) {
+        if (ptid == 0) s_tag[b] = SlotTag{-1, 0, 0, 0};
+        nb_arrive(2 + b, NALL);
+        break;
+      }
+      const int g0 = g * FG;
       const int fg_n = min(FG, a.F - g0);
       uint8_t *slot = smem + b * a.slot_bytes;
-      if (k >= 2) nb_sync(4 + b, NALL);              // consumers are done with slot b (step k-2)
       if (ptid == 0) {
-        const TileRef r = a.tiles[it.tile_begin + k % nt];
+        s_tag[b] = SlotTag{item, g, t, 0};
+        const TileRef r = a.tiles[it.tile_begin + t];
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
         r_bulk(slot, a.blobs + r.off, r.bytes, &bar[b]);
       }
@@ -169,13 +242,33 @@ __global__ void __launch_bounds__(kRunThreads, 1) k_runs(RunArgs a) {
       runs_blob_layout(h.nb, h.n_cols, h.nnz, h.n_u, G, L, &o_rsp, &o_sc, &o_lw, &o_up, &o_lc, &o_w);
       const uint32_t *upix = (const uint32_t *)(slot + o_up);
       uint8_t *s_val = slot + a.off_val;
-      float *s_dark = (float *)(slot + a.off_dark);
+      if constexpr (XC) {
+        // one 128-byte bulk copy per staged pixel from the pixel-major buffer (frame group g);
+        // the staging barrier of slot b expects all of them before any is issued
+        if (ptid == 0)
+          asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(r_smem(&bar[2 + b])),
+                       "r"((uint32_t)h.n_u * (uint32_t)(kXcFrames * 2))
+                       : "memory");
+        asm volatile("bar.sync 6, %0;" ::"r"(NPT) : "memory");
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        const uint16_t *xg = a.xc + (size_t)g * kXcFrames;
+        for (int u = ptid; u < h.n_u; u += NPT) {
+          const uint32_t pix = upix[u];
+          const uint32_t z = pix / (uint32_t)a.ny;
+          const uint32_t c = (uint32_t)__ldg(a.row_off + z) + (pix - z * (uint32_t)a.ny) - (uint32_t)__ldg(a.span_lo + z);
+          uint8_t *row = s_val + (size_t)u * kRunPitch;
+          r_copy(row, xg + (size_t)c * a.xc_pitch, kXcFrames * 2, &bar[2 + b]);
+          *(float *)(row + kXcFrames * 2) = __ldg(a.dark + pix);   // beside the copied bytes
+        }
+        nb_arrive(2 + b, NALL);                       // copies issued, darks written
+        continue;
+      }
       for (int u = ptid; u < h.n_u; u += NPT) {
         const uint32_t pix = upix[u];
         const float d = __ldg(a.dark + pix);
         const T *src = frames + (int64_t)g0 * a.stride + pix;
         uint8_t *row = s_val + (size_t)u * kRunPitch;
-        if (kU16) {
+        if constexpr (kU16) {
           // all FG frames of the pixel in flight at once, packed two per word
           uint32_t v[FG / 2];
 #pragma unroll
@@ -187,46 +280,47 @@ __global__ void __launch_bounds__(kRunThreads, 1) k_runs(RunArgs a) {
           uint4 *dst = (uint4 *)row;
 #pragma unroll
           for (int q = 0; q < FG / 8; ++q) dst[q] = make_uint4(v[4 * q], v[4 * q + 1], v[4 * q + 2], v[4 * q + 3]);
+          *(float *)(row + FG * 2) = d;
+        } else {
+          float v[32];
+#pragma unroll
+          for (int f = 0; f < 32; ++f) v[f] = (f < fg_n) ? r_cvt(__ldg(src + (int64_t)f * a.stride)) - d : 0.0f;
+          float4 *dst = (float4 *)row;
+#pragma unroll
+          for (int q = 0; q < 8; ++q) dst[q] = make_float4(v[4 * q], v[4 * q + 1], v[4 * q + 2], v[4 * q + 3]);
         }
-#pragma unroll
-        for (int c = 0; c < FG; c += 32) {
-          if (kU16) {
-          } else {
-            float v[32];
-#pragma unroll
-            for (int f = 0; f < 32; ++f)
-              v[f] = (c + f < fg_n) ? r_cvt(__ldg(src + (int64_t)(c + f) * a.stride)) - d : 0.0f;
-            float4 *dst = (float4 *)(row + 4 * c);
-#pragma unroll
-            for (int q = 0; q < 8; ++q) dst[q] = make_float4(v[4 * q], v[4 * q + 1], v[4 * q + 2], v[4 * q + 3]);
-          }
-        }
-        s_dark[u] = d;
       }
       nb_arrive(2 + b, NALL);                         // slot b staged
     }
     // take the consumers' last two slot releases so no barrier generation is left open
-    for (int k = n_steps; k < n_steps + 2; ++k)
-      if (k >= 2) nb_sync(4 + (k & 1), NALL);
+    for (int kk = k + 1; kk < k + 3; ++kk)
+      if (kk >= 2) nb_sync(4 + (kk & 1), NALL);
     return;
   }
 
   // ================= consumers: records -> registers -> combine -> cake + lineouts
-  for (int k = 0; k < n_steps; ++k) {
+  for (int k = 0;; ++k) {
     const int b = k & 1;
-    const int g = k / nt, t = k - g * nt;
-    const int g0 = g * FG;
-    const int fg_n = min(FG, a.F - g0);
     const uint8_t *blob = smem + b * a.slot_bytes;
     const uint8_t *s_val = blob + a.off_val;
-    const float *s_dark = (const float *)(blob + a.off_dark);
-    float *s_part = (float *)(smem + b * a.slot_bytes + a.off_val);   // reuses slot b's staging
+    nb_sync(2 + b, NALL);                             // slot b staged (or the end marker)
+    if (s_abort) return;
+    const SlotTag tag = s_tag[b];
+    if (tag.item < 0) {
+      nb_arrive(4 + b, NALL);
+      return;
+    }
+    const WorkItem it = a.items[tag.item];
+    const int nt = it.tile_end - it.tile_begin;
+    const int t = tag.t, g0 = tag.g * FG;
+    const int fg_n = min(FG, a.F - g0);
     if (t == 0)
       for (int i = tid; i < FG * a.rows_max * 2; i += NCT) s_lo[i] = 0.0;
-    nb_sync(2 + b, NALL);                             // slot b staged
-    if (s_abort) return;
-    // the blob was written by the bulk copy (async proxy): observe its completed phase too
+    // the blob and the staging were written by bulk copies (async proxy): observe their phases
     if (!r_wait(&bar[b], (uint32_t)((k >> 1) & 1))) atomicExch(a.err, MI_E_TIMEOUT);
+    if constexpr (XC) {
+      if (!r_wait(&bar[2 + b], (uint32_t)((k >> 1) & 1))) atomicExch(a.err, MI_E_TIMEOUT);
+    }
     const TileHdr h = *(const TileHdr *)blob;
     uint32_t o_rsp, o_sc, o_lw, o_up, o_lc, o_w;
     runs_blob_layout(h.nb, h.n_cols, h.nnz, h.n_u, G, L, &o_rsp, &o_sc, &o_lw, &o_up, &o_lc, &o_w);
@@ -235,48 +329,51 @@ __global__ void __launch_bounds__(kRunThreads, 1) k_runs(RunArgs a) {
     const float *lw = (const float *)(blob + o_lw);
     const uint16_t *lcol = (const uint16_t *)(blob + o_lc);
     const float *wts = (const float *)(blob + o_w);
+    const uint16_t *units = (const uint16_t *)(blob + kRunUnitsOff);
+    const uint32_t *strips = (const uint32_t *)(units + 4 * kRunWarps);   // {first unit | count << 16}
 
     const int ns = h.n_cols;
-    const int K = NC / ns;               // units per strip (>= 1: tiles hold <= NC strips)
-    const int n_units = ns * K;
     float acc[G][FPL];
 #pragma unroll
     for (int i = 0; i < G; ++i)
 #pragma unroll
       for (int p = 0; p < FPL; ++p) acc[i][p] = 0.0f;
-    if (warp < n_units) {
-      const int s = warp / K, kk = warp - s * K;
-      const int rs_lo = ((NRS - 1) * kk) / K, rs_hi = ((NRS - 1) * (kk + 1)) / K;
+    {
+      // this warp's unit: records [j0, j1) of strip s, walked rs by rs
+      const uint2 ud = *(const uint2 *)(units + 4 * warp);
+      const int s = ud.x & 0xFFFF, j0 = ud.x >> 16, j1 = ud.y & 0xFFFF;
       const uint16_t *rp = rsp + s * NRS;
 #pragma unroll
       for (int rs = 0; rs <= G - L; ++rs) {
-        if (rs < rs_lo || rs >= rs_hi) continue;
-        const int jb = rp[rs], je = rp[rs + 1];
-        for (int j = jb; j < je; ++j) {
-          const uint32_t u = lcol[j];
-          const uint8_t *row = s_val + (size_t)u * kRunPitch;
-          float v[FPL];
-          if constexpr (kU16 && FPL == 2) {
-            const uint32_t w2 = ((const uint32_t *)row)[lane];
-            const float d = s_dark[u];
-            v[0] = (float)(w2 & 0xFFFFu) - d;
-            v[1] = (float)(w2 >> 16) - d;
-          } else if constexpr (kU16) {
-            v[0] = (float)((const uint16_t *)row)[lane] - s_dark[u];
-          } else {
-            v[0] = ((const float *)row)[lane];
-          }
-          float w[L];
-          load_weights<L>(wts + (size_t)j * L, w);
+        const int jb = max((int)rp[rs], j0), je = min((int)rp[rs + 1], j1);
+        int j = jb;
+        // two records per iteration: both loads in flight before the conversions and FMAs
+        for (; j + 1 < je; j += 2) {
+          float v0[FPL], v1[FPL], w0[L], w1[L];
+          staged_values<kU16, FPL, FG>(s_val, lcol[j], lane, v0);
+          staged_values<kU16, FPL, FG>(s_val, lcol[j + 1], lane, v1);
+          load_weights<L>(wts + (size_t)j * L, w0);
+          load_weights<L>(wts + (size_t)(j + 1) * L, w1);
 #pragma unroll
           for (int q = 0; q < L; ++q)
 #pragma unroll
-            for (int p = 0; p < FPL; ++p) acc[rs + q][p] = fmaf(w[q], v[p], acc[rs + q][p]);
+            for (int p = 0; p < FPL; ++p) acc[rs + q][p] = fmaf(w0[q], v0[p], acc[rs + q][p]);
+#pragma unroll
+          for (int q = 0; q < L; ++q)
+#pragma unroll
+            for (int p = 0; p < FPL; ++p) acc[rs + q][p] = fmaf(w1[q], v1[p], acc[rs + q][p]);
+        }
+        if (j < je) {
+          float v0[FPL], w0[L];
+          staged_values<kU16, FPL, FG>(s_val, lcol[j], lane, v0);
+          load_weights<L>(wts + (size_t)j * L, w0);
+#pragma unroll
+          for (int q = 0; q < L; ++q)
+#pragma unroll
+            for (int p = 0; p < FPL; ++p) acc[rs + q][p] = fmaf(w0[q], v0[p], acc[rs + q][p]);
         }
       }
-    }
-    nb_sync(1, NCT);                     // staging of slot b consumed: holds the partials now
-    if (warp < n_units) {
+      // unit partials to their own buffer: the slot can be refilled during the combine
 #pragma unroll
       for (int i = 0; i < G; ++i) {
         float *d = s_part + ((size_t)warp * G + i) * FG + lane * FPL;
@@ -284,27 +381,55 @@ __global__ void __launch_bounds__(kRunThreads, 1) k_runs(RunArgs a) {
         else d[0] = acc[i][0];
       }
     }
-    nb_sync(1, NCT);
+    // the strip table, the scales and the header go to registers / private smem before
+    // the slot is handed back
+    uint32_t stp[NC];
+#pragma unroll
+    for (int q = 0; q < NC; ++q) stp[q] = strips[q];
+    for (int i = tid; i < h.nb; i += NCT) {
+      s_sc[i] = scale[i];
+      s_sc[nbp + i] = lw[i];
+    }
+    nb_sync(1, NCT);                     // partials, scales written; slot b no longer read
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    nb_arrive(4 + b, NALL);              // hand slot b back to the producers
 
-    // ---- combine (fixed unit order), scale, lineout partials: warp per row, lanes = frames
-    for (int i = warp; i < h.n_rows; i += NC) {
+    // ---- combine (fixed unit order): warp per row, lanes = frames; sums into registers
+    // first, since the bin results overwrite the partials
+    float v[MAXR][NC][FPL];
+#pragma unroll
+    for (int ri = 0; ri < MAXR; ++ri) {
+      const int i = warp + ri * NC;
+#pragma unroll
+      for (int s = 0; s < NC; ++s) {
+#pragma unroll
+        for (int p = 0; p < FPL; ++p) v[ri][s][p] = 0.0f;
+        if (i < h.n_rows && s < ns) {
+          const int u0 = stp[s] & 0xFFFF, nu = stp[s] >> 16;
+          for (int kk = 0; kk < nu; ++kk) {
+            const float *src = s_part + ((size_t)(u0 + kk) * G + i) * FG + lane * FPL;
+#pragma unroll
+            for (int p = 0; p < FPL; ++p) v[ri][s][p] += src[p];
+          }
+        }
+      }
+    }
+    nb_sync(1, NCT);                     // partials read
+#pragma unroll
+    for (int ri = 0; ri < MAXR; ++ri) {
+      const int i = warp + ri * NC;
+      if (i >= h.n_rows) continue;
       double saw[FPL], ssm[FPL];
 #pragma unroll
       for (int p = 0; p < FPL; ++p) saw[p] = ssm[p] = 0.0;
-      for (int s = 0; s < ns; ++s) {
-        float v[FPL];
 #pragma unroll
-        for (int p = 0; p < FPL; ++p) v[p] = 0.0f;
-        for (int kk = 0; kk < K; ++kk) {
-          const float *src = s_part + ((size_t)(s * K + kk) * G + i) * FG + lane * FPL;
-#pragma unroll
-          for (int p = 0; p < FPL; ++p) v[p] += src[p];
-        }
+      for (int s = 0; s < NC; ++s) {
+        if (s >= ns) continue;
         const int bb = i * ns + s;
-        const float sc = scale[bb], l = lw[bb];
+        const float sc = s_sc[bb], l = s_sc[nbp + bb];
 #pragma unroll
         for (int p = 0; p < FPL; ++p) {
-          const float o = v[p] * sc;
+          const float o = v[ri][s][p] * sc;
           s_out[(lane * FPL + p) * nbp + bb] = o;
           saw[p] += (double)o * (double)l;
           ssm[p] += (l > 0.0f) ? (double)o : 0.0;
@@ -320,8 +445,6 @@ __global__ void __launch_bounds__(kRunThreads, 1) k_runs(RunArgs a) {
       }
     }
     nb_sync(1, NCT);
-    // slot b (blob + staging/partials) is no longer read: hand it back to the producers
-    nb_arrive(4 + b, NALL);
 
     // ---- cake store: warp per frame, lanes over the tile's bins (runs of n_cols contiguous
     // floats per row); row/col from a float reciprocal (exact for b < 2^12)
@@ -349,19 +472,22 @@ __global__ void __launch_bounds__(kRunThreads, 1) k_runs(RunArgs a) {
   }
 }
 
-template <typename T, int G, int L>
+template <typename T, int G, int L, bool XC, int NP>
 static int launch_runs_t(Plan *p, RunArgs &a, cudaStream_t s) {
   const size_t smem = runs_smem_layout(a.blob_cap, std::max(p->max_u, 1), a.nbp, a.rows_max, G,
-                                       runs_frames_per_group(sizeof(T), G), &a.off_val, &a.off_dark, &a.slot_bytes,
-                                       &a.off_out, &a.off_lo, &a.off_bar);
+                                       runs_frames_per_group(sizeof(T), G), &a.off_val, &a.slot_bytes, &a.off_part,
+                                       &a.off_sc, &a.off_lo, &a.off_bar);
   int dev_smem = 0;
   MI_CUDA(cudaDeviceGetAttribute(&dev_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, p->device));
   if (smem + 64 > (size_t)dev_smem)
     return set_error(MI_E_RANGE, "run kernel needs %zu B shared memory (> %d)", smem, dev_smem);
-  MI_CUDA(cudaFuncSetAttribute(k_runs<T, G, L>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  MI_CUDA(cudaFuncSetAttribute(k_runs<T, G, L>, cudaFuncAttributePreferredSharedMemoryCarveout,
-                               cudaSharedmemCarveoutMaxShared));
-  k_runs<T, G, L><<<p->n_items, kRunThreads, smem, s>>>(a);
+  auto kern = k_runs<T, G, L, XC, NP>;
+  MI_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  MI_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, cudaSharedmemCarveoutMaxShared));
+  // persistent: one CTA per SM claims work items (heaviest first) from a counter
+  MI_CUDA(cudaMemsetAsync(p->d_ctr, 0, sizeof(int), s));
+  const int grid = std::max(1, std::min(p->n_items, p->n_sms * kRunCtasPerSm));
+  kern<<<grid, (kRunWarps + NP) * 32, smem, s>>>(a);
   MI_CUDA(cudaGetLastError());
   return MI_OK;
 }
@@ -369,13 +495,24 @@ static int launch_runs_t(Plan *p, RunArgs &a, cudaStream_t s) {
 template <typename T>
 static int launch_runs_gl(Plan *p, RunArgs &a, cudaStream_t s) {
   const int G = p->run_g, L = p->run_l;
-  if (G == 8 && L == 2) return launch_runs_t<T, 8, 2>(p, a, s);
-  if (G == 8 && L == 4) return launch_runs_t<T, 8, 4>(p, a, s);
-  if (G == 16 && L == 4) return launch_runs_t<T, 16, 4>(p, a, s);
-  if (G == 16 && L == 8) return launch_runs_t<T, 16, 8>(p, a, s);
-  if (G == 32 && L == 4) return launch_runs_t<T, 32, 4>(p, a, s);
-  if (G == 32 && L == 8) return launch_runs_t<T, 32, 8>(p, a, s);
+  if (G == 8 && L == 2) return launch_runs_t<T, 8, 2, false, kRunProducerWarps>(p, a, s);
+  if (G == 8 && L == 4) return launch_runs_t<T, 8, 4, false, kRunProducerWarps>(p, a, s);
+  if (G == 16 && L == 4) return launch_runs_t<T, 16, 4, false, kRunProducerWarps>(p, a, s);
+  if (G == 16 && L == 8) return launch_runs_t<T, 16, 8, false, kRunProducerWarps>(p, a, s);
+  if (G == 32 && L == 4) return launch_runs_t<T, 32, 4, false, kRunProducerWarps>(p, a, s);
+  if (G == 32 && L == 8) return launch_runs_t<T, 32, 8, false, kRunProducerWarps>(p, a, s);
   return set_error(MI_E_UNSUPPORTED, "run encoding with G=%d L=%d", G, L);
+}
+
+// pixel-major staging: 8/16-bit frames, 64-frame groups (G <= 16)
+template <typename T>
+static int launch_runs_xc(Plan *p, RunArgs &a, cudaStream_t s) {
+  const int G = p->run_g, L = p->run_l;
+  if (G == 8 && L == 2) return launch_runs_t<T, 8, 2, true, kRunProducersXc>(p, a, s);
+  if (G == 8 && L == 4) return launch_runs_t<T, 8, 4, true, kRunProducersXc>(p, a, s);
+  if (G == 16 && L == 4) return launch_runs_t<T, 16, 4, true, kRunProducersXc>(p, a, s);
+  if (G == 16 && L == 8) return launch_runs_t<T, 16, 8, true, kRunProducersXc>(p, a, s);
+  return set_error(MI_E_UNSUPPORTED, "pixel-major staging with G=%d L=%d", G, L);
 }
 
 int launch_runs(Plan *p, const void *frames, int dtype, int n_frames, int64_t stride, float *cake, bool want_lo,
@@ -400,6 +537,32 @@ int launch_runs(Plan *p, const void *frames, int dtype, int n_frames, int64_t st
   a.blob_cap = (p->max_blob + 15u) & ~15u;
   a.nbp = (p->max_nb | 1);
   a.err = p->d_err;
+  a.n_items = p->n_items;
+  a.counter = p->d_ctr;
+  a.xc = p->d_xc;
+  a.xc_pitch = kXcFrames * kXcGroups;
+  a.span_lo = p->d_span_lo;
+  a.row_off = p->d_row_off;
+  a.ny = p->ny;
+  if (runs_uses_xc(p, dtype)) {
+    // kernel (a) transposes up to 128 frames into the pixel-major buffer, kernel (b) stages
+    // from it; the partial sums of frame f live at row f of the plan's scratch
+    const size_t es = dtype_size(dtype);
+    constexpr int kChunk = kXcFrames * kXcGroups;
+    for (int f0 = 0; f0 < n_frames; f0 += kChunk) {
+      const int nf = std::min(kChunk, n_frames - f0);
+      int rc = launch_xc(p, (const uint8_t *)frames + (size_t)f0 * stride * es, dtype, nf, stride, s);
+      if (rc) return rc;
+      RunArgs b = a;
+      b.F = nf;
+      b.frames = nullptr;
+      b.cake = cake ? cake + (size_t)f0 * p->n_bins : nullptr;
+      b.partial = p->d_partial + (size_t)f0 * p->n_r * p->n_slots * 2;
+      rc = dtype == MI_DT_U16 ? launch_runs_xc<uint16_t>(p, b, s) : launch_runs_xc<uint8_t>(p, b, s);
+      if (rc) return rc;
+    }
+    return MI_OK;
+  }
   switch (dtype) {
     case MI_DT_U8: return launch_runs_gl<uint8_t>(p, a, s);
     case MI_DT_U16: return launch_runs_gl<uint16_t>(p, a, s);
