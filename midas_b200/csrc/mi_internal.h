@@ -138,28 +138,26 @@ __host__ __device__ constexpr int runs_frames_per_group(int sizeof_t, int G) {
 }
 
 // Shared memory of the run kernel (two pipeline slots b = 0, 1):
-//   [blob b: blob_cap][staging b: u_cap x kRunPitch]  x 2
-//   [unit partials: kRunWarps x G x fg floats, then the bin results fg x nbp floats]
-//   [scale, lineout weight: 2 x nbp floats][lineout partials: rows x fg x 2 doubles]
+//   [blob b: blob_cap][staging b: u_cap x kRunPitch; after the record loop, the bin
+//    results fg x nbp floats]  x 2
+//   [unit partials: kRunWarps x G x fg floats][lineout partials: rows x fg x 2 doubles]
 //   [4 mbarriers: blob b, staging b]
 // Offsets of slot 1 are those of slot 0 plus *slot_bytes.
 __host__ __device__ inline uint32_t runs_smem_layout(uint32_t blob_cap, int u_cap, int nbp, int rows, int G, int fg,
                                                      uint32_t *off_val, uint32_t *slot_bytes, uint32_t *off_part,
-                                                     uint32_t *off_sc, uint32_t *off_lo, uint32_t *off_bar) {
+                                                     uint32_t *off_lo, uint32_t *off_bar) {
   auto a16 = [](uint32_t x) { return (x + 15u) & ~15u; };
   const uint32_t ov = a16(blob_cap);                        // staging area of slot 0
-  const uint32_t slot = a16(ov + (uint32_t)u_cap * (uint32_t)kRunPitch);   // [blob | staging]
-  const uint32_t op = 2u * slot;
-  uint32_t part = (uint32_t)kRunWarps * (uint32_t)G * (uint32_t)fg * 4u;
+  uint32_t stage = (uint32_t)u_cap * (uint32_t)kRunPitch;
   const uint32_t outb = (uint32_t)fg * (uint32_t)nbp * 4u;
-  if (outb > part) part = outb;
-  const uint32_t osc = a16(op + part);
-  const uint32_t ol = a16(osc + 8u * (uint32_t)nbp);
+  if (outb > stage) stage = outb;
+  const uint32_t slot = a16(ov + stage);                    // [blob | staging] of one slot
+  const uint32_t op = 2u * slot;
+  const uint32_t ol = a16(op + (uint32_t)kRunWarps * (uint32_t)G * (uint32_t)fg * 4u);
   const uint32_t ob = a16(ol + (uint32_t)fg * (uint32_t)rows * 2u * 8u);
   if (off_val) *off_val = ov;
   if (slot_bytes) *slot_bytes = slot;
   if (off_part) *off_part = op;
-  if (off_sc) *off_sc = osc;
   if (off_lo) *off_lo = ol;
   if (off_bar) *off_bar = ob;
   return ob + 32u;

@@ -581,7 +581,10 @@ static int build_plan(const mi_map_desc &m, const mi_plan_opts &o, Plan *p) {
   L.max_nb = 256;
   L.max_nnz = enc == MI_ENC_RUNS ? 12288 : 4096;
   L.max_cols = enc == MI_ENC_RUNS ? kRunWarps : 1 << 30;
+  // about 12 items per band; item boundaries on 8-column (32-byte) boundaries of the cake
+  // rows when there are enough columns, so no cake sector is written by two items
   L.item_cols = std::max(1, (m.n_eta + 11) / 12);
+  if (m.n_eta >= 96) L.item_cols = (L.item_cols + 7) & ~7;
   int G = 0, RL = 0;
   if (enc == MI_ENC_RUNS) {
     G = L.rows <= 8 ? 8 : (L.rows <= 16 ? 16 : 32);
@@ -649,7 +652,7 @@ static int build_plan(const mi_map_desc &m, const mi_plan_opts &o, Plan *p) {
     const uint32_t cap = (mb + 15u) & ~15u;
     const uint32_t need = enc == MI_ENC_RUNS
                               ? runs_smem_layout(cap, mu, mnb | 1, L.rows, G, runs_frames_per_group(2, G), nullptr,
-                                                 nullptr, nullptr, nullptr, nullptr, nullptr)
+                                                 nullptr, nullptr, nullptr, nullptr)
                               : cake_smem_layout(fpl, cap, mu, mnb | 1, L.rows, nullptr, nullptr, nullptr, nullptr);
     if (need + 1024u <= (uint32_t)dev_smem) break;
     if (attempt >= 12 || L.max_u <= 32)

@@ -17,9 +17,9 @@
 // The kernel is persistent (one CTA per SM) and warp-specialized: producer warps
 // claim work items from a counter (heaviest first), bring each tile's blob in with
 // one bulk copy (TMA) and stage its pixels into one of two slots; consumer warps run
-// the record loop, hand the slot back, then combine the unit partials in a fixed
-// order (a frame's result never depends on the rest of its batch), scale, reduce the
-// lineouts and store the cake.  Staging of 8/16-bit frames comes from the
+// the record loop, combine the unit partials in a fixed order (a frame's result never
+// depends on the rest of its batch), scale, reduce the lineouts, store the cake and
+// hand the slot back.  Staging of 8/16-bit frames comes from the
 // pixel-major buffer written by kernel (a) (mi_stage.cu): one 128-byte bulk copy per
 // pixel per 64-frame group; other frame types are gathered from frame-major memory.
 // The dark is subtracted at use, (float)raw - dark, the reference's arithmetic.
@@ -46,7 +46,7 @@ struct RunArgs {
   int want_cake, want_lo;
   int rows_max;
   uint32_t blob_cap;
-  uint32_t off_val, slot_bytes, off_part, off_sc, off_lo, off_bar;
+  uint32_t off_val, slot_bytes, off_part, off_lo, off_bar;
   int nbp;
   int *err;
   int n_items;
@@ -59,6 +59,7 @@ struct RunArgs {
 };
 
 constexpr uint32_t kRunWaitLimit = 1u << 26;
+constexpr int kRecBatch = 4;   // records whose loads are issued together in the record loop
 
 __device__ __forceinline__ uint32_t r_smem(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
 
@@ -151,7 +152,8 @@ __device__ __forceinline__ void staged_values(const uint8_t *s_val, uint32_t u, 
 // Per-slot schedule record written by the producers: which item, frame group and
 // tile the slot holds (item < 0: no more work for this CTA).
 struct SlotTag {
-  int32_t item, g, t, pad;
+  int32_t item, g, t, nt;          // item, frame group, tile of the item, tiles of the item
+  int32_t r0, n_rows, slot, pad;   // the item's rows and lineout slot
 };
 
 template <typename T, int G, int L, bool XC, int NP>
@@ -164,12 +166,9 @@ __global__ void __launch_bounds__((kRunWarps + NP) * 32, 1) k_runs(RunArgs a) {
   constexpr int NCT = NC * 32;
   constexpr int NPT = NP * 32;                       // producer threads
   constexpr int NALL = NCT + NPT;
-  constexpr int MAXR = (G + NC - 1) / NC;            // rows of a tile per consumer warp
   static_assert(!XC || (kU16 && FG == kXcFrames), "pixel-major staging holds 64 u16 frames per group");
   extern __shared__ __align__(16) uint8_t smem[];
-  float *s_part = (float *)(smem + a.off_part);      // [NC units][G][FG]; then the bin results [FG][nbp]
-  float *s_out = s_part;
-  float *s_sc = (float *)(smem + a.off_sc);          // [2][nbp]: scale, lineout weight of the tile's bins
+  float *s_part = (float *)(smem + a.off_part);      // [NC units][G][FG]
   double *s_lo = (double *)(smem + a.off_lo);        // [rows][FG][2]
   uint64_t *bar = (uint64_t *)(smem + a.off_bar);    // [0,1]: blob of slot b; [2,3]: staging of slot b
   __shared__ SlotTag s_tag[2];
@@ -194,6 +193,9 @@ __global__ void __launch_bounds__((kRunWarps + NP) * 32, 1) k_runs(RunArgs a) {
     const T *frames = (const T *)a.frames;
     int k = 0, item = -1, nt = 0, g = 0, t = 0;
     WorkItem it{};
+    // the claim of the next item is issued when the current one starts, so its latency
+    // overlaps the current item's tiles
+    int next_claim = (ptid == 0) ? atomicAdd(a.counter, 1) : 0;
     for (;; ++k) {
       const int b = k & 1;
       // next (item, group, tile); items are claimed from the launch's counter
@@ -202,20 +204,23 @@ __global__ void __launch_bounds__((kRunWarps + NP) * 32, 1) k_runs(RunArgs a) {
         if (++g == n_groups) item = -1;
       }
       while (item < 0) {
-        if (ptid == 0) s_next = atomicAdd(a.counter, 1);
+        if (ptid == 0) s_next = next_claim;
         asm volatile("bar.sync 6, %0;" ::"r"(NPT) : "memory");
         const int claimed = s_next;
         asm volatile("bar.sync 6, %0;" ::"r"(NPT) : "memory");
         if (claimed >= a.n_items) break;
+        if (ptid == 0) next_claim = atomicAdd(a.counter, 1);
         it = a.items[claimed];
         nt = it.tile_end - it.tile_begin;
         g = 0;
         t = 0;
         if (nt > 0) item = claimed;
       }
+      TileRef tref{};
+      if (ptid == 0 && item >= 0) tref = a.tiles[it.tile_begin + t];   // in flight during the wait
       if (k >= 2) nb_sync(4 + b, NALL);              // consumers are done with slot b (step k-2)
       if (item < 0) {
-        if (ptid == 0) s_tag[b] = SlotTag{-1, 0, 0, 0};
+        if (ptid == 0) s_tag[b] = SlotTag{-1, 0, 0, 0, 0, 0, 0, 0};
         nb_arrive(2 + b, NALL);
         break;
       }
@@ -223,10 +228,9 @@ __global__ void __launch_bounds__((kRunWarps + NP) * 32, 1) k_runs(RunArgs a) {
       const int fg_n = min(FG, a.F - g0);
       uint8_t *slot = smem + b * a.slot_bytes;
       if (ptid == 0) {
-        s_tag[b] = SlotTag{item, g, t, 0};
-        const TileRef r = a.tiles[it.tile_begin + t];
+        s_tag[b] = SlotTag{item, g, t, nt, it.r0, it.n_rows, it.slot, 0};
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-        r_bulk(slot, a.blobs + r.off, r.bytes, &bar[b]);
+        r_bulk(slot, a.blobs + tref.off, tref.bytes, &bar[b]);
       }
       if (!r_wait(&bar[b], (uint32_t)((k >> 1) & 1))) {
         atomicExch(a.err, MI_E_TIMEOUT);
@@ -310,8 +314,7 @@ __global__ void __launch_bounds__((kRunWarps + NP) * 32, 1) k_runs(RunArgs a) {
       nb_arrive(4 + b, NALL);
       return;
     }
-    const WorkItem it = a.items[tag.item];
-    const int nt = it.tile_end - it.tile_begin;
+    const int nt = tag.nt;
     const int t = tag.t, g0 = tag.g * FG;
     const int fg_n = min(FG, a.F - g0);
     if (t == 0)
@@ -347,23 +350,26 @@ __global__ void __launch_bounds__((kRunWarps + NP) * 32, 1) k_runs(RunArgs a) {
       for (int rs = 0; rs <= G - L; ++rs) {
         const int jb = max((int)rp[rs], j0), je = min((int)rp[rs + 1], j1);
         int j = jb;
-        // two records per iteration: both loads in flight before the conversions and FMAs
-        for (; j + 1 < je; j += 2) {
-          float v0[FPL], v1[FPL], w0[L], w1[L];
-          staged_values<kU16, FPL, FG>(s_val, lcol[j], lane, v0);
-          staged_values<kU16, FPL, FG>(s_val, lcol[j + 1], lane, v1);
-          load_weights<L>(wts + (size_t)j * L, w0);
-          load_weights<L>(wts + (size_t)(j + 1) * L, w1);
+        // kRecBatch records per iteration: all their loads in flight before the
+        // conversions and FMAs
+        for (; j + kRecBatch - 1 < je; j += kRecBatch) {
+          uint32_t uu[kRecBatch];
 #pragma unroll
-          for (int q = 0; q < L; ++q)
+          for (int r = 0; r < kRecBatch; ++r) uu[r] = lcol[j + r];
+          float vv[kRecBatch][FPL], ww[kRecBatch][L];
 #pragma unroll
-            for (int p = 0; p < FPL; ++p) acc[rs + q][p] = fmaf(w0[q], v0[p], acc[rs + q][p]);
+          for (int r = 0; r < kRecBatch; ++r) {
+            staged_values<kU16, FPL, FG>(s_val, uu[r], lane, vv[r]);
+            load_weights<L>(wts + (size_t)(j + r) * L, ww[r]);
+          }
 #pragma unroll
-          for (int q = 0; q < L; ++q)
+          for (int r = 0; r < kRecBatch; ++r)
 #pragma unroll
-            for (int p = 0; p < FPL; ++p) acc[rs + q][p] = fmaf(w1[q], v1[p], acc[rs + q][p]);
+            for (int q = 0; q < L; ++q)
+#pragma unroll
+              for (int p = 0; p < FPL; ++p) acc[rs + q][p] = fmaf(ww[r][q], vv[r][p], acc[rs + q][p]);
         }
-        if (j < je) {
+        for (; j < je; ++j) {
           float v0[FPL], w0[L];
           staged_values<kU16, FPL, FG>(s_val, lcol[j], lane, v0);
           load_weights<L>(wts + (size_t)j * L, w0);
@@ -373,7 +379,7 @@ __global__ void __launch_bounds__((kRunWarps + NP) * 32, 1) k_runs(RunArgs a) {
             for (int p = 0; p < FPL; ++p) acc[rs + q][p] = fmaf(w0[q], v0[p], acc[rs + q][p]);
         }
       }
-      // unit partials to their own buffer: the slot can be refilled during the combine
+      // unit partials
 #pragma unroll
       for (int i = 0; i < G; ++i) {
         float *d = s_part + ((size_t)warp * G + i) * FG + lane * FPL;
@@ -381,55 +387,36 @@ __global__ void __launch_bounds__((kRunWarps + NP) * 32, 1) k_runs(RunArgs a) {
         else d[0] = acc[i][0];
       }
     }
-    // the strip table, the scales and the header go to registers / private smem before
-    // the slot is handed back
-    uint32_t stp[NC];
-#pragma unroll
-    for (int q = 0; q < NC; ++q) stp[q] = strips[q];
-    for (int i = tid; i < h.nb; i += NCT) {
-      s_sc[i] = scale[i];
-      s_sc[nbp + i] = lw[i];
-    }
-    nb_sync(1, NCT);                     // partials, scales written; slot b no longer read
-    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-    nb_arrive(4 + b, NALL);              // hand slot b back to the producers
+    nb_sync(1, NCT);                     // unit partials written; staging of slot b consumed
 
-    // ---- combine (fixed unit order): warp per row, lanes = frames; sums into registers
-    // first, since the bin results overwrite the partials
-    float v[MAXR][NC][FPL];
-#pragma unroll
-    for (int ri = 0; ri < MAXR; ++ri) {
-      const int i = warp + ri * NC;
-#pragma unroll
-      for (int s = 0; s < NC; ++s) {
-#pragma unroll
-        for (int p = 0; p < FPL; ++p) v[ri][s][p] = 0.0f;
-        if (i < h.n_rows && s < ns) {
-          const int u0 = stp[s] & 0xFFFF, nu = stp[s] >> 16;
-          for (int kk = 0; kk < nu; ++kk) {
-            const float *src = s_part + ((size_t)(u0 + kk) * G + i) * FG + lane * FPL;
-#pragma unroll
-            for (int p = 0; p < FPL; ++p) v[ri][s][p] += src[p];
-          }
-        }
-      }
-    }
-    nb_sync(1, NCT);                     // partials read
-#pragma unroll
-    for (int ri = 0; ri < MAXR; ++ri) {
-      const int i = warp + ri * NC;
-      if (i >= h.n_rows) continue;
+    // ---- combine (fixed unit order), scale, lineout partials: warp per row, lanes = frames;
+    // the bin results go to slot b's staging area, which the record loop no longer reads
+    float *s_out = (float *)(smem + b * a.slot_bytes + a.off_val);   // [FG][nbp]
+    for (int i = warp; i < h.n_rows; i += NC) {
       double saw[FPL], ssm[FPL];
 #pragma unroll
       for (int p = 0; p < FPL; ++p) saw[p] = ssm[p] = 0.0;
+      for (int s = 0; s < ns; ++s) {
+        const uint32_t st = strips[s];
+        const int u0 = st & 0xFFFF, nu = st >> 16;
+        float v[FPL];
 #pragma unroll
-      for (int s = 0; s < NC; ++s) {
-        if (s >= ns) continue;
+        for (int p = 0; p < FPL; ++p) v[p] = 0.0f;
+        for (int kk = 0; kk < nu; ++kk) {
+          const float *src = s_part + ((size_t)(u0 + kk) * G + i) * FG + lane * FPL;
+          if constexpr (FPL == 2) {
+            const float2 t2 = *(const float2 *)src;
+            v[0] += t2.x;
+            v[1] += t2.y;
+          } else {
+            v[0] += src[0];
+          }
+        }
         const int bb = i * ns + s;
-        const float sc = s_sc[bb], l = s_sc[nbp + bb];
+        const float sc = scale[bb], l = lw[bb];
 #pragma unroll
         for (int p = 0; p < FPL; ++p) {
-          const float o = v[ri][s][p] * sc;
+          const float o = v[p] * sc;
           s_out[(lane * FPL + p) * nbp + bb] = o;
           saw[p] += (double)o * (double)l;
           ssm[p] += (l > 0.0f) ? (double)o : 0.0;
@@ -461,14 +448,18 @@ __global__ void __launch_bounds__((kRunWarps + NP) * 32, 1) k_runs(RunArgs a) {
     }
     if (t == nt - 1 && a.want_lo) {
       for (int f = warp; f < fg_n; f += NC)
-        for (int r = lane; r < it.n_rows; r += 32) {
+        for (int r = lane; r < tag.n_rows; r += 32) {
           const double *src = s_lo + ((size_t)r * FG + f) * 2;
-          double *dst = a.partial + (((int64_t)(g0 + f) * a.n_r + it.r0 + r) * a.n_slots + it.slot) * 2;
+          double *dst = a.partial + (((int64_t)(g0 + f) * a.n_r + tag.r0 + r) * a.n_slots + tag.slot) * 2;
           dst[0] = src[0];
           dst[1] = src[1];
         }
     }
-    nb_sync(1, NCT);                     // s_out / s_lo free for the next step
+    // this warp is done with slot b (blob, bin results): hand it back to the producers, whose
+    // bulk copies (async proxy) will overwrite the bin results written here
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    nb_arrive(4 + b, NALL);
+    nb_sync(1, NCT);                     // s_lo / s_part free for the next step
   }
 }
 
@@ -476,7 +467,7 @@ template <typename T, int G, int L, bool XC, int NP>
 static int launch_runs_t(Plan *p, RunArgs &a, cudaStream_t s) {
   const size_t smem = runs_smem_layout(a.blob_cap, std::max(p->max_u, 1), a.nbp, a.rows_max, G,
                                        runs_frames_per_group(sizeof(T), G), &a.off_val, &a.slot_bytes, &a.off_part,
-                                       &a.off_sc, &a.off_lo, &a.off_bar);
+                                       &a.off_lo, &a.off_bar);
   int dev_smem = 0;
   MI_CUDA(cudaDeviceGetAttribute(&dev_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, p->device));
   if (smem + 64 > (size_t)dev_smem)
