@@ -324,9 +324,15 @@ def main_ours(args):
     mean_step_s = sum(step_ms) / len(step_ms) / 1e3
     achieved = alg / mean_step_s / 1e9
     ref_bytes = map_bytes + F * (info["ref_pixels"] * 2 + w.n_r * w.n_eta * 4)
+    # DRAM bytes (read + write) of the batch's kernels from the committed ncu capture of this
+    # workload at F = 128 (profiles/k_runs_xc_sweep2880_f128.md); other shapes: not captured
+    traffic = None
+    if w.name.startswith("sweep_2880") and F == 128 and info["xc_pixels"] > 0:
+        traffic = {"bytes_per_step": int(0.840295e9 + 0.761555e9 + 1.830098e9 + 1.170938e9),
+                   "kernels": "k_xc + k_runs", "source": "ncu dram__bytes_read.sum + dram__bytes_write.sum"}
     roofline = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
-                "frac": round(achieved / peak, 4), "traffic": None, "peak_kind": peak_kind,
-                "alg_bytes_per_launch": alg,
+                "frac": round(achieved / peak, 4), "traffic": traffic, "peak_kind": peak_kind,
+                "alg_bytes_per_launch": alg, "scope": "whole batch: k_xc + k_runs + k_lineout (k_runs 88 %)",
                 "achieved_touched_bytes": round(ref_bytes / mean_step_s / 1e9, 1)}
 
     out = {"metric": METRIC, "value": round(value, 1), "unit": UNIT, "n_gpus": world, "steps": args.steps,
