@@ -52,6 +52,7 @@ def parse():
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-check", action="store_true")
+    ap.add_argument("--no-fit", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--serve-seconds", type=float, default=8.0,
                     help="duration of the 6-stream serving load (0 = skip)")
@@ -373,6 +374,11 @@ def main_ours(args):
     if not args.no_e2e:
         out["e2e"] = e2e_rate(plan, frames, F, args, w, dev, world)
 
+    # ---- ring fits of every resident frame: all rings in one launch, PV and TCH
+    fit_sample = None
+    if not args.no_fit:
+        out["fits"], fit_sample = fit_bench(plan, frames, w, F, dev)
+
     # ---- serving load: six streams with different maps, Poisson arrivals (rank 0, N = 1)
     served = []
     if rank == 0 and world == 1 and args.serve_seconds > 0:
@@ -404,6 +410,9 @@ def main_ours(args):
                 out["accuracy_vs_reference_integrator"] = ic
             if served:
                 out["serving"]["lineout_max_rel_vs_fp64_oracle"] = served_accuracy(served)
+            if fit_sample is not None:
+                for model, acc in fit_accuracy(fit_sample).items():
+                    out["fits"][model].update(acc)
     if rank == 0:
         print(json.dumps(out), flush=True)
     plan.close()
@@ -536,6 +545,74 @@ def serving_load(args, dev, plain=False, n_distinct=8):
     del streams
     torch.cuda.empty_cache()
     return out, served
+
+
+FIT_HALF_WINDOW = 60   # bins: +-15 px at RBin 0.25 px, 121 samples per window
+
+
+def fit_bench(plan, frames, w, F, dev, reps=5):
+    """Area-weighted lineouts of every resident frame, then every ring of every frame fitted
+    in one launch of the batched LM fitter (kernel d), pseudo-Voigt and TCH.  Returns the
+    timing / iteration summary and a sample of windows for the FP64 check of the CPU leg."""
+    import numpy as np
+    import torch
+
+    from midas_b200 import peakfit, synth
+
+    n = frames.shape[0]
+    lo = torch.empty((n, w.n_r), dtype=torch.float64, device=dev)
+    sm = torch.empty((F, w.n_r), dtype=torch.float64, device=dev)
+    for s0 in range(0, n, F):
+        k = min(F, n - s0)
+        plan.integrate(frames[s0:s0 + k], cake=False, out={"lineout_aw": lo[s0:s0 + k], "lineout_sm": sm[:k]})
+    x = torch.from_numpy(synth.r_centres(w)).to(dev)
+    peaks = torch.from_numpy(synth.ring_peaks(w, FIT_HALF_WINDOW)).to(dev)
+    stream = torch.cuda.current_stream()
+    res, params = {}, {}
+    for model in ("pv", "tch"):
+        kw = dict(model=model, half_window=FIT_HALF_WINDOW, x_bin=w.mapper.RBinSize, max_iter=100,
+                  px_um=w.mapper.px, lsd_um=w.mapper.Lsd)
+        r = peakfit.fit_batch(x, lo, peaks, **kw)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(reps):
+            r = peakfit.fit_batch(x, lo, peaks, **kw)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / reps
+        it = r.iters.cpu().numpy().reshape(-1)
+        edges = [0, 5, 10, 15, 20, 30, 50, 100, 101]
+        hist = np.histogram(np.clip(it, 0, 100), bins=edges)[0]
+        res[model] = {"fits_per_launch": int(it.size), "ms_per_launch": round(ms, 4),
+                      "fits_per_s": round(it.size / (ms / 1e3), 1), "frames": int(n), "rings": int(peaks.numel()),
+                      "window_samples": 2 * FIT_HALF_WINDOW + 1,
+                      "iterations_hist": {f"{edges[i]}-{edges[i + 1] - 1}": int(hist[i]) for i in range(len(hist))},
+                      "iterations_mean": round(float(it[it >= 0].mean()), 2)}
+        params[model] = r.params[:16].cpu().numpy()
+    sample = (synth.r_centres(w), lo[:16].cpu().numpy(), peaks.cpu().numpy(), w, params)
+    return res, sample
+
+
+def fit_accuracy(sample):
+    """FP64 CPU fits (oracle twin of the device LM) of the first 16 frames' windows: largest
+    centre and FWHM differences of the device fits, in px."""
+    import numpy as np
+    import oracle
+    x, lo, peaks, w, params = sample
+    out = {}
+    for mi, model in enumerate(("pv", "tch")):
+        got = params[model]
+        dc, dfw = [], []
+        for f in range(got.shape[0]):
+            for k, c in enumerate(peaks):
+                ref, _ = oracle.fit(x, lo[f], c, half_window=FIT_HALF_WINDOW, model=mi, max_iter=500,
+                                    x_bin=w.mapper.RBinSize, px_um=w.mapper.px, lsd_um=w.mapper.Lsd)
+                dc.append(abs(got[f, k, 1] - ref[1]))
+                dfw.append(abs(got[f, k, 4] - ref[4]))
+        out[model] = {"center_max_abs_err_px_vs_fp64": float(np.max(dc)),
+                      "fwhm_max_abs_err_px_vs_fp64": float(np.max(dfw)), "windows_checked": len(dc)}
+    return out
 
 
 def e2e_rate(plan, frames, F, args, w, dev, world):
