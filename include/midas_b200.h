@@ -137,6 +137,29 @@ int mi_plan_create(const mi_map_desc *map, const mi_plan_opts *opts, int device,
  * The reference subtracts (float)raw - dark[pixel] (IntegratorFitPeaksGPUStream.cu:1156). */
 int mi_plan_set_dark(mi_plan *plan, const float *dark_host);
 int mi_plan_get_info(const mi_plan *plan, mi_plan_info *info);
+
+/* ---- panels: several detectors, one binning, one merged cake ---------------------------
+ * Replaces the per-panel integrate-then-merge of multi-detector setups (one
+ * integrate() + profile_1d() per detector, packages/midas_integrate/midas_integrate/
+ * kernels.py:416,567, and one IntegratorFitPeaksGPUStream per detector).  Each panel has
+ * its own map (geometry, beam centre, mask, dtype) over the SAME n_r x n_eta bins (R or
+ * Q binning).  A bin of the merged cake is the sum of all panels' weighted pixels over
+ * the sum of their areas: one concatenated weight list, as if the panels were one
+ * detector.  The panels' rows are stacked into a virtual detector as wide as the widest
+ * panel (panel i: rows z_off_i .. z_off_i + nz_i - 1, z_off_i = nz_0 + .. + nz_{i-1}).
+ * The plan uses the run encoding (tile_rows <= 16).  mi_integrate_batch and
+ * mi_integrate_plain reject panel plans.                                              */
+int mi_plan_create_panels(const mi_map_desc *maps, int n_panels, const mi_plan_opts *opts,
+                          int device, mi_plan **out);
+/* One dark per panel (ny_i*nz_i floats, host pointers; NULL entries = no dark). */
+int mi_plan_set_dark_panels(mi_plan *plan, const float *const *darks_host);
+/* F frames of every panel (device pointers, panel i frame f at frames[i] + f*strides[i]
+ * elements of dtypes[i]; types may differ between panels) -> merged cake [F][n_r][n_eta]
+ * and lineouts, like mi_integrate_batch.  Kernel (a) transposes each panel's frames into
+ * the plan's pixel-major buffer, then one launch of kernel (b) cakes all panels. */
+int mi_integrate_panels(mi_plan *plan, const void *const *frames, const int *dtypes,
+                        const int64_t *strides, int n_frames, float *cake, double *lineout_aw,
+                        double *lineout_sm, void *stream);
 /* Device-side status of the plan's launches so far: the plan's error word (MI_E_TIMEOUT
  * when a bounded in-kernel wait expired, else 0), which is then cleared.  Synchronises
  * the plan's device. */

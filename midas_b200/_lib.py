@@ -94,6 +94,12 @@ SIGNATURES = [
     ("mi_plan_create", C.c_int, [C.POINTER(MiMapDesc), C.POINTER(MiPlanOpts), C.c_int,
                                  C.POINTER(C.c_void_p)]),
     ("mi_plan_set_dark", C.c_int, [C.c_void_p, C.c_void_p]),
+    ("mi_plan_create_panels", C.c_int, [C.POINTER(MiMapDesc), C.c_int, C.POINTER(MiPlanOpts), C.c_int,
+                                        C.POINTER(C.c_void_p)]),
+    ("mi_plan_set_dark_panels", C.c_int, [C.c_void_p, C.POINTER(C.c_void_p)]),
+    ("mi_integrate_panels", C.c_int, [C.c_void_p, C.POINTER(C.c_void_p), C.POINTER(C.c_int),
+                                      C.POINTER(C.c_int64), C.c_int, C.c_void_p, C.c_void_p, C.c_void_p,
+                                      C.c_void_p]),
     ("mi_plan_get_info", C.c_int, [C.c_void_p, C.POINTER(MiPlanInfo)]),
     ("mi_plan_bytes", C.c_int, [C.c_void_p, C.POINTER(C.c_size_t)]),
     ("mi_plan_status", C.c_int, [C.c_void_p, C.POINTER(C.c_int)]),

@@ -321,8 +321,19 @@ static int launch_fpl(Plan *p, CakeArgs &a, cudaStream_t s) {
   return set_error(MI_E_ARG, "bad frames_per_lane");
 }
 
+int launch_lineout(Plan *p, int n_frames, double *lo_aw, double *lo_sm, cudaStream_t s) {
+  const int64_t n = (int64_t)n_frames * p->n_r;
+  if (n == 0) return MI_OK;
+  k_lineout<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(p->d_partial, n_frames, p->n_r, p->n_slots, p->d_den_aw,
+                                                        p->d_cnt, lo_aw, lo_sm);
+  MI_CUDA(cudaGetLastError());
+  return MI_OK;
+}
+
 int launch_cake(Plan *p, const void *frames, int dtype, int n_frames, int64_t stride, float *cake,
                 double *lo_aw, double *lo_sm, cudaStream_t s) {
+  if (p->panels.size() > 1)
+    return set_error(MI_E_ARG, "a panel plan takes its frames per panel: use mi_integrate_panels");
   CakeArgs a;
   a.items = p->d_items;
   a.tiles = p->d_tiles;
@@ -359,13 +370,7 @@ int launch_cake(Plan *p, const void *frames, int dtype, int n_frames, int64_t st
     default: return set_error(MI_E_ARG, "unknown dtype %d", dtype);
   }
   if (rc) return rc;
-  if (a.want_lo) {
-    const int64_t n = (int64_t)n_frames * p->n_r;
-    k_lineout<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(a.partial, n_frames, p->n_r, p->n_slots, p->d_den_aw,
-                                                          p->d_cnt, lo_aw, lo_sm);
-    MI_CUDA(cudaGetLastError());
-  }
-  return MI_OK;
+  return a.want_lo ? launch_lineout(p, n_frames, lo_aw, lo_sm, s) : MI_OK;
 }
 
 }  // namespace mi

@@ -200,15 +200,19 @@ struct TileLimits {
   int item_cols; // eta columns per work item
 };
 
-// Pixel-major staging of 8/16-bit frames for the run kernel.  The referenced pixels
-// of each detector row are covered by one span [span_lo, span_lo + len) with both ends
-// on 8-pixel boundaries (len may end at ny when ny is not a multiple of 8); the spans,
-// concatenated row by row, give the compact pixel index c.  Kernel (a) writes
-// xc[c][f] (u16, kXcFrames * kXcGroups frames per compact pixel), so a tile stages each
-// of its pixels, one frame group at a time, with one 128-byte bulk copy.  Transpose work
-// is cut into chunks of <= kXcChunk pixels of one span.
-constexpr int kXcFrames = 64;   // frames of one group (one 128-byte staged row)
-constexpr int kXcGroups = 2;    // groups held per launch
+// Pixel-major staging for the run kernel.  The referenced pixels of each detector row
+// are covered by one span [span_lo, span_lo + len) with both ends on 8-pixel boundaries
+// (len may end at ny when ny is not a multiple of 8); the spans, concatenated row by row,
+// give the compact pixel index c.  Kernel (a) writes kXcRowBytes per compact pixel:
+// 8/16-bit frames as u16 (128 frames, groups of 64), other frame types as fp32 with the
+// dark already subtracted (64 frames, groups of 32), so a tile stages each of its pixels,
+// one frame group at a time, with one 128-byte bulk copy.  Transpose work is cut into
+// chunks of <= kXcChunk pixels of one span.
+constexpr int kXcFrames = 64;      // u16 frames of one group (one 128-byte staged row)
+constexpr int kXcGroups = 2;       // u16 groups held per launch
+constexpr int kXcFramesF = 32;     // fp32 frames of one group
+constexpr int kXcGroupsF = 2;      // fp32 groups held per launch
+constexpr int kXcRowBytes = 256;   // bytes per compact pixel
 constexpr int kXcChunk = 256;
 struct XcChunk {
   int32_t z, y0, n, c0;  // detector row, first column, pixels, compact index of the first
@@ -251,7 +255,15 @@ struct Plan {
   int32_t *d_row_off = nullptr;  // per detector row: compact index of the span start
   XcChunk *d_xchunks = nullptr;
   int n_xchunks = 0;
-  uint16_t *d_xc = nullptr;      // [n_xc][kXcFrames * kXcGroups]
+  uint8_t *d_xc = nullptr;       // [n_xc][kXcRowBytes]
+
+  // panels (a plan over several detectors sharing one binning): panel p's rows are rows
+  // [z_off, z_off + nz) of a virtual detector ny pixels wide (ny = the widest panel)
+  struct Panel {
+    int ny, nz, z_off;
+    int chunk_begin, chunk_end;  // its transpose chunks
+  };
+  std::vector<Panel> panels;     // one entry for an ordinary plan
 
   // plain (reference-layout) path
   int32_t *d_nmap = nullptr;     // {count, offset} per bin
@@ -274,7 +286,14 @@ int launch_runs(Plan *p, const void *frames, int dtype, int n_frames, int64_t st
                 cudaStream_t s);
 // true when launch_runs stages this dtype through the pixel-major buffer
 bool runs_uses_xc(const Plan *p, int dtype);
-int launch_xc(Plan *p, const void *frames, int dtype, int F, int64_t stride, cudaStream_t s);
+// Transpose frames [0, F) of panel `panel` into the pixel-major buffer: u16 rows when
+// `as_f32` is false (8/16-bit frames, F <= 128), else fp32 rows minus the dark (F <= 64).
+int launch_xc(Plan *p, int panel, const void *frames, int dtype, int F, int64_t stride, bool as_f32,
+              cudaStream_t s);
+// Caking of frames [0, F) (F <= 128 u16 / 64 fp32) already staged pixel-major.
+int launch_runs_staged(Plan *p, bool as_f32, int F, float *cake, double *partial, bool want_lo, cudaStream_t s);
+// kernel (c): lineouts of frames [0, n_frames) from the plan's partial sums
+int launch_lineout(Plan *p, int n_frames, double *lo_aw, double *lo_sm, cudaStream_t s);
 int launch_plain(Plan *p, const void *frame, int dtype, double *cake, double *lo_aw,
                  double *lo_sm, cudaStream_t s);
 int launch_cast(const void *frames, int dtype, int64_t n_pixels, int n_frames,

@@ -544,7 +544,10 @@ static int upload(T **dst, const T *src, size_t n, size_t *acct) {
   return MI_OK;
 }
 
-static int build_plan(const mi_map_desc &m, const mi_plan_opts &o, Plan *p) {
+// Build a plan.  `pre` (optional) is the weight list already built for the whole detector
+// (panel plans: the panels' lists merged over the virtual detector); `m` then describes the
+// virtual detector and carries no records, and the plain path is not built.
+static int build_plan(const mi_map_desc &m, const mi_plan_opts &o, Plan *p, HostCSR *pre = nullptr) {
   p->mode = o.mode;
   p->normalize = o.normalize ? 1 : 0;
   p->semantics = o.semantics;
@@ -559,8 +562,10 @@ static int build_plan(const mi_map_desc &m, const mi_plan_opts &o, Plan *p) {
   const int64_t n_pix = (int64_t)m.ny * m.nz;
 
   HostCSR csr;
-  int rc = build_host_csr(m, o.mode, o.semantics, &csr);
-  if (rc) return rc;
+  int rc = MI_OK;
+  if (pre) csr = std::move(*pre);
+  else if ((rc = build_host_csr(m, o.mode, o.semantics, &csr))) return rc;
+  if (p->panels.empty()) p->panels.push_back({m.ny, m.nz, 0, 0, 0});
   p->nnz = (int64_t)csr.col.size();
   p->oob = csr.oob;
 
@@ -714,19 +719,25 @@ static int build_plan(const mi_map_desc &m, const mi_plan_opts &o, Plan *p) {
       if (!seen[c]) { seen[c] = 1; ++n; }
     p->ref_pixels = n;
     if (p->encoding == MI_ENC_RUNS && runs_frames_per_group(2, p->run_g) == kXcFrames) {
+      size_t pi = 0;
       for (int z = 0; z < m.nz; ++z) {
+        // chunks are made row by row, so each panel's chunks are one contiguous range
+        while (pi + 1 < p->panels.size() && z >= p->panels[pi + 1].z_off) ++pi;
+        if (z == p->panels[pi].z_off) p->panels[pi].chunk_begin = (int)xchunks.size();
         const uint8_t *row = seen.data() + (int64_t)z * m.ny;
         int lo = 0, hi = m.ny;
         while (lo < m.ny && !row[lo]) ++lo;
         while (hi > lo && !row[hi - 1]) --hi;
         lo &= ~7;
-        if (hi > lo) hi = std::min(m.ny, (hi + 7) & ~7);
+        // the panel's own width bounds the span: the transpose reads the panel's frame rows
+        if (hi > lo) hi = std::min(p->panels[pi].ny, (hi + 7) & ~7);
         else hi = lo;
         span_lo[z] = lo;
         row_off[z] = (int32_t)n_xc;
         for (int y = lo; y < hi; y += kXcChunk)
           xchunks.push_back({z, y, std::min(kXcChunk, hi - y), (int32_t)(n_xc + (y - lo))});
         n_xc += hi - lo;
+        p->panels[pi].chunk_end = (int)xchunks.size();
       }
     }
   }
@@ -777,8 +788,9 @@ static int build_plan(const mi_map_desc &m, const mi_plan_opts &o, Plan *p) {
     p->n_xchunks = (int)xchunks.size();
   }
 
+  if ((rc = upload(&p->d_area_in, csr.area_in.data(), csr.area_in.size(), &acct))) return rc;
   // ---- plain path: reference SoA layout (PrecomputeOffsets_kernel, …Stream.cu:901-924)
-  {
+  if (!pre) {
     const int64_t nrec = m.n_records;
     std::vector<int32_t> off(nrec);
     std::vector<float> w(nrec), aw(nrec), dr(nrec), py(nrec), pz(nrec);
@@ -817,7 +829,6 @@ static int build_plan(const mi_map_desc &m, const mi_plan_opts &o, Plan *p) {
     if ((rc = upload(&p->d_dr, dr.data(), dr.size(), &acct))) return rc;
     if ((rc = upload(&p->d_py, py.data(), py.size(), &acct))) return rc;
     if ((rc = upload(&p->d_pz, pz.data(), pz.size(), &acct))) return rc;
-    if ((rc = upload(&p->d_area_in, csr.area_in.data(), csr.area_in.size(), &acct))) return rc;
     if ((rc = upload(&p->d_area_all, area_all.data(), area_all.size(), &acct))) return rc;
     MI_CUDA(cudaMalloc((void **)&p->d_plain_img, n_pix * sizeof(float)));
     acct += n_pix * sizeof(float);
@@ -874,6 +885,119 @@ int mi_plan_create(const mi_map_desc *map, const mi_plan_opts *opts, int device,
   }
   *out = p;
   return MI_OK;
+}
+
+int mi_plan_create_panels(const mi_map_desc *maps, int n_panels, const mi_plan_opts *opts, int device,
+                          mi_plan **out) {
+  if (!maps || !out || n_panels < 1) return set_error(MI_E_ARG, "mi_plan_create_panels: null argument or no panels");
+  *out = nullptr;
+  int ny_v = 0;
+  int64_t nz_v = 0, n_rec = 0;
+  for (int i = 0; i < n_panels; ++i) {
+    const mi_map_desc &m = maps[i];
+    if (m.n_r != maps[0].n_r || m.n_eta != maps[0].n_eta)
+      return set_error(MI_E_ARG, "mi_plan_create_panels: panel %d has %d x %d bins, panel 0 %d x %d", i, m.n_r,
+                       m.n_eta, maps[0].n_r, maps[0].n_eta);
+    if (m.n_r <= 0 || m.n_eta <= 0 || m.ny < 2 || m.nz < 2)
+      return set_error(MI_E_ARG, "mi_plan_create_panels: panel %d has a bad shape", i);
+    if (!m.nmap || (m.n_records > 0 && !m.records))
+      return set_error(MI_E_ARG, "mi_plan_create_panels: panel %d has null map arrays", i);
+    ny_v = std::max(ny_v, m.ny);
+    nz_v += m.nz;
+    n_rec += m.n_records;
+  }
+  if ((int64_t)ny_v * nz_v > (int64_t)INT32_MAX)
+    return set_error(MI_E_RANGE, "mi_plan_create_panels: panels hold more than 2^31 pixels");
+  mi_plan_opts o{};
+  if (opts) o = *opts;
+  else { o.mode = MI_MODE_FLOOR; o.normalize = 1; o.semantics = MI_SEM_PY; }
+  if (o.mode < 0 || o.mode > 2 || o.semantics < 0 || o.semantics > 2 ||
+      (o.semantics == MI_SEM_IC && o.mode == MI_MODE_FLOOR))
+    return set_error(MI_E_ARG, "mi_plan_create_panels: bad mode %d / semantics %d", o.mode, o.semantics);
+  if (o.encoding == MI_ENC_CSR || o.tile_rows > 16)
+    return set_error(MI_E_UNSUPPORTED, "mi_plan_create_panels: panel plans use the run encoding with tile_rows <= 16");
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
+    return set_error(MI_E_CUDA, "mi_plan_create_panels: no CUDA device available");
+  if (device < 0 || device >= ndev) return set_error(MI_E_ARG, "mi_plan_create_panels: bad device %d", device);
+  // each panel's weights with its own geometry, then merged over the virtual detector:
+  // panel i's pixel (z, y) is virtual pixel (z_off_i + z) * ny_v + y; a bin's terms are
+  // panel 0's, then panel 1's, ... (ascending virtual index); areas add up
+  const int64_t n_bins = (int64_t)maps[0].n_r * maps[0].n_eta;
+  std::vector<HostCSR> part(n_panels);
+  std::vector<Plan::Panel> geo(n_panels);
+  int z_off = 0;
+  for (int i = 0; i < n_panels; ++i) {
+    int rc = build_host_csr(maps[i], o.mode, o.semantics, &part[i]);
+    if (rc) return rc;
+    geo[i] = {maps[i].ny, maps[i].nz, z_off, 0, 0};
+    z_off += maps[i].nz;
+  }
+  HostCSR csr;
+  csr.row_ptr.assign(n_bins + 1, 0);
+  csr.area_in.assign(n_bins, 0.0);
+  csr.area_norm.assign(n_bins, 0.0);
+  for (int64_t b = 0; b < n_bins; ++b) {
+    int64_t c = 0;
+    for (int i = 0; i < n_panels; ++i) {
+      c += part[i].row_ptr[b + 1] - part[i].row_ptr[b];
+      csr.area_in[b] += part[i].area_in[b];
+      csr.area_norm[b] += part[i].area_norm[b];
+    }
+    csr.row_ptr[b + 1] = csr.row_ptr[b] + c;
+  }
+  csr.col.resize(csr.row_ptr[n_bins]);
+  csr.w.resize(csr.row_ptr[n_bins]);
+#pragma omp parallel for schedule(dynamic, 4096)
+  for (int64_t b = 0; b < n_bins; ++b) {
+    int64_t o2 = csr.row_ptr[b];
+    for (int i = 0; i < n_panels; ++i)
+      for (int64_t j = part[i].row_ptr[b]; j < part[i].row_ptr[b + 1]; ++j, ++o2) {
+        const int32_t c = part[i].col[j];
+        const int32_t z = c / geo[i].ny, y = c - z * geo[i].ny;
+        csr.col[o2] = (int32_t)((int64_t)(geo[i].z_off + z) * ny_v + y);
+        csr.w[o2] = part[i].w[j];
+      }
+  }
+  for (int i = 0; i < n_panels; ++i) csr.oob += part[i].oob;
+  std::vector<HostCSR>().swap(part);
+  mi_map_desc vm{};
+  vm.records = nullptr;
+  vm.n_records = n_rec;
+  vm.nmap = nullptr;
+  vm.n_r = maps[0].n_r;
+  vm.n_eta = maps[0].n_eta;
+  vm.ny = ny_v;
+  vm.nz = (int32_t)nz_v;
+  mi_plan *p = new (std::nothrow) mi_plan();
+  if (!p) return set_error(MI_E_OOM, "mi_plan_create_panels: host allocation failed");
+  p->device = device;
+  p->panels = geo;
+  int prev = 0;
+  cudaGetDevice(&prev);
+  int rc = build_plan(vm, o, p, &csr);
+  cudaSetDevice(prev);
+  if (rc == MI_OK && p->n_xc == 0)
+    rc = set_error(MI_E_UNSUPPORTED, "mi_plan_create_panels: the plan has no pixel-major staging");
+  if (rc) {
+    free_plan_mem(p);
+    delete p;
+    return rc;
+  }
+  *out = p;
+  return MI_OK;
+}
+
+int mi_plan_set_dark_panels(mi_plan *p, const float *const *darks) {
+  if (!p || !darks) return set_error(MI_E_ARG, "mi_plan_set_dark_panels: null argument");
+  std::vector<float> v((size_t)p->ny * p->nz, 0.0f);
+  for (size_t i = 0; i < p->panels.size(); ++i) {
+    const Plan::Panel &pn = p->panels[i];
+    if (!darks[i]) continue;
+    for (int z = 0; z < pn.nz; ++z)
+      memcpy(v.data() + (size_t)(pn.z_off + z) * p->ny, darks[i] + (size_t)z * pn.ny, pn.ny * sizeof(float));
+  }
+  return mi_plan_set_dark(p, v.data());
 }
 
 int mi_plan_set_dark(mi_plan *p, const float *dark) {
@@ -941,6 +1065,8 @@ void mi_plan_destroy(mi_plan *p) {
 int mi_integrate_batch(mi_plan *p, const void *frames, int dtype, int n_frames, int64_t stride,
                        float *cake, double *lo_aw, double *lo_sm, void *stream) {
   if (!p || !frames) return set_error(MI_E_ARG, "mi_integrate_batch: null argument");
+  if (p->panels.size() > 1)
+    return set_error(MI_E_ARG, "mi_integrate_batch: a panel plan takes its frames per panel: use mi_integrate_panels");
   if (n_frames < 0) return set_error(MI_E_ARG, "mi_integrate_batch: n_frames < 0");
   if (dtype_size(dtype) == 0) return set_error(MI_E_ARG, "mi_integrate_batch: unknown dtype code %d", dtype);
   if (stride < (int64_t)p->ny * p->nz)
@@ -962,9 +1088,55 @@ int mi_integrate_batch(mi_plan *p, const void *frames, int dtype, int n_frames, 
   return rc;
 }
 
+int mi_integrate_panels(mi_plan *p, const void *const *frames, const int *dtypes, const int64_t *strides,
+                        int n_frames, float *cake, double *lo_aw, double *lo_sm, void *stream) {
+  if (!p || !frames || !dtypes || !strides) return set_error(MI_E_ARG, "mi_integrate_panels: null argument");
+  if (n_frames < 0) return set_error(MI_E_ARG, "mi_integrate_panels: n_frames < 0");
+  if (p->n_xc == 0)
+    return set_error(MI_E_UNSUPPORTED, "mi_integrate_panels: the plan has no pixel-major staging");
+  const int np = (int)p->panels.size();
+  bool as_f32 = false;
+  for (int i = 0; i < np; ++i) {
+    if (!frames[i] && n_frames > 0) return set_error(MI_E_ARG, "mi_integrate_panels: panel %d has no frames", i);
+    if (dtype_size(dtypes[i]) == 0)
+      return set_error(MI_E_ARG, "mi_integrate_panels: panel %d: unknown dtype code %d", i, dtypes[i]);
+    if (strides[i] < (int64_t)p->panels[i].ny * p->panels[i].nz)
+      return set_error(MI_E_ARG, "mi_integrate_panels: panel %d: frame_stride %lld < ny*nz", i,
+                       (long long)strides[i]);
+    if (!(dtypes[i] == MI_DT_U16 || dtypes[i] == MI_DT_U8)) as_f32 = true;
+  }
+  if (n_frames == 0 || (!cake && !lo_aw && !lo_sm)) return MI_OK;
+  int prev = 0;
+  cudaGetDevice(&prev);
+  if (prev != p->device) MI_CUDA(cudaSetDevice(p->device));
+  const cudaStream_t s = (cudaStream_t)stream;
+  const bool want_lo = lo_aw || lo_sm;
+  const int chunk = as_f32 ? kXcFramesF * kXcGroupsF : kXcFrames * kXcGroups;
+  int rc = MI_OK;
+  for (int g0 = 0; g0 < n_frames && rc == MI_OK; g0 += kMaxFramesPerLaunch) {
+    const int ng = std::min(kMaxFramesPerLaunch, n_frames - g0);
+    for (int f0 = 0; f0 < ng && rc == MI_OK; f0 += chunk) {
+      const int nf = std::min(chunk, ng - f0);
+      for (int i = 0; i < np && rc == MI_OK; ++i)
+        rc = launch_xc(p, i, (const uint8_t *)frames[i] + (size_t)(g0 + f0) * strides[i] * dtype_size(dtypes[i]),
+                       dtypes[i], nf, strides[i], as_f32, s);
+      if (rc == MI_OK)
+        rc = launch_runs_staged(p, as_f32, nf, cake ? cake + (size_t)(g0 + f0) * p->n_bins : nullptr,
+                                p->d_partial + (size_t)f0 * p->n_r * p->n_slots * 2, want_lo, s);
+    }
+    if (rc == MI_OK && want_lo)
+      rc = launch_lineout(p, ng, lo_aw ? lo_aw + (size_t)g0 * p->n_r : nullptr,
+                          lo_sm ? lo_sm + (size_t)g0 * p->n_r : nullptr, s);
+  }
+  if (prev != p->device) cudaSetDevice(prev);
+  return rc;
+}
+
 int mi_integrate_plain(mi_plan *p, const void *frame, int dtype, double *cake, double *lo_aw,
                        double *lo_sm, void *stream) {
   if (!p || !frame) return set_error(MI_E_ARG, "mi_integrate_plain: null argument");
+  if (p->panels.size() > 1 || !p->d_plain_img)
+    return set_error(MI_E_UNSUPPORTED, "mi_integrate_plain: a panel plan has no one-frame path");
   if (dtype_size(dtype) == 0) return set_error(MI_E_ARG, "mi_integrate_plain: unknown dtype code %d", dtype);
   if (p->semantics == MI_SEM_IC)
     return set_error(MI_E_UNSUPPORTED, "mi_integrate_plain: the one-frame GPU kernel follows the GPU stream "

@@ -19,10 +19,11 @@
 // one bulk copy (TMA) and stage its pixels into one of two slots; consumer warps run
 // the record loop, combine the unit partials in a fixed order (a frame's result never
 // depends on the rest of its batch), scale, reduce the lineouts, store the cake and
-// hand the slot back.  Staging of 8/16-bit frames comes from the
-// pixel-major buffer written by kernel (a) (mi_stage.cu): one 128-byte bulk copy per
-// pixel per 64-frame group; other frame types are gathered from frame-major memory.
-// The dark is subtracted at use, (float)raw - dark, the reference's arithmetic.
+// hand the slot back.  Staging comes from the pixel-major buffer written by kernel (a)
+// (mi_stage.cu): one 128-byte bulk copy per pixel and frame group (64 u16 frames with the
+// dark subtracted at use as (float)raw - dark, the reference's arithmetic; or 32 fp32
+// frames already dark-subtracted).  Plans without row spans (strips of 32 rows) gather
+// from frame-major memory.
 #include <stdint.h>
 
 #include <algorithm>
@@ -51,8 +52,9 @@ struct RunArgs {
   int *err;
   int n_items;
   int *counter;     // work-item claims of this launch (zero at launch)
-  // pixel-major staging (8/16-bit frames): xc[c * xc_pitch + f], c = row_off[z] + y - span_lo[z]
-  const uint16_t *xc;
+  // pixel-major staging: row of compact pixel c at xc + c * xc_pitch bytes, frame group g at
+  // byte 128 g of the row; c = row_off[z] + y - span_lo[z]
+  const uint8_t *xc;
   int64_t xc_pitch;
   const int32_t *span_lo, *row_off;
   int ny;
@@ -166,7 +168,8 @@ __global__ void __launch_bounds__((kRunWarps + NP) * 32, 1) k_runs(RunArgs a) {
   constexpr int NCT = NC * 32;
   constexpr int NPT = NP * 32;                       // producer threads
   constexpr int NALL = NCT + NPT;
-  static_assert(!XC || (kU16 && FG == kXcFrames), "pixel-major staging holds 64 u16 frames per group");
+  static_assert(!XC || (kU16 && FG == kXcFrames) || (!kU16 && FG == kXcFramesF),
+                "pixel-major staging holds 128-byte frame groups");
   extern __shared__ __align__(16) uint8_t smem[];
   float *s_part = (float *)(smem + a.off_part);      // [NC units][G][FG]
   double *s_lo = (double *)(smem + a.off_lo);        // [rows][FG][2]
@@ -249,20 +252,21 @@ __global__ void __launch_bounds__((kRunWarps + NP) * 32, 1) k_runs(RunArgs a) {
       if constexpr (XC) {
         // one 128-byte bulk copy per staged pixel from the pixel-major buffer (frame group g);
         // the staging barrier of slot b expects all of them before any is issued
+        constexpr uint32_t kRow = 128;
         if (ptid == 0)
           asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(r_smem(&bar[2 + b])),
-                       "r"((uint32_t)h.n_u * (uint32_t)(kXcFrames * 2))
+                       "r"((uint32_t)h.n_u * kRow)
                        : "memory");
         asm volatile("bar.sync 6, %0;" ::"r"(NPT) : "memory");
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-        const uint16_t *xg = a.xc + (size_t)g * kXcFrames;
+        const uint8_t *xg = a.xc + (size_t)g * kRow;
         for (int u = ptid; u < h.n_u; u += NPT) {
           const uint32_t pix = upix[u];
           const uint32_t z = pix / (uint32_t)a.ny;
           const uint32_t c = (uint32_t)__ldg(a.row_off + z) + (pix - z * (uint32_t)a.ny) - (uint32_t)__ldg(a.span_lo + z);
           uint8_t *row = s_val + (size_t)u * kRunPitch;
-          r_copy(row, xg + (size_t)c * a.xc_pitch, kXcFrames * 2, &bar[2 + b]);
-          *(float *)(row + kXcFrames * 2) = __ldg(a.dark + pix);   // beside the copied bytes
+          r_copy(row, xg + (size_t)c * a.xc_pitch, kRow, &bar[2 + b]);
+          if constexpr (kU16) *(float *)(row + kRow) = __ldg(a.dark + pix);   // beside the copied bytes
         }
         nb_arrive(2 + b, NALL);                       // copies issued, darks written
         continue;
@@ -495,7 +499,7 @@ static int launch_runs_gl(Plan *p, RunArgs &a, cudaStream_t s) {
   return set_error(MI_E_UNSUPPORTED, "run encoding with G=%d L=%d", G, L);
 }
 
-// pixel-major staging: 8/16-bit frames, 64-frame groups (G <= 16)
+// pixel-major staging (spans exist for G <= 16): u16 rows (8/16-bit frames) or fp32 rows
 template <typename T>
 static int launch_runs_xc(Plan *p, RunArgs &a, cudaStream_t s) {
   const int G = p->run_g, L = p->run_l;
@@ -506,15 +510,14 @@ static int launch_runs_xc(Plan *p, RunArgs &a, cudaStream_t s) {
   return set_error(MI_E_UNSUPPORTED, "pixel-major staging with G=%d L=%d", G, L);
 }
 
-int launch_runs(Plan *p, const void *frames, int dtype, int n_frames, int64_t stride, float *cake, bool want_lo,
-                cudaStream_t s) {
+static RunArgs run_args(Plan *p, float *cake, bool want_lo) {
   RunArgs a;
   a.items = p->d_items;
   a.tiles = p->d_tiles;
   a.blobs = p->d_blobs;
-  a.frames = frames;
-  a.stride = stride;
-  a.F = n_frames;
+  a.frames = nullptr;
+  a.stride = 0;
+  a.F = 0;
   a.dark = p->d_dark;
   a.cake = cake;
   a.partial = p->d_partial;
@@ -531,25 +534,38 @@ int launch_runs(Plan *p, const void *frames, int dtype, int n_frames, int64_t st
   a.n_items = p->n_items;
   a.counter = p->d_ctr;
   a.xc = p->d_xc;
-  a.xc_pitch = kXcFrames * kXcGroups;
+  a.xc_pitch = kXcRowBytes;
   a.span_lo = p->d_span_lo;
   a.row_off = p->d_row_off;
   a.ny = p->ny;
+  return a;
+}
+
+int launch_runs_staged(Plan *p, bool as_f32, int F, float *cake, double *partial, bool want_lo, cudaStream_t s) {
+  RunArgs a = run_args(p, cake, want_lo);
+  a.F = F;
+  a.partial = partial;
+  return as_f32 ? launch_runs_xc<float>(p, a, s) : launch_runs_xc<uint16_t>(p, a, s);
+}
+
+int launch_runs(Plan *p, const void *frames, int dtype, int n_frames, int64_t stride, float *cake, bool want_lo,
+                cudaStream_t s) {
+  RunArgs a = run_args(p, cake, want_lo);
+  a.frames = frames;
+  a.stride = stride;
+  a.F = n_frames;
   if (runs_uses_xc(p, dtype)) {
-    // kernel (a) transposes up to 128 frames into the pixel-major buffer, kernel (b) stages
+    // kernel (a) transposes a chunk of frames into the pixel-major buffer, kernel (b) stages
     // from it; the partial sums of frame f live at row f of the plan's scratch
+    const bool as_f32 = !(dtype == MI_DT_U16 || dtype == MI_DT_U8);
     const size_t es = dtype_size(dtype);
-    constexpr int kChunk = kXcFrames * kXcGroups;
-    for (int f0 = 0; f0 < n_frames; f0 += kChunk) {
-      const int nf = std::min(kChunk, n_frames - f0);
-      int rc = launch_xc(p, (const uint8_t *)frames + (size_t)f0 * stride * es, dtype, nf, stride, s);
+    const int chunk = as_f32 ? kXcFramesF * kXcGroupsF : kXcFrames * kXcGroups;
+    for (int f0 = 0; f0 < n_frames; f0 += chunk) {
+      const int nf = std::min(chunk, n_frames - f0);
+      int rc = launch_xc(p, 0, (const uint8_t *)frames + (size_t)f0 * stride * es, dtype, nf, stride, as_f32, s);
       if (rc) return rc;
-      RunArgs b = a;
-      b.F = nf;
-      b.frames = nullptr;
-      b.cake = cake ? cake + (size_t)f0 * p->n_bins : nullptr;
-      b.partial = p->d_partial + (size_t)f0 * p->n_r * p->n_slots * 2;
-      rc = dtype == MI_DT_U16 ? launch_runs_xc<uint16_t>(p, b, s) : launch_runs_xc<uint8_t>(p, b, s);
+      rc = launch_runs_staged(p, as_f32, nf, cake ? cake + (size_t)f0 * p->n_bins : nullptr,
+                              p->d_partial + (size_t)f0 * p->n_r * p->n_slots * 2, want_lo, s);
       if (rc) return rc;
     }
     return MI_OK;

@@ -209,6 +209,128 @@ class CakePlan:
         return aw, sm
 
 
+class PanelPlan:
+    """Device-resident plan over several detector panels that share one binning.
+
+    A bin of the merged cake is the sum of every panel's weighted pixels over the sum of
+    their areas (one weight list over all panels); each panel keeps its own map, shape,
+    beam centre, dark and frame type.  ``integrate`` takes one frame tensor per panel and
+    runs kernel (a) once per panel and kernel (b) once for all of them.
+
+    Args:
+        pixmaps: one ``bin_io.PixelMap`` per panel, all with n_r * n_eta bins.
+        shapes: (n_pixels_y, n_pixels_z) of each panel.
+        beam_centres: (bc_y, bc_z) of each panel (used by gradient mode).
+        n_r, n_eta, mode, normalize, semantics, device, tile_rows, tile_pixels, run_len:
+            as for ``CakePlan`` (run encoding, tile_rows <= 16).
+    """
+
+    def __init__(self, pixmaps, *, shapes, n_r: int, n_eta: int, beam_centres=None, mode: str = "floor",
+                 normalize: bool = True, semantics: str = "py", device="cuda", tile_rows: int = 0,
+                 tile_pixels: int = 0, run_len: int = 0):
+        n = len(pixmaps)
+        if n == 0 or len(shapes) != n or (beam_centres is not None and len(beam_centres) != n):
+            raise ValueError("one shape (and beam centre) per panel map is needed")
+        if mode not in L.MODE or semantics not in L.SEM:
+            raise ValueError(f"unknown mode {mode!r} or semantics {semantics!r}")
+        self.device = torch.device("cuda", _device_index(device))
+        self.n_r, self.n_eta, self.shapes = int(n_r), int(n_eta), [(int(a), int(b)) for a, b in shapes]
+        bcs = beam_centres or [(0.0, 0.0)] * n
+        descs = (L.MiMapDesc * n)()
+        self._keep = []
+        for i, pm in enumerate(pixmaps):
+            if pm.n_bins != self.n_r * self.n_eta:
+                raise ValueError(f"panel {i}: PixelMap has {pm.n_bins} bins; n_r * n_eta = {self.n_r * self.n_eta}")
+            recs = np.ascontiguousarray(pm.pxList)
+            nmap = np.ascontiguousarray(pm.nmap_pairs())
+            self._keep += [recs, nmap]
+            ny, nz = self.shapes[i]
+            descs[i] = L.MiMapDesc(recs.ctypes.data if recs.size else None, recs.shape[0], nmap.ctypes.data,
+                                   self.n_r, self.n_eta, ny, nz, float(bcs[i][0]), float(bcs[i][1]))
+        opts = L.MiPlanOpts(L.MODE[mode], int(normalize), L.SEM[semantics], int(tile_rows), int(tile_pixels), 0,
+                            L.ENC["runs"], int(run_len))
+        h = C.c_void_p()
+        L.check(L.lib().mi_plan_create_panels(descs, n, C.byref(opts), self.device.index, C.byref(h)),
+                "mi_plan_create_panels")
+        self._keep = []
+        self._h = h
+
+    def close(self) -> None:
+        if getattr(self, "_h", None) and self._h.value:
+            L.lib().mi_plan_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def info(self) -> Dict[str, int]:
+        inf = L.MiPlanInfo()
+        L.check(L.lib().mi_plan_get_info(self._h, C.byref(inf)), "mi_plan_get_info")
+        return {k: getattr(inf, k) for k, _ in L.MiPlanInfo._fields_}
+
+    def status(self) -> int:
+        st = C.c_int(0)
+        L.check(L.lib().mi_plan_status(self._h, C.byref(st)), "mi_plan_status")
+        return st.value
+
+    def set_dark(self, darks) -> None:
+        """One dark per panel ((nz, ny) floats each, or None)."""
+        arrs = []
+        ptrs = (C.c_void_p * len(self.shapes))()
+        for i, d in enumerate(darks):
+            if d is None:
+                continue
+            ny, nz = self.shapes[i]
+            a = np.ascontiguousarray(np.asarray(d, dtype=np.float32).reshape(-1))
+            if a.size != ny * nz:
+                raise ValueError(f"panel {i}: dark has {a.size} pixels, expected {ny * nz}")
+            arrs.append(a)
+            ptrs[i] = a.ctypes.data
+        L.check(L.lib().mi_plan_set_dark_panels(self._h, ptrs), "mi_plan_set_dark_panels")
+
+    def integrate(self, frames, *, cake: bool = True, lineouts: bool = True, out=None, stream=None):
+        """Frames of every panel (one device tensor (F, nz_i, ny_i) per panel, same F) ->
+        (merged cake [F, n_r, n_eta] float32, lineout_aw [F, n_r], lineout_sm [F, n_r])."""
+        n = len(self.shapes)
+        if len(frames) != n:
+            raise ValueError(f"{len(frames)} frame tensors for {n} panels")
+        F = frames[0].shape[0]
+        ptrs, dts, strides = (C.c_void_p * n)(), (C.c_int * n)(), (C.c_int64 * n)()
+        flats = []
+        for i, fr in enumerate(frames):
+            if fr.device != self.device:
+                raise ValueError(f"panel {i}: frames on {fr.device}, plan on {self.device}")
+            ny, nz = self.shapes[i]
+            if fr.shape[0] != F or fr[0].numel() != ny * nz:
+                raise ValueError(f"panel {i}: frames must be ({F}, {nz}, {ny})")
+            flat = fr.reshape(F, ny * nz)
+            if F and flat.stride(1) != 1:
+                flat = flat.contiguous()
+            flats.append(flat)
+            ptrs[i] = flat.data_ptr() if F else None
+            dts[i] = dtype_code(flat.dtype)
+            strides[i] = flat.stride(0) if F else ny * nz
+        out = out or {}
+        ck = out.get("cake") if cake else None
+        if cake and ck is None:
+            ck = torch.empty((F, self.n_r, self.n_eta), dtype=torch.float32, device=self.device)
+        aw = sm = None
+        if lineouts:
+            aw = out.get("lineout_aw")
+            sm = out.get("lineout_sm")
+            if aw is None:
+                aw = torch.empty((F, self.n_r), dtype=torch.float64, device=self.device)
+            if sm is None:
+                sm = torch.empty((F, self.n_r), dtype=torch.float64, device=self.device)
+        L.check(L.lib().mi_integrate_panels(self._h, ptrs, dts, strides, F, L.ptr(ck), L.ptr(aw), L.ptr(sm),
+                                            L.stream_ptr(stream)), "mi_integrate_panels")
+        return ck, aw, sm
+
+
 # ---------------------------------------------------------------------------
 # midas_integrate-compatible surface
 # ---------------------------------------------------------------------------

@@ -220,6 +220,43 @@ def scaled(w: Workload, factor: int, name: Optional[str] = None) -> Workload:
                    fwhm_px=max(w.fwhm_px, 1.2), n_spots=min(w.n_spots, 8), module_gaps=gaps)
 
 
+def panel_set(q_bin: float = 0.002, eta_bin: float = 2.0, mode: str = "floor") -> List[Workload]:
+    """Uneven multi-panel detector sharing one Q binning (QMin 1.0, QMax 8.0 1/A): four
+    2048x2048 u16 panels around the beam, each with its own beam centre, Lsd in 0.9-1.1 m
+    and tilts <= 0.5 deg, plus one 1475x1679 int32 panel (172 um pixels, module gaps
+    masked).  The rings are the same fcc lattice, so every panel sees them at the same Q."""
+    lam = 0.172979
+    q = dict(QMin=1.0, QMax=8.0, QBinSize=q_bin, Wavelength=lam, EtaMin=-180.0, EtaMax=180.0,
+             EtaBinSize=eta_bin)
+    geo = [(0.90e6, 2100.0, 2100.0, 0.3, -0.2), (1.00e6, -60.0, 2080.0, -0.4, 0.1),
+           (1.05e6, 2090.0, -40.0, 0.2, 0.45), (1.10e6, -50.0, -70.0, -0.1, -0.35)]
+    out = []
+    for i, (lsd, by, bz, ty, tz) in enumerate(geo):
+        m = MapperParams(NrPixelsY=2048, NrPixelsZ=2048, px=200.0, Lsd=lsd, BC_y=by, BC_z=bz, ty=ty, tz=tz, **q)
+        out.append(Workload(f"panel{i}_2048x2048_u16", m, mode, seed=100 + i, tile_rows=16))
+    m = MapperParams(NrPixelsY=1475, NrPixelsZ=1679, px=172.0, Lsd=0.95e6, BC_y=737.6, BC_z=-300.0, ty=0.2,
+                     tz=0.1, **q)
+    out.append(Workload("panel4_1475x1679_i32", m, mode, seed=104, tile_rows=16, frame_dtype="int32",
+                        module_gaps=(487, 7, 195, 17)))
+    return out
+
+
+def scaled_panels(ws: List[Workload], factor: int) -> List[Workload]:
+    """The panel set on detectors `factor` times smaller (same angular coverage and Q bins)."""
+    out = []
+    for w in ws:
+        m = w.mapper
+        m2 = replace(m, NrPixelsY=m.NrPixelsY // factor, NrPixelsZ=m.NrPixelsZ // factor,
+                     BC_y=m.BC_y / factor, BC_z=m.BC_z / factor, px=m.px * factor)
+        gaps = None
+        if w.module_gaps is not None:
+            my, gy, mz, gz = w.module_gaps
+            gaps = (max(1, my // factor), max(1, gy // factor), max(1, mz // factor), max(1, gz // factor))
+        out.append(replace(w, name=f"{w.name}_div{factor}", mapper=m2, fwhm_px=max(w.fwhm_px, 1.2),
+                           module_gaps=gaps))
+    return out
+
+
 def ring_peaks(w: Workload, half_window: int = 15) -> np.ndarray:
     """Ring radii (px) whose +-half_window-bin fit window lies inside the R range."""
     m = w.mapper
