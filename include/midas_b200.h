@@ -123,8 +123,9 @@ typedef struct {
   int64_t oob_records;     /* records whose truncated (y,z) is off the detector        */
   int32_t tile_rows, tile_pixels, frames_per_lane;
   int32_t run_len;         /* register-run length of the tile encoding                 */
-  int64_t xc_pixels;       /* pixels of the pixel-major staging spans (8/16-bit frames
-                              of the run encoding); 0: frames are gathered frame-major */
+  int64_t xc_pixels;       /* pixels of the pixel-major staging spans (run encoding with
+                              tile_rows <= 16); 0: frames are gathered frame-major     */
+  int32_t ref_row_lo, ref_row_hi; /* detector rows [lo, hi) holding referenced pixels  */
 } mi_plan_info;
 
 typedef struct mi_plan mi_plan; /* opaque, immutable after creation except for the dark */
@@ -166,6 +167,15 @@ int mi_integrate_panels(mi_plan *plan, const void *const *frames, const int *dty
 int mi_plan_status(mi_plan *plan, int *device_status);
 int mi_plan_bytes(const mi_plan *plan, size_t *bytes);
 void mi_plan_destroy(mi_plan *plan);
+
+/* Host -> device copy of F frames for this plan: only the band of detector rows that the
+ * map references (ref_row_lo .. ref_row_hi-1) crosses PCIe, as one 2-D copy on `stream`;
+ * the other rows of the device frames are left as they are, and no kernel reads them.
+ * The reference copies every whole frame (IntegratorFitPeaksGPUStream.cu:1633-1683).
+ * `host` should be page-locked for the copy to be asynchronous. */
+int mi_upload_frames(const mi_plan *plan, const void *host, int dtype, int n_frames,
+                     int64_t host_stride, void *device_frames, int64_t device_stride,
+                     void *stream);
 
 /* Cake F frames in one launch.
  *   frames:      device pointer, F frames of ny*nz pixels, frame f at frames + f*frame_stride

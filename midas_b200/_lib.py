@@ -55,7 +55,8 @@ class MiPlanInfo(C.Structure):
                 ("n_items", C.c_int64), ("staged_pixels", C.c_int64), ("ref_pixels", C.c_int64),
                 ("map_bytes", C.c_int64), ("device_bytes", C.c_int64), ("oob_records", C.c_int64),
                 ("tile_rows", C.c_int32), ("tile_pixels", C.c_int32),
-                ("frames_per_lane", C.c_int32), ("run_len", C.c_int32), ("xc_pixels", C.c_int64)]
+                ("frames_per_lane", C.c_int32), ("run_len", C.c_int32), ("xc_pixels", C.c_int64),
+                ("ref_row_lo", C.c_int32), ("ref_row_hi", C.c_int32)]
 
 
 class MiFitOpts(C.Structure):
@@ -108,6 +109,8 @@ SIGNATURES = [
                                      C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     ("mi_integrate_batch_static", C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_int64,
                                             C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
+    ("mi_upload_frames", C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_int64, C.c_void_p, C.c_int64,
+                                   C.c_void_p]),
     ("mi_integrate_plain", C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p,
                                      C.c_void_p, C.c_void_p]),
     ("mi_profile_batch", C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_void_p,

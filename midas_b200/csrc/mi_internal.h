@@ -229,6 +229,7 @@ struct Plan {
   int run_g = 0, run_l = 0;      // run encoding: rows per strip (8/16/32), rows per record
   TileLimits lim{};
   int64_t staged_pixels = 0, ref_pixels = 0;
+  int ref_row_lo = 0, ref_row_hi = 0;   // detector rows holding referenced pixels
 
   // batched path
   uint8_t *d_blobs = nullptr;

@@ -715,9 +715,15 @@ static int build_plan(const mi_map_desc &m, const mi_plan_opts &o, Plan *p, Host
   {
     std::vector<uint8_t> seen(n_pix, 0);
     int64_t n = 0;
-    for (int32_t c : csr.col)
+    int64_t cmin = n_pix, cmax = -1;
+    for (int32_t c : csr.col) {
       if (!seen[c]) { seen[c] = 1; ++n; }
+      cmin = std::min<int64_t>(cmin, c);
+      cmax = std::max<int64_t>(cmax, c);
+    }
     p->ref_pixels = n;
+    p->ref_row_lo = cmax >= 0 ? (int)(cmin / m.ny) : 0;
+    p->ref_row_hi = cmax >= 0 ? (int)(cmax / m.ny) + 1 : 0;
     if (p->encoding == MI_ENC_RUNS && runs_frames_per_group(2, p->run_g) == kXcFrames) {
       size_t pi = 0;
       for (int z = 0; z < m.nz; ++z) {
@@ -1032,6 +1038,8 @@ int mi_plan_get_info(const mi_plan *p, mi_plan_info *info) {
   info->frames_per_lane = p->frames_per_lane;
   info->run_len = p->run_l;
   info->xc_pixels = p->n_xc;
+  info->ref_row_lo = p->ref_row_lo;
+  info->ref_row_hi = p->ref_row_hi;
   return MI_OK;
 }
 
@@ -1130,6 +1138,24 @@ int mi_integrate_panels(mi_plan *p, const void *const *frames, const int *dtypes
   }
   if (prev != p->device) cudaSetDevice(prev);
   return rc;
+}
+
+int mi_upload_frames(const mi_plan *p, const void *host, int dtype, int n_frames, int64_t host_stride,
+                     void *device_frames, int64_t device_stride, void *stream) {
+  if (!p || !host || !device_frames) return set_error(MI_E_ARG, "mi_upload_frames: null argument");
+  if (p->panels.size() > 1) return set_error(MI_E_ARG, "mi_upload_frames: a panel plan has one band per panel");
+  const size_t es = dtype_size(dtype);
+  if (es == 0) return set_error(MI_E_ARG, "mi_upload_frames: unknown dtype code %d", dtype);
+  const int64_t npix = (int64_t)p->ny * p->nz;
+  if (n_frames < 0 || host_stride < npix || device_stride < npix)
+    return set_error(MI_E_ARG, "mi_upload_frames: bad frame count or stride");
+  if (n_frames == 0 || p->ref_row_hi <= p->ref_row_lo) return MI_OK;
+  const size_t off = (size_t)p->ref_row_lo * p->ny * es;
+  const size_t width = (size_t)(p->ref_row_hi - p->ref_row_lo) * p->ny * es;
+  MI_CUDA(cudaMemcpy2DAsync((uint8_t *)device_frames + off, (size_t)device_stride * es, (const uint8_t *)host + off,
+                            (size_t)host_stride * es, width, (size_t)n_frames, cudaMemcpyHostToDevice,
+                            (cudaStream_t)stream));
+  return MI_OK;
 }
 
 int mi_integrate_plain(mi_plan *p, const void *frame, int dtype, double *cake, double *lo_aw,

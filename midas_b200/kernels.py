@@ -180,6 +180,31 @@ class CakePlan:
                                                L.stream_ptr(stream)), "mi_integrate_batch")
         return ck, aw, sm
 
+    def upload(self, host_frames: torch.Tensor, device_frames: torch.Tensor, stream=None) -> None:
+        """Copy host frames (CPU tensor (F, NZ, NY), page-locked for an asynchronous copy) to
+        device frames of the same shape and dtype: only the band of detector rows the map
+        references crosses PCIe (one 2-D copy); the device frames' other rows are left as
+        they are."""
+        if host_frames.device.type != "cpu" or device_frames.device != self.device:
+            raise ValueError("upload copies a CPU tensor into a tensor on the plan's device")
+        if host_frames.dtype != device_frames.dtype or host_frames.shape[0] > device_frames.shape[0]:
+            raise ValueError("host and device frames must have one dtype and room for the frames")
+        hf, F, hs = self._frames_host(host_frames)
+        df = device_frames.reshape(device_frames.shape[0], -1)
+        if df.shape[1] != self.ny * self.nz or (F and df.stride(1) != 1):
+            raise ValueError("device frames must be contiguous frames of ny*nz pixels")
+        L.check(L.lib().mi_upload_frames(self._h, hf.data_ptr(), dtype_code(hf.dtype), F, hs, df.data_ptr(),
+                                         df.stride(0), L.stream_ptr(stream)), "mi_upload_frames")
+
+    def _frames_host(self, frames: torch.Tensor):
+        F = frames.shape[0]
+        flat = frames.reshape(F, -1)
+        if flat.shape[1] != self.ny * self.nz:
+            raise ValueError(f"frame has {flat.shape[1]} pixels, expected {self.ny * self.nz}")
+        if F and flat.stride(1) != 1:
+            raise ValueError("host frames must be contiguous along the pixels")
+        return flat, F, flat.stride(0) if F else self.ny * self.nz
+
     def integrate_plain(self, frame: torch.Tensor, stream=None):
         """The reference algorithm, one frame per launch: (cake float64 [n_r, n_eta], aw, sm)."""
         flat, F, _ = self._frames(frame)

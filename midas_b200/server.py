@@ -284,7 +284,7 @@ class DeviceBackend:
         strm = st["stream"]
         fit = "d_fit" in s
         with torch.cuda.stream(strm):
-            s["d_frames"][:n].copy_(hf[:n], non_blocking=True)
+            st["plan"].upload(hf[:n], s["d_frames"], stream=strm)   # referenced rows only
             if self.plain:
                 code = dtype_code(s["d_frames"].dtype)
                 for i in range(n):

@@ -247,3 +247,27 @@ def test_empty_map_and_empty_batch(cuda):
     assert torch.count_nonzero(ck) == 0 and torch.count_nonzero(aw) == 0
     ck, aw, sm = plan.integrate(torch.ones((0, 8, 8), dtype=torch.uint16, device=cuda))
     assert ck.shape[0] == 0
+
+
+def test_upload_copies_the_referenced_row_band(cuda):
+    """CakePlan.upload moves only the detector rows the map references; caking the
+    uploaded frames equals caking the full frames."""
+    from midas_b200 import synth
+    from midas_b200.mapper import build_map
+    w = synth.scaled(synth.sweep_2880(), 8)
+    m = w.mapper
+    pm, _ = build_map(m, device=0)
+    plan = CakePlan(pm, n_r=w.n_r, n_eta=w.n_eta, n_pixels_y=m.NrPixelsY, n_pixels_z=m.NrPixelsZ, mode=w.mode,
+                    bc_y=m.BC_y, bc_z=m.BC_z, device=cuda)
+    info = plan.info
+    lo, hi = info["ref_row_lo"], info["ref_row_hi"]
+    assert 0 < lo < hi < m.NrPixelsZ
+    fr = w.frames(0, 6)
+    host = fr.cpu().pin_memory()
+    dev = torch.full_like(fr, 7)
+    plan.upload(host, dev)
+    torch.cuda.synchronize()
+    assert torch.equal(dev[:, lo:hi], fr[:, lo:hi])
+    assert bool((dev[:, :lo].int() == 7).all()) and bool((dev[:, hi:].int() == 7).all())
+    for x, y in zip(plan.integrate(dev), plan.integrate(fr)):
+        assert torch.equal(x, y)
