@@ -138,13 +138,21 @@ def dist_setup(args):
 
 
 def dist_max(x: float, world: int) -> float:
+    """Max of x over the ranks (the job's time is its slowest rank's)."""
     if world == 1:
         return x
     import torch
     import torch.distributed as dist
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([x], dtype=torch.float64, device=dev)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
+
+
+def rank_first_frame(rank: int, sweep: int) -> int:
+    """Replicas: rank r cakes its own slice of the omega sweep, frames r*sweep .. (r+1)*sweep-1
+    (weak scaling; the slices never overlap, no data crosses between ranks)."""
+    return rank * sweep
 
 
 def barrier(world):
@@ -268,7 +276,7 @@ def main_ours(args):
     sweep = max(F, (args.sweep_frames // F) * F)
     frames = torch.empty((sweep, nz, ny), dtype=torch.uint16, device=dev)
     for s in range(0, sweep, 256):
-        w.frames(rank * sweep + s, min(256, sweep - s), out=frames[s:s + 256])
+        w.frames(rank_first_frame(rank, sweep) + s, min(256, sweep - s), out=frames[s:s + 256])
     torch.cuda.synchronize()
     n_batches = sweep // F
     cake = torch.empty((F, w.n_r, w.n_eta), dtype=torch.float32, device=dev)
