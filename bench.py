@@ -54,6 +54,8 @@ def parse():
     ap.add_argument("--no-check", action="store_true")
     ap.add_argument("--no-fit", action="store_true")
     ap.add_argument("--no-panels", action="store_true")
+    ap.add_argument("--no-graph", action="store_true", help="skip the CUDA-graph replay of the batched step")
+    ap.add_argument("--autotune", action="store_true", help="time candidate tile shapes / run lengths first")
     ap.add_argument("--panel-frames", type=int, default=256)
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--serve-seconds", type=float, default=8.0,
@@ -263,6 +265,17 @@ def main_ours(args):
     t_setup = time.time()
     pm, _ = build_map(w.mapper, device=local)
     t_map = time.time() - t_setup
+    tuned = None
+    if args.autotune:
+        from midas_b200 import autotune
+        sample = w.frames(0, F, device=dev)
+        t1 = time.time()
+        tuned = autotune.tune(pm, sample, n_r=w.n_r, n_eta=w.n_eta, n_pixels_y=ny, n_pixels_z=nz, mode=w.mode,
+                              bc_y=w.mapper.BC_y, bc_z=w.mapper.BC_z, device=dev)
+        tuned_s = time.time() - t1
+        del sample
+        args.tile_rows, args.run_len, args.tile_pixels = (tuned.best["tile_rows"], tuned.best["run_len"],
+                                                          tuned.best["tile_pixels"])
     t1 = time.time()
     plan = CakePlan(pm, n_r=w.n_r, n_eta=w.n_eta, n_pixels_y=ny, n_pixels_z=nz, mode=w.mode,
                     bc_y=w.mapper.BC_y, bc_z=w.mapper.BC_z, device=dev,
@@ -363,6 +376,27 @@ def main_ours(args):
            "setup_s": {"map_build_gpu": round(t_map, 2), "plan_build": round(t_plan, 2)}}
     if clk:
         out["clocks"] = clk
+    if tuned is not None:
+        out["autotune"] = {"best": tuned.best, "best_ms": tuned.best_ms, "candidates": tuned.table,
+                           "seconds": round(tuned_s, 1)}
+
+    # ---- the same steps replayed from CUDA graphs (one graph per resident batch)
+    if not args.no_graph:
+        graphs = [plan.capture(frames[b * F:(b + 1) * F], bufs) for b in range(n_batches)]
+        for i in range(args.warmup):
+            graphs[i % n_batches].replay()
+        torch.cuda.synchronize()
+        g0, g1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        g0.record(stream)
+        for i in range(args.steps):
+            graphs[(args.warmup + i) % n_batches].replay()
+        g1.record(stream)
+        torch.cuda.synchronize()
+        gms = dist_max(g0.elapsed_time(g1), world)
+        out["graph"] = {"frames_per_s": round(world * args.steps * F / (gms / 1e3), 1),
+                        "ms_per_step": round(gms / args.steps, 4), "graphs": n_batches,
+                        "nodes_per_graph": "memset + k_xc + k_runs per 128 frames, k_lineout"}
+        del graphs
 
     # ---- plain one-frame-per-launch kernel (reference GPU algorithm) on the same frames
     if not args.no_plain:

@@ -180,6 +180,19 @@ class CakePlan:
                                                L.stream_ptr(stream)), "mi_integrate_batch")
         return ck, aw, sm
 
+    def capture(self, frames: torch.Tensor, out: Dict[str, torch.Tensor], *, cake: bool = True,
+                lineouts: bool = True) -> "torch.cuda.CUDAGraph":
+        """Record ``integrate(frames, out=out)`` (every launch of the batch: pixel-major
+        staging, caking, lineouts) as a CUDA graph; ``graph.replay()`` then re-runs it on
+        whatever the same buffers hold.  A first ``integrate`` on the buffers warms up the
+        kernels before the capture."""
+        self.integrate(frames, cake=cake, lineouts=lineouts, out=out)
+        torch.cuda.synchronize(self.device)
+        g = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(g):
+            self.integrate(frames, cake=cake, lineouts=lineouts, out=out)
+        return g
+
     def upload(self, host_frames: torch.Tensor, device_frames: torch.Tensor, stream=None) -> None:
         """Copy host frames (CPU tensor (F, NZ, NY), page-locked for an asynchronous copy) to
         device frames of the same shape and dtype: only the band of detector rows the map

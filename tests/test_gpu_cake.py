@@ -271,3 +271,49 @@ def test_upload_copies_the_referenced_row_band(cuda):
     assert bool((dev[:, :lo].int() == 7).all()) and bool((dev[:, hi:].int() == 7).all())
     for x, y in zip(plan.integrate(dev), plan.integrate(fr)):
         assert torch.equal(x, y)
+
+
+def test_graph_replay_equals_direct_calls(cuda):
+    """A batch captured as a CUDA graph (staging, caking, lineouts) replays to the same results
+    on new frames copied into the captured buffers."""
+    from midas_b200 import synth
+    from midas_b200.mapper import build_map
+    w = synth.scaled(synth.sweep_2880(), 8)
+    m = w.mapper
+    pm, _ = build_map(m, device=0)
+    plan = CakePlan(pm, n_r=w.n_r, n_eta=w.n_eta, n_pixels_y=m.NrPixelsY, n_pixels_z=m.NrPixelsZ, mode=w.mode,
+                    bc_y=m.BC_y, bc_z=m.BC_z, device=cuda)
+    plan.set_dark(w.dark().cpu().numpy())
+    buf = w.frames(0, 40)
+    out = {"cake": torch.empty((40, w.n_r, w.n_eta), dtype=torch.float32, device=cuda),
+           "lineout_aw": torch.empty((40, w.n_r), dtype=torch.float64, device=cuda),
+           "lineout_sm": torch.empty((40, w.n_r), dtype=torch.float64, device=cuda)}
+    g = plan.capture(buf, out)
+    for first in (100, 300):
+        nxt = w.frames(first, 40)
+        buf.copy_(nxt)
+        g.replay()
+        torch.cuda.synchronize()
+        ref = plan.integrate(nxt)
+        for k, r in zip(("cake", "lineout_aw", "lineout_sm"), ref):
+            assert torch.equal(out[k], r)
+    assert plan.status() == 0
+
+
+def test_autotuner_picks_the_fastest_buildable_plan(cuda):
+    from midas_b200 import autotune, synth
+    from midas_b200.mapper import build_map
+    w = synth.scaled(synth.sweep_2880(), 8)
+    m = w.mapper
+    pm, _ = build_map(m, device=0)
+    fr = w.frames(0, 64)
+    cands = [{"tile_rows": 16, "run_len": 0, "tile_pixels": 0}, {"tile_rows": 8, "run_len": 4, "tile_pixels": 0},
+             {"tile_rows": 16, "run_len": 2, "tile_pixels": 0}]     # run_len 2 with 16 rows is refused
+    res = autotune.tune(pm, fr, n_r=w.n_r, n_eta=w.n_eta, n_pixels_y=m.NrPixelsY, n_pixels_z=m.NrPixelsZ,
+                        mode=w.mode, bc_y=m.BC_y, bc_z=m.BC_z, candidates=cands, device=cuda)
+    timed = [r for r in res.table if "ms" in r]
+    assert len(timed) == 2 and "error" in res.table[2]
+    assert res.best_ms == min(r["ms"] for r in timed)
+    again = autotune.tune(pm, fr, n_r=w.n_r, n_eta=w.n_eta, n_pixels_y=m.NrPixelsY, n_pixels_z=m.NrPixelsZ,
+                          mode=w.mode, bc_y=m.BC_y, bc_z=m.BC_z, candidates=cands, device=cuda)
+    assert again is res                                             # cached per map and batch
