@@ -62,6 +62,7 @@ struct RunArgs {
 
 constexpr uint32_t kRunWaitLimit = 1u << 26;
 constexpr int kRecBatch = 4;   // records whose loads are issued together in the record loop
+constexpr int kStoreSlots = 8; // bins per lane in the cake store: tiles hold <= 256 bins
 
 __device__ __forceinline__ uint32_t r_smem(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
 
@@ -159,7 +160,7 @@ struct SlotTag {
 };
 
 template <typename T, int G, int L, bool XC, int NP>
-__global__ void __launch_bounds__((kRunWarps + NP) * 32, 1) k_runs(RunArgs a) {
+__global__ void __launch_bounds__((kRunWarps + NP) * 32, kRunCtasPerSm) k_runs(RunArgs a) {
   constexpr bool kU16 = sizeof(T) <= 2;              // staged as u16
   constexpr int FG = runs_frames_per_group(sizeof(T), G);
   constexpr int FPL = FG / 32;                       // frames per lane
@@ -440,14 +441,23 @@ __global__ void __launch_bounds__((kRunWarps + NP) * 32, 1) k_runs(RunArgs a) {
     // ---- cake store: warp per frame, lanes over the tile's bins (runs of n_cols contiguous
     // floats per row); row/col from a float reciprocal (exact for b < 2^12)
     if (a.want_cake) {
+      // the bins this lane stores (bb = lane + 32 k) and their offsets in a frame's cake,
+      // computed once per tile; tiles hold at most kStoreSlots * 32 bins
       const float inv_ns = 1.0f / (float)ns;
+      int off[kStoreSlots];
+#pragma unroll
+      for (int k = 0; k < kStoreSlots; ++k) {
+        const int bb = lane + 32 * k;
+        const int r = (int)(((float)bb + 0.5f) * inv_ns);
+        off[k] = bb < h.nb ? r * a.n_eta + (bb - r * ns) : -1;
+      }
+      const int64_t tile0 = (int64_t)h.r0 * a.n_eta + h.e0;
       for (int f = warp; f < fg_n; f += NC) {
-        float *dst = a.cake + (int64_t)(g0 + f) * a.n_bins + (int64_t)h.r0 * a.n_eta + h.e0;
-        const float *src = s_out + f * nbp;
-        for (int bb = lane; bb < h.nb; bb += 32) {
-          const int r = (int)(((float)bb + 0.5f) * inv_ns);
-          dst[(int64_t)r * a.n_eta + (bb - r * ns)] = src[bb];
-        }
+        float *dst = a.cake + (int64_t)(g0 + f) * a.n_bins + tile0;
+        const float *src = s_out + f * nbp + lane;
+#pragma unroll
+        for (int k = 0; k < kStoreSlots; ++k)
+          if (off[k] >= 0) dst[off[k]] = src[32 * k];
       }
     }
     if (t == nt - 1 && a.want_lo) {
