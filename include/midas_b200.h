@@ -73,7 +73,7 @@ extern "C" {
 #define MI_DT_I64 3
 #define MI_DT_F32 4
 #define MI_DT_F64 5
-/* code 6 (hybrid) is decoded on the host into u16 + overflow patch before upload */
+#define MI_DT_HYBRID 6       /* u16 base + int64 overflow patch: decoded by mi_decode_hybrid */
 #define MI_DT_I32 7          /* extension: PILATUS-style signed 32-bit frames            */
 
 /* ---- maps ---------------------------------------------------------------- */
@@ -105,6 +105,13 @@ typedef struct {
   int32_t frames_per_lane; /* CSR encoding only: 1, 2 or 4 frames per thread; 0 = auto */
   int32_t encoding;        /* MI_ENC_*: tile encoding of the map                      */
   int32_t run_len;         /* run encoding: rows per record (2, 4 or 8); 0 = auto      */
+  int32_t variance;        /* 1 = variance plan: the cake of a variance map (per-pixel
+                              variances, dark already subtracted) under squared weights,
+                              integrate_with_variance (MI/kernels.py:474-536): bin
+                              variance = sum(w^2 var) / A^2 (normalised) or sum(w^2 var);
+                              lineouts are the propagated variances of profile_1d
+                              (kernels.py:567-628): sum(A^2 var) / (sum A)^2 and
+                              sum(var) / N^2.  mi_integrate_plain rejects such plans.  */
 } mi_plan_opts;
 
 #define MI_ENC_AUTO 0      /* runs                                                       */
@@ -222,6 +229,40 @@ int mi_profile_batch(mi_plan *plan, const void *cake, int cake_dtype, int n_fram
  * 128-bit vector loads.  frames and out are device pointers. */
 int mi_cast_dark(const void *frames, int dtype, int64_t n_pixels, int n_frames,
                  const float *dark, float *out, void *stream);
+
+/* Per-pixel mean of k frames, accumulated in FP64 and stored as float: the dark
+ * average of the stream server's start-up (IntegratorFitPeaksGPUStream.cu:2191-2238,
+ * average_dark_frames, MI/image.py:161-184), on the device.  frames: device pointer,
+ * frame f at frames + f*frame_stride elements of dtype (not MI_DT_HYBRID); out: device
+ * [n_pixels] float.  The result can be passed to mi_plan_set_dark after a copy to the host,
+ * or used on the device directly. */
+int mi_average_frames(const void *frames, int dtype, int64_t n_pixels, int n_frames,
+                      int64_t frame_stride, float *out, void *stream);
+
+/* Decode one hybrid (dtype code 6) socket payload into a float frame of raw counts on
+ * the device.  payload: host bytes as received, [u32 C][u16 base, ny*nz][i32 index, C]
+ * [i64 value, C] (ProcessImageGPU_Hybrid_Impl, IntegratorFitPeaksGPUStream.cu:1497-1560;
+ * decode_hybrid_payload, MI/image.py:83-123), best page-locked.  It crosses PCIe in one
+ * copy into device_staging (>= payload_bytes + 4 bytes, 16-byte aligned, owned by the
+ * caller; reused once the stream has passed the decode), out[p] = (float)base[p], then
+ * out[index[i]] = (float)value[i].  The frame holds raw counts: cake it with dtype
+ * MI_DT_F32 and the plan's dark, which gives (float)raw - dark like the reference.
+ * A payload whose size does not match C and ny*nz is rejected on the host (MI_E_ARG);
+ * an index outside the frame is skipped and sets *device_status (device int) to
+ * MI_E_RANGE. */
+int mi_decode_hybrid(const void *payload, size_t payload_bytes, int ny, int nz,
+                     void *device_staging, float *out, int *device_status, void *stream);
+
+/* Per-bin axis table of a plan, host doubles [n_r*n_eta][MI_BIN_NCOL], bin = r*n_eta + eta:
+ *   R mean (px), 2-theta (deg) = atan(R * px / Lsd), eta mean (deg), bin area (sum of the
+ *   map's areaWeight, float sums like the reference), Q (1/A) = 4 pi / lambda sin(theta)
+ * (the caked output header of IntegratorFitPeaksGPUStream.cu:817-899).  r_lo/r_hi and
+ * eta_lo/eta_hi are the bin edges (host, n_r and n_eta).  Panel plans sum the panels'
+ * areas. */
+#define MI_BIN_NCOL 5
+int mi_plan_bin_table(const mi_plan *plan, const double *r_lo, const double *r_hi,
+                      const double *eta_lo, const double *eta_hi, double px_um,
+                      double lsd_um, double wavelength_a, double *table);
 
 /* ---- peak fitting ----------------------------------------------------------
  * One warp per (frame, peak) window; Levenberg-Marquardt in FP32 with an FP64

@@ -43,7 +43,8 @@ class MiMapDesc(C.Structure):
 class MiPlanOpts(C.Structure):
     _fields_ = [("mode", C.c_int32), ("normalize", C.c_int32), ("semantics", C.c_int32),
                 ("tile_rows", C.c_int32), ("tile_pixels", C.c_int32),
-                ("frames_per_lane", C.c_int32), ("encoding", C.c_int32), ("run_len", C.c_int32)]
+                ("frames_per_lane", C.c_int32), ("encoding", C.c_int32), ("run_len", C.c_int32),
+                ("variance", C.c_int32)]
 
 
 ENC = {"auto": 0, "csr": 1, "runs": 2}
@@ -117,6 +118,12 @@ SIGNATURES = [
                                    C.c_void_p, C.c_void_p]),
     ("mi_cast_dark", C.c_int, [C.c_void_p, C.c_int, C.c_int64, C.c_int, C.c_void_p, C.c_void_p,
                                C.c_void_p]),
+    ("mi_average_frames", C.c_int, [C.c_void_p, C.c_int, C.c_int64, C.c_int, C.c_int64, C.c_void_p,
+                                    C.c_void_p]),
+    ("mi_decode_hybrid", C.c_int, [C.c_void_p, C.c_size_t, C.c_int, C.c_int, C.c_void_p, C.c_void_p,
+                                   C.c_void_p, C.c_void_p]),
+    ("mi_plan_bin_table", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_double,
+                                    C.c_double, C.c_double, C.c_void_p]),
     ("mi_fit_batch", C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_int,
                                C.POINTER(MiFitOpts), C.c_void_p, C.c_void_p, C.c_void_p]),
     ("mi_map_build", C.c_int, [C.POINTER(MiGeometry), C.POINTER(MiBinning), C.c_int,

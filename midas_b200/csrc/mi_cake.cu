@@ -292,7 +292,7 @@ __global__ void k_lineout(const double *partial, int F, int n_r, int n_slots, co
     ssm += p[2 * s + 1];
   }
   const double d = den_aw[r], c = cnt[r];
-  if (lo_aw) lo_aw[i] = d > kAreaThreshold ? saw / d : 0.0;
+  if (lo_aw) lo_aw[i] = d > 0.0 ? saw / d : 0.0;   // d is 0 or a sum of areas > 1e-9
   if (lo_sm) lo_sm[i] = c > 0.0 ? ssm / c : 0.0;
 }
 

@@ -188,6 +188,7 @@ struct HostCSR {
   std::vector<double> w;
   std::vector<double> area_norm;  // normaliser per bin (semantics dependent)
   std::vector<double> area_in;    // in-bounds area per bin (profile weights)
+  std::vector<double> area_gs;    // area of records with 0 <= y < ny, 0 <= z < nz (as floats)
   int64_t oob = 0;
 };
 
@@ -221,6 +222,8 @@ struct XcChunk {
 struct Plan {
   int device = 0;
   int mode = 0, normalize = 1, semantics = 0;
+  int variance = 0;              // squared weights, area^2 normalisation, variance lineouts
+  std::vector<double> area_gs;   // per bin, for mi_plan_bin_table
   int n_r = 0, n_eta = 0, ny = 0, nz = 0;
   double bc_y = 0, bc_z = 0;
   int64_t n_bins = 0, nnz = 0, n_records = 0, oob = 0;

@@ -182,10 +182,13 @@ __global__ void k_plain_integrate(PlainArgs a) {
   a.cake[b] = out;
 }
 
-// one block per (R row, frame); both profiles in one pass
+// one block per (R row, frame); both profiles in one pass.  variance != 0: the cake holds
+// bin variances and the profiles are propagated variances (profile_1d_with_variance,
+// packages/midas_integrate/midas_integrate/kernels.py:604-645): sum(A^2 V) / (sum A)^2 and
+// sum(V) / N^2
 template <typename T>
 __global__ void k_profile(const T *cake, const double *area_in, int n_r, int n_eta, double *lo_aw,
-                          double *lo_sm) {
+                          double *lo_sm, int variance) {
   const int r = blockIdx.x;
   const int64_t f = blockIdx.y;
   if (r >= n_r) return;
@@ -197,7 +200,7 @@ __global__ void k_profile(const T *cake, const double *area_in, int n_r, int n_e
     const double A = area_in[b];
     if (A > kAreaThreshold) {
       const double I = (double)ck[b];
-      s_ia += I * A;
+      s_ia += variance ? I * A * A : I * A;
       s_a += A;
       s_i += I;
       ++n;
@@ -220,8 +223,9 @@ __global__ void k_profile(const T *cake, const double *area_in, int n_r, int n_e
     for (int k = 0; k < (int)(blockDim.x >> 5); ++k) {
       t_ia += sh[0][k]; t_a += sh[1][k]; t_i += sh[2][k]; t_n += sh[3][k];
     }
-    if (lo_aw) lo_aw[f * n_r + r] = t_a > kAreaThreshold ? t_ia / t_a : 0.0;
-    if (lo_sm) lo_sm[f * n_r + r] = t_n > 0 ? t_i / t_n : 0.0;
+    const double d_a = variance ? t_a * t_a : t_a, d_n = variance ? t_n * t_n : t_n;
+    if (lo_aw) lo_aw[f * n_r + r] = t_a > kAreaThreshold ? t_ia / d_a : 0.0;
+    if (lo_sm) lo_sm[f * n_r + r] = t_n > 0 ? t_i / d_n : 0.0;
   }
 }
 
@@ -231,9 +235,11 @@ int launch_profile(Plan *p, const void *cake, int cake_dtype, int n_frames, doub
   if (n_frames > 65535) return set_error(MI_E_RANGE, "mi_profile_batch: more than 65535 frames per call");
   const dim3 grid((unsigned)p->n_r, (unsigned)n_frames);
   if (cake_dtype == MI_DT_F32)
-    k_profile<float><<<grid, 256, 0, s>>>((const float *)cake, p->d_area_in, p->n_r, p->n_eta, lo_aw, lo_sm);
+    k_profile<float><<<grid, 256, 0, s>>>((const float *)cake, p->d_area_in, p->n_r, p->n_eta, lo_aw, lo_sm,
+                                                  p->variance);
   else if (cake_dtype == MI_DT_F64)
-    k_profile<double><<<grid, 256, 0, s>>>((const double *)cake, p->d_area_in, p->n_r, p->n_eta, lo_aw, lo_sm);
+    k_profile<double><<<grid, 256, 0, s>>>((const double *)cake, p->d_area_in, p->n_r, p->n_eta, lo_aw, lo_sm,
+                                                  p->variance);
   else
     return set_error(MI_E_ARG, "mi_profile_batch: cake dtype must be MI_DT_F32 or MI_DT_F64");
   MI_CUDA(cudaGetLastError());

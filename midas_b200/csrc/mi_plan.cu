@@ -200,6 +200,7 @@ int build_host_csr(const mi_map_desc &m, int mode, int sem, HostCSR *out) {
   out->area_in.assign(n_bins, 0.0);
   out->area_norm.assign(n_bins, 0.0);
   std::vector<double> area_all(n_bins, 0.0);
+  out->area_gs.assign(n_bins, 0.0);
   int64_t oob_total = 0;
   // pass 1: term counts
 #pragma omp parallel reduction(+ : oob_total)
@@ -215,6 +216,19 @@ int build_host_csr(const mi_map_desc &m, int mode, int sem, HostCSR *out) {
       out->area_in[b] = ain;
       area_all[b] = aall;
       oob_total += oob;
+      // initialize_PerFrameArr_Area_kernel (IntegratorFitPeaksGPUStream.cu:858-873): the
+      // record's float position inside [0, ny) x [0, nz), and its flat index
+      // (long long)z * ny + y, evaluated in float, below ny * nz
+      double ags = 0.0;
+      const int64_t n_pix = (int64_t)m.ny * m.nz;
+      for (int32_t k = 0; k < m.nmap[2 * b]; ++k) {
+        const mi_map_record &r = m.records[(int64_t)m.nmap[2 * b + 1] + k];
+        if (r.y < 0 || r.y >= m.ny || r.z < 0 || r.z >= m.nz) continue;
+        const float flat = (float)((int64_t)r.z * m.ny) + r.y;
+        if ((int64_t)flat >= n_pix) continue;
+        ags += r.areaWeight;
+      }
+      out->area_gs[b] = ags;
     }
   }
   out->row_ptr.assign(n_bins + 1, 0);
@@ -335,8 +349,11 @@ static inline void bin_scale(const HostCSR &csr, const Plan *p, int64_t b, float
     sc = an > kAreaThreshold ? (p->normalize ? 1.0 / an : 1.0) : 0.0;
   else
     sc = p->normalize ? (ai > kAreaThreshold ? 1.0 / ai : 0.0) : 1.0;
+  // variance plans (integrate_with_variance, kernels.py:551-559; profile_1d_with_variance,
+  // kernels.py:604-645): Var = sum w^2 var / A^2, lineout weight A^2
+  if (p->variance) sc *= sc;
   *scale = (float)sc;
-  *lw = ai > kAreaThreshold ? (float)ai : 0.0f;
+  *lw = ai > kAreaThreshold ? (float)(p->variance ? ai * ai : ai) : 0.0f;
 }
 
 // staged pixel set of a tile (ascending), with lut[pixel] = local index
@@ -565,6 +582,9 @@ static int build_plan(const mi_map_desc &m, const mi_plan_opts &o, Plan *p, Host
   int rc = MI_OK;
   if (pre) csr = std::move(*pre);
   else if ((rc = build_host_csr(m, o.mode, o.semantics, &csr))) return rc;
+  p->variance = o.variance ? 1 : 0;
+  if (p->variance)
+    for (double &x : csr.w) x *= x;   // _square_csr (kernels.py:378-400) of the coalesced weights
   if (p->panels.empty()) p->panels.push_back({m.ny, m.nz, 0, 0, 0});
   p->nnz = (int64_t)csr.col.size();
   p->oob = csr.oob;
@@ -755,13 +775,19 @@ static int build_plan(const mi_map_desc &m, const mi_plan_opts &o, Plan *p, Host
   for (int i = 0; i < n_items; ++i) items_sorted[i] = items[order[i]];
   p->n_items = n_items;
 
-  // lineout denominators
+  // lineout denominators (variance plans: squared, kernels.py:625-640)
   std::vector<double> den(m.n_r, 0.0), cnt(m.n_r, 0.0);
-  for (int r = 0; r < m.n_r; ++r)
+  for (int r = 0; r < m.n_r; ++r) {
     for (int e = 0; e < m.n_eta; ++e) {
       double a = csr.area_in[(int64_t)r * m.n_eta + e];
       if (a > kAreaThreshold) { den[r] += a; cnt[r] += 1.0; }
     }
+    if (p->variance) {
+      den[r] = den[r] > kAreaThreshold ? den[r] * den[r] : 0.0;
+      cnt[r] *= cnt[r];
+    }
+  }
+  p->area_gs = csr.area_gs;
 
   size_t acct = 0;
   MI_CUDA(cudaSetDevice(p->device));
@@ -943,12 +969,14 @@ int mi_plan_create_panels(const mi_map_desc *maps, int n_panels, const mi_plan_o
   csr.row_ptr.assign(n_bins + 1, 0);
   csr.area_in.assign(n_bins, 0.0);
   csr.area_norm.assign(n_bins, 0.0);
+  csr.area_gs.assign(n_bins, 0.0);
   for (int64_t b = 0; b < n_bins; ++b) {
     int64_t c = 0;
     for (int i = 0; i < n_panels; ++i) {
       c += part[i].row_ptr[b + 1] - part[i].row_ptr[b];
       csr.area_in[b] += part[i].area_in[b];
       csr.area_norm[b] += part[i].area_norm[b];
+      csr.area_gs[b] += part[i].area_gs[b];
     }
     csr.row_ptr[b + 1] = csr.row_ptr[b] + c;
   }
@@ -1167,6 +1195,8 @@ int mi_integrate_plain(mi_plan *p, const void *frame, int dtype, double *cake, d
   if (p->semantics == MI_SEM_IC)
     return set_error(MI_E_UNSUPPORTED, "mi_integrate_plain: the one-frame GPU kernel follows the GPU stream "
                                        "or midas_integrate semantics, not IntegrationCore's");
+  if (p->variance)
+    return set_error(MI_E_UNSUPPORTED, "mi_integrate_plain: variance plans are caked by mi_integrate_batch");
   int prev = 0;
   cudaGetDevice(&prev);
   if (prev != p->device) MI_CUDA(cudaSetDevice(p->device));
@@ -1185,6 +1215,27 @@ int mi_profile_batch(mi_plan *p, const void *cake, int cake_dtype, int n_frames,
   int rc = launch_profile(p, cake, cake_dtype, n_frames, lo_aw, lo_sm, (cudaStream_t)stream);
   if (prev != p->device) cudaSetDevice(prev);
   return rc;
+}
+
+int mi_plan_bin_table(const mi_plan *p, const double *r_lo, const double *r_hi, const double *eta_lo,
+                      const double *eta_hi, double px_um, double lsd_um, double wavelength_a, double *table) {
+  if (!p || !r_lo || !r_hi || !eta_lo || !eta_hi || !table) return set_error(MI_E_ARG, "mi_plan_bin_table: null argument");
+  if (lsd_um == 0.0) return set_error(MI_E_ARG, "mi_plan_bin_table: Lsd must be non-zero");
+  // initialize_PerFrameArr_Area_kernel (IntegratorFitPeaksGPUStream.cu:817-899)
+  const double rad2deg = 180.0 / M_PI;
+  for (int r = 0; r < p->n_r; ++r)
+    for (int e = 0; e < p->n_eta; ++e) {
+      const int64_t b = (int64_t)r * p->n_eta + e;
+      const double rm = (r_lo[r] + r_hi[r]) * 0.5, em = (eta_lo[e] + eta_hi[e]) * 0.5;
+      const double tth = atan(rm * px_um / lsd_um);
+      double *t = table + b * MI_BIN_NCOL;
+      t[0] = rm;
+      t[1] = rad2deg * tth;
+      t[2] = em;
+      t[3] = p->area_gs[b];
+      t[4] = wavelength_a > 0 ? (4.0 * M_PI / wavelength_a) * sin(tth / 2.0) : 0.0;
+    }
+  return MI_OK;
 }
 
 int mi_cast_dark(const void *frames, int dtype, int64_t n_pixels, int n_frames, const float *dark,

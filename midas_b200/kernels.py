@@ -63,13 +63,18 @@ class CakePlan:
         tile_rows, tile_pixels, frames_per_lane: tiling knobs (0 = default).
         encoding: 'auto' (= 'runs') | 'runs' (register-blocked radial runs) | 'csr'
             (per-bin term lists); run_len: rows per run record (2, 4, 8; 0 = auto).
+        variance: a variance plan (integrate_with_variance, kernels.py:474-536): frames
+            are per-pixel variance maps, caked with the squared coalesced weights and
+            divided by the squared bin area; its lineouts are the propagated variances of
+            profile_1d_with_variance (kernels.py:604-645).
     """
 
     def __init__(self, pixmap: PixelMap, *, n_r: int, n_eta: int, n_pixels_y: int,
                  n_pixels_z: int, mode: str = "floor", normalize: bool = True,
                  semantics: str = "py", bc_y: float = 0.0, bc_z: float = 0.0,
                  device="cuda", tile_rows: int = 0, tile_pixels: int = 0,
-                 frames_per_lane: int = 0, encoding: str = "auto", run_len: int = 0):
+                 frames_per_lane: int = 0, encoding: str = "auto", run_len: int = 0,
+                 variance: bool = False):
         if pixmap.n_bins != n_r * n_eta:
             raise ValueError(f"PixelMap has {pixmap.n_bins} bins; n_r * n_eta = {n_r * n_eta}")
         if mode not in L.MODE:
@@ -81,6 +86,7 @@ class CakePlan:
         self.ny, self.nz = int(n_pixels_y), int(n_pixels_z)
         self.mode, self.normalize, self.semantics = mode, bool(normalize), semantics
         self.bc_y, self.bc_z = float(bc_y), float(bc_z)
+        self.variance = bool(variance)
         recs = np.ascontiguousarray(pixmap.pxList)
         nmap = np.ascontiguousarray(pixmap.nmap_pairs())
         desc = L.MiMapDesc(recs.ctypes.data if recs.size else None, recs.shape[0],
@@ -90,7 +96,7 @@ class CakePlan:
             raise ValueError(f"unknown encoding {encoding!r}; expected 'auto' | 'csr' | 'runs'")
         opts = L.MiPlanOpts(L.MODE[mode], int(self.normalize), L.SEM[semantics],
                             int(tile_rows), int(tile_pixels), int(frames_per_lane),
-                            L.ENC[encoding], int(run_len))
+                            L.ENC[encoding], int(run_len), int(self.variance))
         h = C.c_void_p()
         L.check(L.lib().mi_plan_create(C.byref(desc), C.byref(opts), self.device.index,
                                        C.byref(h)), "mi_plan_create")
@@ -230,6 +236,23 @@ class CakePlan:
                                            ck.data_ptr(), aw.data_ptr(), sm.data_ptr(),
                                            L.stream_ptr(stream)), "mi_integrate_plain")
         return ck, aw, sm
+
+    def bin_table(self, r_lo, r_hi, eta_lo, eta_hi, *, px: float, lsd: float,
+                  wavelength: float = 0.0) -> np.ndarray:
+        """Per-bin axes [n_r * n_eta, 5]: R mean (px), 2-theta (deg), eta mean (deg), bin
+        area (areaWeight of the records on the detector), Q (1/A; 0 without a wavelength),
+        as the GPU stream's static output header (IntegratorFitPeaksGPUStream.cu:817-899).
+        px and lsd in one unit (um)."""
+        edges = [np.ascontiguousarray(np.asarray(a, dtype=np.float64).reshape(-1)) for a in (r_lo, r_hi)]
+        edges += [np.ascontiguousarray(np.asarray(a, dtype=np.float64).reshape(-1)) for a in (eta_lo, eta_hi)]
+        if edges[0].size != self.n_r or edges[1].size != self.n_r:
+            raise ValueError(f"R edges need {self.n_r} values")
+        if edges[2].size != self.n_eta or edges[3].size != self.n_eta:
+            raise ValueError(f"eta edges need {self.n_eta} values")
+        out = np.empty((self.n_bins, 5), dtype=np.float64)
+        L.check(L.lib().mi_plan_bin_table(self._h, *[e.ctypes.data for e in edges], float(px), float(lsd),
+                                          float(wavelength), out.ctypes.data), "mi_plan_bin_table")
+        return out
 
     def profile(self, cake: torch.Tensor, stream=None):
         """Kernel (c) on a given cake [F, n_r, n_eta] (float32/float64) -> (aw, sm) [F, n_r]."""
@@ -388,7 +411,8 @@ class CSRGeometry:
     semantics: str = "py"
     build_modes: Tuple[str, ...] = ("floor", "bilinear", "gradient")
     dtype: torch.dtype = torch.float32
-    plans: Dict[Tuple[str, bool], CakePlan] = field(default_factory=dict)
+    compute_variance: bool = False
+    plans: Dict[Tuple[str, bool, bool], CakePlan] = field(default_factory=dict)
 
     @property
     def n_bins(self) -> int:
@@ -398,19 +422,31 @@ class CSRGeometry:
     def device(self) -> torch.device:
         return self.area_per_bin.device
 
-    def plan(self, mode: str, normalize: bool = True) -> CakePlan:
+    def plan(self, mode: str, normalize: bool = True, variance: bool = False) -> CakePlan:
         if mode not in L.MODE:
             raise ValueError(f"unknown integration mode {mode!r}; expected 'floor' | 'bilinear' | 'gradient'")
         if mode not in self.build_modes:
             raise RuntimeError(f"build_csr was called without {mode!r} in build_modes; "
                                "rebuild with build_modes including this mode.")
-        key = (mode, bool(normalize))
+        if variance and not self.compute_variance:
+            raise RuntimeError(
+                f"build_csr was called without compute_variance=True (mode={mode!r}); "
+                "rebuild with compute_variance=True to use integrate_with_variance.")
+        key = (mode, bool(normalize), bool(variance))
         if key not in self.plans:
             self.plans[key] = CakePlan(self.pixmap, n_r=self.n_r, n_eta=self.n_eta,
                                        n_pixels_y=self.n_pixels_y, n_pixels_z=self.n_pixels_z,
                                        mode=mode, normalize=normalize, semantics=self.semantics,
-                                       bc_y=self.bc_y, bc_z=self.bc_z, device=self.device)
+                                       bc_y=self.bc_y, bc_z=self.bc_z, device=self.device,
+                                       variance=variance)
         return self.plans[key]
+
+    def any_plan(self, variance: bool = False) -> CakePlan:
+        """A plan of this geometry for the eta reductions (all plans share the bin areas)."""
+        for (_, _, v), p in self.plans.items():
+            if v == variance:
+                return p
+        return self.plan(self.build_modes[0], True, variance)
 
 
 def _area_in(pixmap: PixelMap, ny: int, nz: int) -> np.ndarray:
@@ -438,9 +474,10 @@ def _area_in(pixmap: PixelMap, ny: int, nz: int) -> np.ndarray:
 def build_csr(pixmap: PixelMap, *, n_r: int, n_eta: int, n_pixels_y: int, n_pixels_z: int,
               device="cuda", dtype: torch.dtype = torch.float32, bc_y: float = 0.0,
               bc_z: float = 0.0, build_modes: Tuple[str, ...] = ("floor", "bilinear", "gradient"),
-              semantics: str = "py") -> CSRGeometry:
+              compute_variance: bool = False, semantics: str = "py") -> CSRGeometry:
     """Prepare a map for integration (kernels.py:build_csr).  The per-mode device plans
-    are built lazily by the first ``integrate`` call of that mode."""
+    are built lazily by the first ``integrate`` call of that mode; ``compute_variance``
+    allows the variance plans of ``integrate_with_variance``."""
     if pixmap.n_bins != n_r * n_eta:
         raise ValueError(f"PixelMap has {pixmap.n_bins} bins; n_r * n_eta = {n_r * n_eta}")
     dev = torch.device("cuda", _device_index(device))
@@ -448,30 +485,64 @@ def build_csr(pixmap: PixelMap, *, n_r: int, n_eta: int, n_pixels_y: int, n_pixe
     return CSRGeometry(pixmap=pixmap, area_per_bin=torch.from_numpy(area).to(dev, dtype),
                        n_r=n_r, n_eta=n_eta, n_pixels_y=n_pixels_y, n_pixels_z=n_pixels_z,
                        bc_y=bc_y, bc_z=bc_z, semantics=semantics,
-                       build_modes=tuple(build_modes), dtype=dtype)
+                       build_modes=tuple(build_modes), dtype=dtype,
+                       compute_variance=bool(compute_variance))
 
 
 def integrate(image: torch.Tensor, geom: CSRGeometry, *, mode: str = "floor",
               normalize: bool = True) -> torch.Tensor:
     """Integrate one (dark-subtracted) image to the (n_r, n_eta) grid (kernels.py:integrate)."""
     plan = geom.plan(mode, normalize)
+    flat = _flat_image(image, geom, "image")
+    ck, _, _ = plan.integrate(flat.reshape(1, -1), cake=True, lineouts=False)
+    return ck[0].to(geom.dtype)
+
+
+def _flat_image(image: torch.Tensor, geom: CSRGeometry, what: str) -> torch.Tensor:
     flat = image.reshape(-1)
     if flat.numel() != geom.n_pixels_y * geom.n_pixels_z:
-        raise ValueError(f"image numel {flat.numel()} != n_pixels {geom.n_pixels_y * geom.n_pixels_z}")
+        raise ValueError(f"{what} numel {flat.numel()} != n_pixels {geom.n_pixels_y * geom.n_pixels_z}")
     flat = flat.to(geom.device)
     if flat.dtype not in _TORCH_DT:
         flat = flat.to(torch.float32)
-    ck, _, _ = plan.integrate(flat.reshape(1, -1), cake=True, lineouts=False)
-    return ck[0].to(geom.dtype)
+    return flat
+
+
+def integrate_with_variance(image: torch.Tensor, geom: CSRGeometry, *, mode: str = "floor",
+                            normalize: bool = True, variance_image: Optional[torch.Tensor] = None):
+    """Integrate one frame and propagate per-pixel variance (kernels.py:474-536):
+    (intensity, variance), both (n_r, n_eta).  ``variance_image`` None = Poisson (the
+    image is its own variance).  The variance is the cake of the variance image under
+    the squared coalesced weights, over the squared bin area when normalising."""
+    flat = _flat_image(image, geom, "image")
+    vflat = flat if variance_image is None else _flat_image(variance_image, geom, "variance_image")
+    vplan = geom.plan(mode, normalize, variance=True)
+    iplan = geom.plan(mode, normalize)
+    ck, _, _ = iplan.integrate(flat.reshape(1, -1), cake=True, lineouts=False)
+    vk, _, _ = vplan.integrate(vflat.reshape(1, -1), cake=True, lineouts=False)
+    return ck[0].to(geom.dtype), vk[0].to(geom.dtype)
 
 
 def profile_1d(int2d: torch.Tensor, geom: CSRGeometry, *, mode: str = "area_weighted") -> torch.Tensor:
     """Reduce (n_r, n_eta) -> (n_r,) over eta (kernels.py:profile_1d)."""
     if mode not in ("area_weighted", "simple_mean"):
         raise ValueError(f"unknown profile_1d mode {mode!r}")
-    plan = next(iter(geom.plans.values()), None) or geom.plan(geom.build_modes[0], True)
-    aw, sm = plan.profile(int2d.to(geom.device).reshape(1, geom.n_r, geom.n_eta))
+    aw, sm = geom.any_plan().profile(int2d.to(geom.device).reshape(1, geom.n_r, geom.n_eta))
     return (aw[0] if mode == "area_weighted" else sm[0]).to(geom.dtype)
+
+
+def profile_1d_with_variance(int2d: torch.Tensor, var2d: torch.Tensor, geom: CSRGeometry, *,
+                             mode: str = "area_weighted"):
+    """(I_1d, Var_1d) over eta (kernels.py:604-645): Var_1d = sum(A^2 Var) / (sum A)^2
+    (area_weighted) or sum(Var) / N^2 (simple_mean)."""
+    if mode not in ("area_weighted", "simple_mean"):
+        raise ValueError(f"unknown profile_1d_with_variance mode {mode!r}")
+    shape = (1, geom.n_r, geom.n_eta)
+    aw, sm = geom.any_plan().profile(int2d.to(geom.device).reshape(shape))
+    vaw, vsm = geom.any_plan(variance=True).profile(var2d.to(geom.device).reshape(shape))
+    if mode == "area_weighted":
+        return aw[0].to(geom.dtype), vaw[0].to(geom.dtype)
+    return sm[0].to(geom.dtype), vsm[0].to(geom.dtype)
 
 
 def r_axis(*, n_r: int, RMin: float, RBinSize: float) -> np.ndarray:

@@ -64,3 +64,35 @@ def fit_peaks(x, intensity, peak_locations, *, x_bin_size: float, fit_roi_paddin
     pt = torch.as_tensor(np.asarray(peak_locations, np.float64), device=device)
     r = fit_batch(xt, yt, pt, model=model, half_window=fit_roi_padding, x_bin=x_bin_size)
     return r.params[0, :, :7].cpu().numpy()
+
+
+PEAK_ROW_DTYPE = np.dtype([("frame_idx", "<i4"), ("eta_idx", "<i4"), ("peak_nr", "<i4"), ("eta_deg", "<f8"),
+                           ("area", "<f8"), ("sig", "<f8"), ("gam", "<f8"), ("FWHM_deg", "<f8"),
+                           ("eta_mix", "<f8"), ("chi_sq", "<f8"), ("center_2theta", "<f8"),
+                           ("d_spacing_A", "<f8")])
+
+
+def peak_rows(params, *, px_um: float, lsd_um: float, wavelength_a: float, eta_deg=None,
+              first_frame: int = 0, eta_idx: int = -1) -> np.ndarray:
+    """Output rows of the fitted peaks, one per (frame, peak), as pfio_make_row builds them
+    (FF_HEDM/src/PeakFitIO.c:52-82): the first seven fit outputs, the centre converted to
+    2-theta = atan(center * px / Lsd) (deg) and the d-spacing lambda / (2 sin theta)
+    (0 when theta <= 1e-10 rad).  params: [F, n_peaks, >= 7] fit outputs (``FitResult.params``)."""
+    p = params.detach().cpu().numpy() if hasattr(params, "detach") else np.asarray(params)
+    p = p.reshape(-1, p.shape[-2], p.shape[-1]) if p.ndim >= 2 else p.reshape(1, 1, -1)
+    F, n_peaks = p.shape[0], p.shape[1]
+    rows = np.zeros(F * n_peaks, dtype=PEAK_ROW_DTYPE)
+    flat = p.reshape(F * n_peaks, -1)
+    rows["frame_idx"] = np.repeat(np.arange(F, dtype=np.int32) + first_frame, n_peaks)
+    rows["eta_idx"] = eta_idx
+    rows["peak_nr"] = np.tile(np.arange(n_peaks, dtype=np.int32), F)
+    rows["eta_deg"] = 0.0 if eta_deg is None else eta_deg
+    for k, name in enumerate(("area", None, "sig", "gam", "FWHM_deg", "eta_mix", "chi_sq")):
+        if name:
+            rows[name] = flat[:, k]
+    tth = np.arctan(flat[:, 1] * px_um / lsd_um) * 180.0 / np.pi
+    theta = tth * np.pi / 360.0
+    rows["center_2theta"] = tth
+    with np.errstate(divide="ignore"):
+        rows["d_spacing_A"] = np.where(theta > 1e-10, wavelength_a / (2.0 * np.sin(theta)), 0.0)
+    return rows

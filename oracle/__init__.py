@@ -47,6 +47,8 @@ def lib() -> C.CDLL:
         L.or_integrate.restype = i
         L.or_area_in.argtypes = [vp, vp, C.c_int64, i, i, vp]
         L.or_area_in.restype = None
+        L.or_integrate_var.argtypes = [vp, vp, C.c_int64, i, i, d, d, vp, i, i, i, vp]
+        L.or_integrate_var.restype = i
         L.or_profile.argtypes = [vp, vp, i, i, vp, vp]
         L.or_profile.restype = None
         L.or_fit.argtypes = [vp, vp, i, d, i, i, i, d, d, d, vp]
@@ -95,6 +97,83 @@ def integrate(records, nmap, n_bins, ny, nz, image, *, mode="floor", semantics="
     if rc:
         raise ValueError(f"or_integrate failed ({rc})")
     return cake, area
+
+
+def integrate_var(records, nmap, n_bins, ny, nz, var_image, *, mode="floor", semantics="py", normalize=True,
+                  bc_y=0.0, bc_z=0.0):
+    """FP64 propagated bin variance (n_bins,) of a per-pixel variance image
+    (integrate_with_variance, kernels.py:474-536)."""
+    rec = _c(records, REC_DTYPE)
+    nm = _c(nmap, np.int32).reshape(-1)
+    img = _c(var_image, np.float64).reshape(-1)
+    out = np.zeros(n_bins)
+    rc = lib().or_integrate_var(rec.ctypes.data if rec.size else None, nm.ctypes.data, n_bins, ny, nz, bc_y, bc_z,
+                                img.ctypes.data, MODES[mode], SEMS[semantics], int(normalize), out.ctypes.data)
+    if rc:
+        raise ValueError(f"or_integrate_var failed ({rc})")
+    return out
+
+
+def profile_var(var_cake, area, n_r, n_eta):
+    """Variance halves of profile_1d_with_variance (kernels.py:604-645):
+    sum(A^2 V) / (sum A)^2 and sum(V) / N^2 over the valid (A > 1e-9) eta bins."""
+    v = _c(var_cake, np.float64).reshape(n_r, n_eta)
+    a = _c(area, np.float64).reshape(n_r, n_eta)
+    ok = a > 1e-9
+    av = np.where(ok, a, 0.0)
+    sa = av.sum(1)
+    n = ok.sum(1).astype(np.float64)
+    vaw = np.where(sa > 1e-9, (v * av * av).sum(1) / np.maximum(sa, 1e-9) ** 2, 0.0)
+    vsm = np.where(n > 0, np.where(ok, v, 0.0).sum(1) / np.maximum(n, 1.0) ** 2, 0.0)
+    return vaw, vsm
+
+
+def average_frames(frames):
+    """Per-pixel mean of k frames as the stream server's start-up computes it
+    (IntegratorFitPeaksGPUStream.cu:2216-2232): sequential FP64 sum, divide, cast to float."""
+    f = np.asarray(frames)
+    acc = np.zeros(f.shape[1:], dtype=np.float64)
+    for k in range(f.shape[0]):
+        acc += f[k].astype(np.float64)
+    return (acc / f.shape[0]).astype(np.float32)
+
+
+def decode_hybrid(payload: bytes, ny: int, nz: int):
+    """dtype-6 payload -> (nz, ny) float32 raw counts (image.py:83-123)."""
+    n = ny * nz
+    c = int(np.frombuffer(payload, dtype=np.uint32, count=1)[0])
+    if len(payload) != 4 + 2 * n + 12 * c:
+        raise ValueError("hybrid payload size mismatch")
+    out = np.frombuffer(payload, dtype=np.uint16, count=n, offset=4).astype(np.float32)
+    idx = np.frombuffer(payload, dtype=np.int32, count=c, offset=4 + 2 * n)
+    val = np.frombuffer(payload, dtype=np.int64, count=c, offset=4 + 2 * n + 4 * c)
+    out[idx] = val.astype(np.float32)
+    return out.reshape(nz, ny)
+
+
+def bin_table(records, nmap, n_r, n_eta, ny, nz, r_lo, r_hi, eta_lo, eta_hi, px, lsd, lam):
+    """[n_r*n_eta, 5] R mean, 2-theta (deg), eta mean, area, Q: the static header of the GPU
+    stream output (initialize_PerFrameArr_Area_kernel, IntegratorFitPeaksGPUStream.cu:817-899)."""
+    rec = _c(records, REC_DTYPE)
+    nm = _c(nmap, np.int32).reshape(-1, 2)
+    out = np.zeros((n_r * n_eta, 5))
+    for b in range(n_r * n_eta):
+        j, k = divmod(b, n_eta)
+        rm = (r_lo[j] + r_hi[j]) * 0.5
+        em = (eta_lo[k] + eta_hi[k]) * 0.5
+        tth = np.arctan(rm * px / lsd)
+        area = 0.0
+        for e in rec[nm[b, 1]:nm[b, 1] + max(nm[b, 0], 0)]:
+            y, z = e["y"], e["z"]
+            if y < 0 or y >= ny or z < 0 or z >= nz:
+                continue
+            flat = np.float32(np.float32(int(z) * ny) + y)
+            if int(flat) >= ny * nz:
+                continue
+            area += float(e["areaWeight"])
+        out[b] = (rm, (180.0 / np.pi) * tth, em, area,
+                  (4.0 * np.pi / lam) * np.sin(tth / 2.0) if lam > 0 else 0.0)
+    return out
 
 
 def area_in(records, nmap, n_bins, ny, nz):

@@ -15,6 +15,8 @@
  *      record's position, gradient shift in FP64 only when deltaR != 0 and R > 1, base
  *      pixel from floorf() of the float-rounded position, clamps under-then-over;
  *      normaliser = sum of all areaWeight); no floor mode.
+ * or_integrate_var follows integrate_with_variance (kernels.py:474-536): coalesced weights
+ *   squared against the variance image, over the squared normaliser.
  * or_profile follows profile_1d (kernels.py:567-601) = calculate_1D_profile_kernel and
  * calculate_1D_profile_simple_mean_kernel (IntegratorFitPeaksGPUStream.cu:1162-1334).
  * or_fit is the FP64 twin of the device Levenberg-Marquardt fitter (same window, same
@@ -24,6 +26,7 @@
 #include "oracle.h"
 
 #include <math.h>
+#include <stdlib.h>
 #include <string.h>
 
 #define AREA_THRESHOLD 1e-9
@@ -135,6 +138,129 @@ int or_integrate(const or_record *rec, const int32_t *nmap, int64_t n_bins, int 
     }
     cake[b] = out;
   }
+  return 0;
+}
+
+/* ------------------------------------------------------------------ variance
+ * or_integrate_var: integrate_with_variance (kernels.py:474-536).  The per-(bin, pixel)
+ * weights of every record (the terms or_integrate sums) are coalesced per bin, as the
+ * CSR's sum_duplicates does (_square_csr, kernels.py:378-400), squared and applied to the
+ * variance image; normalised bins divide by the squared normaliser. */
+typedef struct { long pix; double w; } or_term;
+
+static int term_cmp(const void *a, const void *b) {
+  const long x = ((const or_term *)a)->pix, y = ((const or_term *)b)->pix;
+  return (x > y) - (x < y);
+}
+
+static int corner_terms(int ny, int nz, long iy, long iz, double fy, double fz, double frac, or_term *t) {
+  (void)nz;
+  const long o = iz * (long)ny + iy;
+  t[0].pix = o;          t[0].w = frac * (1 - fy) * (1 - fz);
+  t[1].pix = o + 1;      t[1].w = frac * fy * (1 - fz);
+  t[2].pix = o + ny;     t[2].w = frac * (1 - fy) * fz;
+  t[3].pix = o + ny + 1; t[3].w = frac * fy * fz;
+  return 4;
+}
+
+/* the terms one record adds to its bin, per (mode, semantics), as or_integrate samples */
+static int record_terms(const or_record *e, int ny, int nz, double bc_y, double bc_z, int mode, int sem,
+                        or_term *t) {
+  const long npix = (long)ny * nz;
+  const double y = e->y, z = e->z;
+  if (mode == 0) {
+    if (sem == 1) {
+      long long zz = (long long)e->z;
+      float s = (float)(zz * (long long)ny) + e->y;
+      long long o = (long long)s;
+      if (o < 0 || o >= npix) return 0;
+      t[0].pix = (long)o; t[0].w = e->frac;
+      return 1;
+    }
+    const long ty = (long)y, tz = (long)z;
+    if (!(ty >= 0 && ty < ny && tz >= 0 && tz < nz)) return 0;
+    t[0].pix = tz * ny + ty; t[0].w = e->frac;
+    return 1;
+  }
+  double sy = y, sz = z;
+  if (sem == 2) {
+    if (mode == 2 && e->deltaR != 0.0f) {
+      double dy = y - bc_y, dz = z - bc_z;
+      double R = sqrt(dy * dy + dz * dz);
+      if (R > 1.0) { sy -= e->deltaR * dy / R; sz -= e->deltaR * dz / R; }
+    }
+    int iy = (int)floorf((float)sy), iz = (int)floorf((float)sz);
+    double fy = sy - iy, fz = sz - iz;
+    if (iy < 0) { iy = 0; fy = 0; }
+    if (iy >= ny - 1) { iy = ny - 2; fy = 1; }
+    if (iz < 0) { iz = 0; fz = 0; }
+    if (iz >= nz - 1) { iz = nz - 2; fz = 1; }
+    return corner_terms(ny, nz, iy, iz, fy, fz, e->frac, t);
+  }
+  if (mode == 2) {
+    if (sem == 1) {
+      float dy = e->y - (float)bc_y, dz = e->z - (float)bc_z;
+      float R = sqrtf(dy * dy + dz * dz);
+      float ry = e->y, rz = e->z;
+      if (R > 1.0f) { ry -= e->deltaR * dy / R; rz -= e->deltaR * dz / R; }
+      sy = ry; sz = rz;
+    } else {
+      double dy = y - bc_y, dz = z - bc_z;
+      double R = sqrt(dy * dy + dz * dz);
+      double sc = R > 1.0 ? (double)e->deltaR / R : 0.0;
+      sy = y - sc * dy; sz = z - sc * dz;
+    }
+  }
+  long iy = (long)floor(sy), iz = (long)floor(sz);
+  double fy = sy - (double)iy, fz = sz - (double)iz;
+  const int over_y = iy >= ny - 1, under_y = iy < 0, over_z = iz >= nz - 1, under_z = iz < 0;
+  if (over_y) { iy = ny - 2; fy = 1.0; }
+  if (under_y) { iy = 0; fy = 0.0; }
+  if (over_z) { iz = nz - 2; fz = 1.0; }
+  if (under_z) { iz = 0; fz = 0.0; }
+  return corner_terms(ny, nz, iy, iz, fy, fz, e->frac, t);
+}
+
+int or_integrate_var(const or_record *rec, const int32_t *nmap, int64_t n_bins, int ny, int nz, double bc_y,
+                     double bc_z, const double *var_image, int mode, int sem, int normalize, double *var_cake) {
+  if (sem == 2 && mode == 0) return -3;
+  or_term *buf = NULL;
+  long cap = 0;
+  for (int64_t b = 0; b < n_bins; ++b) {
+    const int cnt = nmap[2 * b], off = nmap[2 * b + 1];
+    if (cnt < 0) { free(buf); return -2; }
+    if (4L * cnt > cap) {
+      cap = 4L * cnt;
+      or_term *nb = (or_term *)realloc(buf, (size_t)cap * sizeof(or_term));
+      if (!nb) { free(buf); return -1; }
+      buf = nb;
+    }
+    long n = 0;
+    double A_in = 0.0, A_all = 0.0;
+    for (int k = 0; k < cnt; ++k) {
+      const or_record *e = rec + off + k;
+      const long ty = (long)(double)e->y, tz = (long)(double)e->z;
+      A_all += e->areaWeight;
+      if (ty >= 0 && ty < ny && tz >= 0 && tz < nz) A_in += e->areaWeight;
+      n += record_terms(e, ny, nz, bc_y, bc_z, mode, sem, buf + n);
+    }
+    qsort(buf, (size_t)n, sizeof(or_term), term_cmp);
+    double V = 0.0;
+    for (long i = 0; i < n;) {
+      double w = 0.0;
+      long j = i;
+      for (; j < n && buf[j].pix == buf[i].pix; ++j) w += buf[j].w;
+      V += w * w * var_image[buf[i].pix];
+      i = j;
+    }
+    double out;
+    if (sem == 1 || sem == 2)
+      out = A_all > AREA_THRESHOLD ? (normalize ? V / (A_all * A_all) : V) : 0.0;
+    else
+      out = normalize ? (A_in > AREA_THRESHOLD ? V / (A_in * A_in) : 0.0) : V;
+    var_cake[b] = out;
+  }
+  free(buf);
   return 0;
 }
 

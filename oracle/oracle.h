@@ -32,6 +32,12 @@ int or_integrate(const or_record *rec, const int32_t *nmap, int64_t n_bins, int 
 void or_area_in(const or_record *rec, const int32_t *nmap, int64_t n_bins, int ny, int nz,
                 double *area);
 
+/* integrate_with_variance: var_cake = sum over pixels of (coalesced weight)^2 * var_image,
+ * over the squared normaliser when normalising */
+int or_integrate_var(const or_record *rec, const int32_t *nmap, int64_t n_bins, int ny, int nz,
+                     double bc_y, double bc_z, const double *var_image, int mode, int sem, int normalize,
+                     double *var_cake);
+
 /* profile_1d: area-weighted (lo_aw) and simple-mean (lo_sm) eta reductions */
 void or_profile(const double *cake, const double *area_in, int n_r, int n_eta, double *lo_aw,
                 double *lo_sm);

@@ -45,6 +45,21 @@ def load_kernels_case(tag):
     return g
 
 
+def load_variance_case(tag):
+    g = dict(np.load(GOLDEN / f"variance_{tag}.npz"))
+    g["records"] = g["records"].view(REC_DTYPE)
+    g["nmap"] = np.stack([g["counts"], g["offsets"]], 1).astype(np.int32)
+    for k in ("ny", "nz", "n_r", "n_eta"):
+        g[k] = int(g[k])
+    for k in ("bc_y", "bc_z"):
+        g[k] = float(g[k])
+    return g
+
+
+def load_image_case():
+    return dict(np.load(GOLDEN / "image.npz"))
+
+
 def load_mapper_case(tag):
     g = dict(np.load(GOLDEN / f"mapper_{tag}.npz"))
     g["records"] = g["records"].view(REC_DTYPE)
@@ -57,6 +72,7 @@ def load_mapper_case(tag):
 
 KERNEL_CASES = ["a", "b", "c", "d"]
 MAPPER_CASES = ["m1", "m2", "m3"]
+VARIANCE_CASES = ["a", "b", "d"]
 
 
 def rel_err(x, ref, tau_frac=1e-3):

@@ -19,6 +19,13 @@ the reference's C mapper and integrator compiled into oracle/_ref, and writes:
                   (integration_apply_map) sums on a seeded image
   peakfit.npz     lineouts and the reference scipy TRF fit (peakfit.fit_peaks)
   header.npz      Map.bin header bytes and parameter hashes
+  variance_*.npz  the kernels_* maps with a variance image: integrate_with_variance
+                  (build_csr(compute_variance=True)) and profile_1d_with_variance, FP64,
+                  every mode, normalize on/off
+  image.npz       hybrid (dtype 6) payloads decoded by decode_hybrid_payload and a
+                  multi-frame int64 dark averaged by average_dark_frames
+
+Selected groups only: python tests/golden/make_golden.py variance image
 
 The fixtures are inputs/outputs only; nothing of the reference's source is copied.
 """
@@ -43,7 +50,7 @@ def ref_modules():
     pkg.__path__ = [str(PKG)]
     sys.modules["midas_integrate"] = pkg
     mods = {}
-    for name in ("bin_io", "kernels", "peakfit"):
+    for name in ("bin_io", "kernels", "peakfit", "image"):
         spec = importlib.util.spec_from_file_location(f"midas_integrate.{name}", PKG / f"{name}.py")
         m = importlib.util.module_from_spec(spec)
         sys.modules[f"midas_integrate.{name}"] = m
@@ -78,16 +85,88 @@ def random_pixmap(rng, ny, nz, n_r, n_eta, avg=6, oob_fraction=0.05, frac_y=Fals
     return recs, bins
 
 
+KERNEL_CASES = [
+    ("a", 0xC0FFEE, 64, 48, 8, 12, False),
+    ("b", 0xBEE, 33, 29, 5, 7, True),     # ragged shape, fractional sub-pixel y/z
+    ("c", 0xDEAD, 16, 16, 4, 6, False),
+    ("d", 123, 50, 70, 9, 11, True),
+]
+
+
+def variance_cases(M):
+    """The kernels_* maps again (same seeds), each with a variance image."""
+    import torch
+    bin_io, kernels = M["bin_io"], M["kernels"]
+    for tag, seed, ny, nz, n_r, n_eta, frac in KERNEL_CASES[:2] + KERNEL_CASES[3:]:
+        rng = np.random.default_rng(seed)
+        recs, bins = random_pixmap(rng, ny, nz, n_r, n_eta, frac_y=frac)
+        counts = np.array([len(b) for b in bins], np.int32)
+        offsets = np.zeros_like(counts)
+        offsets[1:] = np.cumsum(counts[:-1])
+        flat = [recs[i] for b in bins for i in b]
+        px = np.array(flat, dtype=bin_io.PXLIST_DTYPE)
+        pixmap = bin_io.PixelMap(pxList=px, counts=counts, offsets=offsets, map_header=None,
+                                 nmap_header=None)
+        vr = np.random.default_rng(seed + 1)
+        image = vr.uniform(0, 1000, size=(nz, ny))
+        var_image = image * vr.uniform(0.8, 1.5, size=(nz, ny)) + 4.0   # gain and read noise
+        bc_y, bc_z = ny / 2 + 0.3, nz / 2 - 0.2
+        geom = kernels.build_csr(pixmap, n_r=n_r, n_eta=n_eta, n_pixels_y=ny, n_pixels_z=nz,
+                                 dtype=torch.float64, bc_y=bc_y, bc_z=bc_z, compute_variance=True)
+        out = dict(records=px.view(np.uint8).copy(), counts=counts, offsets=offsets, image=image,
+                   var_image=var_image, ny=ny, nz=nz, n_r=n_r, n_eta=n_eta, bc_y=bc_y, bc_z=bc_z,
+                   area_per_bin=geom.area_per_bin.numpy())
+        for mode in ("floor", "bilinear", "gradient"):
+            for norm in (True, False):
+                key = f"{mode}_{'n' if norm else 'r'}"
+                I, V = kernels.integrate_with_variance(torch.from_numpy(image), geom, mode=mode, normalize=norm,
+                                                       variance_image=torch.from_numpy(var_image))
+                out[f"int_{key}"] = I.numpy().reshape(-1)
+                out[f"var_{key}"] = V.numpy().reshape(-1)
+                for pm in ("area_weighted", "simple_mean"):
+                    i1, v1 = kernels.profile_1d_with_variance(I, V, geom, mode=pm)
+                    out[f"i1_{pm}_{key}"] = i1.numpy()
+                    out[f"v1_{pm}_{key}"] = v1.numpy()
+        # Poisson default: variance_image=None uses the image itself
+        I, V = kernels.integrate_with_variance(torch.from_numpy(image), geom, mode="bilinear", normalize=True)
+        out["var_poisson_bilinear_n"] = V.numpy().reshape(-1)
+        np.savez_compressed(OUT / f"variance_{tag}.npz", **out)
+        print("wrote", OUT / f"variance_{tag}.npz", px.shape[0], "records")
+
+
+def image_case(M):
+    """Hybrid payloads (no overflow, a few overflows, overflows on the first and last
+    pixel) and an int64 multi-frame dark file, through the reference's decoders."""
+    import tempfile
+    im = M["image"]
+    rng = np.random.default_rng(606)
+    ny, nz = 37, 23
+    n = ny * nz
+    out = dict(ny=ny, nz=nz)
+    for k, n_over in enumerate((0, 9, 2)):
+        base = rng.integers(0, 65535, size=n).astype(np.uint16)
+        idx = rng.choice(n, size=n_over, replace=False).astype(np.int32)
+        if k == 2:
+            idx = np.array([0, n - 1], np.int32)
+        val = rng.integers(65536, 1 << 40, size=n_over).astype(np.int64)
+        payload = (np.array([n_over], np.uint32).tobytes() + base.tobytes() + idx.tobytes() + val.tobytes())
+        out[f"payload_{k}"] = np.frombuffer(payload, np.uint8).copy()
+        out[f"decoded_{k}"] = im.decode_hybrid_payload(payload, n_pixels_y=ny, n_pixels_z=nz)
+    dark = rng.integers(90, 130, size=(7, nz, ny)).astype(np.int64)
+    dark[:, 0, 0] = (1 << 40) + np.arange(7)        # large counts: the FP64 sum matters
+    with tempfile.TemporaryDirectory() as td:
+        f = Path(td) / "dark.bin"
+        dark.tofile(f)
+        out["dark_frames"] = dark
+        out["dark_mean"] = im.average_dark_frames(f, n_pixels_y=ny, n_pixels_z=nz, dtype="int64")
+    np.savez_compressed(OUT / "image.npz", **out)
+    print("wrote", OUT / "image.npz")
+
+
 def kernels_cases(M):
     import torch
     bin_io, kernels = M["bin_io"], M["kernels"]
-    cases = [
-        ("a", 0xC0FFEE, 64, 48, 8, 12, False),
-        ("b", 0xBEE, 33, 29, 5, 7, True),     # ragged shape, fractional sub-pixel y/z
-        ("c", 0xDEAD, 16, 16, 4, 6, False),
-        ("d", 123, 50, 70, 9, 11, True),
-    ]
-    for tag, seed, ny, nz, n_r, n_eta, frac in cases:
+    for tag, seed, ny, nz, n_r, n_eta, frac in KERNEL_CASES:
         rng = np.random.default_rng(seed)
         recs, bins = random_pixmap(rng, ny, nz, n_r, n_eta, frac_y=frac)
         counts = np.array([len(b) for b in bins], np.int32)
@@ -188,10 +267,11 @@ def header_case(M):
 
 def main():
     M = ref_modules()
-    kernels_cases(M)
-    mapper_cases()
-    peakfit_case(M)
-    header_case(M)
+    groups = {"kernels": lambda: kernels_cases(M), "mapper": mapper_cases, "peakfit": lambda: peakfit_case(M),
+              "header": lambda: header_case(M), "variance": lambda: variance_cases(M),
+              "image": lambda: image_case(M)}
+    for name in (sys.argv[1:] or list(groups)):
+        groups[name]()
 
 
 if __name__ == "__main__":

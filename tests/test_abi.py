@@ -73,3 +73,30 @@ def test_synth_descriptor_validation():
     d = L.MiSynthDesc()
     d.ny = 1
     assert L.lib().mi_synth_dark(C.byref(d), None, None) == L.MI_E_ARG
+
+
+def test_frame_preparation_argument_checks():
+    """Hybrid payload size and shape checks and the dark-average arguments are validated
+    on the host before any device call (buffers here are host memory never touched)."""
+    lib = L.lib()
+    buf = np.zeros(64, np.uint8)
+    p = buf.ctypes.data
+    assert lib.mi_decode_hybrid(None, 0, 4, 4, p, p, p, None) == L.MI_E_ARG
+    assert lib.mi_decode_hybrid(p, 10, 4, 4, p, p, p, None) == L.MI_E_ARG     # smaller than count + base
+    assert b"smaller" in lib.mi_last_error()
+    payload = np.zeros(4 + 2 * 16 + 12, np.uint8)
+    payload[:4] = np.frombuffer(np.uint32(2).tobytes(), np.uint8)            # claims 2 overflows, holds 1
+    assert lib.mi_decode_hybrid(payload.ctypes.data, payload.size, 4, 4, p, p, p, None) == L.MI_E_ARG
+    assert b"need" in lib.mi_last_error()
+    assert lib.mi_decode_hybrid(p, 40, 0, 4, p, p, p, None) == L.MI_E_ARG
+    assert lib.mi_average_frames(None, 1, 16, 2, 16, None, None) == L.MI_E_ARG
+    assert lib.mi_average_frames(p, 1, 16, 0, 16, p, None) == L.MI_E_ARG      # no frames
+    assert lib.mi_average_frames(p, 1, 16, 2, 8, p, None) == L.MI_E_ARG       # stride < pixels
+    assert lib.mi_average_frames(p, 6, 16, 2, 16, p, None) == L.MI_E_ARG      # hybrid is not a frame dtype
+    assert lib.mi_plan_bin_table(None, p, p, p, p, 1.0, 1.0, 0.0, p) == L.MI_E_ARG
+
+
+def test_plan_opts_layout_matches_header():
+    """mi_plan_opts: nine int32 fields, variance last."""
+    assert C.sizeof(L.MiPlanOpts) == 9 * 4
+    assert L.MiPlanOpts._fields_[-1][0] == "variance"

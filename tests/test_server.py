@@ -195,3 +195,24 @@ def test_threaded_server_with_concurrent_submitters():
             np.testing.assert_array_equal(r.lineout_aw, np.arange(1, 6) * f.sum())
     lat = srv.latency_ms()
     assert lat["n"] == 120 and lat["p99"] >= lat["p50"] > 0
+
+
+def test_peak_rows_two_theta_and_d_spacing():
+    """pfio_make_row (PeakFitIO.c:52-82): 2-theta from the centre in px, Bragg d-spacing."""
+    import math
+    from midas_b200.peakfit import peak_rows
+    params = np.zeros((2, 3, 11))
+    params[..., 0] = 5.0
+    params[..., 1] = [[300.0, 512.5, 0.0], [301.0, 700.0, 1e-9]]
+    params[..., 4] = 0.01
+    rows = peak_rows(params, px_um=200.0, lsd_um=1e6, wavelength_a=0.172979, first_frame=10)
+    assert rows.shape == (6,)
+    assert list(rows["frame_idx"]) == [10, 10, 10, 11, 11, 11]
+    assert list(rows["peak_nr"]) == [0, 1, 2, 0, 1, 2]
+    for r, c in zip(rows, params[..., 1].reshape(-1)):
+        tth = math.atan(c * 200.0 / 1e6) * 180.0 / math.pi
+        th = tth * math.pi / 360.0
+        assert r["center_2theta"] == tth
+        assert r["d_spacing_A"] == (0.172979 / (2.0 * math.sin(th)) if th > 1e-10 else 0.0)
+    assert rows["d_spacing_A"][2] == 0.0 and rows["d_spacing_A"][5] == 0.0
+    assert np.all(rows["area"] == 5.0) and np.all(rows["FWHM_deg"] == 0.01)
