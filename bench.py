@@ -46,7 +46,7 @@ def parse():
     ap.add_argument("--tile-rows", type=int, default=0)
     ap.add_argument("--tile-pixels", type=int, default=0)
     ap.add_argument("--fpl", type=int, default=0)
-    ap.add_argument("--encoding", default="auto", choices=["auto", "runs", "csr"])
+    ap.add_argument("--encoding", default="auto", choices=["auto", "runs", "csr", "mma"])
     ap.add_argument("--run-len", type=int, default=0)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-plain", action="store_true")

@@ -117,6 +117,11 @@ typedef struct {
 #define MI_ENC_AUTO 0      /* runs                                                       */
 #define MI_ENC_CSR 1       /* per-bin term lists, one warp per bin, lane = frame         */
 #define MI_ENC_RUNS 2      /* per-pixel radial runs: one staged value feeds run_len bins */
+#define MI_ENC_MMA 3       /* tensor cores (8/16-bit frames only): 12 x 4-bin tiles as dense
+                              int8 MMAs, frames split into two byte planes and weights into
+                              32-bit fixed point (relative to the bin's largest weight), exact
+                              int32 accumulation, FP64 recombination; other frame types get
+                              MI_E_UNSUPPORTED                                            */
 
 typedef struct {
   int64_t n_bins, n_r, n_eta;

@@ -47,7 +47,7 @@ class MiPlanOpts(C.Structure):
                 ("variance", C.c_int32)]
 
 
-ENC = {"auto": 0, "csr": 1, "runs": 2}
+ENC = {"auto": 0, "csr": 1, "runs": 2, "mma": 3}
 
 
 class MiPlanInfo(C.Structure):

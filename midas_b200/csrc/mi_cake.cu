@@ -357,7 +357,19 @@ int launch_cake(Plan *p, const void *frames, int dtype, int n_frames, int64_t st
   a.err = p->d_err;
   if (!a.want_cake && !a.want_lo) return MI_OK;
   int rc = MI_OK;
-  if (p->encoding == MI_ENC_RUNS) {
+  if (p->encoding == MI_ENC_MMA) {
+    // kernel (a) splits a chunk of frames into byte planes, then kernel (b) on the tensor cores
+    if (!(dtype == MI_DT_U16 || dtype == MI_DT_U8))
+      return set_error(MI_E_UNSUPPORTED, "MMA plans cake 8/16-bit frames only (dtype %d)", dtype);
+    const size_t es = dtype_size(dtype);
+    for (int f0 = 0; f0 < n_frames && rc == MI_OK; f0 += kMmaFrames) {
+      const int nf = std::min(kMmaFrames, n_frames - f0);
+      rc = launch_xc(p, 0, (const uint8_t *)frames + (size_t)f0 * stride * es, dtype, nf, stride, false, s);
+      if (rc == MI_OK)
+        rc = launch_mma(p, nf, cake ? cake + (size_t)f0 * p->n_bins : nullptr,
+                        p->d_partial + (size_t)f0 * p->n_r * p->n_slots * 2, a.want_lo, s);
+    }
+  } else if (p->encoding == MI_ENC_RUNS) {
     rc = launch_runs(p, frames, dtype, n_frames, stride, cake, a.want_lo, s);
   } else switch (dtype) {
     case MI_DT_U8: rc = launch_fpl<uint8_t>(p, a, s); break;

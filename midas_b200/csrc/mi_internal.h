@@ -219,6 +219,64 @@ struct XcChunk {
   int32_t z, y0, n, c0;  // detector row, first column, pixels, compact index of the first
 };
 
+// ---------------------------------------------------------------------------
+// MMA encoding (MI_ENC_MMA, kernel k_mma of mi_mma.cu): caking of 8/16-bit frames on the
+// tensor cores with exact integer arithmetic.  A tile is kMmaRows x kMmaCols bins (bin
+// n = row * kMmaCols + col) and its staged pixels in K slots; a frame batch is the M = 128
+// rows of the MMA.  Frames are split into two byte planes (lo, hi), weights into four
+// byte planes of a 32-bit fixed-point value q = round(w / w_max(bin) * (2^32 - 1)); the
+// eight u8 x u8 products accumulate exactly in int32 (five accumulators, one per byte
+// shift 0..4), and the epilogue recombines them in FP64:
+//   cake = fac * sum_k 2^(8k) acc_k - dk,  fac = w_max / (2^32 - 1) * scale,
+//   dk = fac * sum q * dark (the dark term of the bin, set with the dark).
+// The pixel-major buffer of an MMA plan holds two byte planes, [lo: n_xc x 128][hi: n_xc x
+// 128]: row c of a plane is compact pixel c's byte of 128 frames, its 16-byte granule g
+// (frames 16g .. 16g+15) at position g ^ (c % 8).
+// Blob of a tile (16-byte aligned arrays):
+//   MmaHdr                              32 B
+//   double fac[48], dk[48]; float lw[48]  per bin n of the tile (zeros for bins outside it);
+//                                       dk is written by the dark kernel when a dark is set
+//   uint2  runs[n_runs]                 {c, k0 | len << 8}: len consecutive K slots k0.. of a
+//                                       step staged from pixel-major rows c.. (one bulk copy
+//                                       per byte plane); slot k holds a pixel with
+//                                       c % 8 == k % 8 (the swizzle phase of its row)
+//   uint32 run_ptr[n_k + 1]             runs of K step s: [run_ptr[s], run_ptr[s+1])
+//   uint32 xrow[32 * n_k]               compact index of each slot, 0xFFFFFFFF = empty
+//   uint32 step_ptr[n_k + 1]            terms of K step s
+//   uint2  terms[n_terms]               {q, k | n << 16}, sorted by k
+struct MmaHdr {
+  int32_t n_rows, n_cols, r0, e0, n_k, n_terms;
+  int32_t box_rows;   // rows of the item's sub-band (12, 6, 3 or 1): the cake store's box height
+  int32_t n_runs;
+};
+static_assert(sizeof(MmaHdr) == 32, "MmaHdr layout");
+constexpr int kMmaRows = 12;           // R rows per tile
+constexpr int kMmaCols = 4;            // eta columns per tile (one 16-byte cake segment)
+constexpr int kMmaN = kMmaRows * kMmaCols;  // 48 bins: the N of every MMA
+constexpr int kMmaFrames = 128;        // frames per launch: the M of every MMA
+constexpr int kMmaKStep = 32;          // K slots (staged pixels) per MMA step
+constexpr uint32_t kMmaEmpty = 0xFFFFFFFFu;
+constexpr int kMmaMaxBinTerms = 16000; // int32 accumulators: 2 x 255 x 255 per term
+constexpr uint32_t kMmaBlobCap = 24 * 1024;  // largest tile blob (blob slots in shared memory)
+constexpr uint32_t kMmaBinsOff = 32;   // fac, dk, lw after the header
+constexpr uint32_t kMmaBinsBytes = kMmaN * (8 + 8 + 4);
+
+struct MmaBlob {
+  uint32_t runs, run_ptr, xrow, step_ptr, terms, bytes;
+};
+__host__ __device__ inline MmaBlob mma_blob_layout(int n_k, int n_runs, int n_terms) {
+  auto a16 = [](uint32_t x) { return (x + 15u) & ~15u; };
+  MmaBlob b;
+  uint32_t o = a16(kMmaBinsOff + kMmaBinsBytes);
+  b.runs = o;     o = a16(o + 8u * (uint32_t)n_runs);
+  b.run_ptr = o;  o = a16(o + 4u * (uint32_t)(n_k + 1));
+  b.xrow = o;     o = a16(o + 4u * (uint32_t)kMmaKStep * (uint32_t)n_k);
+  b.step_ptr = o; o = a16(o + 4u * (uint32_t)(n_k + 1));
+  b.terms = o;    o = a16(o + 8u * (uint32_t)n_terms);
+  b.bytes = o;
+  return b;
+}
+
 struct Plan {
   int device = 0;
   int mode = 0, normalize = 1, semantics = 0;
@@ -260,6 +318,7 @@ struct Plan {
   XcChunk *d_xchunks = nullptr;
   int n_xchunks = 0;
   uint8_t *d_xc = nullptr;       // [n_xc][kXcRowBytes]
+  int32_t *d_xc_pix = nullptr;   // MMA encoding: virtual pixel of each compact index
 
   // panels (a plan over several detectors sharing one binning): panel p's rows are rows
   // [z_off, z_off + nz) of a virtual detector ny pixels wide (ny = the widest panel)
@@ -296,6 +355,10 @@ int launch_xc(Plan *p, int panel, const void *frames, int dtype, int F, int64_t 
               cudaStream_t s);
 // Caking of frames [0, F) (F <= 128 u16 / 64 fp32) already staged pixel-major.
 int launch_runs_staged(Plan *p, bool as_f32, int F, float *cake, double *partial, bool want_lo, cudaStream_t s);
+// MMA encoding (mi_mma.cu): caking of frames [0, F) (F <= 128) staged as byte planes, and
+// the per-bin dark terms (after a dark is set)
+int launch_mma(Plan *p, int F, float *cake, double *partial, bool want_lo, cudaStream_t s);
+int launch_mma_dark(Plan *p, cudaStream_t s);
 // kernel (c): lineouts of frames [0, n_frames) from the plan's partial sums
 int launch_lineout(Plan *p, int n_frames, double *lo_aw, double *lo_sm, cudaStream_t s);
 int launch_plain(Plan *p, const void *frame, int dtype, double *cake, double *lo_aw,

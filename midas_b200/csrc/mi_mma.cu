@@ -1,0 +1,640 @@
+// mi_mma.cu -- kernel (b), MMA encoding: batched caking on the tensor cores (tcgen05, int8).
+//
+// Same contract as the run kernel (integrate() of packages/midas_integrate/midas_integrate/
+// kernels.py:416-473, integrate_noMapMask of FF_HEDM/src/IntegratorFitPeaksGPUStream.cu:
+// 975-1050): cake = diag(scale) W (frames - dark) plus the eta partial sums of both
+// lineouts, here for batches of up to 128 frames of 8/16-bit pixels.
+//
+// A tile (kMmaRows x kMmaCols = 48 bins) is a dense int8 product on the tensor cores:
+//   D[frame][bin] (int32, TMEM) += A[frame][pixel] (a byte plane of the frames)
+//                                  x B[pixel][bin] (a byte plane of the weights q)
+// two frame planes x four weight planes = eight tcgen05.mma per K step of 32 staged pixels,
+// into five int32 accumulators (one per byte shift 0..4).  Every product and sum is exact;
+// the epilogue forms sum_k 2^(8k) acc_k in FP64, subtracts the bin's dark term and scales:
+// cake = fac * value - dk.  The only approximation is the 32-bit fixed-point weight
+// (2^-33 of the bin's largest weight); the reference's fp32 (raw - dark) and fp32 sums are
+// replaced by exact integer sums, so the result is closer to the FP64 one.
+//
+// Operands in shared memory, per pipeline stage (one K step):
+//   A (frames): MN-major, 128B swizzle; slot k of the step is the 128-byte row
+//     (k % 8) * 128 + (k / 8) * 1024 holding the pixel's 128 frame bytes, 16-byte granule g
+//     at position g ^ (k % 8).  Kernel (a) writes each pixel-major row with its granules
+//     already in that order for phase c % 8, and the tiler puts pixel c in a slot with
+//     k % 8 == c % 8, so a slot is filled by one plain 128-byte bulk copy per plane.
+//   B (weights): K-major, no swizzle; byte (n, k) at (n % 8) * 16 + (n / 8) * 256 +
+//     (k % 16) + (k / 16) * 128, zeroed and then scattered from the step's terms.
+//
+// Roles (one persistent CTA per SM, 14 warps):
+//   warp 0          TMEM allocation (512 columns: two accumulator sets of 5 x 48) and, on one
+//                   lane, the MMA issue: 8 MMAs per K step, a commit that frees the stage, and
+//                   at a tile's last step a commit that hands the accumulators to the epilogue
+//   warp 1          loader: claims work items (heaviest first) and brings each tile's blob
+//                   into one of three blob slots with one bulk copy
+//   warps 2,3,12,13 producers: K step g (counted over the CTA's tiles) is built by producer
+//                   g % 4 into stage g % 6
+//   warps 4-11      epilogue: warp w reads TMEM lanes 32 (w % 4) + 0..31 (= frames) and half
+//                   of the tile's bins (8 bins x 5 accumulators at a time), recombines, puts the
+//                   cake values into a shared-memory tile that one TMA tensor store writes to
+//                   the [F][n_r][n_eta] cake (double-buffered), and accumulates the lineout
+//                   partial sums of the item's rows in registers (a frame's result does not
+//                   depend on the rest of its batch)
+// Every wait is an mbarrier poll with an iteration limit; on expiry the kernel sets the
+// plan's error word (MI_E_TIMEOUT) and the role leaves its loop.
+#include <cuda.h>
+#include <stdint.h>
+#include <string.h>
+
+#include <algorithm>
+
+#include "mi_internal.h"
+
+namespace mi {
+
+constexpr int kMmaStages = 6;
+constexpr int kMmaProducers = 4;
+constexpr int kMmaEpiWarps = 8;
+constexpr int kMmaWarps = 14;
+constexpr int kMmaThreads = kMmaWarps * 32;
+constexpr uint32_t kMmaStageBytes = 14336;   // A lo 4096 | A hi 4096 | B 4 x 1536
+constexpr uint32_t kMmaBPlane = 1536;
+constexpr int kMmaBlobSlotsMax = 4;
+constexpr int kMmaTmemCols = 512;
+constexpr int kMmaAccCols = 256;            // columns per accumulator set (5 x 48 used)
+constexpr uint32_t kMmaWaitLimit = 1u << 26;
+constexpr uint32_t kMmaOutBytes = kMmaFrames * kMmaN * 4;   // one cake tile: [128][rows][4] floats
+constexpr int kMmaBoxes = 4;                // cake store boxes of 12, 6, 3 and 1 rows
+
+struct MmaArgs {
+  CUtensorMap tmap[kMmaBoxes];  // the call's cake as (n_eta, n_r, F) floats, box 4 x h x 128
+  const WorkItem *items;
+  const TileRef *tiles;
+  const uint8_t *blobs;
+  const uint8_t *xc_lo, *xc_hi;   // pixel-major byte planes, 128 bytes per compact pixel
+  float *cake;
+  double *partial;          // [F][n_r][n_slots][2]
+  int F, n_r, n_eta, n_slots;
+  int64_t n_bins;
+  int want_cake, want_lo, use_tma;
+  int n_items;
+  int *counter;
+  int *err;
+  uint32_t blob_cap;
+  int n_blob;               // blob slots (3 or 4, as shared memory allows)
+};
+
+// Per-slot and per-stage tags passed between the roles through shared memory.
+struct MmaTag {
+  int32_t end, slot, first, last;   // end of work; item's lineout slot; first/last tile of item
+  int32_t r0, n_rows, e0, n_cols;   // the tile's bins
+  int32_t tile, step, n_k, box;     // tile sequence number of the CTA, K step, K steps, box rows
+};
+
+struct MmaSmem {
+  uint32_t off_out, off_blob, off_shdr, off_btag, off_atag, off_bar, off_tmem, total;
+};
+
+__host__ __device__ inline MmaSmem mma_smem_layout(uint32_t blob_cap, int n_blob) {
+  MmaSmem L;
+  uint32_t o = (uint32_t)kMmaStages * kMmaStageBytes;
+  L.off_out = o;   o += 2u * kMmaOutBytes;
+  L.off_blob = o;  o += (uint32_t)n_blob * blob_cap;
+  L.off_shdr = o;  o += (uint32_t)kMmaStages * sizeof(MmaTag);
+  L.off_btag = o;  o += (uint32_t)kMmaBlobSlotsMax * sizeof(MmaTag);
+  L.off_atag = o;  o += 2u * sizeof(MmaTag);
+  L.off_bar = o;   o += 8u * (2u * kMmaStages + 2u * kMmaBlobSlotsMax + 4u);
+  L.off_tmem = o;  o += 16u;
+  L.total = o + 1024u;   // the base is rounded up to 1024 bytes inside the kernel
+  return L;
+}
+
+__device__ __forceinline__ uint32_t m_smem(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ bool m_wait(uint64_t *bar, uint32_t parity) {
+  const uint32_t a = m_smem(bar);
+  for (uint32_t it = 0; it < kMmaWaitLimit; ++it) {
+    uint32_t done;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(done)
+        : "r"(a), "r"(parity)
+        : "memory");
+    if (done) return true;
+  }
+  return false;
+}
+
+__device__ __forceinline__ void m_arrive(uint64_t *bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(m_smem(bar)) : "memory");
+}
+__device__ __forceinline__ void m_arrive_tx(uint64_t *bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(m_smem(bar)), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ void m_expect_tx(uint64_t *bar, uint32_t bytes) {
+  asm volatile("mbarrier.expect_tx.relaxed.cta.shared::cta.b64 [%0], %1;" ::"r"(m_smem(bar)), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ void m_copy(void *dst, const void *src, uint32_t bytes, uint64_t *bar) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(m_smem(dst)),
+      "l"(src), "r"(bytes), "r"(m_smem(bar))
+      : "memory");
+}
+
+// shared-memory matrix descriptors (version 1): start address, leading / stride byte
+// offsets in 16-byte units, layout type in bits 61-63 (0 = no swizzle, 2 = 128B swizzle)
+__device__ __forceinline__ uint64_t m_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo, uint32_t layout) {
+  return (uint64_t)((saddr >> 4) & 0x3FFFu) | ((uint64_t)((lbo >> 4) & 0x3FFFu) << 16) |
+         ((uint64_t)((sbo >> 4) & 0x3FFFu) << 32) | (1ull << 46) | ((uint64_t)layout << 61);
+}
+
+// instruction descriptor, kind::i8: D s32, A u8 MN-major, B u8 K-major, M = 128, N = 48
+constexpr uint32_t kMmaIdesc = (2u << 4) | (1u << 15) | ((uint32_t)(kMmaN >> 3) << 17) | ((uint32_t)(kMmaFrames >> 4) << 24);
+
+__device__ __forceinline__ void m_mma(uint32_t d_tmem, uint64_t adesc, uint64_t bdesc, uint32_t accumulate) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n" ::"r"(d_tmem),
+      "l"(adesc), "l"(bdesc), "r"(kMmaIdesc), "r"(accumulate), "r"(0u), "r"(0u), "r"(0u), "r"(0u));
+}
+__device__ __forceinline__ void m_commit(uint64_t *bar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(m_smem(bar))
+               : "memory");
+}
+__device__ __forceinline__ void m_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void m_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+
+__device__ __forceinline__ void m_ld16(uint32_t taddr, uint32_t *r) {
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
+      "%15}, [%16];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]), "=r"(r[8]),
+        "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+      : "r"(taddr));
+}
+__device__ __forceinline__ void m_ld8(uint32_t taddr, uint32_t *r) {
+  asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+               : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7])
+               : "r"(taddr));
+}
+__device__ __forceinline__ void m_ld_wait() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
+
+// non-negative int32 -> double exactly, on the FP64 pipe: 2^52 + x has x in its low bits
+__device__ __forceinline__ double m_u2d(uint32_t x) { return __hiloint2double(0x43300000, (int)x) - 4503599627370496.0; }
+
+__global__ void __launch_bounds__(kMmaThreads, 1) k_mma(const __grid_constant__ MmaArgs a) {
+  extern __shared__ uint8_t smem_raw[];
+  // 1024-byte aligned base: the swizzled A operand's atoms start on 1024-byte boundaries
+  const uint32_t raw = m_smem(smem_raw);
+  uint8_t *smem = smem_raw + (((raw + 1023u) & ~1023u) - raw);
+  const MmaSmem L = mma_smem_layout(a.blob_cap, a.n_blob);
+  const int NB = a.n_blob;
+  MmaTag *s_shdr = (MmaTag *)(smem + L.off_shdr);
+  MmaTag *s_btag = (MmaTag *)(smem + L.off_btag);
+  MmaTag *s_atag = (MmaTag *)(smem + L.off_atag);
+  uint64_t *bar = (uint64_t *)(smem + L.off_bar);
+  uint64_t *full = bar, *empty = bar + kMmaStages;
+  uint64_t *bfull = bar + 2 * kMmaStages, *bempty = bfull + kMmaBlobSlotsMax;
+  uint64_t *afull = bempty + kMmaBlobSlotsMax, *aempty = afull + 2;
+  uint32_t *s_tmem = (uint32_t *)(smem + L.off_tmem);
+
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  if (tid == 0) {
+    for (int q = 0; q < kMmaStages; ++q) {
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(m_smem(&full[q])) : "memory");
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(m_smem(&empty[q])) : "memory");
+    }
+    for (int q = 0; q < kMmaBlobSlotsMax; ++q) {
+      // a blob slot is free again when the producers have built its stages and the epilogue
+      // has used its per-bin factors
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(m_smem(&bfull[q])) : "memory");
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(m_smem(&bempty[q])),
+                   "r"(kMmaProducers + kMmaEpiWarps)
+                   : "memory");
+    }
+    for (int q = 0; q < 2; ++q) {
+      // two arrivals: the MMA lane's (after it wrote the set's tag) and the commit of the
+      // tile's last MMAs
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 2;" ::"r"(m_smem(&afull[q])) : "memory");
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(m_smem(&aempty[q])), "r"(kMmaEpiWarps)
+                   : "memory");
+    }
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(m_smem(s_tmem)),
+                 "r"(kMmaTmemCols)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  m_fence_before();
+  __syncthreads();
+  m_fence_after();
+  const uint32_t tmem = *s_tmem;
+
+  if (warp == 0) {
+    // ================= MMA issue (one lane)
+    if (lane == 0) {
+      bool ok = true;
+      for (uint32_t g = 0;; ++g) {
+        const int q = (int)(g % kMmaStages);
+        if (!m_wait(&full[q], (g / kMmaStages) & 1u)) { ok = false; break; }
+        const MmaTag h = s_shdr[q];
+        if (h.end) {
+          // no more tiles: pass the end marker to the epilogue through the next set
+          const int ab = h.tile & 1;
+          if (!m_wait(&aempty[ab], ((uint32_t)(h.tile >> 1) & 1u) ^ 1u)) { ok = false; break; }
+          s_atag[ab] = h;
+          m_arrive(&afull[ab]);
+          m_arrive(&afull[ab]);
+          break;
+        }
+        const int ab = h.tile & 1;
+        if (h.step == 0) {
+          if (!m_wait(&aempty[ab], ((uint32_t)(h.tile >> 1) & 1u) ^ 1u)) { ok = false; break; }
+          s_atag[ab] = h;
+          m_arrive(&afull[ab]);
+        }
+        m_fence_after();
+        const uint32_t sb = m_smem(smem + (size_t)q * kMmaStageBytes);
+        const uint32_t dbase = tmem + (uint32_t)(ab * kMmaAccCols);
+#pragma unroll
+        for (int v = 0; v < 2; ++v) {
+          const uint64_t ad = m_desc(sb + 4096u * v, 0u, 1024u, 2u);
+#pragma unroll
+          for (int j = 0; j < 4; ++j) {
+            const uint64_t bd = m_desc(sb + 8192u + kMmaBPlane * j, 128u, 256u, 0u);
+            const int k = v + j;
+            // the first product into each accumulator of a tile starts it from zero
+            const uint32_t acc = (h.step > 0 || (v == 1 && j < 3)) ? 1u : 0u;
+            m_mma(dbase + (uint32_t)(k * kMmaN), ad, bd, acc);
+          }
+        }
+        m_commit(&empty[q]);
+        if (h.step == h.n_k - 1) m_commit(&afull[ab]);
+      }
+      if (!ok) atomicExch(a.err, MI_E_TIMEOUT);
+    }
+    __syncwarp();
+  } else if (warp == 1) {
+    // ================= loader: items -> tile blobs
+    int j = 0;
+    bool ok = true;
+    for (;;) {
+      int claimed = 0;
+      if (lane == 0) claimed = atomicAdd(a.counter, 1);
+      claimed = __shfl_sync(0xffffffffu, claimed, 0);
+      if (claimed >= a.n_items) break;
+      const WorkItem it = a.items[claimed];
+      const int nt = it.tile_end - it.tile_begin;
+      for (int t = 0; t < nt && ok; ++t, ++j) {
+        const int sl = j % NB;
+        if (lane == 0) {
+          const TileRef tr = a.tiles[it.tile_begin + t];
+          if (!m_wait(&bempty[sl], ((uint32_t)(j / NB) & 1u) ^ 1u)) {
+            ok = false;
+          } else {
+            MmaTag tg{};
+            tg.end = 0;
+            tg.slot = it.slot;
+            tg.first = (t == 0);
+            tg.last = (t == nt - 1);
+            tg.tile = j;
+            s_btag[sl] = tg;
+            uint8_t *dst = smem + L.off_blob + (size_t)sl * a.blob_cap;
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+            m_arrive_tx(&bfull[sl], tr.bytes);
+            m_copy(dst, a.blobs + tr.off, tr.bytes, &bfull[sl]);
+          }
+        }
+        ok = __shfl_sync(0xffffffffu, ok ? 1 : 0, 0) != 0;
+      }
+      if (!ok) break;
+    }
+    if (lane == 0) {
+      const int sl = j % NB;
+      if (ok && m_wait(&bempty[sl], ((uint32_t)(j / NB) & 1u) ^ 1u)) {
+        MmaTag tg{};
+        tg.end = 1;
+        tg.tile = j;
+        s_btag[sl] = tg;
+        m_arrive(&bfull[sl]);
+      } else {
+        atomicExch(a.err, MI_E_TIMEOUT);
+      }
+    }
+    __syncwarp();
+  } else if (warp == 2 || warp == 3 || warp >= 4 + kMmaEpiWarps) {
+    // ================= producers: stages (weight planes + frame planes) of K steps
+    const int pw = warp < 4 ? warp - 2 : warp - (2 + kMmaEpiWarps);
+    uint32_t g = 0;
+    bool ok = true;
+    for (int j = 0; ok; ++j) {
+      const int sl = j % NB;
+      if (!m_wait(&bfull[sl], (uint32_t)(j / NB) & 1u)) { ok = false; break; }
+      const MmaTag bt = s_btag[sl];
+      const uint8_t *blob = smem + L.off_blob + (size_t)sl * a.blob_cap;
+      if (bt.end) {
+        if ((int)(g % kMmaProducers) == pw) {
+          const int q = (int)(g % kMmaStages);
+          if (lane == 0) {
+            if (m_wait(&empty[q], ((g / kMmaStages) & 1u) ^ 1u)) {
+              MmaTag e = bt;
+              s_shdr[q] = e;
+              m_arrive(&full[q]);
+            } else {
+              atomicExch(a.err, MI_E_TIMEOUT);
+            }
+          }
+        }
+        break;
+      }
+      const MmaHdr hd = *(const MmaHdr *)blob;
+      const MmaBlob BL = mma_blob_layout(hd.n_k, hd.n_runs, hd.n_terms);
+      const uint2 *runs = (const uint2 *)(blob + BL.runs);
+      const uint32_t *rptr = (const uint32_t *)(blob + BL.run_ptr);
+      const uint32_t *sp = (const uint32_t *)(blob + BL.step_ptr);
+      const uint2 *terms = (const uint2 *)(blob + BL.terms);
+      for (int s = 0; s < hd.n_k; ++s, ++g) {
+        if ((int)(g % kMmaProducers) != pw) continue;
+        const int q = (int)(g % kMmaStages);
+        bool got = true;
+        if (lane == 0) got = m_wait(&empty[q], ((g / kMmaStages) & 1u) ^ 1u);
+        if (!__shfl_sync(0xffffffffu, got ? 1 : 0, 0)) { ok = false; break; }
+        uint8_t *st = smem + (size_t)q * kMmaStageBytes;
+        // frame planes: one bulk copy per run of consecutive pixels and plane; slot k of the
+        // step is the 128-byte row k of each plane's operand
+        const int r0s = (int)rptr[s], nrun = (int)rptr[s + 1] - r0s;   // <= 32
+        uint2 rn = make_uint2(0u, 0u);
+        if (lane < nrun) rn = runs[r0s + lane];
+        const uint32_t len = rn.y >> 8;
+        const uint32_t bytes = __reduce_add_sync(0xffffffffu, len) * 256u;
+        if (lane == 0) m_expect_tx(&full[q], bytes);
+        __syncwarp();
+        if (len) {
+          const uint32_t ro = (rn.y & 0xFFu) * 128u;
+          m_copy(st + ro, a.xc_lo + (size_t)rn.x * 128u, len * 128u, &full[q]);
+          m_copy(st + 4096u + ro, a.xc_hi + (size_t)rn.x * 128u, len * 128u, &full[q]);
+        }
+        // weight planes: zero, then the step's terms
+        uint4 *bz = (uint4 *)(st + 8192u);
+        for (int i = lane; i < (int)(4u * kMmaBPlane / 16u); i += 32) bz[i] = make_uint4(0u, 0u, 0u, 0u);
+        __syncwarp();
+        const int t0 = (int)sp[s], t1 = (int)sp[s + 1];
+        for (int t = t0 + lane; t < t1; t += 32) {
+          const uint2 tm = terms[t];
+          const uint32_t kk = (tm.y & 0xFFFFu) - (uint32_t)s * kMmaKStep, n = tm.y >> 16;
+          const uint32_t off = (n & 7u) * 16u + (n >> 3) * 256u + (kk & 15u) + (kk >> 4) * 128u;
+          uint8_t *b0 = st + 8192u + off;
+          b0[0] = (uint8_t)(tm.x & 0xFFu);
+          b0[kMmaBPlane] = (uint8_t)((tm.x >> 8) & 0xFFu);
+          b0[2 * kMmaBPlane] = (uint8_t)((tm.x >> 16) & 0xFFu);
+          b0[3 * kMmaBPlane] = (uint8_t)(tm.x >> 24);
+        }
+        if (lane == 0) {
+          MmaTag h = bt;
+          h.r0 = hd.r0;
+          h.n_rows = hd.n_rows;
+          h.e0 = hd.e0;
+          h.n_cols = hd.n_cols;
+          h.step = s;
+          h.n_k = hd.n_k;
+          h.box = hd.box_rows;
+          s_shdr[q] = h;
+        }
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        __syncwarp();
+        if (lane == 0) m_arrive(&full[q]);
+      }
+      __syncwarp();
+      if (lane == 0) m_arrive(&bempty[sl]);
+    }
+    if (!ok && lane == 0) atomicExch(a.err, MI_E_TIMEOUT);
+    __syncwarp();
+  } else {
+    // ================= epilogue: TMEM -> cake tile (TMA store) + lineout partials
+    constexpr int kHalf = kMmaN / 2;               // bins per epilogue warp
+    constexpr int kHalfRows = kHalf / kMmaCols;
+    const int e = warp - 4, quad = warp & 3, half = e >> 2;
+    const int m = quad * 32 + lane;                 // frame of the launch
+    const bool live = m < a.F;
+    const bool issuer = e == 0 && lane == 0;
+    double saw[kHalfRows], ssm[kHalfRows];
+#pragma unroll
+    for (int i = 0; i < kHalfRows; ++i) saw[i] = ssm[i] = 0.0;
+    for (int j = 0;; ++j) {
+      const int ab = j & 1;
+      bool got = true;
+      if (lane == 0) got = m_wait(&afull[ab], (uint32_t)(j >> 1) & 1u);
+      if (!__shfl_sync(0xffffffffu, got ? 1 : 0, 0)) {
+        if (lane == 0) atomicExch(a.err, MI_E_TIMEOUT);
+        break;
+      }
+      m_fence_after();
+      const MmaTag tg = s_atag[ab];
+      if (tg.end) break;
+      if (tg.first) {
+#pragma unroll
+        for (int i = 0; i < kHalfRows; ++i) saw[i] = ssm[i] = 0.0;
+      }
+      float *ot = (float *)(smem + L.off_out + (uint32_t)(j & 1) * kMmaOutBytes);   // [128][box][4]
+      if (a.use_tma) {
+        // the store issued from this buffer two tiles ago has read it
+        if (issuer) asm volatile("cp.async.bulk.wait_group.read 1;" ::: "memory");
+        asm volatile("bar.sync 1, %0;" ::"r"(kMmaEpiWarps * 32) : "memory");
+      }
+      const uint32_t tbase = tmem + ((uint32_t)(quad * 32) << 16) + (uint32_t)(ab * kMmaAccCols + kHalf * half);
+      float *crow = a.cake + (size_t)m * (size_t)a.n_bins;
+      // the tile's per-bin factors stay in its blob slot until every epilogue warp is done
+      const uint8_t *bb = smem + L.off_blob + (size_t)(j % NB) * a.blob_cap + kMmaBinsOff;
+      const double *bfac = (const double *)bb + kHalf * half;
+      const double *bdk = (const double *)bb + kMmaN + kHalf * half;
+      const float *blw = (const float *)(bb + 16 * kMmaN) + kHalf * half;
+#pragma unroll
+      for (int c = 0; c < kHalf / 8; ++c) {
+        uint32_t r[5][8];
+#pragma unroll
+        for (int k = 0; k < 5; ++k) m_ld8(tbase + (uint32_t)(k * kMmaN + 8 * c), r[k]);
+        m_ld_wait();
+        if (c == kHalf / 8 - 1) {
+          // every accumulator of the set has been read: hand it back to the MMA lane
+          m_fence_before();
+          __syncwarp();
+          if (lane == 0) m_arrive(&aempty[ab]);
+        }
+        // bins outside the tile have fac = dk = lw = 0: no branches
+        float o[8];
+#pragma unroll
+        for (int i = 0; i < 8; ++i) {
+          const int lrow = (8 * c + i) / kMmaCols;
+          const double x4 = m_u2d(r[4][i]), x3 = m_u2d(r[3][i]), x2 = m_u2d(r[2][i]), x1 = m_u2d(r[1][i]),
+                       x0 = m_u2d(r[0][i]);
+          const double v = fma(fma(x4, 256.0, x3), 65536.0, fma(fma(x2, 256.0, x1), 256.0, x0));
+          const double res = fma(bfac[8 * c + i], v, -bdk[8 * c + i]);
+          const float l = blw[8 * c + i];
+          o[i] = (float)res;
+          saw[lrow] = fma(res, (double)l, saw[lrow]);
+          ssm[lrow] += (l > 0.0f) ? res : 0.0;
+        }
+        if (!a.use_tma && live && a.want_cake) {
+#pragma unroll
+          for (int i = 0; i < 8; ++i) {
+            const int n = kHalf * half + 8 * c + i, row = n / kMmaCols, col = n % kMmaCols;
+            if (row < tg.n_rows && col < tg.n_cols) crow[(int64_t)(tg.r0 + row) * a.n_eta + tg.e0 + col] = o[i];
+          }
+        }
+        if (a.use_tma) {
+          // rows 2c, 2c+1 of this warp's half: one float4 each, if inside the store box
+#pragma unroll
+          for (int q = 0; q < 2; ++q) {
+            const int row = kHalfRows * half + 2 * c + q;
+            if (row < tg.box) *(float4 *)(ot + ((size_t)m * tg.box + row) * kMmaCols) =
+                make_float4(o[4 * q], o[4 * q + 1], o[4 * q + 2], o[4 * q + 3]);
+          }
+        }
+      }
+      if (a.use_tma) {
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        asm volatile("bar.sync 1, %0;" ::"r"(kMmaEpiWarps * 32) : "memory");
+        if (issuer) {
+          const int bi = tg.box == kMmaRows ? 0 : (tg.box == 6 ? 1 : (tg.box == 3 ? 2 : 3));
+          asm volatile(
+              "cp.async.bulk.tensor.3d.global.shared::cta.bulk_group [%0, {%1, %2, %3}], [%4];" ::"l"(&a.tmap[bi]),
+              "r"(tg.e0), "r"(tg.r0), "r"(0), "r"(m_smem(ot))
+              : "memory");
+          asm volatile("cp.async.bulk.commit_group;" ::: "memory");
+        }
+      }
+      __syncwarp();
+      if (lane == 0) m_arrive(&bempty[j % NB]);   // this warp is done with the tile's blob
+      if (tg.last && a.want_lo && live) {
+#pragma unroll
+        for (int i = 0; i < kHalfRows; ++i) {
+          const int row = kHalfRows * half + i;
+          if (row < tg.n_rows) {
+            double *dst = a.partial + (((int64_t)m * a.n_r + tg.r0 + row) * a.n_slots + tg.slot) * 2;
+            dst[0] = saw[i];
+            dst[1] = ssm[i];
+          }
+        }
+      }
+    }
+    if (issuer) asm volatile("cp.async.bulk.wait_group 0;" ::: "memory");
+  }
+  m_fence_before();
+  __syncthreads();
+  if (warp == 0) {
+    m_fence_after();
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kMmaTmemCols) : "memory");
+  }
+}
+
+// dark term of each bin: dk = fac * sum over the bin's terms of q * dark[pixel], written into
+// the tile's blob; one block per tile, thread n summing bin n's terms in blob order
+// (deterministic)
+__global__ void k_mma_dark(const TileRef *tiles, uint8_t *blobs, const int32_t *xc_pix, const float *dark,
+                           int has_dark) {
+  const TileRef tr = tiles[blockIdx.x];
+  uint8_t *blob = blobs + tr.off;
+  const MmaHdr hd = *(const MmaHdr *)blob;
+  const MmaBlob BL = mma_blob_layout(hd.n_k, hd.n_runs, hd.n_terms);
+  const uint32_t *xrow = (const uint32_t *)(blob + BL.xrow);
+  const uint2 *terms = (const uint2 *)(blob + BL.terms);
+  const int n = threadIdx.x;
+  if (n >= kMmaN) return;
+  const double *fac = (const double *)(blob + kMmaBinsOff);
+  double *dk = (double *)(blob + kMmaBinsOff) + kMmaN;
+  double d = 0.0;
+  if (has_dark)
+    for (int t = 0; t < hd.n_terms; ++t) {
+      const uint2 tm = terms[t];
+      if ((int)(tm.y >> 16) != n) continue;
+      d += (double)tm.x * (double)dark[xc_pix[xrow[tm.y & 0xFFFFu]]];
+    }
+  dk[n] = fac[n] * d;
+}
+
+typedef CUresult (*EncodeTiledFn)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
+                                  const cuuint64_t *, const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave,
+                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+// cuTensorMapEncodeTiled through the runtime's driver entry point (no link to libcuda)
+static EncodeTiledFn encode_tiled() {
+  static EncodeTiledFn fn = nullptr;
+  static bool tried = false;
+  if (!tried) {
+    tried = true;
+    void *f = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPointByVersion("cuTensorMapEncodeTiled", &f, 12000, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = (EncodeTiledFn)f;
+  }
+  return fn;
+}
+
+int launch_mma(Plan *p, int F, float *cake, double *partial, bool want_lo, cudaStream_t s) {
+  if (F <= 0 || F > kMmaFrames) return set_error(MI_E_ARG, "launch_mma: %d frames (1..%d)", F, kMmaFrames);
+  MmaArgs a;
+  memset(&a, 0, sizeof(a));
+  a.items = p->d_items;
+  a.tiles = p->d_tiles;
+  a.blobs = p->d_blobs;
+  a.xc_lo = p->d_xc;
+  a.xc_hi = p->d_xc + (size_t)p->n_xc * 128;
+  a.cake = cake;
+  a.partial = partial;
+  a.F = F;
+  a.n_r = p->n_r;
+  a.n_eta = p->n_eta;
+  a.n_slots = p->n_slots;
+  a.n_bins = p->n_bins;
+  a.want_cake = cake != nullptr;
+  a.want_lo = want_lo;
+  a.n_items = p->n_items;
+  a.counter = p->d_ctr;
+  a.err = p->d_err;
+  a.blob_cap = (p->max_blob + 15u) & ~15u;
+  if (a.blob_cap > kMmaBlobCap) return set_error(MI_E_RANGE, "launch_mma: tile blob of %u B", a.blob_cap);
+  // cake tiles leave through TMA tensor stores when the cake rows are 16-byte multiples
+  // (n_eta % 4 == 0) and the cake is 16-byte aligned; otherwise through plain stores
+  a.use_tma = 0;
+  if (cake && p->n_eta % kMmaCols == 0 && (uintptr_t)cake % 16 == 0) {
+    EncodeTiledFn enc = encode_tiled();
+    if (!enc) return set_error(MI_E_CUDA, "launch_mma: cuTensorMapEncodeTiled is not available");
+    const cuuint64_t dims[3] = {(cuuint64_t)p->n_eta, (cuuint64_t)p->n_r, (cuuint64_t)F};
+    const cuuint64_t strides[2] = {(cuuint64_t)p->n_eta * 4u, (cuuint64_t)p->n_bins * 4u};
+    const cuuint32_t estr[3] = {1, 1, 1};
+    const int rows[kMmaBoxes] = {kMmaRows, 6, 3, 1};
+    for (int i = 0; i < kMmaBoxes; ++i) {
+      const cuuint32_t box[3] = {(cuuint32_t)kMmaCols, (cuuint32_t)rows[i], (cuuint32_t)kMmaFrames};
+      const CUresult r = enc(&a.tmap[i], CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, cake, dims, strides, box, estr,
+                             CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                             CU_TENSOR_MAP_L2_PROMOTION_NONE, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+      if (r != CUDA_SUCCESS) return set_error(MI_E_CUDA, "launch_mma: cuTensorMapEncodeTiled failed (%d)", (int)r);
+    }
+    a.use_tma = 1;
+  }
+  // four blob slots when shared memory allows, else three
+  int dev_smem = 0;
+  MI_CUDA(cudaDeviceGetAttribute(&dev_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, p->device));
+  a.n_blob = kMmaBlobSlotsMax;
+  while (a.n_blob > 3 && mma_smem_layout(a.blob_cap, a.n_blob).total > (uint32_t)dev_smem) --a.n_blob;
+  const MmaSmem L = mma_smem_layout(a.blob_cap, a.n_blob);
+  if (L.total > (uint32_t)dev_smem)
+    return set_error(MI_E_RANGE, "launch_mma: %u B of shared memory needed (device allows %d)", L.total, dev_smem);
+  MI_CUDA(cudaFuncSetAttribute(k_mma, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.total));
+  MI_CUDA(cudaMemsetAsync(p->d_ctr, 0, sizeof(int), s));
+  const int grid = std::max(1, std::min(p->n_items, p->n_sms));
+  k_mma<<<grid, kMmaThreads, L.total, s>>>(a);
+  MI_CUDA(cudaGetLastError());
+  return MI_OK;
+}
+
+int launch_mma_dark(Plan *p, cudaStream_t s) {
+  if (p->n_tiles == 0) return MI_OK;
+  k_mma_dark<<<(unsigned)p->n_tiles, 64, 0, s>>>(p->d_tiles, p->d_blobs, p->d_xc_pix, p->d_dark, p->has_dark);
+  MI_CUDA(cudaGetLastError());
+  return MI_OK;
+}
+
+}  // namespace mi

@@ -342,7 +342,8 @@ static int tile_item(const Builder &B, int r0, int nrows, int e_begin, int e_end
 }
 
 // normalisation factor and lineout weight of bin b (see mi_internal.h)
-static inline void bin_scale(const HostCSR &csr, const Plan *p, int64_t b, float *scale, float *lw) {
+static inline void bin_scale(const HostCSR &csr, const Plan *p, int64_t b, float *scale, float *lw,
+                             double *scale64 = nullptr) {
   const double an = csr.area_norm[b], ai = csr.area_in[b];
   double sc;
   if (p->semantics != MI_SEM_PY)
@@ -352,6 +353,7 @@ static inline void bin_scale(const HostCSR &csr, const Plan *p, int64_t b, float
   // variance plans (integrate_with_variance, kernels.py:551-559; profile_1d_with_variance,
   // kernels.py:604-645): Var = sum w^2 var / A^2, lineout weight A^2
   if (p->variance) sc *= sc;
+  if (scale64) *scale64 = sc;
   *scale = (float)sc;
   *lw = ai > kAreaThreshold ? (float)(p->variance ? ai * ai : ai) : 0.0f;
 }
@@ -546,7 +548,8 @@ static int free_plan_mem(Plan *p) {
   void *ptrs[] = {p->d_blobs, p->d_tiles, p->d_items, p->d_den_aw, p->d_cnt, p->d_partial,
                   p->d_dark, p->d_err, p->d_nmap, p->d_sorted, p->d_off, p->d_w, p->d_aw,
                   p->d_dr, p->d_py, p->d_pz, p->d_area_in, p->d_area_all, p->d_plain_img,
-                  p->d_ctr, p->d_span_lo, p->d_row_off, p->d_xchunks, p->d_xc};
+                  p->d_ctr, p->d_span_lo, p->d_row_off, p->d_xchunks, p->d_xc,
+                  p->d_xc_pix};
   for (void *q : ptrs)
     if (q) cudaFree(q);
   return MI_OK;
@@ -558,6 +561,231 @@ static int upload(T **dst, const T *src, size_t n, size_t *acct) {
   MI_CUDA(cudaMalloc((void **)dst, bytes));
   *acct += bytes;
   if (n) MI_CUDA(cudaMemcpy(*dst, src, n * sizeof(T), cudaMemcpyHostToDevice));
+  return MI_OK;
+}
+
+// ---- MMA encoding: tiles of up to kMmaRows x kMmaCols bins (see MmaHdr).  Each band of
+// kMmaRows rows is cut into sub-bands of h rows (h = 12, 6, 3, 1: the largest whose tile
+// blobs all fit the kernel's blob slots); a work item is a sub-band x item_cols columns,
+// its tiles the item's groups of kMmaCols columns, all on the item's rows.
+static int mma_tile_blob(const HostCSR &csr, const mi_map_desc &m, const std::vector<int32_t> &span_lo,
+                         const std::vector<int32_t> &row_off, const std::vector<double> &wmax,
+                         const std::vector<double> &fac, const std::vector<float> &lw, int r0, int nr, int box_rows,
+                         int e0, int nc, std::vector<int32_t> &lut, std::vector<uint8_t> &blob, int *nnz_out,
+                         int *nu_out) {
+  std::vector<int32_t> pix;
+  for (int i = 0; i < nr; ++i)
+    for (int j = 0; j < nc; ++j) {
+      const int64_t b = (int64_t)(r0 + i) * m.n_eta + e0 + j;
+      for (int64_t t = csr.row_ptr[b]; t < csr.row_ptr[b + 1]; ++t)
+        if (lut[csr.col[t]] < 0) {
+          lut[csr.col[t]] = 0;
+          pix.push_back(csr.col[t]);
+        }
+    }
+  // K slots in ascending compact index, slot k with k % 8 == c % 8 (the row's swizzle phase)
+  std::vector<std::pair<int64_t, int32_t>> cp(pix.size());
+  for (size_t u = 0; u < pix.size(); ++u) {
+    const int32_t z = pix[u] / m.ny, y = pix[u] - z * m.ny;
+    cp[u] = {(int64_t)row_off[z] + y - span_lo[z], pix[u]};
+  }
+  std::sort(cp.begin(), cp.end());
+  int prev = -1;
+  for (auto &e : cp) {
+    int k = prev + 1;
+    k += (int)(((e.first & 7) - (k & 7) + 8) & 7);
+    lut[e.second] = k;
+    prev = k;
+  }
+  const int n_k = std::max(1, (prev + 1 + kMmaKStep - 1) / kMmaKStep);
+  if (n_k * kMmaKStep > 65535) {
+    for (int32_t q : pix) lut[q] = -1;
+    return set_error(MI_E_RANGE, "MMA tile at row %d, column %d stages more than 65535 pixel slots", r0, e0);
+  }
+  std::vector<uint32_t> xrow((size_t)n_k * kMmaKStep, kMmaEmpty);
+  for (auto &e : cp) xrow[lut[e.second]] = (uint32_t)e.first;
+  // runs: consecutive slots of one step holding consecutive compact indices
+  std::vector<uint2> runs;
+  std::vector<uint32_t> rptr(n_k + 1, 0);
+  for (int s = 0; s < n_k; ++s) {
+    rptr[s] = (uint32_t)runs.size();
+    for (int k = 0; k < kMmaKStep;) {
+      const uint32_t c = xrow[s * kMmaKStep + k];
+      if (c == kMmaEmpty) { ++k; continue; }
+      int len = 1;
+      while (k + len < kMmaKStep && xrow[s * kMmaKStep + k + len] == c + (uint32_t)len) ++len;
+      runs.push_back(make_uint2(c, (uint32_t)k | ((uint32_t)len << 8)));
+      k += len;
+    }
+  }
+  rptr[n_k] = (uint32_t)runs.size();
+  std::vector<uint2> terms;
+  double bfac[kMmaN] = {0}, bdk[kMmaN] = {0};
+  float blw[kMmaN] = {0};
+  for (int i = 0; i < nr; ++i)
+    for (int j = 0; j < nc; ++j) {
+      const int64_t b = (int64_t)(r0 + i) * m.n_eta + e0 + j;
+      const uint32_t n = (uint32_t)(i * kMmaCols + j);
+      bfac[n] = fac[b];
+      blw[n] = lw[b];
+      const double wm = wmax[b];
+      for (int64_t t = csr.row_ptr[b]; t < csr.row_ptr[b + 1]; ++t) {
+        double qd = wm > 0.0 ? std::llround(csr.w[t] / wm * 4294967295.0) : 0.0;
+        qd = std::min(std::max(qd, 0.0), 4294967295.0);
+        terms.push_back(make_uint2((uint32_t)qd, (uint32_t)lut[csr.col[t]] | (n << 16)));
+      }
+    }
+  std::stable_sort(terms.begin(), terms.end(),
+                   [](const uint2 &x, const uint2 &y) { return (x.y & 0xFFFFu) < (y.y & 0xFFFFu); });
+  std::vector<uint32_t> sp(n_k + 1, 0);
+  for (const uint2 &t : terms) ++sp[(t.y & 0xFFFFu) / kMmaKStep + 1];
+  for (int s = 0; s < n_k; ++s) sp[s + 1] += sp[s];
+  for (int32_t q : pix) lut[q] = -1;
+  const MmaBlob L = mma_blob_layout(n_k, (int)runs.size(), (int)terms.size());
+  blob.assign(L.bytes, 0);
+  MmaHdr h{nr, nc, r0, e0, n_k, (int32_t)terms.size(), box_rows, (int32_t)runs.size()};
+  memcpy(blob.data(), &h, sizeof(h));
+  memcpy(blob.data() + kMmaBinsOff, bfac, sizeof(bfac));
+  memcpy(blob.data() + kMmaBinsOff + sizeof(bfac), bdk, sizeof(bdk));
+  memcpy(blob.data() + kMmaBinsOff + sizeof(bfac) + sizeof(bdk), blw, sizeof(blw));
+  if (!runs.empty()) memcpy(blob.data() + L.runs, runs.data(), runs.size() * 8);
+  memcpy(blob.data() + L.run_ptr, rptr.data(), rptr.size() * 4);
+  memcpy(blob.data() + L.xrow, xrow.data(), xrow.size() * 4);
+  memcpy(blob.data() + L.step_ptr, sp.data(), sp.size() * 4);
+  if (!terms.empty()) memcpy(blob.data() + L.terms, terms.data(), terms.size() * 8);
+  *nnz_out = (int)terms.size();
+  *nu_out = (int)pix.size();
+  return MI_OK;
+}
+
+static int build_mma_tiles(const HostCSR &csr, const mi_map_desc &m, Plan *p, const std::vector<int32_t> &span_lo,
+                           const std::vector<int32_t> &row_off, int *n_slots_out, std::vector<TileRef> *tiles_out,
+                           std::vector<WorkItem> *items_out, std::vector<uint8_t> *blobs_out) {
+  const int64_t n_bins = (int64_t)m.n_r * m.n_eta, n_pix = (int64_t)m.ny * m.nz;
+  std::vector<double> wmax(n_bins, 0.0), fac(n_bins, 0.0);
+  std::vector<float> lw(n_bins, 0.0f);
+  for (int64_t b = 0; b < n_bins; ++b) {
+    if (csr.row_ptr[b + 1] - csr.row_ptr[b] > kMmaMaxBinTerms)
+      return set_error(MI_E_RANGE, "bin %lld has more than %d terms: use the run encoding", (long long)b,
+                       kMmaMaxBinTerms);
+    double wm = 0.0;
+    for (int64_t t = csr.row_ptr[b]; t < csr.row_ptr[b + 1]; ++t) wm = std::max(wm, csr.w[t]);
+    wmax[b] = wm;
+    float sc32;
+    double sc;
+    bin_scale(csr, p, b, &sc32, &lw[b], &sc);
+    fac[b] = wm / 4294967295.0 * sc;
+  }
+  // items of about 12 per band, on 8-column (32-byte) cake boundaries when there are enough
+  // columns, always on kMmaCols boundaries
+  int item_cols = std::max(1, (m.n_eta + 11) / 12);
+  item_cols = m.n_eta >= 96 ? (item_cols + 7) & ~7 : (item_cols + kMmaCols - 1) / kMmaCols * kMmaCols;
+  const int n_slots = (m.n_eta + item_cols - 1) / item_cols;
+  const int n_bands = (m.n_r + kMmaRows - 1) / kMmaRows;
+  struct BandOut {
+    std::vector<WorkItem> items;
+    std::vector<std::vector<uint8_t>> blobs;
+    std::vector<int> nu;
+  };
+  std::vector<BandOut> bands(n_bands);
+  int err = MI_OK;
+  const int nthr = std::min(omp_get_max_threads(), 16);
+#pragma omp parallel num_threads(nthr)
+  {
+    std::vector<int32_t> lut(n_pix, -1);
+#pragma omp for schedule(dynamic, 1)
+    for (int bi = 0; bi < n_bands; ++bi) {
+      BandOut &bo = bands[bi];
+      const int br0 = bi * kMmaRows, bnr = std::min(kMmaRows, m.n_r - br0);
+      for (int h : {kMmaRows, 6, 3, 1}) {
+        bo.items.clear();
+        bo.blobs.clear();
+        bo.nu.clear();
+        bool fits = true;
+        for (int r0 = br0; r0 < br0 + bnr && fits; r0 += h) {
+          const int nr = std::min(h, br0 + bnr - r0);
+          for (int sl = 0; sl < n_slots && fits; ++sl) {
+            WorkItem w{};
+            w.tile_begin = (int)bo.blobs.size();
+            w.r0 = r0;
+            w.n_rows = nr;
+            w.slot = sl;
+            const int e_end = std::min(m.n_eta, (sl + 1) * item_cols);
+            for (int e0 = sl * item_cols; e0 < e_end; e0 += kMmaCols) {
+              bo.blobs.emplace_back();
+              int nnz = 0, nu = 0;
+              const int e = mma_tile_blob(csr, m, span_lo, row_off, wmax, fac, lw, r0, nr, h, e0,
+                                          std::min(kMmaCols, e_end - e0), lut, bo.blobs.back(), &nnz, &nu);
+              if (e) {
+#pragma omp critical
+                err = e;
+                fits = false;
+                break;
+              }
+              if (bo.blobs.back().size() > kMmaBlobCap) {
+                fits = false;
+                break;
+              }
+              w.nnz += nnz;
+              bo.nu.push_back(nu);
+            }
+            w.tile_end = (int)bo.blobs.size();
+            bo.items.push_back(w);
+          }
+        }
+        if (fits || err) break;
+        if (h == 1) {
+#pragma omp critical
+          err = set_error(MI_E_RANGE, "an MMA tile of one row at row %d exceeds %u B; use the run encoding", br0,
+                          kMmaBlobCap);
+          break;
+        }
+      }
+    }
+  }
+  if (err) return err;
+  // arena
+  std::vector<TileRef> &tiles = *tiles_out;
+  std::vector<WorkItem> &items = *items_out;
+  tiles.clear();
+  items.clear();
+  uint64_t arena = 0;
+  uint32_t max_blob = 0;
+  int max_u = 0;
+  int64_t staged = 0;
+  for (BandOut &bo : bands)
+    for (WorkItem w : bo.items) {
+      const int tb = (int)tiles.size();
+      for (int k = w.tile_begin; k < w.tile_end; ++k) {
+        const uint32_t bytes = (uint32_t)bo.blobs[k].size();
+        tiles.push_back({arena, bytes, 0});
+        arena += bytes;
+        max_blob = std::max(max_blob, bytes);
+        max_u = std::max(max_u, bo.nu[k]);
+        staged += bo.nu[k];
+      }
+      w.tile_end = (int)tiles.size();
+      w.tile_begin = tb;
+      items.push_back(w);
+    }
+  blobs_out->assign(arena, 0);
+  size_t ti = 0;
+  for (BandOut &bo : bands)
+    for (WorkItem w : bo.items)
+      for (int k = w.tile_begin; k < w.tile_end; ++k, ++ti) {
+        memcpy(blobs_out->data() + tiles[ti].off, bo.blobs[k].data(), bo.blobs[k].size());
+        std::vector<uint8_t>().swap(bo.blobs[k]);
+      }
+  p->n_tiles = (int)tiles.size();
+  p->max_blob = max_blob;
+  p->max_u = max_u;
+  p->max_nb = kMmaN;
+  p->staged_pixels = staged;
+  p->n_slots = n_slots;
+  p->lim.rows = kMmaRows;
+  p->lim.max_u = max_u;
+  p->lim.item_cols = item_cols;
+  *n_slots_out = n_slots;
   return MI_OK;
 }
 
@@ -590,8 +818,8 @@ static int build_plan(const mi_map_desc &m, const mi_plan_opts &o, Plan *p, Host
   p->oob = csr.oob;
 
   // ---- encoding and limits
-  const int enc = (o.encoding == MI_ENC_CSR) ? MI_ENC_CSR : MI_ENC_RUNS;
-  if (o.encoding < 0 || o.encoding > 2) return set_error(MI_E_ARG, "unknown encoding %d", o.encoding);
+  const int enc = (o.encoding == MI_ENC_CSR) ? MI_ENC_CSR : (o.encoding == MI_ENC_MMA ? MI_ENC_MMA : MI_ENC_RUNS);
+  if (o.encoding < 0 || o.encoding > 3) return set_error(MI_E_ARG, "unknown encoding %d", o.encoding);
   p->encoding = enc;
   int fpl = o.frames_per_lane > 0 ? o.frames_per_lane : 1;
   if (fpl != 1 && fpl != 2 && fpl != 4) return set_error(MI_E_ARG, "frames_per_lane must be 1, 2 or 4");
@@ -628,106 +856,6 @@ static int build_plan(const mi_map_desc &m, const mi_plan_opts &o, Plan *p, Host
     dev_smem = std::min(dev_smem, sm_smem / kRunCtasPerSm - 1024);
   }
 
-  // ---- items and tiles; shrink the tile limits until the kernel's shared memory fits
-  const int n_bands = (m.n_r + L.rows - 1) / L.rows;
-  const int n_slots = (m.n_eta + L.item_cols - 1) / L.item_cols;
-  p->n_slots = n_slots;
-  const int n_items = n_bands * n_slots;
-  std::vector<std::vector<HostTile>> item_tiles(n_items);
-  std::vector<std::vector<std::vector<uint8_t>>> item_blobs(n_items);
-  for (int attempt = 0;; ++attempt) {
-    int err = MI_OK;
-    int nthr = std::min(omp_get_max_threads(), 16);
-#pragma omp parallel num_threads(nthr)
-    {
-      std::vector<int32_t> stamp(n_pix, 0), lut(n_pix, -1);
-      int32_t sid = 0;
-#pragma omp for schedule(dynamic, 1)
-      for (int it = 0; it < n_items; ++it) {
-        item_tiles[it].clear();
-        item_blobs[it].clear();
-        int band = it / n_slots, slot = it % n_slots;
-        int r0 = band * L.rows, nr = std::min(L.rows, m.n_r - r0);
-        int e0 = slot * L.item_cols, e1 = std::min(m.n_eta, e0 + L.item_cols);
-        int e = tile_item(Builder(csr, m.n_r, m.n_eta, n_pix, L), r0, nr, e0, e1, stamp, sid,
-                          item_tiles[it]);
-        if (e) {
-#pragma omp critical
-          err = e;
-          continue;
-        }
-        for (const HostTile &t : item_tiles[it]) {
-          item_blobs[it].emplace_back();
-          if (enc == MI_ENC_RUNS)
-            runs_blob(csr, m, p, t, t.r0 - r0, G, RL, lut, item_blobs[it].back());
-          else
-            csr_blob(csr, m, p, t, t.r0 - r0, lut, item_blobs[it].back());
-        }
-      }
-    }
-    if (err) return err;
-    uint32_t mb = 0;
-    int mu = 1, mnb = 1;
-    for (int it = 0; it < n_items; ++it)
-      for (size_t k = 0; k < item_tiles[it].size(); ++k) {
-        mb = std::max(mb, (uint32_t)item_blobs[it][k].size());
-        mu = std::max(mu, item_tiles[it][k].n_u);
-        mnb = std::max(mnb, item_tiles[it][k].n_rows * item_tiles[it][k].n_cols);
-      }
-    const uint32_t cap = (mb + 15u) & ~15u;
-    const uint32_t need = enc == MI_ENC_RUNS
-                              ? runs_smem_layout(cap, mu, mnb | 1, L.rows, G, runs_frames_per_group(2, G), nullptr,
-                                                 nullptr, nullptr, nullptr, nullptr)
-                              : cake_smem_layout(fpl, cap, mu, mnb | 1, L.rows, nullptr, nullptr, nullptr, nullptr);
-    if (need + 1024u <= (uint32_t)dev_smem) break;
-    if (attempt >= 12 || L.max_u <= 32)
-      return set_error(MI_E_RANGE, "tiles need %u B of shared memory (device allows %d); lower tile_rows",
-                       need, dev_smem);
-    L.max_u = std::max(32, L.max_u * 4 / 5);
-    L.max_nnz = std::max(256, L.max_nnz * 4 / 5);
-    L.max_nb = std::max(16, L.max_nb * 4 / 5);
-  }
-  p->lim = L;
-
-  // ---- blob arena
-  std::vector<TileRef> tiles;
-  std::vector<WorkItem> items(n_items);
-  uint64_t arena = 0;
-  uint32_t max_blob = 0;
-  int max_u = 0, max_nb = 0;
-  int64_t staged = 0;
-  for (int it = 0; it < n_items; ++it) {
-    int band = it / n_slots, slot = it % n_slots;
-    WorkItem &w = items[it];
-    w.tile_begin = (int)tiles.size();
-    w.r0 = band * L.rows;
-    w.n_rows = std::min(L.rows, m.n_r - w.r0);
-    w.slot = slot;
-    w.nnz = 0;
-    for (size_t k = 0; k < item_tiles[it].size(); ++k) {
-      const HostTile &t = item_tiles[it][k];
-      const uint32_t bytes = (uint32_t)item_blobs[it][k].size();
-      tiles.push_back({arena, bytes, 0});
-      arena += bytes;
-      max_blob = std::max(max_blob, bytes);
-      max_u = std::max(max_u, t.n_u);
-      max_nb = std::max(max_nb, t.n_rows * t.n_cols);
-      staged += t.n_u;
-      w.nnz += t.nnz;
-    }
-    w.tile_end = (int)tiles.size();
-  }
-  p->n_tiles = (int)tiles.size();
-  p->max_blob = max_blob;
-  p->max_u = max_u;
-  p->max_nb = max_nb;
-  p->staged_pixels = staged;
-  std::vector<uint8_t> blobs(arena, 0);
-  for (int it = 0, ti = 0; it < n_items; ++it)
-    for (size_t k = 0; k < item_blobs[it].size(); ++k, ++ti) {
-      memcpy(blobs.data() + tiles[ti].off, item_blobs[it][k].data(), item_blobs[it][k].size());
-      std::vector<uint8_t>().swap(item_blobs[it][k]);
-    }
   // distinct referenced pixels, and their row spans for pixel-major staging
   std::vector<int32_t> span_lo(m.nz, 0), row_off(m.nz, 0);
   std::vector<XcChunk> xchunks;
@@ -744,7 +872,8 @@ static int build_plan(const mi_map_desc &m, const mi_plan_opts &o, Plan *p, Host
     p->ref_pixels = n;
     p->ref_row_lo = cmax >= 0 ? (int)(cmin / m.ny) : 0;
     p->ref_row_hi = cmax >= 0 ? (int)(cmax / m.ny) + 1 : 0;
-    if (p->encoding == MI_ENC_RUNS && runs_frames_per_group(2, p->run_g) == kXcFrames) {
+    if ((p->encoding == MI_ENC_RUNS && runs_frames_per_group(2, p->run_g) == kXcFrames) ||
+        p->encoding == MI_ENC_MMA) {
       size_t pi = 0;
       for (int z = 0; z < m.nz; ++z) {
         // chunks are made row by row, so each panel's chunks are one contiguous range
@@ -767,6 +896,115 @@ static int build_plan(const mi_map_desc &m, const mi_plan_opts &o, Plan *p, Host
       }
     }
   }
+  int n_slots = 0, n_items = 0;
+  std::vector<TileRef> tiles;
+  std::vector<WorkItem> items;
+  std::vector<uint8_t> blobs;
+  if (enc == MI_ENC_MMA) {
+    if ((rc = build_mma_tiles(csr, m, p, span_lo, row_off, &n_slots, &tiles, &items, &blobs))) return rc;
+    n_items = (int)items.size();
+  } else {
+    // ---- items and tiles; shrink the tile limits until the kernel's shared memory fits
+    const int n_bands = (m.n_r + L.rows - 1) / L.rows;
+    n_slots = (m.n_eta + L.item_cols - 1) / L.item_cols;
+    p->n_slots = n_slots;
+    n_items = n_bands * n_slots;
+    std::vector<std::vector<HostTile>> item_tiles(n_items);
+    std::vector<std::vector<std::vector<uint8_t>>> item_blobs(n_items);
+    for (int attempt = 0;; ++attempt) {
+      int err = MI_OK;
+      int nthr = std::min(omp_get_max_threads(), 16);
+  #pragma omp parallel num_threads(nthr)
+      {
+        std::vector<int32_t> stamp(n_pix, 0), lut(n_pix, -1);
+        int32_t sid = 0;
+  #pragma omp for schedule(dynamic, 1)
+        for (int it = 0; it < n_items; ++it) {
+          item_tiles[it].clear();
+          item_blobs[it].clear();
+          int band = it / n_slots, slot = it % n_slots;
+          int r0 = band * L.rows, nr = std::min(L.rows, m.n_r - r0);
+          int e0 = slot * L.item_cols, e1 = std::min(m.n_eta, e0 + L.item_cols);
+          int e = tile_item(Builder(csr, m.n_r, m.n_eta, n_pix, L), r0, nr, e0, e1, stamp, sid,
+                            item_tiles[it]);
+          if (e) {
+  #pragma omp critical
+            err = e;
+            continue;
+          }
+          for (const HostTile &t : item_tiles[it]) {
+            item_blobs[it].emplace_back();
+            if (enc == MI_ENC_RUNS)
+              runs_blob(csr, m, p, t, t.r0 - r0, G, RL, lut, item_blobs[it].back());
+            else
+              csr_blob(csr, m, p, t, t.r0 - r0, lut, item_blobs[it].back());
+          }
+        }
+      }
+      if (err) return err;
+      uint32_t mb = 0;
+      int mu = 1, mnb = 1;
+      for (int it = 0; it < n_items; ++it)
+        for (size_t k = 0; k < item_tiles[it].size(); ++k) {
+          mb = std::max(mb, (uint32_t)item_blobs[it][k].size());
+          mu = std::max(mu, item_tiles[it][k].n_u);
+          mnb = std::max(mnb, item_tiles[it][k].n_rows * item_tiles[it][k].n_cols);
+        }
+      const uint32_t cap = (mb + 15u) & ~15u;
+      const uint32_t need = enc == MI_ENC_RUNS
+                                ? runs_smem_layout(cap, mu, mnb | 1, L.rows, G, runs_frames_per_group(2, G), nullptr,
+                                                   nullptr, nullptr, nullptr, nullptr)
+                                : cake_smem_layout(fpl, cap, mu, mnb | 1, L.rows, nullptr, nullptr, nullptr, nullptr);
+      if (need + 1024u <= (uint32_t)dev_smem) break;
+      if (attempt >= 12 || L.max_u <= 32)
+        return set_error(MI_E_RANGE, "tiles need %u B of shared memory (device allows %d); lower tile_rows",
+                         need, dev_smem);
+      L.max_u = std::max(32, L.max_u * 4 / 5);
+      L.max_nnz = std::max(256, L.max_nnz * 4 / 5);
+      L.max_nb = std::max(16, L.max_nb * 4 / 5);
+    }
+    p->lim = L;
+
+    // ---- blob arena
+    items.assign(n_items, WorkItem{});
+    uint64_t arena = 0;
+    uint32_t max_blob = 0;
+    int max_u = 0, max_nb = 0;
+    int64_t staged = 0;
+    for (int it = 0; it < n_items; ++it) {
+      int band = it / n_slots, slot = it % n_slots;
+      WorkItem &w = items[it];
+      w.tile_begin = (int)tiles.size();
+      w.r0 = band * L.rows;
+      w.n_rows = std::min(L.rows, m.n_r - w.r0);
+      w.slot = slot;
+      w.nnz = 0;
+      for (size_t k = 0; k < item_tiles[it].size(); ++k) {
+        const HostTile &t = item_tiles[it][k];
+        const uint32_t bytes = (uint32_t)item_blobs[it][k].size();
+        tiles.push_back({arena, bytes, 0});
+        arena += bytes;
+        max_blob = std::max(max_blob, bytes);
+        max_u = std::max(max_u, t.n_u);
+        max_nb = std::max(max_nb, t.n_rows * t.n_cols);
+        staged += t.n_u;
+        w.nnz += t.nnz;
+      }
+      w.tile_end = (int)tiles.size();
+    }
+    p->n_tiles = (int)tiles.size();
+    p->max_blob = max_blob;
+    p->max_u = max_u;
+    p->max_nb = max_nb;
+    p->staged_pixels = staged;
+    blobs.assign(arena, 0);
+    for (int it = 0, ti = 0; it < n_items; ++it)
+      for (size_t k = 0; k < item_blobs[it].size(); ++k, ++ti) {
+        memcpy(blobs.data() + tiles[ti].off, item_blobs[it][k].data(), item_blobs[it][k].size());
+        std::vector<uint8_t>().swap(item_blobs[it][k]);
+      }
+  }
+
   // heaviest-first launch order
   std::vector<int> order(n_items);
   std::iota(order.begin(), order.end(), 0);
@@ -797,6 +1035,7 @@ static int build_plan(const mi_map_desc &m, const mi_plan_opts &o, Plan *p, Host
   if ((rc = upload(&p->d_items, items_sorted.data(), items_sorted.size(), &acct))) return rc;
   if ((rc = upload(&p->d_den_aw, den.data(), den.size(), &acct))) return rc;
   if ((rc = upload(&p->d_cnt, cnt.data(), cnt.size(), &acct))) return rc;
+
   {
     size_t bytes = (size_t)kMaxFramesPerLaunch * m.n_r * n_slots * 2 * sizeof(double);
     MI_CUDA(cudaMalloc((void **)&p->d_partial, bytes));
@@ -813,6 +1052,14 @@ static int build_plan(const mi_map_desc &m, const mi_plan_opts &o, Plan *p, Host
     if ((rc = upload(&p->d_span_lo, span_lo.data(), span_lo.size(), &acct))) return rc;
     if ((rc = upload(&p->d_row_off, row_off.data(), row_off.size(), &acct))) return rc;
     if ((rc = upload(&p->d_xchunks, xchunks.data(), xchunks.size(), &acct))) return rc;
+    if (enc == MI_ENC_MMA) {
+      std::vector<int32_t> xpix(n_xc);
+      for (int z = 0; z < m.nz; ++z) {
+        const int64_t c1 = z + 1 < m.nz ? row_off[z + 1] : n_xc;
+        for (int64_t c = row_off[z]; c < c1; ++c) xpix[c] = (int32_t)((int64_t)z * m.ny + span_lo[z] + (c - row_off[z]));
+      }
+      if ((rc = upload(&p->d_xc_pix, xpix.data(), xpix.size(), &acct))) return rc;
+    }
     const size_t bytes = (size_t)n_xc * kXcFrames * kXcGroups * sizeof(uint16_t);
     MI_CUDA(cudaMalloc((void **)&p->d_xc, bytes));
     acct += bytes;
@@ -946,8 +1193,9 @@ int mi_plan_create_panels(const mi_map_desc *maps, int n_panels, const mi_plan_o
   if (o.mode < 0 || o.mode > 2 || o.semantics < 0 || o.semantics > 2 ||
       (o.semantics == MI_SEM_IC && o.mode == MI_MODE_FLOOR))
     return set_error(MI_E_ARG, "mi_plan_create_panels: bad mode %d / semantics %d", o.mode, o.semantics);
-  if (o.encoding == MI_ENC_CSR || o.tile_rows > 16)
-    return set_error(MI_E_UNSUPPORTED, "mi_plan_create_panels: panel plans use the run encoding with tile_rows <= 16");
+  if (o.encoding == MI_ENC_CSR || (o.encoding != MI_ENC_MMA && o.tile_rows > 16))
+    return set_error(MI_E_UNSUPPORTED,
+                     "mi_plan_create_panels: panel plans use the run encoding with tile_rows <= 16 or the MMA encoding");
   int ndev = 0;
   if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
     return set_error(MI_E_CUDA, "mi_plan_create_panels: no CUDA device available");
@@ -1043,8 +1291,14 @@ int mi_plan_set_dark(mi_plan *p, const float *dark) {
   if (dark) MI_CUDA(cudaMemcpy(p->d_dark, dark, n * sizeof(float), cudaMemcpyHostToDevice));
   else MI_CUDA(cudaMemset(p->d_dark, 0, n * sizeof(float)));
   p->has_dark = dark ? 1 : 0;
+  int rc = MI_OK;
+  if (p->encoding == MI_ENC_MMA) {
+    // the per-bin dark terms, computed once per dark on the legacy stream
+    rc = launch_mma_dark(p, nullptr);
+    if (rc == MI_OK) MI_CUDA(cudaDeviceSynchronize());
+  }
   cudaSetDevice(prev);
-  return MI_OK;
+  return rc;
 }
 
 int mi_plan_get_info(const mi_plan *p, mi_plan_info *info) {
@@ -1147,6 +1401,8 @@ int mi_integrate_panels(mi_plan *p, const void *const *frames, const int *dtypes
   if (prev != p->device) MI_CUDA(cudaSetDevice(p->device));
   const cudaStream_t s = (cudaStream_t)stream;
   const bool want_lo = lo_aw || lo_sm;
+  if (as_f32 && p->encoding == MI_ENC_MMA)
+    return set_error(MI_E_UNSUPPORTED, "mi_integrate_panels: MMA plans take 8/16-bit frames only");
   const int chunk = as_f32 ? kXcFramesF * kXcGroupsF : kXcFrames * kXcGroups;
   int rc = MI_OK;
   for (int g0 = 0; g0 < n_frames && rc == MI_OK; g0 += kMaxFramesPerLaunch) {
@@ -1156,7 +1412,10 @@ int mi_integrate_panels(mi_plan *p, const void *const *frames, const int *dtypes
       for (int i = 0; i < np && rc == MI_OK; ++i)
         rc = launch_xc(p, i, (const uint8_t *)frames[i] + (size_t)(g0 + f0) * strides[i] * dtype_size(dtypes[i]),
                        dtypes[i], nf, strides[i], as_f32, s);
-      if (rc == MI_OK)
+      if (rc == MI_OK && p->encoding == MI_ENC_MMA)
+        rc = launch_mma(p, nf, cake ? cake + (size_t)(g0 + f0) * p->n_bins : nullptr,
+                        p->d_partial + (size_t)f0 * p->n_r * p->n_slots * 2, want_lo, s);
+      else if (rc == MI_OK)
         rc = launch_runs_staged(p, as_f32, nf, cake ? cake + (size_t)(g0 + f0) * p->n_bins : nullptr,
                                 p->d_partial + (size_t)f0 * p->n_r * p->n_slots * 2, want_lo, s);
     }

@@ -23,9 +23,15 @@
 
 namespace mi {
 
-template <typename T, bool VEC>
+// PLANES (MMA encoding): two byte planes [lo: n_xc x 128][hi: n_xc x 128] (the buffer's
+// n_xc x 256 bytes); row c of a plane holds that byte of compact pixel c's 128 frames, the
+// 16-byte granule of frames 16g .. 16g+15 at position g ^ (c % 8): the 128-byte swizzle
+// phase the tensor-core operand of a K slot with k % 8 == c % 8 expects, so a run of
+// consecutive pixels is staged with one plain bulk copy per plane.
+template <typename T, bool VEC, bool PLANES>
 __global__ void __launch_bounds__(256) k_xc(const T *__restrict__ frames, int64_t stride, int F, int ny, int z_off,
-                                            const XcChunk *__restrict__ chunks, uint8_t *__restrict__ xc) {
+                                            const XcChunk *__restrict__ chunks, uint8_t *__restrict__ xc,
+                                            int64_t n_xc) {
   constexpr int kPitch = kXcRowBytes / 2;  // u16 per compact pixel
   __shared__ __align__(16) uint16_t S[kXcFrames][kXcChunk + 8];
   const XcChunk ch = chunks[blockIdx.x];
@@ -63,7 +69,15 @@ __global__ void __launch_bounds__(256) k_xc(const T *__restrict__ frames, int64_
 #pragma unroll
       for (int j = 0; j < 8; j += 2)
         w[j / 2] = (uint32_t)S[8 * q + j][col] | ((uint32_t)S[8 * q + j + 1][col] << 16);
-      *(uint4 *)(out + (int64_t)(ch.c0 + p) * kPitch + h * kXcFrames + 8 * q) = make_uint4(w[0], w[1], w[2], w[3]);
+      if constexpr (PLANES) {
+        const int cc = ch.c0 + p, fr = h * kXcFrames + 8 * q;
+        uint8_t *row = xc + (int64_t)cc * 128 + 16 * ((fr >> 4) ^ (cc & 7)) + (fr & 8);
+        *(uint2 *)row = make_uint2(__byte_perm(w[0], w[1], 0x6420), __byte_perm(w[2], w[3], 0x6420));
+        *(uint2 *)(row + n_xc * 128) =
+            make_uint2(__byte_perm(w[0], w[1], 0x7531), __byte_perm(w[2], w[3], 0x7531));
+      } else {
+        *(uint4 *)(out + (int64_t)(ch.c0 + p) * kPitch + h * kXcFrames + 8 * q) = make_uint4(w[0], w[1], w[2], w[3]);
+      }
     }
   }
 }
@@ -118,21 +132,29 @@ int launch_xc(Plan *p, int panel, const void *frames, int dtype, int F, int64_t 
   if (grid == 0) return MI_OK;
   const XcChunk *chunks = p->d_xchunks + pn.chunk_begin;
   if (!as_f32) {
+    const bool planes = p->encoding == MI_ENC_MMA;
     if (dtype == MI_DT_U16) {
       const bool vec = ((uintptr_t)frames % 16 == 0) && ((stride * 2) % 16 == 0) && ((pn.ny * 2) % 16 == 0);
-      if (vec)
-        k_xc<uint16_t, true><<<grid, 256, 0, s>>>((const uint16_t *)frames, stride, F, pn.ny, pn.z_off, chunks,
-                                                  p->d_xc);
+      const uint16_t *f16 = (const uint16_t *)frames;
+      if (vec && planes)
+        k_xc<uint16_t, true, true><<<grid, 256, 0, s>>>(f16, stride, F, pn.ny, pn.z_off, chunks, p->d_xc, p->n_xc);
+      else if (vec)
+        k_xc<uint16_t, true, false><<<grid, 256, 0, s>>>(f16, stride, F, pn.ny, pn.z_off, chunks, p->d_xc, p->n_xc);
+      else if (planes)
+        k_xc<uint16_t, false, true><<<grid, 256, 0, s>>>(f16, stride, F, pn.ny, pn.z_off, chunks, p->d_xc, p->n_xc);
       else
-        k_xc<uint16_t, false><<<grid, 256, 0, s>>>((const uint16_t *)frames, stride, F, pn.ny, pn.z_off, chunks,
-                                                   p->d_xc);
+        k_xc<uint16_t, false, false><<<grid, 256, 0, s>>>(f16, stride, F, pn.ny, pn.z_off, chunks, p->d_xc, p->n_xc);
     } else if (dtype == MI_DT_U8) {
-      k_xc<uint8_t, false><<<grid, 256, 0, s>>>((const uint8_t *)frames, stride, F, pn.ny, pn.z_off, chunks,
-                                                p->d_xc);
+      const uint8_t *f8 = (const uint8_t *)frames;
+      if (planes)
+        k_xc<uint8_t, false, true><<<grid, 256, 0, s>>>(f8, stride, F, pn.ny, pn.z_off, chunks, p->d_xc, p->n_xc);
+      else
+        k_xc<uint8_t, false, false><<<grid, 256, 0, s>>>(f8, stride, F, pn.ny, pn.z_off, chunks, p->d_xc, p->n_xc);
     } else {
       return set_error(MI_E_ARG, "launch_xc: dtype %d does not fit u16 staging", dtype);
     }
   } else {
+    if (p->encoding == MI_ENC_MMA) return set_error(MI_E_UNSUPPORTED, "launch_xc: MMA plans stage 8/16-bit frames only");
     switch (dtype) {
       case MI_DT_U8: xcf_launch<uint8_t>(p, pn, frames, F, stride, s); break;
       case MI_DT_U16: xcf_launch<uint16_t>(p, pn, frames, F, stride, s); break;

@@ -62,7 +62,8 @@ class CakePlan:
         device: CUDA device.
         tile_rows, tile_pixels, frames_per_lane: tiling knobs (0 = default).
         encoding: 'auto' (= 'runs') | 'runs' (register-blocked radial runs) | 'csr'
-            (per-bin term lists); run_len: rows per run record (2, 4, 8; 0 = auto).
+            (per-bin term lists) | 'mma' (tensor cores, exact int8 products; 8/16-bit
+            frames only); run_len: rows per run record (2, 4, 8; 0 = auto).
         variance: a variance plan (integrate_with_variance, kernels.py:474-536): frames
             are per-pixel variance maps, caked with the squared coalesced weights and
             divided by the squared bin area; its lineouts are the propagated variances of
@@ -93,7 +94,7 @@ class CakePlan:
                            nmap.ctypes.data, self.n_r, self.n_eta, self.ny, self.nz,
                            self.bc_y, self.bc_z)
         if encoding not in L.ENC:
-            raise ValueError(f"unknown encoding {encoding!r}; expected 'auto' | 'csr' | 'runs'")
+            raise ValueError(f"unknown encoding {encoding!r}; expected 'auto' | 'csr' | 'runs' | 'mma'")
         opts = L.MiPlanOpts(L.MODE[mode], int(self.normalize), L.SEM[semantics],
                             int(tile_rows), int(tile_pixels), int(frames_per_lane),
                             L.ENC[encoding], int(run_len), int(self.variance))
@@ -284,12 +285,15 @@ class PanelPlan:
         beam_centres: (bc_y, bc_z) of each panel (used by gradient mode).
         n_r, n_eta, mode, normalize, semantics, device, tile_rows, tile_pixels, run_len:
             as for ``CakePlan`` (run encoding, tile_rows <= 16).
+        encoding: 'runs' or 'mma' (tensor cores; every panel's frames 8/16-bit).
     """
 
     def __init__(self, pixmaps, *, shapes, n_r: int, n_eta: int, beam_centres=None, mode: str = "floor",
                  normalize: bool = True, semantics: str = "py", device="cuda", tile_rows: int = 0,
-                 tile_pixels: int = 0, run_len: int = 0):
+                 tile_pixels: int = 0, run_len: int = 0, encoding: str = "runs"):
         n = len(pixmaps)
+        if encoding not in ("runs", "mma"):
+            raise ValueError(f"panel plans use the 'runs' or 'mma' encoding, not {encoding!r}")
         if n == 0 or len(shapes) != n or (beam_centres is not None and len(beam_centres) != n):
             raise ValueError("one shape (and beam centre) per panel map is needed")
         if mode not in L.MODE or semantics not in L.SEM:
@@ -309,7 +313,7 @@ class PanelPlan:
             descs[i] = L.MiMapDesc(recs.ctypes.data if recs.size else None, recs.shape[0], nmap.ctypes.data,
                                    self.n_r, self.n_eta, ny, nz, float(bcs[i][0]), float(bcs[i][1]))
         opts = L.MiPlanOpts(L.MODE[mode], int(normalize), L.SEM[semantics], int(tile_rows), int(tile_pixels), 0,
-                            L.ENC["runs"], int(run_len))
+                            L.ENC[encoding], int(run_len))
         h = C.c_void_p()
         L.check(L.lib().mi_plan_create_panels(descs, n, C.byref(opts), self.device.index, C.byref(h)),
                 "mi_plan_create_panels")
