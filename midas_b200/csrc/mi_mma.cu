@@ -8,30 +8,31 @@
 // A tile (kMmaRows x kMmaCols = 48 bins) is a dense int8 product on the tensor cores:
 //   D[frame][bin] (int32, TMEM) += A[frame][pixel] (a byte plane of the frames)
 //                                  x B[pixel][bin] (a byte plane of the weights q)
-// two frame planes x four weight planes = eight tcgen05.mma per K step of 32 staged pixels,
-// into five int32 accumulators (one per byte shift 0..4).  Every product and sum is exact;
+// two frame planes x four weight planes, issued as two tcgen05.mma of N = 192 per K step of
+// 32 staged pixels, into five int32 accumulators (one per byte shift 0..4).  Every product and sum is exact;
 // the epilogue forms sum_k 2^(8k) acc_k in FP64, subtracts the bin's dark term and scales:
 // cake = fac * value - dk.  The only approximation is the 32-bit fixed-point weight
 // (2^-33 of the bin's largest weight); the reference's fp32 (raw - dark) and fp32 sums are
 // replaced by exact integer sums, so the result is closer to the FP64 one.
 //
-// Operands in shared memory, per pipeline stage (one K step):
-//   A (frames): MN-major, 128B swizzle; slot k of the step is the 128-byte row
+// Operands in shared memory, per pipeline stage (two K steps, 64 pixel slots):
+//   A (frames): MN-major, 128B swizzle; slot k of the stage is the 128-byte row
 //     (k % 8) * 128 + (k / 8) * 1024 holding the pixel's 128 frame bytes, 16-byte granule g
 //     at position g ^ (k % 8).  Kernel (a) writes each pixel-major row with its granules
 //     already in that order for phase c % 8, and the tiler puts pixel c in a slot with
 //     k % 8 == c % 8, so a slot is filled by one plain 128-byte bulk copy per plane.
-//   B (weights): K-major, no swizzle; byte (n, k) at (n % 8) * 16 + (n / 8) * 256 +
-//     (k % 16) + (k / 16) * 128, zeroed and then scattered from the step's terms.
+//   B (weights): K-major, no swizzle, the four byte planes as rows n' = 48 j + n; byte (n', k)
+//     at (n' % 8) * 16 + (n' / 8) * 512 + (k % 16) + (k / 16) * 128, zeroed and then
+//     scattered from the stage's terms.
 //
 // Roles (one persistent CTA per SM, 14 warps):
 //   warp 0          TMEM allocation (512 columns: two accumulator sets of 5 x 48) and, on one
-//                   lane, the MMA issue: 8 MMAs per K step, a commit that frees the stage, and
+//                   lane, the MMA issue: 2 MMAs per K step, a commit that frees the stage, and
 //                   at a tile's last step a commit that hands the accumulators to the epilogue
 //   warp 1          loader: claims work items (heaviest first) and brings each tile's blob
-//                   into one of three blob slots with one bulk copy
-//   warps 2,3,12,13 producers: K step g (counted over the CTA's tiles) is built by producer
-//                   g % 4 into stage g % 6
+//                   into one of its blob slots with one bulk copy
+//   warps 2,3,12,13 producers: stage g (counted over the CTA's tiles) is built by producer
+//                   g % 4 into stage slot g % 4
 //   warps 4-11      epilogue: warp w reads TMEM lanes 32 (w % 4) + 0..31 (= frames) and half
 //                   of the tile's bins (8 bins x 5 accumulators at a time), recombines, puts the
 //                   cake values into a shared-memory tile that one TMA tensor store writes to
@@ -50,14 +51,18 @@
 
 namespace mi {
 
-constexpr int kMmaStages = 6;
+constexpr int kMmaStages = 4;
+constexpr int kMmaStepsPerStage = 2;        // K steps (32 pixel slots each) per pipeline stage
 constexpr int kMmaProducers = 4;
 constexpr int kMmaEpiWarps = 8;
 constexpr int kMmaWarps = 14;
 constexpr int kMmaThreads = kMmaWarps * 32;
-constexpr uint32_t kMmaStageBytes = 14336;   // A lo 4096 | A hi 4096 | B 4 x 1536
-constexpr uint32_t kMmaBPlane = 1536;
+constexpr uint32_t kMmaStageBytes = 28672;   // A lo 8192 | A hi 8192 | B 12288 (64 pixel slots)
+constexpr uint32_t kMmaAHi = 8192, kMmaB = 16384;
+constexpr uint32_t kMmaBPlane = 3072;        // 48 rows of the K-major weight operand, 64 K
 constexpr int kMmaBlobSlotsMax = 4;
+constexpr int kMmaFacSlots = 6;             // ring of the tiles' per-bin factors (epilogue)
+constexpr uint32_t kMmaFacBytes = 1024;      // one ring entry: fac, dk, lw of 48 bins (960 B)
 constexpr int kMmaTmemCols = 512;
 constexpr int kMmaAccCols = 256;            // columns per accumulator set (5 x 48 used)
 constexpr uint32_t kMmaWaitLimit = 1u << 26;
@@ -79,18 +84,19 @@ struct MmaArgs {
   int *counter;
   int *err;
   uint32_t blob_cap;
-  int n_blob;               // blob slots (3 or 4, as shared memory allows)
+  int n_blob;               // blob slots (2 to 4, as shared memory allows)
 };
 
 // Per-slot and per-stage tags passed between the roles through shared memory.
 struct MmaTag {
-  int32_t end, slot, first, last;   // end of work; item's lineout slot; first/last tile of item
+  int32_t end, tile, step, n_k;     // end of work; tile sequence number of the CTA; stage of the
+                                    // tile; K steps of the tile (the MMA lane reads these 16 B)
+  int32_t slot, first, last, box;   // item's lineout slot; first/last tile of item; box rows
   int32_t r0, n_rows, e0, n_cols;   // the tile's bins
-  int32_t tile, step, n_k, box;     // tile sequence number of the CTA, K step, K steps, box rows
 };
 
 struct MmaSmem {
-  uint32_t off_out, off_blob, off_shdr, off_btag, off_atag, off_bar, off_tmem, total;
+  uint32_t off_out, off_blob, off_fac, off_shdr, off_btag, off_atag, off_bar, off_tmem, total;
 };
 
 __host__ __device__ inline MmaSmem mma_smem_layout(uint32_t blob_cap, int n_blob) {
@@ -98,10 +104,11 @@ __host__ __device__ inline MmaSmem mma_smem_layout(uint32_t blob_cap, int n_blob
   uint32_t o = (uint32_t)kMmaStages * kMmaStageBytes;
   L.off_out = o;   o += 2u * kMmaOutBytes;
   L.off_blob = o;  o += (uint32_t)n_blob * blob_cap;
+  L.off_fac = o;   o += (uint32_t)kMmaFacSlots * kMmaFacBytes;
   L.off_shdr = o;  o += (uint32_t)kMmaStages * sizeof(MmaTag);
   L.off_btag = o;  o += (uint32_t)kMmaBlobSlotsMax * sizeof(MmaTag);
   L.off_atag = o;  o += 2u * sizeof(MmaTag);
-  L.off_bar = o;   o += 8u * (2u * kMmaStages + 2u * kMmaBlobSlotsMax + 4u);
+  L.off_bar = o;   o += 8u * (2u * kMmaStages + 2u * kMmaBlobSlotsMax + 2u * kMmaFacSlots + 4u);
   L.off_tmem = o;  o += 16u;
   L.total = o + 1024u;   // the base is rounded up to 1024 bytes inside the kernel
   return L;
@@ -148,13 +155,17 @@ __device__ __forceinline__ uint64_t m_desc(uint32_t saddr, uint32_t lbo, uint32_
 }
 
 // instruction descriptor, kind::i8: D s32, A u8 MN-major, B u8 K-major, M = 128, N = 48
-constexpr uint32_t kMmaIdesc = (2u << 4) | (1u << 15) | ((uint32_t)(kMmaN >> 3) << 17) | ((uint32_t)(kMmaFrames >> 4) << 24);
+// with N = 192 (the four weight planes, 48 bins each, side by side), 144 (planes 0-2) or 48
+__host__ __device__ constexpr uint32_t mma_idesc(int n) {
+  return (2u << 4) | (1u << 15) | ((uint32_t)(n >> 3) << 17) | ((uint32_t)(kMmaFrames >> 4) << 24);
+}
 
-__device__ __forceinline__ void m_mma(uint32_t d_tmem, uint64_t adesc, uint64_t bdesc, uint32_t accumulate) {
+__device__ __forceinline__ void m_mma(uint32_t d_tmem, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
+                                      uint32_t accumulate) {
   asm volatile(
       "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
       "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n" ::"r"(d_tmem),
-      "l"(adesc), "l"(bdesc), "r"(kMmaIdesc), "r"(accumulate), "r"(0u), "r"(0u), "r"(0u), "r"(0u));
+      "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate), "r"(0u), "r"(0u), "r"(0u), "r"(0u));
 }
 __device__ __forceinline__ void m_commit(uint64_t *bar) {
   asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(m_smem(bar))
@@ -195,6 +206,7 @@ __global__ void __launch_bounds__(kMmaThreads, 1) k_mma(const __grid_constant__ 
   uint64_t *full = bar, *empty = bar + kMmaStages;
   uint64_t *bfull = bar + 2 * kMmaStages, *bempty = bfull + kMmaBlobSlotsMax;
   uint64_t *afull = bempty + kMmaBlobSlotsMax, *aempty = afull + 2;
+  uint64_t *ffull = aempty + 2, *fempty = ffull + kMmaFacSlots;
   uint32_t *s_tmem = (uint32_t *)(smem + L.off_tmem);
 
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -204,11 +216,15 @@ __global__ void __launch_bounds__(kMmaThreads, 1) k_mma(const __grid_constant__ 
       asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(m_smem(&empty[q])) : "memory");
     }
     for (int q = 0; q < kMmaBlobSlotsMax; ++q) {
-      // a blob slot is free again when the producers have built its stages and the epilogue
-      // has used its per-bin factors
+      // a blob slot is free again when the producers have built its stages
       asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(m_smem(&bfull[q])) : "memory");
-      asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(m_smem(&bempty[q])),
-                   "r"(kMmaProducers + kMmaEpiWarps)
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(m_smem(&bempty[q])), "r"(kMmaProducers)
+                   : "memory");
+    }
+    for (int q = 0; q < kMmaFacSlots; ++q) {
+      // a factor entry is free again when every epilogue warp has used it
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(m_smem(&ffull[q])) : "memory");
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(m_smem(&fempty[q])), "r"(kMmaEpiWarps)
                    : "memory");
     }
     for (int q = 0; q < 2; ++q) {
@@ -238,39 +254,48 @@ __global__ void __launch_bounds__(kMmaThreads, 1) k_mma(const __grid_constant__ 
       for (uint32_t g = 0;; ++g) {
         const int q = (int)(g % kMmaStages);
         if (!m_wait(&full[q], (g / kMmaStages) & 1u)) { ok = false; break; }
-        const MmaTag h = s_shdr[q];
-        if (h.end) {
+        const int4 hq = *(const int4 *)&s_shdr[q];   // end, tile, step, n_k
+        const int ab = hq.y & 1;
+        if (hq.x) {
           // no more tiles: pass the end marker to the epilogue through the next set
-          const int ab = h.tile & 1;
-          if (!m_wait(&aempty[ab], ((uint32_t)(h.tile >> 1) & 1u) ^ 1u)) { ok = false; break; }
-          s_atag[ab] = h;
+          if (!m_wait(&aempty[ab], ((uint32_t)(hq.y >> 1) & 1u) ^ 1u)) { ok = false; break; }
+          s_atag[ab] = s_shdr[q];
           m_arrive(&afull[ab]);
           m_arrive(&afull[ab]);
           break;
         }
-        const int ab = h.tile & 1;
-        if (h.step == 0) {
-          if (!m_wait(&aempty[ab], ((uint32_t)(h.tile >> 1) & 1u) ^ 1u)) { ok = false; break; }
-          s_atag[ab] = h;
+        if (hq.z == 0) {
+          if (!m_wait(&aempty[ab], ((uint32_t)(hq.y >> 1) & 1u) ^ 1u)) { ok = false; break; }
+          m_fence_after();
+          s_atag[ab] = s_shdr[q];
           m_arrive(&afull[ab]);
         }
-        m_fence_after();
         const uint32_t sb = m_smem(smem + (size_t)q * kMmaStageBytes);
         const uint32_t dbase = tmem + (uint32_t)(ab * kMmaAccCols);
+        // the four weight planes are one N = 192 operand (plane j = rows 48 j ..): the low
+        // frame plane's product lands on accumulators 0-3 (columns 0..191), the high plane's,
+        // one byte up, on accumulators 1-4 (columns 48..239).  At a tile's first K step the
+        // first product into each accumulator starts it from zero, so the high plane's
+        // product is split there into planes 0-2 (accumulate) and plane 3 (fresh).
 #pragma unroll
-        for (int v = 0; v < 2; ++v) {
-          const uint64_t ad = m_desc(sb + 4096u * v, 0u, 1024u, 2u);
-#pragma unroll
-          for (int j = 0; j < 4; ++j) {
-            const uint64_t bd = m_desc(sb + 8192u + kMmaBPlane * j, 128u, 256u, 0u);
-            const int k = v + j;
-            // the first product into each accumulator of a tile starts it from zero
-            const uint32_t acc = (h.step > 0 || (v == 1 && j < 3)) ? 1u : 0u;
-            m_mma(dbase + (uint32_t)(k * kMmaN), ad, bd, acc);
+        for (int hs = 0; hs < kMmaStepsPerStage; ++hs) {
+          if (kMmaStepsPerStage * hq.z + hs >= hq.w) break;
+          const uint64_t alo = m_desc(sb + 4096u * hs, 0u, 1024u, 2u);
+          const uint64_t ahi = m_desc(sb + kMmaAHi + 4096u * hs, 0u, 1024u, 2u);
+          const uint32_t bsa = sb + kMmaB + 256u * hs;
+          const uint64_t bd = m_desc(bsa, 128u, 512u, 0u);
+          const bool first = hq.z == 0 && hs == 0;
+          m_mma(dbase, alo, bd, mma_idesc(4 * kMmaN), first ? 0u : 1u);
+          if (!first) {
+            m_mma(dbase + (uint32_t)kMmaN, ahi, bd, mma_idesc(4 * kMmaN), 1u);
+          } else {
+            m_mma(dbase + (uint32_t)kMmaN, ahi, bd, mma_idesc(3 * kMmaN), 1u);
+            m_mma(dbase + (uint32_t)(4 * kMmaN), ahi, m_desc(bsa + 3u * kMmaBPlane, 128u, 512u, 0u),
+                  mma_idesc(kMmaN), 0u);
           }
         }
         m_commit(&empty[q]);
-        if (h.step == h.n_k - 1) m_commit(&afull[ab]);
+        if (kMmaStepsPerStage * (hq.z + 1) >= hq.w) m_commit(&afull[ab]);
       }
       if (!ok) atomicExch(a.err, MI_E_TIMEOUT);
     }
@@ -290,7 +315,9 @@ __global__ void __launch_bounds__(kMmaThreads, 1) k_mma(const __grid_constant__ 
         const int sl = j % NB;
         if (lane == 0) {
           const TileRef tr = a.tiles[it.tile_begin + t];
-          if (!m_wait(&bempty[sl], ((uint32_t)(j / NB) & 1u) ^ 1u)) {
+          const int fs = j % kMmaFacSlots;
+          if (!m_wait(&bempty[sl], ((uint32_t)(j / NB) & 1u) ^ 1u) ||
+              !m_wait(&fempty[fs], ((uint32_t)(j / kMmaFacSlots) & 1u) ^ 1u)) {
             ok = false;
           } else {
             MmaTag tg{};
@@ -304,6 +331,10 @@ __global__ void __launch_bounds__(kMmaThreads, 1) k_mma(const __grid_constant__ 
             asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
             m_arrive_tx(&bfull[sl], tr.bytes);
             m_copy(dst, a.blobs + tr.off, tr.bytes, &bfull[sl]);
+            // the per-bin factors also go to the epilogue's ring, which outlives the blob slot
+            m_arrive_tx(&ffull[fs], kMmaBinsBytes);
+            m_copy(smem + L.off_fac + (size_t)fs * kMmaFacBytes, a.blobs + tr.off + kMmaBinsOff, kMmaBinsBytes,
+                   &ffull[fs]);
           }
         }
         ok = __shfl_sync(0xffffffffu, ok ? 1 : 0, 0) != 0;
@@ -354,37 +385,50 @@ __global__ void __launch_bounds__(kMmaThreads, 1) k_mma(const __grid_constant__ 
       const uint32_t *rptr = (const uint32_t *)(blob + BL.run_ptr);
       const uint32_t *sp = (const uint32_t *)(blob + BL.step_ptr);
       const uint2 *terms = (const uint2 *)(blob + BL.terms);
-      for (int s = 0; s < hd.n_k; ++s, ++g) {
+      const int n_st = (hd.n_k + kMmaStepsPerStage - 1) / kMmaStepsPerStage;
+      for (int s2 = 0; s2 < n_st; ++s2, ++g) {
         if ((int)(g % kMmaProducers) != pw) continue;
         const int q = (int)(g % kMmaStages);
         bool got = true;
         if (lane == 0) got = m_wait(&empty[q], ((g / kMmaStages) & 1u) ^ 1u);
         if (!__shfl_sync(0xffffffffu, got ? 1 : 0, 0)) { ok = false; break; }
         uint8_t *st = smem + (size_t)q * kMmaStageBytes;
-        // frame planes: one bulk copy per run of consecutive pixels and plane; slot k of the
-        // step is the 128-byte row k of each plane's operand
-        const int r0s = (int)rptr[s], nrun = (int)rptr[s + 1] - r0s;   // <= 32
-        uint2 rn = make_uint2(0u, 0u);
-        if (lane < nrun) rn = runs[r0s + lane];
-        const uint32_t len = rn.y >> 8;
-        const uint32_t bytes = __reduce_add_sync(0xffffffffu, len) * 256u;
+        const int s0 = kMmaStepsPerStage * s2, s1 = min(s0 + kMmaStepsPerStage, hd.n_k);
+        // frame planes: one bulk copy per run of consecutive pixels and plane; pixel slot k of
+        // the stage is the 128-byte row k of each plane's operand (a K step is 32 rows)
+        uint2 rn[kMmaStepsPerStage];
+        uint32_t len[kMmaStepsPerStage], bytes = 0;
+#pragma unroll
+        for (int hs = 0; hs < kMmaStepsPerStage; ++hs) {
+          rn[hs] = make_uint2(0u, 0u);
+          if (s0 + hs < s1) {
+            const int r0s = (int)rptr[s0 + hs], nrun = (int)rptr[s0 + hs + 1] - r0s;   // <= 32
+            if (lane < nrun) rn[hs] = runs[r0s + lane];
+          }
+          len[hs] = rn[hs].y >> 8;
+          bytes += __reduce_add_sync(0xffffffffu, len[hs]) * 256u;
+        }
         if (lane == 0) m_expect_tx(&full[q], bytes);
         __syncwarp();
-        if (len) {
-          const uint32_t ro = (rn.y & 0xFFu) * 128u;
-          m_copy(st + ro, a.xc_lo + (size_t)rn.x * 128u, len * 128u, &full[q]);
-          m_copy(st + 4096u + ro, a.xc_hi + (size_t)rn.x * 128u, len * 128u, &full[q]);
-        }
-        // weight planes: zero, then the step's terms
-        uint4 *bz = (uint4 *)(st + 8192u);
+#pragma unroll
+        for (int hs = 0; hs < kMmaStepsPerStage; ++hs)
+          if (len[hs]) {
+            const uint32_t ro = (uint32_t)(kMmaKStep * hs + (rn[hs].y & 0xFFu)) * 128u;
+            m_copy(st + ro, a.xc_lo + (size_t)rn[hs].x * 128u, len[hs] * 128u, &full[q]);
+            m_copy(st + kMmaAHi + ro, a.xc_hi + (size_t)rn[hs].x * 128u, len[hs] * 128u, &full[q]);
+          }
+        // weight planes: zero, then the stage's terms; byte (n', k) of the K-major operand at
+        // (n' % 8) * 16 + (n' / 8) * 512 + (k % 16) + (k / 16) * 128, n' = 48 j + n
+        uint4 *bz = (uint4 *)(st + kMmaB);
         for (int i = lane; i < (int)(4u * kMmaBPlane / 16u); i += 32) bz[i] = make_uint4(0u, 0u, 0u, 0u);
         __syncwarp();
-        const int t0 = (int)sp[s], t1 = (int)sp[s + 1];
+        const int t0 = (int)sp[s0], t1 = (int)sp[s1];
+        const uint32_t kbase = (uint32_t)(kMmaKStep * s0);
         for (int t = t0 + lane; t < t1; t += 32) {
           const uint2 tm = terms[t];
-          const uint32_t kk = (tm.y & 0xFFFFu) - (uint32_t)s * kMmaKStep, n = tm.y >> 16;
-          const uint32_t off = (n & 7u) * 16u + (n >> 3) * 256u + (kk & 15u) + (kk >> 4) * 128u;
-          uint8_t *b0 = st + 8192u + off;
+          const uint32_t kk = (tm.y & 0xFFFFu) - kbase, n = tm.y >> 16;
+          const uint32_t off = (n & 7u) * 16u + (n >> 3) * 512u + (kk & 15u) + (kk >> 4) * 128u;
+          uint8_t *b0 = st + kMmaB + off;
           b0[0] = (uint8_t)(tm.x & 0xFFu);
           b0[kMmaBPlane] = (uint8_t)((tm.x >> 8) & 0xFFu);
           b0[2 * kMmaBPlane] = (uint8_t)((tm.x >> 16) & 0xFFu);
@@ -396,7 +440,7 @@ __global__ void __launch_bounds__(kMmaThreads, 1) k_mma(const __grid_constant__ 
           h.n_rows = hd.n_rows;
           h.e0 = hd.e0;
           h.n_cols = hd.n_cols;
-          h.step = s;
+          h.step = s2;
           h.n_k = hd.n_k;
           h.box = hd.box_rows;
           s_shdr[q] = h;
@@ -444,8 +488,14 @@ __global__ void __launch_bounds__(kMmaThreads, 1) k_mma(const __grid_constant__ 
       }
       const uint32_t tbase = tmem + ((uint32_t)(quad * 32) << 16) + (uint32_t)(ab * kMmaAccCols + kHalf * half);
       float *crow = a.cake + (size_t)m * (size_t)a.n_bins;
-      // the tile's per-bin factors stay in its blob slot until every epilogue warp is done
-      const uint8_t *bb = smem + L.off_blob + (size_t)(j % NB) * a.blob_cap + kMmaBinsOff;
+      // the tile's per-bin factors, in its entry of the factor ring
+      const int fs = j % kMmaFacSlots;
+      if (lane == 0) got = m_wait(&ffull[fs], (uint32_t)(j / kMmaFacSlots) & 1u);
+      if (!__shfl_sync(0xffffffffu, got ? 1 : 0, 0)) {
+        if (lane == 0) atomicExch(a.err, MI_E_TIMEOUT);
+        break;
+      }
+      const uint8_t *bb = smem + L.off_fac + (size_t)fs * kMmaFacBytes;
       const double *bfac = (const double *)bb + kHalf * half;
       const double *bdk = (const double *)bb + kMmaN + kHalf * half;
       const float *blw = (const float *)(bb + 16 * kMmaN) + kHalf * half;
@@ -506,7 +556,7 @@ __global__ void __launch_bounds__(kMmaThreads, 1) k_mma(const __grid_constant__ 
         }
       }
       __syncwarp();
-      if (lane == 0) m_arrive(&bempty[j % NB]);   // this warp is done with the tile's blob
+      if (lane == 0) m_arrive(&fempty[fs]);   // this warp is done with the tile's factors
       if (tg.last && a.want_lo && live) {
 #pragma unroll
         for (int i = 0; i < kHalfRows; ++i) {
@@ -615,11 +665,12 @@ int launch_mma(Plan *p, int F, float *cake, double *partial, bool want_lo, cudaS
     }
     a.use_tma = 1;
   }
-  // four blob slots when shared memory allows, else three
+  // up to four blob slots, as shared memory allows (two suffice for progress: the epilogue
+  // holds one, the producers use the next)
   int dev_smem = 0;
   MI_CUDA(cudaDeviceGetAttribute(&dev_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, p->device));
   a.n_blob = kMmaBlobSlotsMax;
-  while (a.n_blob > 3 && mma_smem_layout(a.blob_cap, a.n_blob).total > (uint32_t)dev_smem) --a.n_blob;
+  while (a.n_blob > 2 && mma_smem_layout(a.blob_cap, a.n_blob).total > (uint32_t)dev_smem) --a.n_blob;
   const MmaSmem L = mma_smem_layout(a.blob_cap, a.n_blob);
   if (L.total > (uint32_t)dev_smem)
     return set_error(MI_E_RANGE, "launch_mma: %u B of shared memory needed (device allows %d)", L.total, dev_smem);
