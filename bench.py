@@ -31,6 +31,12 @@ REPO = Path(__file__).resolve().parent
 sys.path.insert(0, str(REPO))
 
 METRIC = "caked_frames_per_s"
+# DRAM bytes (read + write) per 128-frame batch of the sweep_2880 workload, from the committed
+# ncu captures (profiles/): the transpose kernel k_xc plus the caking kernel of the encoding
+TRAFFIC = {"runs": {"bytes_per_step": int(0.840295e9 + 0.761555e9 + 1.830098e9 + 1.170938e9),
+                    "kernels": "k_xc + k_runs"}}
+SCOPE = {"runs": "whole batch: k_xc + k_runs + k_lineout (k_runs 88 %)",
+         "mma": "whole batch: k_xc + k_mma + k_lineout"}
 UNIT = "frames/s"
 
 
@@ -46,7 +52,8 @@ def parse():
     ap.add_argument("--tile-rows", type=int, default=0)
     ap.add_argument("--tile-pixels", type=int, default=0)
     ap.add_argument("--fpl", type=int, default=0)
-    ap.add_argument("--encoding", default="auto", choices=["auto", "runs", "csr", "mma"])
+    ap.add_argument("--encoding", default="mma", choices=["auto", "runs", "csr", "mma"],
+                    help="tile encoding of the batched plan (mma: tensor cores, the default for these u16 sweeps)")
     ap.add_argument("--run-len", type=int, default=0)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-plain", action="store_true")
@@ -350,13 +357,13 @@ def main_ours(args):
     ref_bytes = map_bytes + F * (info["ref_pixels"] * 2 + w.n_r * w.n_eta * 4)
     # DRAM bytes (read + write) of the batch's kernels from the committed ncu capture of this
     # workload at F = 128 (profiles/k_runs_xc_sweep2880_f128.md); other shapes: not captured
+    enc = args.encoding if args.encoding != "auto" else "runs"
     traffic = None
-    if w.name.startswith("sweep_2880") and F == 128 and info["xc_pixels"] > 0:
-        traffic = {"bytes_per_step": int(0.840295e9 + 0.761555e9 + 1.830098e9 + 1.170938e9),
-                   "kernels": "k_xc + k_runs", "source": "ncu dram__bytes_read.sum + dram__bytes_write.sum"}
+    if w.name.startswith("sweep_2880") and F == 128 and info["xc_pixels"] > 0 and enc in TRAFFIC:
+        traffic = dict(TRAFFIC[enc], source="ncu dram__bytes_read.sum + dram__bytes_write.sum")
     roofline = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                 "frac": round(achieved / peak, 4), "traffic": traffic, "peak_kind": peak_kind,
-                "alg_bytes_per_launch": alg, "scope": "whole batch: k_xc + k_runs + k_lineout (k_runs 88 %)",
+                "alg_bytes_per_launch": alg, "scope": SCOPE.get(enc, "whole batch"),
                 "achieved_touched_bytes": round(ref_bytes / mean_step_s / 1e9, 1)}
 
     out = {"metric": METRIC, "value": round(value, 1), "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -367,7 +374,7 @@ def main_ours(args):
                       "map_records": info["n_records"], "tiles": info["n_tiles"],
                       "tile_rows": info["tile_rows"], "tile_pixels": info["tile_pixels"],
                       "frames_per_lane": info["frames_per_lane"],
-                      "encoding": args.encoding if args.encoding != "auto" else "runs",
+                      "encoding": enc,
                       "run_len": info["run_len"], "staged_pixels_per_frame": info["staged_pixels"],
                       "referenced_pixels": info["ref_pixels"], "map_bytes": info["map_bytes"],
                       "l2": "inputs larger than L2: each step reads a new %.1f GB batch" % (F * frame_bytes / 1e9),
@@ -395,7 +402,7 @@ def main_ours(args):
         gms = dist_max(g0.elapsed_time(g1), world)
         out["graph"] = {"frames_per_s": round(world * args.steps * F / (gms / 1e3), 1),
                         "ms_per_step": round(gms / args.steps, 4), "graphs": n_batches,
-                        "nodes_per_graph": "memset + k_xc + k_runs per 128 frames, k_lineout"}
+                        "nodes_per_graph": "memset + k_xc + caking kernel per 128 frames, k_lineout"}
         del graphs
 
     # ---- plain one-frame-per-launch kernel (reference GPU algorithm) on the same frames
