@@ -15,14 +15,14 @@
 // (2^-33 of the bin's largest weight); the reference's fp32 (raw - dark) and fp32 sums are
 // replaced by exact integer sums, so the result is closer to the FP64 one.
 //
-// Operands in shared memory, per pipeline stage (two K steps, 64 pixel slots):
+// Operands in shared memory, per pipeline stage (kMmaStepsPerStage K steps of 32 pixel slots):
 //   A (frames): MN-major, 128B swizzle; slot k of the stage is the 128-byte row
 //     (k % 8) * 128 + (k / 8) * 1024 holding the pixel's 128 frame bytes, 16-byte granule g
 //     at position g ^ (k % 8).  Kernel (a) writes each pixel-major row with its granules
 //     already in that order for phase c % 8, and the tiler puts pixel c in a slot with
 //     k % 8 == c % 8, so a slot is filled by one plain 128-byte bulk copy per plane.
 //   B (weights): K-major, no swizzle, the four byte planes as rows n' = 48 j + n; byte (n', k)
-//     at (n' % 8) * 16 + (n' / 8) * 512 + (k % 16) + (k / 16) * 128, zeroed and then
+//     at (n' % 8) * 16 + (n' / 8) * kMmaBSbo + (k % 16) + (k / 16) * 128, zeroed and then
 //     scattered from the stage's terms.
 //
 // Roles (one persistent CTA per SM, 14 warps):
@@ -32,7 +32,7 @@
 //   warp 1          loader: claims work items (heaviest first) and brings each tile's blob
 //                   into one of its blob slots with one bulk copy
 //   warps 2,3,12,13 producers: stage g (counted over the CTA's tiles) is built by producer
-//                   g % 4 into stage slot g % 4
+//                   g % 4 into stage slot g % kMmaStages
 //   warps 4-11      epilogue: warp w reads TMEM lanes 32 (w % 4) + 0..31 (= frames) and half
 //                   of the tile's bins (8 bins x 5 accumulators at a time), recombines, puts the
 //                   cake values into a shared-memory tile that one TMA tensor store writes to
@@ -51,15 +51,21 @@
 
 namespace mi {
 
-constexpr int kMmaStages = 4;
-constexpr int kMmaStepsPerStage = 2;        // K steps (32 pixel slots each) per pipeline stage
+#ifndef MI_MMA_STAGES
+#define MI_MMA_STAGES 8
+#define MI_MMA_STEPS 1
+#endif
+constexpr int kMmaStages = MI_MMA_STAGES;
+constexpr int kMmaStepsPerStage = MI_MMA_STEPS;   // K steps (32 pixel slots each) per stage
 constexpr int kMmaProducers = 4;
 constexpr int kMmaEpiWarps = 8;
 constexpr int kMmaWarps = 14;
 constexpr int kMmaThreads = kMmaWarps * 32;
-constexpr uint32_t kMmaStageBytes = 28672;   // A lo 8192 | A hi 8192 | B 12288 (64 pixel slots)
-constexpr uint32_t kMmaAHi = 8192, kMmaB = 16384;
-constexpr uint32_t kMmaBPlane = 3072;        // 48 rows of the K-major weight operand, 64 K
+// per stage: A lo 4096 | A hi 4096 | B 6144 per K step
+constexpr uint32_t kMmaStageBytes = 14336u * kMmaStepsPerStage;
+constexpr uint32_t kMmaAHi = 4096u * kMmaStepsPerStage, kMmaB = 8192u * kMmaStepsPerStage;
+constexpr uint32_t kMmaBPlane = 1536u * kMmaStepsPerStage;   // 48 rows of the K-major weight operand
+constexpr uint32_t kMmaBSbo = 256u * kMmaStepsPerStage;      // bytes per 8-row group of that operand
 constexpr int kMmaBlobSlotsMax = 4;
 constexpr int kMmaFacSlots = 6;             // ring of the tiles' per-bin factors (epilogue)
 constexpr uint32_t kMmaFacBytes = 1024;      // one ring entry: fac, dk, lw of 48 bins (960 B)
@@ -283,14 +289,14 @@ __global__ void __launch_bounds__(kMmaThreads, 1) k_mma(const __grid_constant__ 
           const uint64_t alo = m_desc(sb + 4096u * hs, 0u, 1024u, 2u);
           const uint64_t ahi = m_desc(sb + kMmaAHi + 4096u * hs, 0u, 1024u, 2u);
           const uint32_t bsa = sb + kMmaB + 256u * hs;
-          const uint64_t bd = m_desc(bsa, 128u, 512u, 0u);
+          const uint64_t bd = m_desc(bsa, 128u, kMmaBSbo, 0u);
           const bool first = hq.z == 0 && hs == 0;
           m_mma(dbase, alo, bd, mma_idesc(4 * kMmaN), first ? 0u : 1u);
           if (!first) {
             m_mma(dbase + (uint32_t)kMmaN, ahi, bd, mma_idesc(4 * kMmaN), 1u);
           } else {
             m_mma(dbase + (uint32_t)kMmaN, ahi, bd, mma_idesc(3 * kMmaN), 1u);
-            m_mma(dbase + (uint32_t)(4 * kMmaN), ahi, m_desc(bsa + 3u * kMmaBPlane, 128u, 512u, 0u),
+            m_mma(dbase + (uint32_t)(4 * kMmaN), ahi, m_desc(bsa + 3u * kMmaBPlane, 128u, kMmaBSbo, 0u),
                   mma_idesc(kMmaN), 0u);
           }
         }
@@ -418,7 +424,7 @@ __global__ void __launch_bounds__(kMmaThreads, 1) k_mma(const __grid_constant__ 
             m_copy(st + kMmaAHi + ro, a.xc_hi + (size_t)rn[hs].x * 128u, len[hs] * 128u, &full[q]);
           }
         // weight planes: zero, then the stage's terms; byte (n', k) of the K-major operand at
-        // (n' % 8) * 16 + (n' / 8) * 512 + (k % 16) + (k / 16) * 128, n' = 48 j + n
+        // (n' % 8) * 16 + (n' / 8) * kMmaBSbo + (k % 16) + (k / 16) * 128, n' = 48 j + n
         uint4 *bz = (uint4 *)(st + kMmaB);
         for (int i = lane; i < (int)(4u * kMmaBPlane / 16u); i += 32) bz[i] = make_uint4(0u, 0u, 0u, 0u);
         __syncwarp();
@@ -427,7 +433,7 @@ __global__ void __launch_bounds__(kMmaThreads, 1) k_mma(const __grid_constant__ 
         for (int t = t0 + lane; t < t1; t += 32) {
           const uint2 tm = terms[t];
           const uint32_t kk = (tm.y & 0xFFFFu) - kbase, n = tm.y >> 16;
-          const uint32_t off = (n & 7u) * 16u + (n >> 3) * 512u + (kk & 15u) + (kk >> 4) * 128u;
+          const uint32_t off = (n & 7u) * 16u + (n >> 3) * kMmaBSbo + (kk & 15u) + (kk >> 4) * 128u;
           uint8_t *b0 = st + kMmaB + off;
           b0[0] = (uint8_t)(tm.x & 0xFFu);
           b0[kMmaBPlane] = (uint8_t)((tm.x >> 8) & 0xFFu);
