@@ -112,6 +112,8 @@ typedef struct {
                               lineouts are the propagated variances of profile_1d
                               (kernels.py:567-628): sum(A^2 var) / (sum A)^2 and
                               sum(var) / N^2.  mi_integrate_plain rejects such plans.  */
+  int32_t host_threads;    /* host threads building the plan (0 = all): a server that
+                              admits a stream while serving others leaves cores to them */
 } mi_plan_opts;
 
 #define MI_ENC_AUTO 0      /* runs                                                       */

@@ -44,7 +44,7 @@ class MiPlanOpts(C.Structure):
     _fields_ = [("mode", C.c_int32), ("normalize", C.c_int32), ("semantics", C.c_int32),
                 ("tile_rows", C.c_int32), ("tile_pixels", C.c_int32),
                 ("frames_per_lane", C.c_int32), ("encoding", C.c_int32), ("run_len", C.c_int32),
-                ("variance", C.c_int32)]
+                ("variance", C.c_int32), ("host_threads", C.c_int32)]
 
 
 ENC = {"auto": 0, "csr": 1, "runs": 2, "mma": 3}

@@ -57,9 +57,12 @@ namespace mi {
 #endif
 constexpr int kMmaStages = MI_MMA_STAGES;
 constexpr int kMmaStepsPerStage = MI_MMA_STEPS;   // K steps (32 pixel slots each) per stage
-constexpr int kMmaProducers = 4;
+#ifndef MI_MMA_PRODUCERS
+#define MI_MMA_PRODUCERS 4
+#endif
+constexpr int kMmaProducers = MI_MMA_PRODUCERS;
 constexpr int kMmaEpiWarps = 8;
-constexpr int kMmaWarps = 14;
+constexpr int kMmaWarps = 2 + kMmaProducers + 8;   // MMA/TMEM, loader, producers, epilogue
 constexpr int kMmaThreads = kMmaWarps * 32;
 // per stage: A lo 4096 | A hi 4096 | B 6144 per K step
 constexpr uint32_t kMmaStageBytes = 14336u * kMmaStepsPerStage;

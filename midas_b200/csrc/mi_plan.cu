@@ -789,6 +789,21 @@ static int build_mma_tiles(const HostCSR &csr, const mi_map_desc &m, Plan *p, co
   return MI_OK;
 }
 
+// Caps the OpenMP threads of the calling thread's parallel regions for a scope (the
+// host_threads plan option); the previous setting is restored on exit.
+struct HostThreads {
+  int prev = 0;
+  explicit HostThreads(int n) {
+    if (n > 0) {
+      prev = omp_get_max_threads();
+      omp_set_num_threads(n);
+    }
+  }
+  ~HostThreads() {
+    if (prev > 0) omp_set_num_threads(prev);
+  }
+};
+
 // Build a plan.  `pre` (optional) is the weight list already built for the whole detector
 // (panel plans: the panels' lists merged over the virtual detector); `m` then describes the
 // virtual detector and carries no records, and the plain path is not built.
@@ -1155,6 +1170,7 @@ int mi_plan_create(const mi_map_desc *map, const mi_plan_opts *opts, int device,
   p->device = device;
   int prev = 0;
   cudaGetDevice(&prev);
+  HostThreads ht(o.host_threads);
   int rc = build_plan(*map, o, p);
   cudaSetDevice(prev);
   if (rc) {
@@ -1190,6 +1206,7 @@ int mi_plan_create_panels(const mi_map_desc *maps, int n_panels, const mi_plan_o
   mi_plan_opts o{};
   if (opts) o = *opts;
   else { o.mode = MI_MODE_FLOOR; o.normalize = 1; o.semantics = MI_SEM_PY; }
+  HostThreads ht(o.host_threads);
   if (o.mode < 0 || o.mode > 2 || o.semantics < 0 || o.semantics > 2 ||
       (o.semantics == MI_SEM_IC && o.mode == MI_MODE_FLOOR))
     return set_error(MI_E_ARG, "mi_plan_create_panels: bad mode %d / semantics %d", o.mode, o.semantics);

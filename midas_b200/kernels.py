@@ -68,6 +68,7 @@ class CakePlan:
             are per-pixel variance maps, caked with the squared coalesced weights and
             divided by the squared bin area; its lineouts are the propagated variances of
             profile_1d_with_variance (kernels.py:604-645).
+        host_threads: host threads that build the plan (0 = all cores).
     """
 
     def __init__(self, pixmap: PixelMap, *, n_r: int, n_eta: int, n_pixels_y: int,
@@ -75,7 +76,7 @@ class CakePlan:
                  semantics: str = "py", bc_y: float = 0.0, bc_z: float = 0.0,
                  device="cuda", tile_rows: int = 0, tile_pixels: int = 0,
                  frames_per_lane: int = 0, encoding: str = "auto", run_len: int = 0,
-                 variance: bool = False):
+                 variance: bool = False, host_threads: int = 0):
         if pixmap.n_bins != n_r * n_eta:
             raise ValueError(f"PixelMap has {pixmap.n_bins} bins; n_r * n_eta = {n_r * n_eta}")
         if mode not in L.MODE:
@@ -97,7 +98,7 @@ class CakePlan:
             raise ValueError(f"unknown encoding {encoding!r}; expected 'auto' | 'csr' | 'runs' | 'mma'")
         opts = L.MiPlanOpts(L.MODE[mode], int(self.normalize), L.SEM[semantics],
                             int(tile_rows), int(tile_pixels), int(frames_per_lane),
-                            L.ENC[encoding], int(run_len), int(self.variance))
+                            L.ENC[encoding], int(run_len), int(self.variance), int(host_threads))
         h = C.c_void_p()
         L.check(L.lib().mi_plan_create(C.byref(desc), C.byref(opts), self.device.index,
                                        C.byref(h)), "mi_plan_create")

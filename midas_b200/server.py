@@ -30,6 +30,7 @@ from __future__ import annotations
 import collections
 import ctypes as C
 import itertools
+import os
 import threading
 import time
 from concurrent.futures import Future
@@ -171,10 +172,12 @@ class DeviceBackend:
     """
 
     def __init__(self, device: int = 0, max_batch: int = 32, max_inflight: int = 2, plain: bool = False,
-                 pinned_bytes: int = 2 << 30):
+                 pinned_bytes: int = 2 << 30, build_threads: int = 0):
         import torch
         self.torch = torch
         self.device = torch.device("cuda", device)
+        # host threads building an admitted stream's plan: a quarter of the cores (at most 4)
+        self.build_threads = build_threads or max(1, min(4, (os.cpu_count() or 4) // 4))
         self.max_batch = max_batch
         self.max_inflight = max_inflight
         self.plain = plain
@@ -219,9 +222,11 @@ class DeviceBackend:
             for tok in tokens:
                 self.pool.release(tok)
             raise
+        # a stream admitted while others are served builds its plan on a few host cores, so
+        # the scheduler thread and the callers submitting frames keep theirs
         plan = CakePlan(cfg.pixmap, n_r=cfg.n_r, n_eta=cfg.n_eta, n_pixels_y=cfg.n_pixels_y,
                         n_pixels_z=cfg.n_pixels_z, mode=cfg.mode, bc_y=cfg.bc_y, bc_z=cfg.bc_z,
-                        device=self.device, tile_rows=cfg.tile_rows)
+                        device=self.device, tile_rows=cfg.tile_rows, host_threads=self.build_threads)
         if cfg.dark is not None:
             plan.set_dark(cfg.dark)
         slots = []

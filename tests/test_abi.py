@@ -97,6 +97,6 @@ def test_frame_preparation_argument_checks():
 
 
 def test_plan_opts_layout_matches_header():
-    """mi_plan_opts: nine int32 fields, variance last."""
-    assert C.sizeof(L.MiPlanOpts) == 9 * 4
-    assert L.MiPlanOpts._fields_[-1][0] == "variance"
+    """mi_plan_opts: ten int32 fields, host_threads last."""
+    assert C.sizeof(L.MiPlanOpts) == 10 * 4
+    assert [f for f, _ in L.MiPlanOpts._fields_][-2:] == ["variance", "host_threads"]
