@@ -35,8 +35,9 @@
 //                   g % 4 into stage slot g % kMmaStages
 //   warps 4-11      epilogue: warp w reads TMEM lanes 32 (w % 4) + 0..31 (= frames) and half
 //                   of the tile's bins (8 bins x 5 accumulators at a time), recombines, puts the
-//                   cake values into a shared-memory tile that one TMA tensor store writes to
-//                   the [F][n_r][n_eta] cake (double-buffered), and accumulates the lineout
+//                   cake values into a shared-memory tile holding two adjacent tiles of the item
+//                   (8 columns: 32-byte rows, whole sectors) that one TMA tensor store writes
+//                   to the [F][n_r][n_eta] cake, and accumulates the lineout
 //                   partial sums of the item's rows in registers (a frame's result does not
 //                   depend on the rest of its batch)
 // Every wait is an mbarrier poll with an iteration limit; on expiry the kernel sets the
@@ -76,10 +77,11 @@ constexpr int kMmaTmemCols = 512;
 constexpr int kMmaAccCols = 256;            // columns per accumulator set (5 x 48 used)
 constexpr uint32_t kMmaWaitLimit = 1u << 26;
 constexpr uint32_t kMmaOutBytes = kMmaFrames * kMmaN * 4;   // one cake tile: [128][rows][4] floats
-constexpr int kMmaBoxes = 4;                // cake store boxes of 12, 6, 3 and 1 rows
+// The epilogue stores two adjacent tiles of an item (8 columns) with one box: 32-byte rows
+constexpr int kMmaBoxes = 8;                // cake store boxes of 4 and 8 columns x 12, 6, 3, 1 rows
 
 struct MmaArgs {
-  CUtensorMap tmap[kMmaBoxes];  // the call's cake as (n_eta, n_r, F) floats, box 4 x h x 128
+  CUtensorMap tmap[kMmaBoxes];  // the call's cake as (n_eta, n_r, F) floats, box w x h x 128
   const WorkItem *items;
   const TileRef *tiles;
   const uint8_t *blobs;
@@ -102,6 +104,7 @@ struct MmaTag {
                                     // tile; K steps of the tile (the MMA lane reads these 16 B)
   int32_t slot, first, last, box;   // item's lineout slot; first/last tile of item; box rows
   int32_t r0, n_rows, e0, n_cols;   // the tile's bins
+  int32_t pos, pad0, pad1, pad2;    // index of the tile in its item
 };
 
 struct MmaSmem {
@@ -334,6 +337,7 @@ __global__ void __launch_bounds__(kMmaThreads, 1) k_mma(const __grid_constant__ 
             tg.slot = it.slot;
             tg.first = (t == 0);
             tg.last = (t == nt - 1);
+            tg.pos = t;
             tg.tile = j;
             s_btag[sl] = tg;
             uint8_t *dst = smem + L.off_blob + (size_t)sl * a.blob_cap;
@@ -489,10 +493,15 @@ __global__ void __launch_bounds__(kMmaThreads, 1) k_mma(const __grid_constant__ 
 #pragma unroll
         for (int i = 0; i < kHalfRows; ++i) saw[i] = ssm[i] = 0.0;
       }
-      float *ot = (float *)(smem + L.off_out + (uint32_t)(j & 1) * kMmaOutBytes);   // [128][box][4]
-      if (a.use_tma) {
-        // the store issued from this buffer two tiles ago has read it
-        if (issuer) asm volatile("cp.async.bulk.wait_group.read 1;" ::: "memory");
+      // cake tiles go out in pairs: the item's tiles 2i and 2i+1 share one [128][box][8] tile of
+      // shared memory and one 8-column store; an item's odd last tile goes alone, [128][box][4]
+      float *ot = (float *)(smem + L.off_out);
+      const bool second = (tg.pos & 1) != 0;
+      const int pitch = (second || !tg.last) ? 2 * kMmaCols : kMmaCols;
+      const int coff = second ? kMmaCols : 0;
+      if (a.use_tma && !second) {
+        // the previous store has read the tile's shared memory
+        if (issuer) asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");
         asm volatile("bar.sync 1, %0;" ::"r"(kMmaEpiWarps * 32) : "memory");
       }
       const uint32_t tbase = tmem + ((uint32_t)(quad * 32) << 16) + (uint32_t)(ab * kMmaAccCols + kHalf * half);
@@ -547,19 +556,19 @@ __global__ void __launch_bounds__(kMmaThreads, 1) k_mma(const __grid_constant__ 
 #pragma unroll
           for (int q = 0; q < 2; ++q) {
             const int row = kHalfRows * half + 2 * c + q;
-            if (row < tg.box) *(float4 *)(ot + ((size_t)m * tg.box + row) * kMmaCols) =
+            if (row < tg.box) *(float4 *)(ot + ((size_t)m * tg.box + row) * pitch + coff) =
                 make_float4(o[4 * q], o[4 * q + 1], o[4 * q + 2], o[4 * q + 3]);
           }
         }
       }
-      if (a.use_tma) {
+      if (a.use_tma && (second || tg.last)) {
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
         asm volatile("bar.sync 1, %0;" ::"r"(kMmaEpiWarps * 32) : "memory");
         if (issuer) {
-          const int bi = tg.box == kMmaRows ? 0 : (tg.box == 6 ? 1 : (tg.box == 3 ? 2 : 3));
+          const int bi = (tg.box == kMmaRows ? 0 : (tg.box == 6 ? 1 : (tg.box == 3 ? 2 : 3))) + (second ? 4 : 0);
           asm volatile(
               "cp.async.bulk.tensor.3d.global.shared::cta.bulk_group [%0, {%1, %2, %3}], [%4];" ::"l"(&a.tmap[bi]),
-              "r"(tg.e0), "r"(tg.r0), "r"(0), "r"(m_smem(ot))
+              "r"(tg.e0 - coff), "r"(tg.r0), "r"(0), "r"(m_smem(ot))
               : "memory");
           asm volatile("cp.async.bulk.commit_group;" ::: "memory");
         }
@@ -664,9 +673,10 @@ int launch_mma(Plan *p, int F, float *cake, double *partial, bool want_lo, cudaS
     const cuuint64_t dims[3] = {(cuuint64_t)p->n_eta, (cuuint64_t)p->n_r, (cuuint64_t)F};
     const cuuint64_t strides[2] = {(cuuint64_t)p->n_eta * 4u, (cuuint64_t)p->n_bins * 4u};
     const cuuint32_t estr[3] = {1, 1, 1};
-    const int rows[kMmaBoxes] = {kMmaRows, 6, 3, 1};
+    const int rows[4] = {kMmaRows, 6, 3, 1};
     for (int i = 0; i < kMmaBoxes; ++i) {
-      const cuuint32_t box[3] = {(cuuint32_t)kMmaCols, (cuuint32_t)rows[i], (cuuint32_t)kMmaFrames};
+      const cuuint32_t box[3] = {(cuuint32_t)(i < 4 ? kMmaCols : 2 * kMmaCols), (cuuint32_t)rows[i % 4],
+                                 (cuuint32_t)kMmaFrames};
       const CUresult r = enc(&a.tmap[i], CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, cake, dims, strides, box, estr,
                              CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
                              CU_TENSOR_MAP_L2_PROMOTION_NONE, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
