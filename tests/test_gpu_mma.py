@@ -169,3 +169,19 @@ def test_mma_panels(cuda):
     b = pr.integrate(frames)
     for x, y in zip(a, b):
         assert rel_err(x.cpu().numpy(), y.cpu().numpy())[0] <= 2 * TOL
+
+
+def test_host_threads_option_builds_the_same_plan(cuda):
+    """A plan built on two host threads (the serving loop's admission setting) cakes
+    bit-identically to one built on all cores, for both encodings."""
+    g = load_kernels_case("b")
+    pm = from_arrays(g["records"], g["nmap"])
+    rng = np.random.default_rng(12)
+    frames = torch.from_numpy(rng.integers(0, 60000, size=(5, g["nz"], g["ny"])).astype(np.uint16)).to(cuda)
+    for enc in ("mma", "runs"):
+        kw = dict(n_r=g["n_r"], n_eta=g["n_eta"], n_pixels_y=g["ny"], n_pixels_z=g["nz"], mode="gradient",
+                  bc_y=g["bc_y"], bc_z=g["bc_z"], device=cuda, encoding=enc)
+        a = CakePlan(pm, host_threads=2, **kw).integrate(frames)
+        b = CakePlan(pm, **kw).integrate(frames)
+        for x, y in zip(a, b):
+            assert torch.equal(x, y)
