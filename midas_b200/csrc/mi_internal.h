@@ -241,7 +241,6 @@ struct XcChunk {
 //                                       per byte plane); slot k holds a pixel with
 //                                       c % 8 == k % 8 (the swizzle phase of its row)
 //   uint32 run_ptr[n_k + 1]             runs of K step s: [run_ptr[s], run_ptr[s+1])
-//   uint32 xrow[32 * n_k]               compact index of each slot, 0xFFFFFFFF = empty
 //   uint32 step_ptr[n_k + 1]            terms of K step s
 //   uint2  terms[n_terms]               {q, k | n << 16}, sorted by k
 struct MmaHdr {
@@ -262,7 +261,7 @@ constexpr uint32_t kMmaBinsOff = 32;   // fac, dk, lw after the header
 constexpr uint32_t kMmaBinsBytes = kMmaN * (8 + 8 + 4);
 
 struct MmaBlob {
-  uint32_t runs, run_ptr, xrow, step_ptr, terms, bytes;
+  uint32_t runs, run_ptr, step_ptr, terms, bytes;
 };
 __host__ __device__ inline MmaBlob mma_blob_layout(int n_k, int n_runs, int n_terms) {
   auto a16 = [](uint32_t x) { return (x + 15u) & ~15u; };
@@ -270,7 +269,6 @@ __host__ __device__ inline MmaBlob mma_blob_layout(int n_k, int n_runs, int n_te
   uint32_t o = a16(kMmaBinsOff + kMmaBinsBytes);
   b.runs = o;     o = a16(o + 8u * (uint32_t)n_runs);
   b.run_ptr = o;  o = a16(o + 4u * (uint32_t)(n_k + 1));
-  b.xrow = o;     o = a16(o + 4u * (uint32_t)kMmaKStep * (uint32_t)n_k);
   b.step_ptr = o; o = a16(o + 4u * (uint32_t)(n_k + 1));
   b.terms = o;    o = a16(o + 8u * (uint32_t)n_terms);
   b.bytes = o;

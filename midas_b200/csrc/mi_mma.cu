@@ -606,7 +606,8 @@ __global__ void k_mma_dark(const TileRef *tiles, uint8_t *blobs, const int32_t *
   uint8_t *blob = blobs + tr.off;
   const MmaHdr hd = *(const MmaHdr *)blob;
   const MmaBlob BL = mma_blob_layout(hd.n_k, hd.n_runs, hd.n_terms);
-  const uint32_t *xrow = (const uint32_t *)(blob + BL.xrow);
+  const uint2 *runs = (const uint2 *)(blob + BL.runs);
+  const uint32_t *rptr = (const uint32_t *)(blob + BL.run_ptr);
   const uint2 *terms = (const uint2 *)(blob + BL.terms);
   const int n = threadIdx.x;
   if (n >= kMmaN) return;
@@ -617,7 +618,14 @@ __global__ void k_mma_dark(const TileRef *tiles, uint8_t *blobs, const int32_t *
     for (int t = 0; t < hd.n_terms; ++t) {
       const uint2 tm = terms[t];
       if ((int)(tm.y >> 16) != n) continue;
-      d += (double)tm.x * (double)dark[xc_pix[xrow[tm.y & 0xFFFFu]]];
+      // the term's pixel: the run of its K step that covers its slot
+      const uint32_t k = tm.y & 0xFFFFu, s = k / kMmaKStep, kk = k % kMmaKStep;
+      uint32_t c = 0;
+      for (uint32_t r = rptr[s]; r < rptr[s + 1]; ++r) {
+        const uint32_t k0 = runs[r].y & 0xFFu, len = runs[r].y >> 8;
+        if (kk >= k0 && kk < k0 + len) { c = runs[r].x + (kk - k0); break; }
+      }
+      d += (double)tm.x * (double)dark[xc_pix[c]];
     }
   dk[n] = fac[n] * d;
 }

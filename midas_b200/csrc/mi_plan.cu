@@ -650,7 +650,6 @@ static int mma_tile_blob(const HostCSR &csr, const mi_map_desc &m, const std::ve
   memcpy(blob.data() + kMmaBinsOff + sizeof(bfac) + sizeof(bdk), blw, sizeof(blw));
   if (!runs.empty()) memcpy(blob.data() + L.runs, runs.data(), runs.size() * 8);
   memcpy(blob.data() + L.run_ptr, rptr.data(), rptr.size() * 4);
-  memcpy(blob.data() + L.xrow, xrow.data(), xrow.size() * 4);
   memcpy(blob.data() + L.step_ptr, sp.data(), sp.size() * 4);
   if (!terms.empty()) memcpy(blob.data() + L.terms, terms.data(), terms.size() * 8);
   *nnz_out = (int)terms.size();
