@@ -256,7 +256,7 @@ constexpr int kMmaFrames = 128;        // frames per launch: the M of every MMA
 constexpr int kMmaKStep = 32;          // K slots (staged pixels) per MMA step
 constexpr uint32_t kMmaEmpty = 0xFFFFFFFFu;
 constexpr int kMmaMaxBinTerms = 16000; // int32 accumulators: 2 x 255 x 255 per term
-constexpr uint32_t kMmaBlobCap = 20 * 1024;  // largest tile blob (blob slots in shared memory)
+constexpr uint32_t kMmaBlobCap = 24 * 1024;  // largest tile blob (blob slots in shared memory)
 constexpr uint32_t kMmaBinsOff = 32;   // fac, dk, lw after the header
 constexpr uint32_t kMmaBinsBytes = kMmaN * (8 + 8 + 4);
 

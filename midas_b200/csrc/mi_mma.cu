@@ -53,7 +53,7 @@
 namespace mi {
 
 #ifndef MI_MMA_STAGES
-#define MI_MMA_STAGES 8
+#define MI_MMA_STAGES 7
 #define MI_MMA_STEPS 1
 #endif
 constexpr int kMmaStages = MI_MMA_STAGES;
