@@ -185,3 +185,29 @@ def test_host_threads_option_builds_the_same_plan(cuda):
         b = CakePlan(pm, **kw).integrate(frames)
         for x, y in zip(a, b):
             assert torch.equal(x, y)
+
+
+def test_mma_coarse_bins_split_bands(cuda):
+    """A 2048^2 powder map with coarse bins (990 x 72: 1 px in R, 5 deg in eta): tile blobs
+    of whole 12-row bands exceed the kernel's blob slots, so bands are cut into 6-, 3- or
+    1-row sub-bands with their own cake store boxes. Agrees with the run encoding."""
+    from midas_b200 import synth
+    from midas_b200.mapper import build_map
+    w = synth.powder_2048()
+    m = w.mapper
+    pm, _ = build_map(m, device=0)
+    kw = dict(n_r=w.n_r, n_eta=w.n_eta, n_pixels_y=m.NrPixelsY, n_pixels_z=m.NrPixelsZ, mode=w.mode,
+              bc_y=m.BC_y, bc_z=m.BC_z, device=cuda)
+    mma = CakePlan(pm, encoding="mma", **kw)
+    runs = CakePlan(pm, encoding="runs", **kw)
+    # unsplit: one item per band of 12 rows and slot of 8 columns (9 slots of 72 columns)
+    assert mma.info["n_items"] > (w.n_r + 11) // 12 * 9
+    dark = w.dark().cpu().numpy()
+    mma.set_dark(dark)
+    runs.set_dark(dark)
+    frames = w.frames(0, 130)
+    a = mma.integrate(frames)
+    b = runs.integrate(frames)
+    assert mma.status() == 0
+    for x, y in zip(a, b):
+        assert rel_err(x.cpu().numpy(), y.cpu().numpy())[0] <= 2 * TOL
