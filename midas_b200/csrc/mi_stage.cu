@@ -62,20 +62,35 @@ __global__ void __launch_bounds__(256) k_xc(const T *__restrict__ frames, int64_
       *(uint4 *)&S[f][8 * (v ^ ((f >> 3) & 7))] = val;
     }
     __syncthreads();
-    for (int i = threadIdx.x; i < ch.n * 8; i += blockDim.x) {
-      const int p = i >> 3, q = i & 7;
-      const int col = 8 * ((p >> 3) ^ q) + (p & 7);
-      uint32_t w[4];
+    if constexpr (PLANES) {
+      // pixel p, 16-frame granule g of this half (frame octets 2g, 2g+1): one 16-byte store
+      // per byte plane, four consecutive threads writing one pixel's half row
+      for (int i = threadIdx.x; i < ch.n * 4; i += blockDim.x) {
+        const int p = i >> 2, g = i & 3;
+        uint32_t w[8];
 #pragma unroll
-      for (int j = 0; j < 8; j += 2)
-        w[j / 2] = (uint32_t)S[8 * q + j][col] | ((uint32_t)S[8 * q + j + 1][col] << 16);
-      if constexpr (PLANES) {
-        const int cc = ch.c0 + p, fr = h * kXcFrames + 8 * q;
-        uint8_t *row = xc + (int64_t)cc * 128 + 16 * ((fr >> 4) ^ (cc & 7)) + (fr & 8);
-        *(uint2 *)row = make_uint2(__byte_perm(w[0], w[1], 0x6420), __byte_perm(w[2], w[3], 0x6420));
-        *(uint2 *)(row + n_xc * 128) =
-            make_uint2(__byte_perm(w[0], w[1], 0x7531), __byte_perm(w[2], w[3], 0x7531));
-      } else {
+        for (int o = 0; o < 2; ++o) {
+          const int q = 2 * g + o;
+          const int col = 8 * ((p >> 3) ^ q) + (p & 7);
+#pragma unroll
+          for (int j = 0; j < 8; j += 2)
+            w[4 * o + j / 2] = (uint32_t)S[8 * q + j][col] | ((uint32_t)S[8 * q + j + 1][col] << 16);
+        }
+        const int cc = ch.c0 + p;
+        uint8_t *row = xc + (int64_t)cc * 128 + 16 * ((4 * h + g) ^ (cc & 7));
+        *(uint4 *)row = make_uint4(__byte_perm(w[0], w[1], 0x6420), __byte_perm(w[2], w[3], 0x6420),
+                                   __byte_perm(w[4], w[5], 0x6420), __byte_perm(w[6], w[7], 0x6420));
+        *(uint4 *)(row + n_xc * 128) = make_uint4(__byte_perm(w[0], w[1], 0x7531), __byte_perm(w[2], w[3], 0x7531),
+                                                  __byte_perm(w[4], w[5], 0x7531), __byte_perm(w[6], w[7], 0x7531));
+      }
+    } else {
+      for (int i = threadIdx.x; i < ch.n * 8; i += blockDim.x) {
+        const int p = i >> 3, q = i & 7;
+        const int col = 8 * ((p >> 3) ^ q) + (p & 7);
+        uint32_t w[4];
+#pragma unroll
+        for (int j = 0; j < 8; j += 2)
+          w[j / 2] = (uint32_t)S[8 * q + j][col] | ((uint32_t)S[8 * q + j + 1][col] << 16);
         *(uint4 *)(out + (int64_t)(ch.c0 + p) * kPitch + h * kXcFrames + 8 * q) = make_uint4(w[0], w[1], w[2], w[3]);
       }
     }
