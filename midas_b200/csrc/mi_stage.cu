@@ -28,6 +28,8 @@ namespace mi {
 // 16-byte granule of frames 16g .. 16g+15 at position g ^ (c % 8): the 128-byte swizzle
 // phase the tensor-core operand of a K slot with k % 8 == c % 8 expects, so a run of
 // consecutive pixels is staged with one plain bulk copy per plane.
+constexpr int kXcLoads = 8;
+
 template <typename T, bool VEC, bool PLANES>
 __global__ void __launch_bounds__(256) k_xc(const T *__restrict__ frames, int64_t stride, int F, int ny, int z_off,
                                             const XcChunk *__restrict__ chunks, uint8_t *__restrict__ xc,
@@ -41,25 +43,40 @@ __global__ void __launch_bounds__(256) k_xc(const T *__restrict__ frames, int64_
   for (int h = 0; h * kXcFrames < F; ++h) {
     const int fh = min(kXcFrames, F - h * kXcFrames);
     if (h) __syncthreads();
-    for (int i = threadIdx.x; i < kXcFrames * nv; i += blockDim.x) {
-      const int f = i / nv, v = i - f * nv;
-      uint4 val = make_uint4(0u, 0u, 0u, 0u);
-      if (f < fh) {
-        const T *src = frames + (int64_t)(h * kXcFrames + f) * stride + base + 8 * v;
-        if constexpr (VEC) {
-          val = __ldg((const uint4 *)src);
-        } else {
-          uint32_t t[4];
+    // kXcLoads groups per thread per pass, all loads issued before the first shared-memory
+    // store, so each thread keeps that many 16-byte reads in flight
+    const int n_items = kXcFrames * nv;
+    for (int i0 = threadIdx.x; i0 < n_items; i0 += kXcLoads * blockDim.x) {
+      uint4 val[kXcLoads];
 #pragma unroll
-          for (int j = 0; j < 8; j += 2) {
-            const uint32_t lo = (8 * v + j < ch.n) ? (uint32_t)(uint16_t)__ldg(src + j) : 0u;
-            const uint32_t hi = (8 * v + j + 1 < ch.n) ? (uint32_t)(uint16_t)__ldg(src + j + 1) : 0u;
-            t[j / 2] = lo | (hi << 16);
+      for (int u = 0; u < kXcLoads; ++u) {
+        const int i = i0 + u * blockDim.x;
+        const int f = i / nv, v = i - f * nv;
+        val[u] = make_uint4(0u, 0u, 0u, 0u);
+        if (i < n_items && f < fh) {
+          const T *src = frames + (int64_t)(h * kXcFrames + f) * stride + base + 8 * v;
+          if constexpr (VEC) {
+            val[u] = __ldg((const uint4 *)src);
+          } else {
+            uint32_t t[4];
+#pragma unroll
+            for (int j = 0; j < 8; j += 2) {
+              const uint32_t lo = (8 * v + j < ch.n) ? (uint32_t)(uint16_t)__ldg(src + j) : 0u;
+              const uint32_t hi = (8 * v + j + 1 < ch.n) ? (uint32_t)(uint16_t)__ldg(src + j + 1) : 0u;
+              t[j / 2] = lo | (hi << 16);
+            }
+            val[u] = make_uint4(t[0], t[1], t[2], t[3]);
           }
-          val = make_uint4(t[0], t[1], t[2], t[3]);
         }
       }
-      *(uint4 *)&S[f][8 * (v ^ ((f >> 3) & 7))] = val;
+#pragma unroll
+      for (int u = 0; u < kXcLoads; ++u) {
+        const int i = i0 + u * blockDim.x;
+        if (i < n_items) {
+          const int f = i / nv, v = i - f * nv;
+          *(uint4 *)&S[f][8 * (v ^ ((f >> 3) & 7))] = val[u];
+        }
+      }
     }
     __syncthreads();
     if constexpr (PLANES) {
