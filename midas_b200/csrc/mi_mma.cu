@@ -263,20 +263,27 @@ __global__ void __launch_bounds__(kMmaThreads, 1) k_mma(const __grid_constant__ 
     // ================= MMA issue (one lane)
     if (lane == 0) {
       bool ok = true;
+      // the stages of a tile arrive in order, so the lane counts them itself and reads a stage
+      // tag only at a tile's first stage (or the end marker): shared memory is busy with the
+      // producers' and the epilogue's traffic, and a read on this serial path costs every stage
+      int st = 0, n_st = 0, nk = 0, ab = 0;
       for (uint32_t g = 0;; ++g) {
         const int q = (int)(g % kMmaStages);
         if (!m_wait(&full[q], (g / kMmaStages) & 1u)) { ok = false; break; }
-        const int4 hq = *(const int4 *)&s_shdr[q];   // end, tile, step, n_k
-        const int ab = hq.y & 1;
-        if (hq.x) {
-          // no more tiles: pass the end marker to the epilogue through the next set
-          if (!m_wait(&aempty[ab], ((uint32_t)(hq.y >> 1) & 1u) ^ 1u)) { ok = false; break; }
-          s_atag[ab] = s_shdr[q];
-          m_arrive(&afull[ab]);
-          m_arrive(&afull[ab]);
-          break;
-        }
-        if (hq.z == 0) {
+        if (st == n_st) {
+          const int4 hq = *(const int4 *)&s_shdr[q];   // end, tile, step, n_k
+          ab = hq.y & 1;
+          if (hq.x) {
+            // no more tiles: pass the end marker to the epilogue through the next set
+            if (!m_wait(&aempty[ab], ((uint32_t)(hq.y >> 1) & 1u) ^ 1u)) { ok = false; break; }
+            s_atag[ab] = s_shdr[q];
+            m_arrive(&afull[ab]);
+            m_arrive(&afull[ab]);
+            break;
+          }
+          nk = hq.w;
+          n_st = (nk + kMmaStepsPerStage - 1) / kMmaStepsPerStage;
+          st = 0;
           if (!m_wait(&aempty[ab], ((uint32_t)(hq.y >> 1) & 1u) ^ 1u)) { ok = false; break; }
           m_fence_after();
           s_atag[ab] = s_shdr[q];
@@ -291,12 +298,12 @@ __global__ void __launch_bounds__(kMmaThreads, 1) k_mma(const __grid_constant__ 
         // product is split there into planes 0-2 (accumulate) and plane 3 (fresh).
 #pragma unroll
         for (int hs = 0; hs < kMmaStepsPerStage; ++hs) {
-          if (kMmaStepsPerStage * hq.z + hs >= hq.w) break;
+          if (kMmaStepsPerStage * st + hs >= nk) break;
           const uint64_t alo = m_desc(sb + 4096u * hs, 0u, 1024u, 2u);
           const uint64_t ahi = m_desc(sb + kMmaAHi + 4096u * hs, 0u, 1024u, 2u);
           const uint32_t bsa = sb + kMmaB + 256u * hs;
           const uint64_t bd = m_desc(bsa, 128u, kMmaBSbo, 0u);
-          const bool first = hq.z == 0 && hs == 0;
+          const bool first = st == 0 && hs == 0;
           m_mma(dbase, alo, bd, mma_idesc(4 * kMmaN), first ? 0u : 1u);
           if (!first) {
             m_mma(dbase + (uint32_t)kMmaN, ahi, bd, mma_idesc(4 * kMmaN), 1u);
@@ -307,7 +314,7 @@ __global__ void __launch_bounds__(kMmaThreads, 1) k_mma(const __grid_constant__ 
           }
         }
         m_commit(&empty[q]);
-        if (kMmaStepsPerStage * (hq.z + 1) >= hq.w) m_commit(&afull[ab]);
+        if (++st == n_st) m_commit(&afull[ab]);
       }
       if (!ok) atomicExch(a.err, MI_E_TIMEOUT);
     }
