@@ -25,14 +25,14 @@
 //     at (n' % 8) * 16 + (n' / 8) * kMmaBSbo + (k % 16) + (k / 16) * 128, zeroed and then
 //     scattered from the stage's terms.
 //
-// Roles (one persistent CTA per SM, 14 warps):
+// Roles (one persistent CTA per SM, 16 warps):
 //   warp 0          TMEM allocation (512 columns: two accumulator sets of 5 x 48) and, on one
 //                   lane, the MMA issue: 2 MMAs per K step, a commit that frees the stage, and
 //                   at a tile's last step a commit that hands the accumulators to the epilogue
 //   warp 1          loader: claims work items (heaviest first) and brings each tile's blob
 //                   into one of its blob slots with one bulk copy
-//   warps 2,3,12,13 producers: stage g (counted over the CTA's tiles) is built by producer
-//                   g % 4 into stage slot g % kMmaStages
+//   warps 2,3,12-15 producers: stage g (counted over the CTA's tiles) is built by producer
+//                   g % 6 into stage slot g % kMmaStages
 //   warps 4-11      epilogue: warp w reads TMEM lanes 32 (w % 4) + 0..31 (= frames) and half
 //                   of the tile's bins (8 bins x 5 accumulators at a time), recombines, puts the
 //                   cake values into a shared-memory tile holding two adjacent tiles of the item
@@ -59,9 +59,13 @@ namespace mi {
 constexpr int kMmaStages = MI_MMA_STAGES;
 constexpr int kMmaStepsPerStage = MI_MMA_STEPS;   // K steps (32 pixel slots each) per stage
 #ifndef MI_MMA_PRODUCERS
-#define MI_MMA_PRODUCERS 4
+#define MI_MMA_PRODUCERS 6
 #endif
 constexpr int kMmaProducers = MI_MMA_PRODUCERS;
+// A producer waits for its stage slot by the parity of the slot's empty barrier, which is sound
+// only while the barrier is at most one phase behind the waiter.  The producer of stage g has
+// seen stage g - producers - stages consumed; stage g - 2 stages must be: producers <= stages.
+static_assert(MI_MMA_PRODUCERS <= MI_MMA_STAGES, "more producers than stage slots aliases barrier phases");
 constexpr int kMmaEpiWarps = 8;
 constexpr int kMmaWarps = 2 + kMmaProducers + 8;   // MMA/TMEM, loader, producers, epilogue
 constexpr int kMmaThreads = kMmaWarps * 32;
@@ -444,15 +448,24 @@ __global__ void __launch_bounds__(kMmaThreads, 1) k_mma(const __grid_constant__ 
         __syncwarp();
         const int t0 = (int)sp[s0], t1 = (int)sp[s1];
         const uint32_t kbase = (uint32_t)(kMmaKStep * s0);
-        for (int t = t0 + lane; t < t1; t += 32) {
-          const uint2 tm = terms[t];
-          const uint32_t kk = (tm.y & 0xFFFFu) - kbase, n = tm.y >> 16;
-          const uint32_t off = (n & 7u) * 16u + (n >> 3) * kMmaBSbo + (kk & 15u) + (kk >> 4) * 128u;
-          uint8_t *b0 = st + kMmaB + off;
-          b0[0] = (uint8_t)(tm.x & 0xFFu);
-          b0[kMmaBPlane] = (uint8_t)((tm.x >> 8) & 0xFFu);
-          b0[2 * kMmaBPlane] = (uint8_t)((tm.x >> 16) & 0xFFu);
-          b0[3 * kMmaBPlane] = (uint8_t)(tm.x >> 24);
+        // four terms per lane loaded before any store: the terms and the planes share shared
+        // memory, so the compiler cannot hoist the next loads above the stores by itself
+        for (int t = t0 + lane; t < t1; t += 4 * 32) {
+          uint2 tmv[4];
+#pragma unroll
+          for (int u = 0; u < 4; ++u) tmv[u] = t + 32 * u < t1 ? terms[t + 32 * u] : make_uint2(0u, 0u);
+#pragma unroll
+          for (int u = 0; u < 4; ++u) {
+            if (t + 32 * u >= t1) break;
+            const uint2 tm = tmv[u];
+            const uint32_t kk = (tm.y & 0xFFFFu) - kbase, n = tm.y >> 16;
+            const uint32_t off = (n & 7u) * 16u + (n >> 3) * kMmaBSbo + (kk & 15u) + (kk >> 4) * 128u;
+            uint8_t *b0 = st + kMmaB + off;
+            b0[0] = (uint8_t)(tm.x & 0xFFu);
+            b0[kMmaBPlane] = (uint8_t)((tm.x >> 8) & 0xFFu);
+            b0[2 * kMmaBPlane] = (uint8_t)((tm.x >> 16) & 0xFFu);
+            b0[3 * kMmaBPlane] = (uint8_t)(tm.x >> 24);
+          }
         }
         if (lane == 0) {
           MmaTag h = bt;
