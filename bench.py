@@ -35,7 +35,7 @@ METRIC = "caked_frames_per_s"
 # ncu captures (profiles/): the transpose kernel k_xc plus the caking kernel of the encoding
 TRAFFIC = {"runs": {"bytes_per_step": int(0.840295e9 + 0.761555e9 + 1.830098e9 + 1.170938e9),
                     "kernels": "k_xc + k_runs"},
-           "mma": {"bytes_per_step": int(0.841459e9 + 0.767582e9 + 1.285997e9 + 0.862188e9),
+           "mma": {"bytes_per_step": int(0.839712e9 + 0.764601e9 + 1.282986e9 + 0.862686e9),
                    "kernels": "k_xc + k_mma"}}
 SCOPE = {"runs": "whole batch: k_xc + k_runs + k_lineout (k_runs 88 %)",
          "mma": "whole batch: k_xc + k_mma + k_lineout"}
