@@ -541,12 +541,15 @@ def serving_load(args, dev, plain=False, n_distinct=8):
         t0 = time.perf_counter()
         try:
             c = cfg_of(late_w, late_rate)
+            t1 = time.perf_counter()
             sid = srv.admit(c)
         except AdmissionError as e:
             late_info.update(admitted=False, reason=str(e))
             return
-        late_info.update(admitted=True, admit_s=round(time.perf_counter() - t0, 3), name=c.name,
-                         window=(t0, time.perf_counter()))
+        t2 = time.perf_counter()
+        # map_s: map on the device, dark, ring windows; plan_s: plan build, dark upload, buffers
+        late_info.update(admitted=True, admit_s=round(t2 - t0, 3), map_s=round(t1 - t0, 3),
+                         plan_s=round(t2 - t1, 3), name=c.name, window=(t0, t2))
         producer(c.name, sid, late_rate, late_frames, 99, stop_at[0])
 
     # the host loop is Python: keep the cyclic garbage collector's pauses out of the window
@@ -592,13 +595,25 @@ def serving_load(args, dev, plain=False, n_distinct=8):
         late_info["p99_ms_outside_admission"] = round(float(np.percentile(steady, 99)), 3)
         late_info["frames_during_admission"] = int(sum(lo <= r.t_arrival <= hi for v in results.values()
                                                        for r in v))
+    # where the slowest 1 % of frames waited: arrival -> submit() (the producer thread late),
+    # submit -> launch of its batch (queued in the server), launch -> result in host memory
+    allr = [r for v in results.values() for r in v]
+    tail_split = None
+    if allr:
+        cut = np.percentile([r.latency_s for r in allr], 99)
+        worst = [r for r in allr if r.latency_s >= cut]
+        tail_split = {k: round(float(np.median([f(r) for r in worst])) * 1e3, 3) for k, f in (
+            ("submit_late_ms", lambda r: r.t_submit - r.t_arrival),
+            ("queued_ms", lambda r: r.t_dispatch - r.t_submit),
+            ("in_flight_ms", lambda r: r.t_complete - r.t_dispatch))}
+        tail_split["frames"] = len(worst)
     out = {"streams": len(streams) + (1 if late_info.get("admitted") else 0), "seconds": round(T, 2),
            "offered_frames": sum(offered.values()), "completed_frames": n_done,
            "frames_per_s": round(n_done / wall, 1), "p50_ms": round(lat["p50"], 3), "p99_ms": round(lat["p99"], 3),
            "max_ms": round(lat["max"], 3), "hbm_alg_gb_s": round(backend.alg_bytes / wall / 1e9, 2),
            "launch_calls": backend.launches, "batches": srv.batches,
            "mode": "plain one-frame-per-launch" if plain else "continuous batching",
-           "late_stream": late_info, "per_stream": streams_out,
+           "late_stream": late_info, "p99_tail_median_split": tail_split, "per_stream": streams_out,
            "latency": "scheduled Poisson arrival -> lineouts and ring fits in host memory"}
     # each producer's first request carried frames[0] of its stream
     served = [(c, fr[0], results[c.name][0].lineout_aw) for c, _, fr in streams if results.get(c.name)]
