@@ -772,7 +772,7 @@ def fit_accuracy(sample):
 
 
 def e2e_rate(plan, frames, F, args, w, dev, world):
-    """Host (pinned) frames -> H2D of the referenced row band (CakePlan.upload) -> batched
+    """Host (pinned) frames -> H2D of the referenced pixels (CakePlan.upload) -> batched
     caking -> D2H lineouts, double-buffered on two streams so the copy of batch i+1 overlaps
     the caking of batch i."""
     import torch
@@ -818,11 +818,12 @@ def e2e_rate(plan, frames, F, args, w, dev, world):
     dev_ms = dist_max(a.elapsed_time(b), world)
     rate = world * args.steps * F / (dev_ms / 1e3)
     info = plan.info
-    band = (info["ref_row_hi"] - info["ref_row_lo"]) * ny
-    return {"value": round(rate, 1), "unit": UNIT, "h2d_bytes_per_step": F * band * 2,
+    up = info["upload_pixels"]
+    return {"value": round(rate, 1), "unit": UNIT, "h2d_bytes_per_step": F * up * 2,
             "d2h_bytes_per_step": 2 * F * w.n_r * 8, "wall_s": round(wall, 3),
-            "pipeline": "2 streams, double-buffered H2D of the referenced row band "
-                        f"({info['ref_row_hi'] - info['ref_row_lo']} of {nz} rows)"}
+            "pipeline": "2 streams, double-buffered H2D of the referenced columns of each 16-row "
+                        f"group of the referenced band ({info['ref_row_hi'] - info['ref_row_lo']} of {nz} "
+                        f"rows, {up} of {nz * ny} pixels per frame)"}
 
 
 # ---------------------------------------------------------------------------

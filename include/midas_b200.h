@@ -140,6 +140,8 @@ typedef struct {
   int64_t xc_pixels;       /* pixels of the pixel-major staging spans (run encoding with
                               tile_rows <= 16); 0: frames are gathered frame-major     */
   int32_t ref_row_lo, ref_row_hi; /* detector rows [lo, hi) holding referenced pixels  */
+  int64_t upload_pixels;   /* pixels of one frame mi_upload_frames copies: per group of 16
+                              rows of the band, the columns any of them references       */
 } mi_plan_info;
 
 typedef struct mi_plan mi_plan; /* opaque, immutable after creation except for the dark */
@@ -182,11 +184,14 @@ int mi_plan_status(mi_plan *plan, int *device_status);
 int mi_plan_bytes(const mi_plan *plan, size_t *bytes);
 void mi_plan_destroy(mi_plan *plan);
 
-/* Host -> device copy of F frames for this plan: only the band of detector rows that the
- * map references (ref_row_lo .. ref_row_hi-1) crosses PCIe, as one 2-D copy on `stream`;
- * the other rows of the device frames are left as they are, and no kernel reads them.
- * The reference copies every whole frame (IntegratorFitPeaksGPUStream.cu:1633-1683).
- * `host` should be page-locked for the copy to be asynchronous. */
+/* Host -> device copy of F frames for this plan: only the pixels the map can read cross
+ * PCIe.  Per group of 16 detector rows of the referenced band (ref_row_lo .. ref_row_hi-1)
+ * the columns any row of the group references (rounded out to 8 pixels), all F frames in one
+ * 3-D copy on `stream` (upload_pixels of mi_plan_info per frame); when a stride is not a
+ * whole number of rows, the band's full rows in one 2-D copy.  The other pixels of the
+ * device frames are left as they are, and no kernel reads them.  The reference copies every
+ * whole frame (IntegratorFitPeaksGPUStream.cu:1633-1683).  `host` should be page-locked for
+ * the copy to be asynchronous. */
 int mi_upload_frames(const mi_plan *plan, const void *host, int dtype, int n_frames,
                      int64_t host_stride, void *device_frames, int64_t device_stride,
                      void *stream);

@@ -57,7 +57,7 @@ class MiPlanInfo(C.Structure):
                 ("map_bytes", C.c_int64), ("device_bytes", C.c_int64), ("oob_records", C.c_int64),
                 ("tile_rows", C.c_int32), ("tile_pixels", C.c_int32),
                 ("frames_per_lane", C.c_int32), ("run_len", C.c_int32), ("xc_pixels", C.c_int64),
-                ("ref_row_lo", C.c_int32), ("ref_row_hi", C.c_int32)]
+                ("ref_row_lo", C.c_int32), ("ref_row_hi", C.c_int32), ("upload_pixels", C.c_int64)]
 
 
 class MiFitOpts(C.Structure):

@@ -215,6 +215,7 @@ constexpr int kXcFramesF = 32;     // fp32 frames of one group
 constexpr int kXcGroupsF = 2;      // fp32 groups held per launch
 constexpr int kXcRowBytes = 256;   // bytes per compact pixel
 constexpr int kXcChunk = 256;
+constexpr int kUploadRows = 16;   // detector rows per column range of mi_upload_frames
 struct XcChunk {
   int32_t z, y0, n, c0;  // detector row, first column, pixels, compact index of the first
 };
@@ -289,6 +290,10 @@ struct Plan {
   TileLimits lim{};
   int64_t staged_pixels = 0, ref_pixels = 0;
   int ref_row_lo = 0, ref_row_hi = 0;   // detector rows holding referenced pixels
+  // host -> device upload of frames (mi_upload_frames): per group of kUploadRows detector
+  // rows, the columns any of its rows references, rounded out to 8 pixels as the transpose
+  // reads them: {first row, end row, first column, end column}
+  std::vector<int4> upload_groups;
 
   // batched path
   uint8_t *d_blobs = nullptr;

@@ -886,6 +886,20 @@ static int build_plan(const mi_map_desc &m, const mi_plan_opts &o, Plan *p, Host
     p->ref_pixels = n;
     p->ref_row_lo = cmax >= 0 ? (int)(cmin / m.ny) : 0;
     p->ref_row_hi = cmax >= 0 ? (int)(cmax / m.ny) + 1 : 0;
+    if (p->panels.size() == 1) {
+      for (int z0 = p->ref_row_lo; z0 < p->ref_row_hi; z0 += kUploadRows) {
+        const int z1 = std::min(z0 + kUploadRows, p->ref_row_hi);
+        int lo = m.ny, hi = 0;
+        for (int z = z0; z < z1; ++z) {
+          const uint8_t *row = seen.data() + (int64_t)z * m.ny;
+          int a = 0, b = m.ny;
+          while (a < m.ny && !row[a]) ++a;
+          while (b > a && !row[b - 1]) --b;
+          if (b > a) { lo = std::min(lo, a); hi = std::max(hi, b); }
+        }
+        if (hi > lo) p->upload_groups.push_back(make_int4(z0, z1, lo & ~7, std::min(m.ny, (hi + 7) & ~7)));
+      }
+    }
     if ((p->encoding == MI_ENC_RUNS && runs_frames_per_group(2, p->run_g) == kXcFrames) ||
         p->encoding == MI_ENC_MMA) {
       size_t pi = 0;
@@ -1338,6 +1352,8 @@ int mi_plan_get_info(const mi_plan *p, mi_plan_info *info) {
   info->xc_pixels = p->n_xc;
   info->ref_row_lo = p->ref_row_lo;
   info->ref_row_hi = p->ref_row_hi;
+  info->upload_pixels = 0;
+  for (const int4 &g : p->upload_groups) info->upload_pixels += (int64_t)(g.y - g.x) * (g.w - g.z);
   return MI_OK;
 }
 
@@ -1453,6 +1469,22 @@ int mi_upload_frames(const mi_plan *p, const void *host, int dtype, int n_frames
   if (n_frames < 0 || host_stride < npix || device_stride < npix)
     return set_error(MI_E_ARG, "mi_upload_frames: bad frame count or stride");
   if (n_frames == 0 || p->ref_row_hi <= p->ref_row_lo) return MI_OK;
+  if (!p->upload_groups.empty() && host_stride % p->ny == 0 && device_stride % p->ny == 0) {
+    // one 3-D copy per row group: its referenced columns x its rows x the frames, so only
+    // the referenced part of each row crosses PCIe (a frame is host_stride / ny rows deep)
+    const size_t pitch = (size_t)p->ny * es;
+    for (const int4 &g : p->upload_groups) {
+      cudaMemcpy3DParms c = {};
+      c.srcPtr = make_cudaPitchedPtr(const_cast<void *>(host), pitch, pitch, (size_t)(host_stride / p->ny));
+      c.dstPtr = make_cudaPitchedPtr(device_frames, pitch, pitch, (size_t)(device_stride / p->ny));
+      c.srcPos = make_cudaPos((size_t)g.z * es, (size_t)g.x, 0);
+      c.dstPos = c.srcPos;
+      c.extent = make_cudaExtent((size_t)(g.w - g.z) * es, (size_t)(g.y - g.x), (size_t)n_frames);
+      c.kind = cudaMemcpyHostToDevice;
+      MI_CUDA(cudaMemcpy3DAsync(&c, (cudaStream_t)stream));
+    }
+    return MI_OK;
+  }
   const size_t off = (size_t)p->ref_row_lo * p->ny * es;
   const size_t width = (size_t)(p->ref_row_hi - p->ref_row_lo) * p->ny * es;
   MI_CUDA(cudaMemcpy2DAsync((uint8_t *)device_frames + off, (size_t)device_stride * es, (const uint8_t *)host + off,

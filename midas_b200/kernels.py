@@ -203,9 +203,10 @@ class CakePlan:
 
     def upload(self, host_frames: torch.Tensor, device_frames: torch.Tensor, stream=None) -> None:
         """Copy host frames (CPU tensor (F, NZ, NY), page-locked for an asynchronous copy) to
-        device frames of the same shape and dtype: only the band of detector rows the map
-        references crosses PCIe (one 2-D copy); the device frames' other rows are left as
-        they are."""
+        device frames of the same shape and dtype: only the pixels the map can read cross
+        PCIe -- per group of 16 rows of the referenced band, the columns the group references
+        (``info["upload_pixels"]`` per frame), one 3-D copy per group; the device frames'
+        other pixels are left as they are."""
         if host_frames.device.type != "cpu" or device_frames.device != self.device:
             raise ValueError("upload copies a CPU tensor into a tensor on the plan's device")
         if host_frames.dtype != device_frames.dtype or host_frames.shape[0] > device_frames.shape[0]:

@@ -249,8 +249,9 @@ def test_empty_map_and_empty_batch(cuda):
     assert ck.shape[0] == 0
 
 
-def test_upload_copies_the_referenced_row_band(cuda):
-    """CakePlan.upload moves only the detector rows the map references; caking the
+def test_upload_copies_the_referenced_columns(cuda):
+    """CakePlan.upload moves only the referenced columns of each 16-row group of the
+    referenced band (upload_pixels per frame, fewer than the band's full rows); caking the
     uploaded frames equals caking the full frames."""
     from midas_b200 import synth
     from midas_b200.mapper import build_map
@@ -263,12 +264,19 @@ def test_upload_copies_the_referenced_row_band(cuda):
     lo, hi = info["ref_row_lo"], info["ref_row_hi"]
     assert 0 < lo < hi < m.NrPixelsZ
     fr = w.frames(0, 6)
+    f32 = fr.cpu().int()   # uint16 reductions and masks are compared on the host
+    sentinel = int(f32.max()) + 1
+    assert sentinel < 65536
     host = fr.cpu().pin_memory()
-    dev = torch.full_like(fr, 7)
+    dev = torch.full_like(fr, sentinel)
     plan.upload(host, dev)
     torch.cuda.synchronize()
-    assert torch.equal(dev[:, lo:hi], fr[:, lo:hi])
-    assert bool((dev[:, :lo].int() == 7).all()) and bool((dev[:, hi:].int() == 7).all())
+    d32 = dev.cpu().int()
+    copied = d32 != sentinel
+    assert int(copied.sum()) == fr.shape[0] * info["upload_pixels"]
+    assert 0 < info["upload_pixels"] < (hi - lo) * m.NrPixelsY
+    assert torch.equal(d32[copied], f32[copied])
+    assert not bool(copied[:, :lo].any()) and not bool(copied[:, hi:].any())
     for x, y in zip(plan.integrate(dev), plan.integrate(fr)):
         assert torch.equal(x, y)
 
