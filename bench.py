@@ -513,6 +513,7 @@ def serving_load(args, dev, plain=False, n_distinct=8):
         f.result(timeout=300)
     srv.latencies.clear()
     srv.completed = srv.batches = 0
+    srv.reset_pass_stats()
     backend.alg_bytes = backend.launches = 0
     per_stream = {}
     offered = {}
@@ -607,13 +608,19 @@ def serving_load(args, dev, plain=False, n_distinct=8):
             ("queued_ms", lambda r: r.t_dispatch - r.t_submit),
             ("in_flight_ms", lambda r: r.t_complete - r.t_dispatch))}
         tail_split["frames"] = len(worst)
+    ps = srv.pass_stats()
+    ps = {k: (round(v, 3) if isinstance(v, float) else int(v)) for k, v in ps.items()}
+    ps["max_pass_at"] = round(ps["max_pass_at"] - t_start, 3)   # seconds into the run
+    if window:
+        ps["admission_s"] = [round(window[0] - t_start, 3), round(window[1] - t_start, 3)]
     out = {"streams": len(streams) + (1 if late_info.get("admitted") else 0), "seconds": round(T, 2),
            "offered_frames": sum(offered.values()), "completed_frames": n_done,
            "frames_per_s": round(n_done / wall, 1), "p50_ms": round(lat["p50"], 3), "p99_ms": round(lat["p99"], 3),
            "max_ms": round(lat["max"], 3), "hbm_alg_gb_s": round(backend.alg_bytes / wall / 1e9, 2),
            "launch_calls": backend.launches, "batches": srv.batches,
            "mode": "plain one-frame-per-launch" if plain else "continuous batching",
-           "late_stream": late_info, "p99_tail_median_split": tail_split, "per_stream": streams_out,
+           "late_stream": late_info, "p99_tail_median_split": tail_split, "scheduler": ps,
+           "per_stream": streams_out,
            "latency": "scheduled Poisson arrival -> lineouts and ring fits in host memory"}
     # each producer's first request carried frames[0] of its stream
     served = [(c, fr[0], results[c.name][0].lineout_aw) for c, _, fr in streams if results.get(c.name)]

@@ -289,7 +289,7 @@ class DeviceBackend:
         strm = st["stream"]
         fit = "d_fit" in s
         with torch.cuda.stream(strm):
-            st["plan"].upload(hf[:n], s["d_frames"], stream=strm)   # referenced rows only
+            st["plan"].upload(hf[:n], s["d_frames"], stream=strm)   # referenced pixels only
             if self.plain:
                 code = dtype_code(s["d_frames"].dtype)
                 for i in range(n):
@@ -365,6 +365,18 @@ class CakeServer:
         self.latencies: List[float] = []
         self.completed = 0
         self.batches = 0
+        self.reset_pass_stats()
+
+    def reset_pass_stats(self) -> None:
+        """Clear the scheduler-pass statistics (see pass_stats)."""
+        self._ps = {"passes": 0, "slow_passes": 0, "max_pass_ms": 0.0, "max_pass_at": 0.0,
+                    "max_ready_ms": 0.0, "max_collect_ms": 0.0, "max_dispatch_ms": 0.0}
+
+    def pass_stats(self) -> Dict[str, float]:
+        """Scheduler-thread statistics since the last reset: passes, passes over 20 ms, the
+        slowest pass (ms, and its time.perf_counter() start), and the slowest single call of
+        each kind (event query, result collection, dispatch of a batch)."""
+        return dict(self._ps)
 
     # -- admission -----------------------------------------------------------
     def admit(self, cfg: StreamConfig) -> int:
@@ -436,13 +448,22 @@ class CakeServer:
     def _pass(self) -> bool:
         """One scheduling pass: complete finished batches, dispatch pending frames."""
         did = False
+        ps, clock = self._ps, time.perf_counter
+        t_pass = clock()
         with self._lock:
             streams = list(self.streams.values())
         for s in streams:
-            while s.inflight and self.backend.ready(s.state, s.inflight[0][0]):
+            while s.inflight:
+                t = clock()
+                ok = self.backend.ready(s.state, s.inflight[0][0])
+                t1 = clock()
+                ps["max_ready_ms"] = max(ps["max_ready_ms"], (t1 - t) * 1e3)
+                if not ok:
+                    break
                 handle, reqs = s.inflight.popleft()
                 res = self.backend.collect(s.state, s.cfg, handle)
-                now = time.perf_counter()
+                now = clock()
+                ps["max_collect_ms"] = max(ps["max_collect_ms"], (now - t1) * 1e3)
                 for r, (aw, sm, fit, cake) in zip(reqs, res):
                     lat = now - r.t_arrival
                     self.latencies.append(lat)
@@ -458,9 +479,15 @@ class CakeServer:
                 for r in reqs:
                     r.t_dispatch = t_disp
                 handle = self.backend.dispatch(s.state, s.cfg, [r.frame for r in reqs])
+                ps["max_dispatch_ms"] = max(ps["max_dispatch_ms"], (clock() - t_disp) * 1e3)
                 s.inflight.append((handle, reqs))
                 self.batches += 1
                 did = True
+        dt = (clock() - t_pass) * 1e3
+        ps["passes"] += 1
+        ps["slow_passes"] += dt > 20.0
+        if dt > ps["max_pass_ms"]:
+            ps["max_pass_ms"], ps["max_pass_at"] = dt, t_pass
         return did
 
     def _loop(self):

@@ -195,6 +195,11 @@ def test_threaded_server_with_concurrent_submitters():
             np.testing.assert_array_equal(r.lineout_aw, np.arange(1, 6) * f.sum())
     lat = srv.latency_ms()
     assert lat["n"] == 120 and lat["p99"] >= lat["p50"] > 0
+    ps = srv.pass_stats()
+    assert ps["passes"] > 0 and ps["max_pass_ms"] > 0 and ps["max_dispatch_ms"] > 0
+    assert ps["max_pass_ms"] >= max(ps["max_ready_ms"], ps["max_collect_ms"], ps["max_dispatch_ms"])
+    srv.reset_pass_stats()
+    assert srv.pass_stats()["passes"] == 0
 
 
 def test_peak_rows_two_theta_and_d_spacing():
