@@ -514,6 +514,7 @@ def serving_load(args, dev, plain=False, n_distinct=8):
     srv.latencies.clear()
     srv.completed = srv.batches = 0
     srv.reset_pass_stats()
+    backend.dispatch_stats(reset=True)
     backend.alg_bytes = backend.launches = 0
     per_stream = {}
     offered = {}
@@ -613,6 +614,7 @@ def serving_load(args, dev, plain=False, n_distinct=8):
     ps["max_pass_at"] = round(ps["max_pass_at"] - t_start, 3)   # seconds into the run
     if window:
         ps["admission_s"] = [round(window[0] - t_start, 3), round(window[1] - t_start, 3)]
+    ps["dispatch_max_ms"] = {k: round(v, 3) for k, v in backend.dispatch_stats().items()}
     out = {"streams": len(streams) + (1 if late_info.get("admitted") else 0), "seconds": round(T, 2),
            "offered_frames": sum(offered.values()), "completed_frames": n_done,
            "frames_per_s": round(n_done / wall, 1), "p50_ms": round(lat["p50"], 3), "p99_ms": round(lat["p99"], 3),

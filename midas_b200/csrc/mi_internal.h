@@ -20,6 +20,8 @@ constexpr double kAreaThreshold = 1e-9;
 constexpr int kMaxFramesPerLaunch = 256;
 
 int set_error(int code, const char *fmt, ...);
+// cudaMemcpy of a large buffer in 4 MB pieces (pageable host memory on either side).
+cudaError_t copy_pieces(void *dst, const void *src, size_t bytes, cudaMemcpyKind kind);
 int cuda_error(cudaError_t e, const char *what, const char *file, int line);
 
 #define MI_CUDA(call)                                                         \

@@ -534,7 +534,7 @@ static int build_device(const MapGeom &g, const MapBins &Bh, const uint8_t *mask
   uint8_t *d_mask = nullptr;
   if (mask_h) {
     MI_DCHK(dalloc((void **)&d_mask, n_pix));
-    MI_DCHK(cudaMemcpy(d_mask, mask_h, n_pix, cudaMemcpyHostToDevice));
+    MI_DCHK(copy_pieces(d_mask, mask_h, n_pix, cudaMemcpyHostToDevice));
   }
   int32_t *d_cnt = nullptr, *d_bmask = nullptr, *d_bcnt = nullptr;
   int64_t *d_off = nullptr;
@@ -593,10 +593,10 @@ static int build_device(const MapGeom &g, const MapBins &Bh, const uint8_t *mask
   std::vector<int32_t> counts(n_bins);
   m->bin_mask.resize(n_bins);
   m->recs.resize(total);
-  MI_DCHK(cudaMemcpy(counts.data(), d_bcnt, sizeof(int32_t) * n_bins, cudaMemcpyDeviceToHost));
-  MI_DCHK(cudaMemcpy(m->bin_mask.data(), d_bmask, sizeof(int32_t) * n_bins, cudaMemcpyDeviceToHost));
+  MI_DCHK(copy_pieces(counts.data(), d_bcnt, sizeof(int32_t) * n_bins, cudaMemcpyDeviceToHost));
+  MI_DCHK(copy_pieces(m->bin_mask.data(), d_bmask, sizeof(int32_t) * n_bins, cudaMemcpyDeviceToHost));
   if (total > 0)
-    MI_DCHK(cudaMemcpy(m->recs.data(), d_recs2, sizeof(mi_map_record) * total, cudaMemcpyDeviceToHost));
+    MI_DCHK(copy_pieces(m->recs.data(), d_recs2, sizeof(mi_map_record) * total, cudaMemcpyDeviceToHost));
   finish_map(m, n_bins, counts);
   cleanup();
 #undef MI_DCHK

@@ -36,6 +36,18 @@ int cuda_error(cudaError_t e, const char *what, const char *file, int line) {
                    cudaGetErrorString(e), what, file, line);
 }
 
+cudaError_t copy_pieces(void *dst, const void *src, size_t bytes, cudaMemcpyKind kind) {
+  // A synchronous copy from or to pageable memory keeps other host threads' copy calls on
+  // the device waiting until it ends (a serving thread's frame upload waited for a plan's
+  // map upload); in pieces, such a call waits for one piece at most.
+  constexpr size_t kPiece = size_t(4) << 20;
+  for (size_t o = 0; o < bytes; o += kPiece) {
+    const cudaError_t e = cudaMemcpy((uint8_t *)dst + o, (const uint8_t *)src + o, std::min(kPiece, bytes - o), kind);
+    if (e != cudaSuccess) return e;
+  }
+  return cudaSuccess;
+}
+
 size_t dtype_size(int dtype) {
   switch (dtype) {
     case MI_DT_U8: return 1;
@@ -560,7 +572,7 @@ static int upload(T **dst, const T *src, size_t n, size_t *acct) {
   size_t bytes = std::max<size_t>(n, 1) * sizeof(T);
   MI_CUDA(cudaMalloc((void **)dst, bytes));
   *acct += bytes;
-  if (n) MI_CUDA(cudaMemcpy(*dst, src, n * sizeof(T), cudaMemcpyHostToDevice));
+  if (n) MI_CUDA(copy_pieces(*dst, src, n * sizeof(T), cudaMemcpyHostToDevice));
   return MI_OK;
 }
 
@@ -1318,14 +1330,15 @@ int mi_plan_set_dark(mi_plan *p, const float *dark) {
   int prev = 0;
   cudaGetDevice(&prev);
   MI_CUDA(cudaSetDevice(p->device));
-  if (dark) MI_CUDA(cudaMemcpy(p->d_dark, dark, n * sizeof(float), cudaMemcpyHostToDevice));
+  if (dark) MI_CUDA(copy_pieces(p->d_dark, dark, n * sizeof(float), cudaMemcpyHostToDevice));
   else MI_CUDA(cudaMemset(p->d_dark, 0, n * sizeof(float)));
   p->has_dark = dark ? 1 : 0;
   int rc = MI_OK;
   if (p->encoding == MI_ENC_MMA) {
-    // the per-bin dark terms, computed once per dark on the legacy stream
+    // the per-bin dark terms, computed once per dark on the legacy stream; waiting for that
+    // stream alone leaves other threads' streams running
     rc = launch_mma_dark(p, nullptr);
-    if (rc == MI_OK) MI_CUDA(cudaDeviceSynchronize());
+    if (rc == MI_OK) MI_CUDA(cudaStreamSynchronize(nullptr));
   }
   cudaSetDevice(prev);
   return rc;

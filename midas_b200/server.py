@@ -178,6 +178,7 @@ class DeviceBackend:
         self.device = torch.device("cuda", device)
         # host threads building an admitted stream's plan: a quarter of the cores (at most 4)
         self.build_threads = build_threads or max(1, min(4, (os.cpu_count() or 4) // 4))
+        self._dmax = dict.fromkeys(("stage_ms", "upload_ms", "integrate_ms", "fit_ms", "results_ms"), 0.0)
         self.max_batch = max_batch
         self.max_inflight = max_inflight
         self.plain = plain
@@ -278,8 +279,18 @@ class DeviceBackend:
                                      L.stream_ptr(strm)), "mi_fit_batch")
         self.launches += 1
 
+    def dispatch_stats(self, reset: bool = False) -> Dict[str, float]:
+        """Slowest step of dispatch() so far, per step (ms): the host staging copy, the
+        upload, the caking launch, the fit launch, the result copies and event record."""
+        out = dict(self._dmax)
+        if reset:
+            self._dmax = dict.fromkeys(self._dmax, 0.0)
+        return out
+
     def dispatch(self, st, cfg: StreamConfig, frames: List[np.ndarray]):
         torch = self.torch
+        clock, dm = time.perf_counter, self._dmax
+        t0 = clock()
         k = st["free"].pop()
         s = st["slots"][k]
         n = len(frames)
@@ -288,8 +299,12 @@ class DeviceBackend:
             hf[i].numpy()[...] = f.reshape(cfg.n_pixels_z, cfg.n_pixels_y)
         strm = st["stream"]
         fit = "d_fit" in s
+        t1 = clock()
+        dm["stage_ms"] = max(dm["stage_ms"], (t1 - t0) * 1e3)
         with torch.cuda.stream(strm):
             st["plan"].upload(hf[:n], s["d_frames"], stream=strm)   # referenced pixels only
+            t2 = clock()
+            dm["upload_ms"] = max(dm["upload_ms"], (t2 - t1) * 1e3)
             if self.plain:
                 code = dtype_code(s["d_frames"].dtype)
                 for i in range(n):
@@ -306,10 +321,14 @@ class DeviceBackend:
                 if cfg.want_cake:
                     out["cake"] = s["d_cake"][:n]
                 st["plan"].integrate(s["d_frames"][:n], cake=cfg.want_cake, out=out, stream=strm)
+                t3 = clock()
+                dm["integrate_ms"] = max(dm["integrate_ms"], (t3 - t2) * 1e3)
                 self.launches += 1
                 self.alg_bytes += st["map_bytes"] + n * st["frame_bytes"]
                 if fit:
                     self._fit(st, cfg, s, 0, n, strm)
+                    dm["fit_ms"] = max(dm["fit_ms"], (clock() - t3) * 1e3)
+            t4 = clock()
             if fit:
                 s["h_fit"][:n].copy_(s["d_fit"][:n], non_blocking=True)
             s["h_aw"][:n].copy_(s["d_aw"][:n], non_blocking=True)
@@ -317,6 +336,7 @@ class DeviceBackend:
             if cfg.want_cake:
                 s["h_cake"][:n].copy_(s["d_cake"][:n], non_blocking=True)
             s["event"].record(strm)
+        dm["results_ms"] = max(dm["results_ms"], (clock() - t4) * 1e3)
         return (k, n)
 
     def ready(self, st, handle) -> bool:
