@@ -498,18 +498,36 @@ static int build_host(const MapGeom &g, const MapBins &B, const uint8_t *mask, m
   return MI_OK;
 }
 
+// The whole build runs on a stream of its own with stream-ordered allocations: nothing in
+// it waits for the device as a whole (cudaFree does), so other host threads' streams, a
+// server's batches among them, keep running while a map is built.
 static int build_device(const MapGeom &g, const MapBins &Bh, const uint8_t *mask_h, int device, mi_map *m) {
   const int64_t n_pix = (int64_t)g.ny * g.nz;
   const int64_t n_bins = (int64_t)Bh.n_r * Bh.n_eta;
   MI_CUDA(cudaSetDevice(device));
+  cudaStream_t st = nullptr;
+  MI_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
   std::vector<void *> owned;
   auto dalloc = [&](void **p, size_t bytes) -> cudaError_t {
-    cudaError_t e = cudaMalloc(p, std::max<size_t>(bytes, 16));
+    cudaError_t e = cudaMallocAsync(p, std::max<size_t>(bytes, 16), st);
     if (e == cudaSuccess) owned.push_back(*p);
     return e;
   };
   auto cleanup = [&]() {
-    for (void *p : owned) cudaFree(p);
+    for (void *p : owned) cudaFreeAsync(p, st);
+    cudaStreamSynchronize(st);
+    cudaStreamDestroy(st);
+  };
+  // host <-> device copies on the build's stream, in 4 MB pieces (pageable host memory)
+  auto copy = [&](void *dst, const void *src, size_t bytes, cudaMemcpyKind kind) -> cudaError_t {
+    constexpr size_t kPiece = size_t(4) << 20;
+    for (size_t o = 0; o < bytes; o += kPiece) {
+      cudaError_t e = cudaMemcpyAsync((uint8_t *)dst + o, (const uint8_t *)src + o, std::min(kPiece, bytes - o),
+                                      kind, st);
+      if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+      if (e != cudaSuccess) return e;
+    }
+    return cudaSuccess;
   };
 #define MI_DCHK(call)                                                     \
   do {                                                                    \
@@ -522,10 +540,10 @@ static int build_device(const MapGeom &g, const MapBins &Bh, const uint8_t *mask
   } while (0)
   double *d_edges = nullptr;
   MI_DCHK(dalloc((void **)&d_edges, sizeof(double) * (2 * Bh.n_r + 2 * Bh.n_eta)));
-  MI_DCHK(cudaMemcpy(d_edges, Bh.rlo, sizeof(double) * Bh.n_r, cudaMemcpyHostToDevice));
-  MI_DCHK(cudaMemcpy(d_edges + Bh.n_r, Bh.rhi, sizeof(double) * Bh.n_r, cudaMemcpyHostToDevice));
-  MI_DCHK(cudaMemcpy(d_edges + 2 * Bh.n_r, Bh.elo, sizeof(double) * Bh.n_eta, cudaMemcpyHostToDevice));
-  MI_DCHK(cudaMemcpy(d_edges + 2 * Bh.n_r + Bh.n_eta, Bh.ehi, sizeof(double) * Bh.n_eta, cudaMemcpyHostToDevice));
+  MI_DCHK(copy(d_edges, Bh.rlo, sizeof(double) * Bh.n_r, cudaMemcpyHostToDevice));
+  MI_DCHK(copy(d_edges + Bh.n_r, Bh.rhi, sizeof(double) * Bh.n_r, cudaMemcpyHostToDevice));
+  MI_DCHK(copy(d_edges + 2 * Bh.n_r, Bh.elo, sizeof(double) * Bh.n_eta, cudaMemcpyHostToDevice));
+  MI_DCHK(copy(d_edges + 2 * Bh.n_r + Bh.n_eta, Bh.ehi, sizeof(double) * Bh.n_eta, cudaMemcpyHostToDevice));
   MapBins B = Bh;
   B.rlo = d_edges;
   B.rhi = d_edges + Bh.n_r;
@@ -534,7 +552,7 @@ static int build_device(const MapGeom &g, const MapBins &Bh, const uint8_t *mask
   uint8_t *d_mask = nullptr;
   if (mask_h) {
     MI_DCHK(dalloc((void **)&d_mask, n_pix));
-    MI_DCHK(copy_pieces(d_mask, mask_h, n_pix, cudaMemcpyHostToDevice));
+    MI_DCHK(copy(d_mask, mask_h, n_pix, cudaMemcpyHostToDevice));
   }
   int32_t *d_cnt = nullptr, *d_bmask = nullptr, *d_bcnt = nullptr;
   int64_t *d_off = nullptr;
@@ -542,24 +560,24 @@ static int build_device(const MapGeom &g, const MapBins &Bh, const uint8_t *mask
   MI_DCHK(dalloc((void **)&d_off, sizeof(int64_t) * (n_pix + 1)));
   MI_DCHK(dalloc((void **)&d_bmask, sizeof(int32_t) * n_bins));
   MI_DCHK(dalloc((void **)&d_bcnt, sizeof(int32_t) * n_bins));
-  MI_DCHK(cudaMemset(d_bmask, 0, sizeof(int32_t) * n_bins));
-  MI_DCHK(cudaMemset(d_bcnt, 0, sizeof(int32_t) * n_bins));
+  MI_DCHK(cudaMemsetAsync(d_bmask, 0, sizeof(int32_t) * n_bins, st));
+  MI_DCHK(cudaMemsetAsync(d_bcnt, 0, sizeof(int32_t) * n_bins, st));
   const int thr = 128;
   const unsigned grid = (unsigned)((n_pix + thr - 1) / thr);
-  k_map_count<<<grid, thr>>>(g, B, d_mask, d_cnt, d_bmask);
+  k_map_count<<<grid, thr, 0, st>>>(g, B, d_mask, d_cnt, d_bmask);
   MI_DCHK(cudaGetLastError());
   // exclusive scan of counts (int64)
   {
     size_t tmp_bytes = 0;
-    MI_DCHK(cub::DeviceScan::ExclusiveSum(nullptr, tmp_bytes, d_cnt, d_off, n_pix + 0));
+    MI_DCHK(cub::DeviceScan::ExclusiveSum(nullptr, tmp_bytes, d_cnt, d_off, n_pix + 0, st));
     void *tmp = nullptr;
     MI_DCHK(dalloc(&tmp, tmp_bytes));
-    MI_DCHK(cub::DeviceScan::ExclusiveSum(tmp, tmp_bytes, d_cnt, d_off, n_pix));
+    MI_DCHK(cub::DeviceScan::ExclusiveSum(tmp, tmp_bytes, d_cnt, d_off, n_pix, st));
   }
   int64_t last_off = 0;
   int32_t last_cnt = 0;
-  MI_DCHK(cudaMemcpy(&last_off, d_off + n_pix - 1, sizeof(int64_t), cudaMemcpyDeviceToHost));
-  MI_DCHK(cudaMemcpy(&last_cnt, d_cnt + n_pix - 1, sizeof(int32_t), cudaMemcpyDeviceToHost));
+  MI_DCHK(copy(&last_off, d_off + n_pix - 1, sizeof(int64_t), cudaMemcpyDeviceToHost));
+  MI_DCHK(copy(&last_cnt, d_cnt + n_pix - 1, sizeof(int32_t), cudaMemcpyDeviceToHost));
   const int64_t total = last_off + last_cnt;
   if (total > INT32_MAX) {
     cleanup();
@@ -573,30 +591,30 @@ static int build_device(const MapGeom &g, const MapBins &Bh, const uint8_t *mask
   MI_DCHK(dalloc((void **)&d_idx2, sizeof(int32_t) * total));
   MI_DCHK(dalloc((void **)&d_recs, sizeof(mi_map_record) * total));
   MI_DCHK(dalloc((void **)&d_recs2, sizeof(mi_map_record) * total));
-  k_map_fill<<<grid, thr>>>(g, B, d_mask, d_off, d_keys, d_recs, d_bcnt);
+  k_map_fill<<<grid, thr, 0, st>>>(g, B, d_mask, d_off, d_keys, d_recs, d_bcnt);
   MI_DCHK(cudaGetLastError());
   if (total > 0) {
-    k_iota<<<(unsigned)((total + 255) / 256), 256>>>(d_idx, total);
+    k_iota<<<(unsigned)((total + 255) / 256), 256, 0, st>>>(d_idx, total);
     MI_DCHK(cudaGetLastError());
     int end_bit = 1;
     while (end_bit < 31 && ((int64_t)1 << end_bit) < n_bins) ++end_bit;
     size_t tmp_bytes = 0;
     MI_DCHK(cub::DeviceRadixSort::SortPairs(nullptr, tmp_bytes, d_keys, d_keys2, d_idx, d_idx2, (int)total, 0,
-                                            end_bit));
+                                            end_bit, st));
     void *tmp = nullptr;
     MI_DCHK(dalloc(&tmp, tmp_bytes));
     MI_DCHK(cub::DeviceRadixSort::SortPairs(tmp, tmp_bytes, d_keys, d_keys2, d_idx, d_idx2, (int)total, 0,
-                                            end_bit));
-    k_gather_recs<<<(unsigned)((total + 255) / 256), 256>>>(d_idx2, d_recs, d_recs2, total);
+                                            end_bit, st));
+    k_gather_recs<<<(unsigned)((total + 255) / 256), 256, 0, st>>>(d_idx2, d_recs, d_recs2, total);
     MI_DCHK(cudaGetLastError());
   }
   std::vector<int32_t> counts(n_bins);
   m->bin_mask.resize(n_bins);
   m->recs.resize(total);
-  MI_DCHK(copy_pieces(counts.data(), d_bcnt, sizeof(int32_t) * n_bins, cudaMemcpyDeviceToHost));
-  MI_DCHK(copy_pieces(m->bin_mask.data(), d_bmask, sizeof(int32_t) * n_bins, cudaMemcpyDeviceToHost));
+  MI_DCHK(copy(counts.data(), d_bcnt, sizeof(int32_t) * n_bins, cudaMemcpyDeviceToHost));
+  MI_DCHK(copy(m->bin_mask.data(), d_bmask, sizeof(int32_t) * n_bins, cudaMemcpyDeviceToHost));
   if (total > 0)
-    MI_DCHK(copy_pieces(m->recs.data(), d_recs2, sizeof(mi_map_record) * total, cudaMemcpyDeviceToHost));
+    MI_DCHK(copy(m->recs.data(), d_recs2, sizeof(mi_map_record) * total, cudaMemcpyDeviceToHost));
   finish_map(m, n_bins, counts);
   cleanup();
 #undef MI_DCHK
