@@ -195,6 +195,12 @@ void mi_plan_destroy(mi_plan *plan);
 int mi_upload_frames(const mi_plan *plan, const void *host, int dtype, int n_frames,
                      int64_t host_stride, void *device_frames, int64_t device_stride,
                      void *stream);
+/* Host -> host copy of F frames (e.g. into the page-locked buffer mi_upload_frames then
+ * sends) of exactly the pixels mi_upload_frames copies (upload_pixels of mi_plan_info per
+ * frame); the destination's other pixels are left as they are.  No device work.  A
+ * server stages a caller's frame with it instead of copying the whole frame. */
+int mi_stage_host_frames(const mi_plan *plan, const void *src, int dtype, int n_frames,
+                         int64_t src_stride, void *dst, int64_t dst_stride);
 
 /* Cake F frames in one launch.
  *   frames:      device pointer, F frames of ny*nz pixels, frame f at frames + f*frame_stride

@@ -112,6 +112,8 @@ SIGNATURES = [
                                             C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     ("mi_upload_frames", C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_int64, C.c_void_p, C.c_int64,
                                    C.c_void_p]),
+    ("mi_stage_host_frames", C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_int64, C.c_void_p,
+                                       C.c_int64]),
     ("mi_integrate_plain", C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p,
                                      C.c_void_p, C.c_void_p]),
     ("mi_profile_batch", C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_void_p,

@@ -1472,6 +1472,27 @@ int mi_integrate_panels(mi_plan *p, const void *const *frames, const int *dtypes
   return rc;
 }
 
+int mi_stage_host_frames(const mi_plan *p, const void *src, int dtype, int n_frames, int64_t src_stride, void *dst,
+                         int64_t dst_stride) {
+  if (!p || !src || !dst) return set_error(MI_E_ARG, "mi_stage_host_frames: null argument");
+  if (p->panels.size() > 1) return set_error(MI_E_ARG, "mi_stage_host_frames: a panel plan has one band per panel");
+  const size_t es = dtype_size(dtype);
+  if (es == 0) return set_error(MI_E_ARG, "mi_stage_host_frames: unknown dtype code %d", dtype);
+  const int64_t npix = (int64_t)p->ny * p->nz;
+  if (n_frames < 0 || src_stride < npix || dst_stride < npix)
+    return set_error(MI_E_ARG, "mi_stage_host_frames: bad frame count or stride");
+  for (int f = 0; f < n_frames; ++f) {
+    const uint8_t *s = (const uint8_t *)src + (size_t)f * src_stride * es;
+    uint8_t *d = (uint8_t *)dst + (size_t)f * dst_stride * es;
+    for (const int4 &g : p->upload_groups)
+      for (int z = g.x; z < g.y; ++z) {
+        const size_t o = ((size_t)z * p->ny + g.z) * es;
+        memcpy(d + o, s + o, (size_t)(g.w - g.z) * es);
+      }
+  }
+  return MI_OK;
+}
+
 int mi_upload_frames(const mi_plan *p, const void *host, int dtype, int n_frames, int64_t host_stride,
                      void *device_frames, int64_t device_stride, void *stream) {
   if (!p || !host || !device_frames) return set_error(MI_E_ARG, "mi_upload_frames: null argument");

@@ -218,6 +218,21 @@ class CakePlan:
         L.check(L.lib().mi_upload_frames(self._h, hf.data_ptr(), dtype_code(hf.dtype), F, hs, df.data_ptr(),
                                          df.stride(0), L.stream_ptr(stream)), "mi_upload_frames")
 
+    def stage_host(self, src: np.ndarray, dst: torch.Tensor) -> None:
+        """Copy host frames ``src`` (numpy (F, NZ, NY) or (NZ, NY), C-contiguous) into the
+        host tensor ``dst`` of the same dtype (e.g. page-locked staging for ``upload``): only
+        the pixels ``upload`` sends (``info["upload_pixels"]`` per frame), in C with the
+        interpreter lock released."""
+        a = np.ascontiguousarray(src)
+        F = a.shape[0] if a.ndim == 3 else 1
+        if a.size != F * self.ny * self.nz or dst.device.type != "cpu":
+            raise ValueError("stage_host copies host frames of ny*nz pixels into a CPU tensor")
+        df = dst.reshape(dst.shape[0] if dst.dim() == 3 else 1, -1)
+        if df.shape[0] < F or df.stride(1) != 1 or str(a.dtype) != str(dst.dtype).replace("torch.", ""):
+            raise ValueError("stage_host needs a contiguous destination of the same dtype with room for the frames")
+        L.check(L.lib().mi_stage_host_frames(self._h, a.ctypes.data, dtype_code(dst.dtype), F, self.ny * self.nz,
+                                             df.data_ptr(), df.stride(0)), "mi_stage_host_frames")
+
     def _frames_host(self, frames: torch.Tensor):
         F = frames.shape[0]
         flat = frames.reshape(F, -1)

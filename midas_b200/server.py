@@ -295,8 +295,12 @@ class DeviceBackend:
         s = st["slots"][k]
         n = len(frames)
         hf = s["h_frames"]
+        hdt = hf.numpy().dtype
         for i, f in enumerate(frames):
-            hf[i].numpy()[...] = f.reshape(cfg.n_pixels_z, cfg.n_pixels_y)
+            if f.dtype == hdt and f.flags.c_contiguous:
+                st["plan"].stage_host(f, hf[i])   # the pixels the upload sends, without the GIL
+            else:
+                hf[i].numpy()[...] = f.reshape(cfg.n_pixels_z, cfg.n_pixels_y)
         strm = st["stream"]
         fit = "d_fit" in s
         t1 = clock()

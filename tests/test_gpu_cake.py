@@ -279,6 +279,17 @@ def test_upload_copies_the_referenced_columns(cuda):
     assert not bool(copied[:, :lo].any()) and not bool(copied[:, hi:].any())
     for x, y in zip(plan.integrate(dev), plan.integrate(fr)):
         assert torch.equal(x, y)
+    # host staging of exactly the pixels the upload sends, then the upload: the same caking
+    staged = torch.full((fr.shape[0],) + tuple(fr.shape[1:]), sentinel, dtype=fr.dtype).pin_memory()
+    plan.stage_host(host.numpy(), staged)
+    s32 = staged.int()
+    moved = s32 != sentinel
+    assert int(moved.sum()) == fr.shape[0] * info["upload_pixels"]
+    assert torch.equal(moved, copied) and torch.equal(s32[moved], f32[moved])
+    dev2 = torch.full_like(fr, sentinel)
+    plan.upload(staged, dev2)
+    for x, y in zip(plan.integrate(dev2), plan.integrate(fr)):
+        assert torch.equal(x, y)
 
 
 def test_graph_replay_equals_direct_calls(cuda):
