@@ -595,21 +595,52 @@ static int mma_tile_blob(const HostCSR &csr, const mi_map_desc &m, const std::ve
           pix.push_back(csr.col[t]);
         }
     }
-  // K slots in ascending compact index, slot k with k % 8 == c % 8 (the row's swizzle phase)
+  // K slots.  The tile's pixels form runs of consecutive compact indices (pieces of detector
+  // rows); a run takes consecutive slots from a slot k with k % 8 == c % 8 (each staged row
+  // carries its compact index's swizzle phase), so it is staged with one bulk copy per plane.
+  // Runs are laid out in compact order, each after the previous one, skipping slots up to
+  // its phase; a run that fits a run of such skipped slots below the end, in phase and within
+  // one K step, goes there instead.  The slots are a summation index: any assignment serves
+  // as long as the weight planes use the same one.
   std::vector<std::pair<int64_t, int32_t>> cp(pix.size());
   for (size_t u = 0; u < pix.size(); ++u) {
     const int32_t z = pix[u] / m.ny, y = pix[u] - z * m.ny;
     cp[u] = {(int64_t)row_off[z] + y - span_lo[z], pix[u]};
   }
   std::sort(cp.begin(), cp.end());
-  int prev = -1;
-  for (auto &e : cp) {
-    int k = prev + 1;
-    k += (int)(((e.first & 7) - (k & 7) + 8) & 7);
-    lut[e.second] = k;
-    prev = k;
+  static_assert(kMmaKStep == 32, "one 32-bit occupancy mask per K step");
+  std::vector<uint32_t> occ;   // per K step, one bit per slot in use
+  int top = 0;                 // slots below are laid out (used or skipped)
+  int lo_step = 0;             // steps before this one are full
+  for (size_t u = 0; u < cp.size();) {
+    size_t v = u + 1;
+    while (v < cp.size() && cp[v].first == cp[v - 1].first + 1) ++v;
+    const int len = (int)(v - u), ph = (int)(cp[u].first & 7);
+    int kpos = -1;
+    if (len <= kMmaKStep - ph) {
+      const uint32_t need = len == kMmaKStep ? 0xFFFFFFFFu : (1u << len) - 1u;
+      const int s_end = std::min((int)occ.size(), top / kMmaKStep + 1);
+      for (int st = lo_step; st < s_end && kpos < 0; ++st)
+        for (int k = ph; k + len <= kMmaKStep && st * kMmaKStep + k + len <= top; k += 8)
+          if ((occ[st] & (need << k)) == 0) {
+            kpos = st * kMmaKStep + k;
+            break;
+          }
+    }
+    if (kpos < 0) {
+      kpos = top + ((ph - (top & 7) + 8) & 7);
+      top = kpos + len;
+    }
+    for (int i = 0; i < len; ++i) {
+      const int k = kpos + i, st = k / kMmaKStep;
+      if (st >= (int)occ.size()) occ.resize(st + 1, 0u);
+      occ[st] |= 1u << (k % kMmaKStep);
+      lut[cp[u + i].second] = k;
+    }
+    while (lo_step < (int)occ.size() && occ[lo_step] == 0xFFFFFFFFu) ++lo_step;
+    u = v;
   }
-  const int n_k = std::max(1, (prev + 1 + kMmaKStep - 1) / kMmaKStep);
+  const int n_k = std::max(1, (top + kMmaKStep - 1) / kMmaKStep);
   if (n_k * kMmaKStep > 65535) {
     for (int32_t q : pix) lut[q] = -1;
     return set_error(MI_E_RANGE, "MMA tile at row %d, column %d stages more than 65535 pixel slots", r0, e0);
