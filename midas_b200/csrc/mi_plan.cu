@@ -599,9 +599,10 @@ static int mma_tile_blob(const HostCSR &csr, const mi_map_desc &m, const std::ve
   // rows); a run takes consecutive slots from a slot k with k % 8 == c % 8 (each staged row
   // carries its compact index's swizzle phase), so it is staged with one bulk copy per plane.
   // Runs are laid out in compact order, each after the previous one, skipping slots up to
-  // its phase; a run that fits a run of such skipped slots below the end, in phase and within
-  // one K step, goes there instead.  The slots are a summation index: any assignment serves
-  // as long as the weight planes use the same one.
+  // its phase.  Before that, the run fills runs of such skipped slots below the end: a piece
+  // of at least two of its pixels (or its last pixel) goes to the first skipped slot of its
+  // phase with room, each piece staged with a bulk copy of its own.  The slots are a
+  // summation index: any assignment serves as long as the weight planes use the same one.
   std::vector<std::pair<int64_t, int32_t>> cp(pix.size());
   for (size_t u = 0; u < pix.size(); ++u) {
     const int32_t z = pix[u] / m.ny, y = pix[u] - z * m.ny;
@@ -615,27 +616,41 @@ static int mma_tile_blob(const HostCSR &csr, const mi_map_desc &m, const std::ve
   for (size_t u = 0; u < cp.size();) {
     size_t v = u + 1;
     while (v < cp.size() && cp[v].first == cp[v - 1].first + 1) ++v;
-    const int len = (int)(v - u), ph = (int)(cp[u].first & 7);
-    int kpos = -1;
-    if (len <= kMmaKStep - ph) {
-      const uint32_t need = len == kMmaKStep ? 0xFFFFFFFFu : (1u << len) - 1u;
+    const int len = (int)(v - u);
+    auto put = [&](int i0, int n, int kpos) {
+      for (int i = 0; i < n; ++i) {
+        const int k = kpos + i, st = k / kMmaKStep;
+        if (st >= (int)occ.size()) occ.resize(st + 1, 0u);
+        occ[st] |= 1u << (k % kMmaKStep);
+        lut[cp[u + i0 + i].second] = k;
+      }
+    };
+    int i = 0;
+    while (i < len) {
+      // the first skipped slot of the next pixel's phase with room for a piece
+      const int ph = (int)(cp[u + i].first & 7), want = std::min(2, len - i);
       const int s_end = std::min((int)occ.size(), top / kMmaKStep + 1);
+      int kpos = -1, room = 0;
       for (int st = lo_step; st < s_end && kpos < 0; ++st)
-        for (int k = ph; k + len <= kMmaKStep && st * kMmaKStep + k + len <= top; k += 8)
-          if ((occ[st] & (need << k)) == 0) {
+        for (int k = ph; k < kMmaKStep && st * kMmaKStep + k < top; k += 8) {
+          int h = 0;
+          while (k + h < kMmaKStep && st * kMmaKStep + k + h < top && !(occ[st] >> (k + h) & 1u)) ++h;
+          if (h >= want) {
             kpos = st * kMmaKStep + k;
+            room = h;
             break;
           }
+        }
+      if (kpos < 0) break;
+      const int n = std::min(room, len - i);
+      put(i, n, kpos);
+      i += n;
     }
-    if (kpos < 0) {
-      kpos = top + ((ph - (top & 7) + 8) & 7);
-      top = kpos + len;
-    }
-    for (int i = 0; i < len; ++i) {
-      const int k = kpos + i, st = k / kMmaKStep;
-      if (st >= (int)occ.size()) occ.resize(st + 1, 0u);
-      occ[st] |= 1u << (k % kMmaKStep);
-      lut[cp[u + i].second] = k;
+    if (i < len) {
+      const int ph = (int)(cp[u + i].first & 7);
+      const int kpos = top + ((ph - (top & 7) + 8) & 7);
+      put(i, len - i, kpos);
+      top = kpos + len - i;
     }
     while (lo_step < (int)occ.size() && occ[lo_step] == 0xFFFFFFFFu) ++lo_step;
     u = v;
