@@ -18,6 +18,10 @@
 
 #include "mi_internal.h"
 
+#ifndef MI_MMA_MIN_PIECE
+#define MI_MMA_MIN_PIECE 2   // fewest pixels of a run piece placed in skipped slots
+#endif
+
 namespace mi {
 
 static thread_local char g_err[1024] = "";
@@ -628,7 +632,7 @@ static int mma_tile_blob(const HostCSR &csr, const mi_map_desc &m, const std::ve
     int i = 0;
     while (i < len) {
       // the first skipped slot of the next pixel's phase with room for a piece
-      const int ph = (int)(cp[u + i].first & 7), want = std::min(2, len - i);
+      const int ph = (int)(cp[u + i].first & 7), want = std::min(MI_MMA_MIN_PIECE, len - i);
       const int s_end = std::min((int)occ.size(), top / kMmaKStep + 1);
       int kpos = -1, room = 0;
       for (int st = lo_step; st < s_end && kpos < 0; ++st)
