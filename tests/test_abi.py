@@ -46,6 +46,10 @@ def test_null_arguments_are_rejected():
     assert b"null" in lib.mi_last_error()
     assert lib.mi_integrate_batch(None, None, 1, 1, 1, None, None, None, None) == L.MI_E_ARG
     assert lib.mi_cast_dark(None, 1, 1, 1, None, None, None) == L.MI_E_ARG
+    buf = np.zeros(16, np.uint16)
+    assert lib.mi_upload_frames(None, buf.ctypes.data, 1, 1, 16, buf.ctypes.data, 16, None) == L.MI_E_ARG
+    assert lib.mi_stage_host_frames(None, buf.ctypes.data, 1, 1, 16, buf.ctypes.data, 16) == L.MI_E_ARG
+    assert b"mi_stage_host_frames" in lib.mi_last_error()
     opts = L.MiFitOpts(9, 15, 10, 1.0, 0.0, 0.0)
     x = np.zeros(4)
     assert lib.mi_fit_batch(x.ctypes.data, x.ctypes.data, 1, 4, x.ctypes.data, 1, C.byref(opts),
