@@ -104,3 +104,26 @@ def test_plan_opts_layout_matches_header():
     """mi_plan_opts: ten int32 fields, host_threads last."""
     assert C.sizeof(L.MiPlanOpts) == 10 * 4
     assert [f for f, _ in L.MiPlanOpts._fields_][-2:] == ["variance", "host_threads"]
+
+
+def test_without_a_gpu_plans_fail_loudly():
+    """No CUDA device: the Python plan and the C ABI both refuse with an error; nothing falls
+    back to a host computation."""
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("checks the behaviour on a host without a GPU")
+    import oracle
+    from midas_b200.bin_io import from_arrays
+    from midas_b200.kernels import CakePlan
+    recs = np.zeros(1, dtype=oracle.REC_DTYPE)
+    recs["y"], recs["z"], recs["frac"], recs["areaWeight"] = 2.0, 3.0, 1.0, 1.0
+    nmap = np.zeros((12, 2), np.int32)
+    nmap[0] = (1, 0)
+    with pytest.raises(RuntimeError, match="CUDA device"):
+        CakePlan(from_arrays(recs, nmap), n_r=3, n_eta=4, n_pixels_y=8, n_pixels_z=8, device="cuda")
+    desc = L.MiMapDesc(recs.ctypes.data, 1, nmap.ctypes.data, 3, 4, 8, 8, 0.0, 0.0)
+    opts = L.MiPlanOpts(L.MODE["floor"], 1, L.SEM["py"], 0, 0, 0, L.ENC["auto"], 0, 0, 0)
+    h = C.c_void_p()
+    rc = L.lib().mi_plan_create(C.byref(desc), C.byref(opts), 0, C.byref(h))
+    assert rc != 0 and not h.value
+    assert L.lib().mi_last_error()
