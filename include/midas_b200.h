@@ -20,6 +20,8 @@
  *   mi_fit_batch         <- fitPeaks()                 FF_HEDM/src/PeakFit.c:275 (called per frame at
  *                           IntegratorFitPeaksGPUStream.cu:2630-2702) and fit_peaks()
  *                           packages/midas_integrate/midas_integrate/peakfit.py:334
+ *   mi_fit_plan_*        <- fitPeaks() job construction and joint fits, PeakFit.c:292-545, and the
+ *                           per-eta fits of FF_HEDM/src/IntegratorZarrOMP.c:1902-2030
  *   mi_map_build         <- mapper_build_map()         FF_HEDM/src/MapperCore.c:45 (DetectorMapper)
  *   mi_last_error        <- (new) the reference aborts the process on any CUDA error
  *                           (gpuAssert, IntegratorFitPeaksGPUStream.cu:299-308); this library
@@ -124,6 +126,12 @@ typedef struct {
                               32-bit fixed point (relative to the bin's largest weight), exact
                               int32 accumulation, FP64 recombination; other frame types get
                               MI_E_UNSUPPORTED                                            */
+#define MI_ENC_MMAD 4      /* tensor cores reading the frames in place (u16/u8 frames): the
+                              tiles of MI_ENC_MMA, pixels in 8-pixel row granules loaded per
+                              frame into tensor memory (one vector load per granule when rows
+                              are a multiple of 8 pixels and frames and strides 16-byte
+                              aligned), 24-bit fixed-point weights, four int32 accumulators;
+                              no pixel-major staging pass                                 */
 
 typedef struct {
   int64_t n_bins, n_r, n_eta;
@@ -218,14 +226,16 @@ int mi_integrate_batch(mi_plan *plan, const void *frames, int dtype, int n_frame
 
 /* mi_integrate_batch that allocates nothing (no counterpart in the reference).
  * For callers that cannot have device memory allocated for them once running -- a
- * detector front-end that owns the whole device memory budget, or a host recording its
- * per-batch work into a CUDA graph -- the batched kernels keep their only scratch, the
+ * detector front-end that reserves the device's whole memory budget at start-up and
+ * hands the library only its own buffers -- the batched kernels keep their only scratch, the
  * per-row lineout partial sums, in a fixed 8 MiB array inside the library (held on every
  * GPU that loads it until exit).  Same arguments and results as mi_integrate_batch;
  * frames are processed in chunks that fit the array; a plan needing more than the array
  * for one frame (n_r x 12 x 2 doubles > 1,048,576) gets MI_E_RANGE.  The first call on a
  * device looks up the array's address: make it before any stream capture.  Calls that
- * overlap on the GPU share the array and race. */
+ * overlap on the GPU share the array and race.  A device reset while the library is loaded
+ * is not supported (the looked-up address is kept).  On a tensor-core (MMA) plan the chunk
+ * is bounded by the array (11 frames per launch for 3960 x 360 bins), which costs speed. */
 int mi_integrate_batch_static(mi_plan *plan, const void *frames, int dtype, int n_frames,
                               int64_t frame_stride, float *cake, double *lineout_aw,
                               double *lineout_sm, void *stream);
@@ -312,6 +322,65 @@ typedef struct {
 int mi_fit_batch(const double *x, const double *lineouts, int n_frames, int n_x,
                  const double *peaks, int n_peaks, const mi_fit_opts *opts,
                  double *out, int32_t *iters, void *stream);
+
+/* ---- fit plans: multi-peak fit jobs ---------------------------------------
+ * A fit plan fixes the reference's fit jobs once per (x axis, peak list, options) and
+ * fits every job of every series of a batch in one launch (one warp per series;
+ * Levenberg-Marquardt with the step projected onto the reference's box bounds, FP32
+ * model and Jacobian, FP64 normal equations and Cholesky solve).
+ *   MI_FIT_KIND_PEAKS <- fitPeaks()  FF_HEDM/src/PeakFit.c:275-545 and fit_peaks()
+ *                        packages/midas_integrate/midas_integrate/peakfit.py:334: nearest
+ *                        bin per peak (kept when closer than 2 x_bin), ROI = bin +-
+ *                        half_window, overlapping ROIs merged into one joint job (at most
+ *                        MI_FIT_JOB_MAX_PEAKS peaks; a longer overlapping run starts a new
+ *                        job), area-normalised TCH pseudo-Voigt per peak + bg0 + bg1 * xn.
+ *   MI_FIT_KIND_ETA   <- the per-eta-bin fits of FF_HEDM/src/IntegratorZarrOMP.c:1902-2030
+ *                        (pf_fit_single_peak / pf_fit_doublet_peak, PeakFit.c:1174-1195, PV
+ *                        mode): series with fewer than 5 nonzero samples are skipped; each
+ *                        peak, or each pair of adjacent peaks closer than doublet_sep, is
+ *                        fit on the bins whose centre lies within half_window bins of it;
+ *                        height-normalised pseudo-Voigt, one mixing, flat background.
+ * Output rows: MI_FIT_NOUT doubles per (series, peak), in the caller's peak order:
+ *   PEAKS: [area, center, sig, gam, fwhm, eta, chi2_dof, height, bg0, bg1, two_theta_deg]
+ *   ETA:   [0, center, 0, 0, 0, 0, snr, height, bg, 0, two_theta_deg] when snr > 1 (the
+ *          reference's per-eta row), else zeros
+ * iters per (series, peak): iterations of its job, -1 peak not fit (no nearest bin within
+ * 2 x_bin, or no ROI), -2 job with no more samples than parameters, -3 series skipped. */
+#define MI_FIT_KIND_PEAKS 0
+#define MI_FIT_KIND_ETA 1
+#define MI_FIT_JOB_MAX_PEAKS 8
+
+typedef struct {
+  int32_t kind;         /* MI_FIT_KIND_*                                              */
+  int32_t half_window;  /* ROI padding in bins (FitROIPadding)                        */
+  int32_t max_iter;     /* LM iteration cap per job (<= 0: 200)                       */
+  int32_t pad;
+  double x_bin;         /* bin size of the x axis                                     */
+  double doublet_sep;   /* KIND_ETA: adjacent peaks closer than this are one job; 0 = none */
+  double px_um;         /* pixel size (um) for the 2-theta column; 0 = skip           */
+  double lsd_um;        /* sample-detector distance (um)                              */
+} mi_fit_job_opts;
+
+typedef struct mi_fit_plan mi_fit_plan;
+
+/* x: host [n_x] bin centres (ascending), peaks: host [n_peaks] positions.  device < 0 makes
+ * a host-only plan (its job table for mi_fit_plan_info / mi_fit_plan_jobs; it cannot run). */
+int mi_fit_plan_create(const double *x, int n_x, const double *peaks, int n_peaks,
+                       const mi_fit_job_opts *opts, int device, mi_fit_plan **out);
+/* jobs formed, peaks placed in a job, most peaks in one job */
+int mi_fit_plan_info(const mi_fit_plan *plan, int *n_jobs, int *n_valid, int *max_job_peaks);
+/* The job table: jobs [n_jobs][4] = {first sample, last sample, peaks, first entry}, and
+ * peak_ids [n_valid] = the caller's index of each entry (either pointer may be NULL). */
+int mi_fit_plan_jobs(const mi_fit_plan *plan, int32_t *jobs, int32_t *peak_ids);
+/* Fit n_series x n_sub series: sample i of series (f, e) at
+ * src + f*ld_series + e*ld_sub + i*ld_x elements (src_dtype MI_DT_F32 or MI_DT_F64, device
+ * memory).  Lineouts [F][n_x]: n_sub 1, ld_series n_x, ld_x 1.  Eta columns of a cake
+ * [F][n_r][n_eta]: n_sub n_eta, ld_series n_r*n_eta, ld_sub 1, ld_x n_eta.
+ * out: device [n_series*n_sub][n_peaks][MI_FIT_NOUT]; iters: device [n_series*n_sub][n_peaks]. */
+int mi_fit_plan_run(const mi_fit_plan *plan, const void *src, int src_dtype, int n_series, int n_sub,
+                    int64_t ld_series, int64_t ld_sub, int64_t ld_x, double *out, int32_t *iters,
+                    void *stream);
+void mi_fit_plan_destroy(mi_fit_plan *plan);
 
 /* ---- map building (DetectorMapper on the device) -------------------------- */
 typedef struct {

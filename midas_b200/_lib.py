@@ -27,6 +27,8 @@ SEM = {"py": 0, "gpustream": 1, "ic": 2}
 DT_U8, DT_U16, DT_U32, DT_I64, DT_F32, DT_F64, DT_I32 = 0, 1, 2, 3, 4, 5, 7
 FIT_PV, FIT_TCH = 0, 1
 FIT_NOUT = 11
+FIT_KIND_PEAKS, FIT_KIND_ETA = 0, 1
+FIT_JOB_MAX_PEAKS = 8
 
 
 class MiMapRecord(C.Structure):
@@ -47,7 +49,7 @@ class MiPlanOpts(C.Structure):
                 ("variance", C.c_int32), ("host_threads", C.c_int32)]
 
 
-ENC = {"auto": 0, "csr": 1, "runs": 2, "mma": 3}
+ENC = {"auto": 0, "csr": 1, "runs": 2, "mma": 3, "mmad": 4}
 
 
 class MiPlanInfo(C.Structure):
@@ -63,6 +65,12 @@ class MiPlanInfo(C.Structure):
 class MiFitOpts(C.Structure):
     _fields_ = [("model", C.c_int32), ("half_window", C.c_int32), ("max_iter", C.c_int32),
                 ("x_bin", C.c_double), ("px_um", C.c_double), ("lsd_um", C.c_double)]
+
+
+class MiFitJobOpts(C.Structure):
+    _fields_ = [("kind", C.c_int32), ("half_window", C.c_int32), ("max_iter", C.c_int32), ("pad", C.c_int32),
+                ("x_bin", C.c_double), ("doublet_sep", C.c_double), ("px_um", C.c_double),
+                ("lsd_um", C.c_double)]
 
 
 class MiGeometry(C.Structure):
@@ -128,6 +136,13 @@ SIGNATURES = [
                                     C.c_double, C.c_double, C.c_void_p]),
     ("mi_fit_batch", C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_int,
                                C.POINTER(MiFitOpts), C.c_void_p, C.c_void_p, C.c_void_p]),
+    ("mi_fit_plan_create", C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_int, C.POINTER(MiFitJobOpts), C.c_int,
+                                     C.POINTER(C.c_void_p)]),
+    ("mi_fit_plan_info", C.c_int, [C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int)]),
+    ("mi_fit_plan_jobs", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
+    ("mi_fit_plan_run", C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int64, C.c_int64,
+                                  C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p]),
+    ("mi_fit_plan_destroy", None, [C.c_void_p]),
     ("mi_map_build", C.c_int, [C.POINTER(MiGeometry), C.POINTER(MiBinning), C.c_int,
                                C.POINTER(C.c_void_p)]),
     ("mi_map_sizes", C.c_int, [C.c_void_p, C.POINTER(C.c_int64), C.POINTER(C.c_int64)]),

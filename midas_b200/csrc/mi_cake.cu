@@ -321,17 +321,17 @@ static int launch_fpl(Plan *p, CakeArgs &a, cudaStream_t s) {
   return set_error(MI_E_ARG, "bad frames_per_lane");
 }
 
-int launch_lineout(Plan *p, int n_frames, double *lo_aw, double *lo_sm, cudaStream_t s) {
+int launch_lineout(Plan *p, const double *partial, int n_frames, double *lo_aw, double *lo_sm, cudaStream_t s) {
   const int64_t n = (int64_t)n_frames * p->n_r;
   if (n == 0) return MI_OK;
-  k_lineout<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(p->d_partial, n_frames, p->n_r, p->n_slots, p->d_den_aw,
+  k_lineout<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(partial, n_frames, p->n_r, p->n_slots, p->d_den_aw,
                                                         p->d_cnt, lo_aw, lo_sm);
   MI_CUDA(cudaGetLastError());
   return MI_OK;
 }
 
 int launch_cake(Plan *p, const void *frames, int dtype, int n_frames, int64_t stride, float *cake,
-                double *lo_aw, double *lo_sm, cudaStream_t s) {
+                double *lo_aw, double *lo_sm, double *partial, cudaStream_t s) {
   if (p->panels.size() > 1)
     return set_error(MI_E_ARG, "a panel plan takes its frames per panel: use mi_integrate_panels");
   CakeArgs a;
@@ -343,7 +343,7 @@ int launch_cake(Plan *p, const void *frames, int dtype, int n_frames, int64_t st
   a.F = n_frames;
   a.dark = p->d_dark;
   a.cake = cake;
-  a.partial = p->d_partial;
+  a.partial = partial;
   a.n_slots = p->n_slots;
   a.n_r = p->n_r;
   a.n_eta = p->n_eta;
@@ -367,10 +367,21 @@ int launch_cake(Plan *p, const void *frames, int dtype, int n_frames, int64_t st
       rc = launch_xc(p, 0, (const uint8_t *)frames + (size_t)f0 * stride * es, dtype, nf, stride, false, s);
       if (rc == MI_OK)
         rc = launch_mma(p, nf, cake ? cake + (size_t)f0 * p->n_bins : nullptr,
-                        p->d_partial + (size_t)f0 * p->n_r * p->n_slots * 2, a.want_lo, s);
+                        partial + (size_t)f0 * p->n_r * p->n_slots * 2, a.want_lo, s);
+    }
+  } else if (p->encoding == MI_ENC_MMAD) {
+    // kernel (b) on the tensor cores, reading the frames in place: no staging pass
+    if (!(dtype == MI_DT_U16 || dtype == MI_DT_U8))
+      return set_error(MI_E_UNSUPPORTED, "direct MMA plans cake 8/16-bit frames only (dtype %d)", dtype);
+    const size_t es = dtype_size(dtype);
+    for (int f0 = 0; f0 < n_frames && rc == MI_OK; f0 += kMmaFrames) {
+      const int nf = std::min(kMmaFrames, n_frames - f0);
+      rc = launch_mmad(p, (const uint8_t *)frames + (size_t)f0 * stride * es, dtype, nf, stride,
+                       cake ? cake + (size_t)f0 * p->n_bins : nullptr, partial + (size_t)f0 * p->n_r * p->n_slots * 2,
+                       a.want_lo, s);
     }
   } else if (p->encoding == MI_ENC_RUNS) {
-    rc = launch_runs(p, frames, dtype, n_frames, stride, cake, a.want_lo, s);
+    rc = launch_runs(p, frames, dtype, n_frames, stride, cake, partial, a.want_lo, s);
   } else switch (dtype) {
     case MI_DT_U8: rc = launch_fpl<uint8_t>(p, a, s); break;
     case MI_DT_U16: rc = launch_fpl<uint16_t>(p, a, s); break;
@@ -382,7 +393,7 @@ int launch_cake(Plan *p, const void *frames, int dtype, int n_frames, int64_t st
     default: return set_error(MI_E_ARG, "unknown dtype %d", dtype);
   }
   if (rc) return rc;
-  return a.want_lo ? launch_lineout(p, n_frames, lo_aw, lo_sm, s) : MI_OK;
+  return a.want_lo ? launch_lineout(p, partial, n_frames, lo_aw, lo_sm, s) : MI_OK;
 }
 
 }  // namespace mi

@@ -278,6 +278,42 @@ __host__ __device__ inline MmaBlob mma_blob_layout(int n_k, int n_runs, int n_te
   return b;
 }
 
+// Direct MMA encoding (MI_ENC_MMAD, kernel k_mmad of mi_mmad.cu): the tiles, bins and
+// epilogue of the MMA encoding, with the frames read by the kernel straight from their
+// frame-major layout (no pixel-major buffer).  A tile's pixels are covered by 8-pixel
+// granules (8 consecutive pixels of one detector row, the first at a multiple of 8); a K
+// step of 32 slots is four granules, slot k holding pixel k % 8 of granule k / 8.  The
+// producer warps load a frame's granule with one 16-byte load per frame (u16 frames), split
+// it into its low and high byte planes and store both into tensor memory, where they are
+// the A operand of the MMAs.  Weights are 24-bit fixed point, q = round(w / w_max(bin) x
+// (2^24 - 1)), in three byte planes (the B operand, N = 144), so four int32 accumulators
+// (byte shifts 0..3) hold the exact products:
+//   cake = fac * sum_k 2^(8k) acc_k - dk,  fac = w_max / (2^24 - 1) * scale.
+// Blob of a tile (16-byte aligned arrays):
+//   MmaHdr                       32 B (n_runs: 0)
+//   double fac[48], dk[48]; float lw[48]
+//   uint32 gran[n_k][4]          granule z | y0 << 16 (kMmadEmpty: none)
+//   uint32 step_ptr[n_k + 1]     terms of K step s
+//   uint2  terms[n_terms]        {q, k | n << 16}, sorted by slot k (k / 32 = K step)
+constexpr int kMmadGran = 4;           // granules per K step
+constexpr int kMmadGranPx = 8;         // pixels per granule
+constexpr uint32_t kMmadEmpty = 0xFFFFFFFFu;
+constexpr double kMmadQMax = 16777215.0;  // 2^24 - 1
+
+struct MmadBlob {
+  uint32_t gran, step_ptr, terms, bytes;
+};
+__host__ __device__ inline MmadBlob mmad_blob_layout(int n_k, int n_terms) {
+  auto a16 = [](uint32_t x) { return (x + 15u) & ~15u; };
+  MmadBlob b;
+  uint32_t o = a16(kMmaBinsOff + kMmaBinsBytes);
+  b.gran = o;     o = a16(o + 4u * kMmadGran * (uint32_t)n_k);
+  b.step_ptr = o; o = a16(o + 4u * (uint32_t)(n_k + 1));
+  b.terms = o;    o = a16(o + 8u * (uint32_t)n_terms);
+  b.bytes = o;
+  return b;
+}
+
 struct Plan {
   int device = 0;
   int mode = 0, normalize = 1, semantics = 0;
@@ -348,10 +384,12 @@ struct Plan {
 int build_host_csr(const mi_map_desc &m, int mode, int semantics, HostCSR *out);
 
 // Launchers (mi_cake.cu, mi_plain.cu)
+// `partial` is the lineout scratch, [n_frames][n_r][n_slots][2] doubles (the plan's d_partial,
+// or a caller-provided array of that size)
 int launch_cake(Plan *p, const void *frames, int dtype, int n_frames, int64_t stride,
-                float *cake, double *lo_aw, double *lo_sm, cudaStream_t s);
-int launch_runs(Plan *p, const void *frames, int dtype, int n_frames, int64_t stride, float *cake, bool want_lo,
-                cudaStream_t s);
+                float *cake, double *lo_aw, double *lo_sm, double *partial, cudaStream_t s);
+int launch_runs(Plan *p, const void *frames, int dtype, int n_frames, int64_t stride, float *cake, double *partial,
+                bool want_lo, cudaStream_t s);
 // true when launch_runs stages this dtype through the pixel-major buffer
 bool runs_uses_xc(const Plan *p, int dtype);
 // Transpose frames [0, F) of panel `panel` into the pixel-major buffer: u16 rows when
@@ -364,8 +402,13 @@ int launch_runs_staged(Plan *p, bool as_f32, int F, float *cake, double *partial
 // the per-bin dark terms (after a dark is set)
 int launch_mma(Plan *p, int F, float *cake, double *partial, bool want_lo, cudaStream_t s);
 int launch_mma_dark(Plan *p, cudaStream_t s);
-// kernel (c): lineouts of frames [0, n_frames) from the plan's partial sums
-int launch_lineout(Plan *p, int n_frames, double *lo_aw, double *lo_sm, cudaStream_t s);
+// Direct MMA encoding (mi_mmad.cu): caking of frames [0, F) (F <= 128, u16 or u8) read in
+// place at frames + f * stride, and the per-bin dark terms
+int launch_mmad(Plan *p, const void *frames, int dtype, int F, int64_t stride, float *cake, double *partial,
+                bool want_lo, cudaStream_t s);
+int launch_mmad_dark(Plan *p, cudaStream_t s);
+// kernel (c): lineouts of frames [0, n_frames) from the partial sums in `partial`
+int launch_lineout(Plan *p, const double *partial, int n_frames, double *lo_aw, double *lo_sm, cudaStream_t s);
 int launch_plain(Plan *p, const void *frame, int dtype, double *cake, double *lo_aw,
                  double *lo_sm, cudaStream_t s);
 int launch_cast(const void *frames, int dtype, int64_t n_pixels, int n_frames,

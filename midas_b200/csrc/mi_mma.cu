@@ -49,6 +49,7 @@
 #include <algorithm>
 
 #include "mi_internal.h"
+#include "mi_tc.cuh"
 
 namespace mi {
 
@@ -79,7 +80,6 @@ constexpr int kMmaFacSlots = 6;             // ring of the tiles' per-bin factor
 constexpr uint32_t kMmaFacBytes = 1024;      // one ring entry: fac, dk, lw of 48 bins (960 B)
 constexpr int kMmaTmemCols = 512;
 constexpr int kMmaAccCols = 256;            // columns per accumulator set (5 x 48 used)
-constexpr uint32_t kMmaWaitLimit = 1u << 26;
 constexpr uint32_t kMmaOutBytes = kMmaFrames * kMmaN * 4;   // one cake tile: [128][rows][4] floats
 // The epilogue stores two adjacent tiles of an item (8 columns) with one box: 32-byte rows
 constexpr int kMmaBoxes = 8;                // cake store boxes of 4 and 8 columns x 12, 6, 3, 1 rows
@@ -130,46 +130,6 @@ __host__ __device__ inline MmaSmem mma_smem_layout(uint32_t blob_cap, int n_blob
   return L;
 }
 
-__device__ __forceinline__ uint32_t m_smem(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
-
-__device__ __forceinline__ bool m_wait(uint64_t *bar, uint32_t parity) {
-  const uint32_t a = m_smem(bar);
-  for (uint32_t it = 0; it < kMmaWaitLimit; ++it) {
-    uint32_t done;
-    asm volatile(
-        "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-        "selp.u32 %0, 1, 0, p;\n\t}"
-        : "=r"(done)
-        : "r"(a), "r"(parity)
-        : "memory");
-    if (done) return true;
-  }
-  return false;
-}
-
-__device__ __forceinline__ void m_arrive(uint64_t *bar) {
-  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(m_smem(bar)) : "memory");
-}
-__device__ __forceinline__ void m_arrive_tx(uint64_t *bar, uint32_t bytes) {
-  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(m_smem(bar)), "r"(bytes) : "memory");
-}
-__device__ __forceinline__ void m_expect_tx(uint64_t *bar, uint32_t bytes) {
-  asm volatile("mbarrier.expect_tx.relaxed.cta.shared::cta.b64 [%0], %1;" ::"r"(m_smem(bar)), "r"(bytes) : "memory");
-}
-__device__ __forceinline__ void m_copy(void *dst, const void *src, uint32_t bytes, uint64_t *bar) {
-  asm volatile(
-      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(m_smem(dst)),
-      "l"(src), "r"(bytes), "r"(m_smem(bar))
-      : "memory");
-}
-
-// shared-memory matrix descriptors (version 1): start address, leading / stride byte
-// offsets in 16-byte units, layout type in bits 61-63 (0 = no swizzle, 2 = 128B swizzle)
-__device__ __forceinline__ uint64_t m_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo, uint32_t layout) {
-  return (uint64_t)((saddr >> 4) & 0x3FFFu) | ((uint64_t)((lbo >> 4) & 0x3FFFu) << 16) |
-         ((uint64_t)((sbo >> 4) & 0x3FFFu) << 32) | (1ull << 46) | ((uint64_t)layout << 61);
-}
-
 // instruction descriptor, kind::i8: D s32, A u8 MN-major, B u8 K-major, M = 128, N = 48
 // with N = 192 (the four weight planes, 48 bins each, side by side), 144 (planes 0-2) or 48
 __host__ __device__ constexpr uint32_t mma_idesc(int n) {
@@ -183,31 +143,6 @@ __device__ __forceinline__ void m_mma(uint32_t d_tmem, uint64_t adesc, uint64_t 
       "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n" ::"r"(d_tmem),
       "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate), "r"(0u), "r"(0u), "r"(0u), "r"(0u));
 }
-__device__ __forceinline__ void m_commit(uint64_t *bar) {
-  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(m_smem(bar))
-               : "memory");
-}
-__device__ __forceinline__ void m_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
-__device__ __forceinline__ void m_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
-
-__device__ __forceinline__ void m_ld16(uint32_t taddr, uint32_t *r) {
-  asm volatile(
-      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
-      "%15}, [%16];"
-      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]), "=r"(r[8]),
-        "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
-      : "r"(taddr));
-}
-__device__ __forceinline__ void m_ld8(uint32_t taddr, uint32_t *r) {
-  asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
-               : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7])
-               : "r"(taddr));
-}
-__device__ __forceinline__ void m_ld_wait() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
-
-// non-negative int32 -> double exactly, on the FP64 pipe: 2^52 + x has x in its low bits
-__device__ __forceinline__ double m_u2d(uint32_t x) { return __hiloint2double(0x43300000, (int)x) - 4503599627370496.0; }
-
 __global__ void __launch_bounds__(kMmaThreads, 1) k_mma(const __grid_constant__ MmaArgs a) {
   extern __shared__ uint8_t smem_raw[];
   // 1024-byte aligned base: the swizzled A operand's atoms start on 1024-byte boundaries
@@ -648,25 +583,6 @@ __global__ void k_mma_dark(const TileRef *tiles, uint8_t *blobs, const int32_t *
       d += (double)tm.x * (double)dark[xc_pix[c]];
     }
   dk[n] = fac[n] * d;
-}
-
-typedef CUresult (*EncodeTiledFn)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
-                                  const cuuint64_t *, const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave,
-                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
-
-// cuTensorMapEncodeTiled through the runtime's driver entry point (no link to libcuda)
-static EncodeTiledFn encode_tiled() {
-  static EncodeTiledFn fn = nullptr;
-  static bool tried = false;
-  if (!tried) {
-    tried = true;
-    void *f = nullptr;
-    cudaDriverEntryPointQueryResult q;
-    if (cudaGetDriverEntryPointByVersion("cuTensorMapEncodeTiled", &f, 12000, cudaEnableDefault, &q) == cudaSuccess &&
-        q == cudaDriverEntryPointSuccess)
-      fn = (EncodeTiledFn)f;
-  }
-  return fn;
 }
 
 int launch_mma(Plan *p, int F, float *cake, double *partial, bool want_lo, cudaStream_t s) {

@@ -719,9 +719,84 @@ static int mma_tile_blob(const HostCSR &csr, const mi_map_desc &m, const std::ve
   return MI_OK;
 }
 
+// ---- Direct MMA encoding (see MmadBlob): the tile's pixels covered by 8-pixel row granules
+// in (row, column) order, four granules per K step; pixel (z, y) of granule g sits in slot
+// 8 g + (y - y0).  Weights in 24-bit fixed point relative to the bin's largest weight.
+static int mmad_tile_blob(const HostCSR &csr, const mi_map_desc &m, const std::vector<double> &wmax,
+                          const std::vector<double> &fac, const std::vector<float> &lw, int r0, int nr, int box_rows,
+                          int e0, int nc, std::vector<int32_t> &lut, std::vector<uint8_t> &blob, int *nnz_out,
+                          int *nu_out) {
+  std::vector<int32_t> pix;
+  for (int i = 0; i < nr; ++i)
+    for (int j = 0; j < nc; ++j) {
+      const int64_t b = (int64_t)(r0 + i) * m.n_eta + e0 + j;
+      for (int64_t t = csr.row_ptr[b]; t < csr.row_ptr[b + 1]; ++t)
+        if (lut[csr.col[t]] < 0) {
+          lut[csr.col[t]] = 0;
+          pix.push_back(csr.col[t]);
+        }
+    }
+  std::sort(pix.begin(), pix.end());
+  // granules in ascending flat order = (row, column) order
+  std::vector<uint32_t> gran;
+  int64_t last = -1;
+  for (int32_t q : pix) {
+    const int32_t z = q / m.ny, y = q - z * m.ny, y0 = y & ~(kMmadGranPx - 1);
+    const int64_t key = (int64_t)z * m.ny + y0;
+    if (key != last) {
+      gran.push_back((uint32_t)z | ((uint32_t)y0 << 16));
+      last = key;
+    }
+    lut[q] = (int32_t)((gran.size() - 1) * kMmadGranPx + (y - y0));
+  }
+  const int n_k = std::max(1, (int)((gran.size() + kMmadGran - 1) / kMmadGran));
+  if ((int64_t)n_k * kMmaKStep > 65535) {
+    for (int32_t q : pix) lut[q] = -1;
+    return set_error(MI_E_RANGE, "MMA tile at row %d, column %d stages more than 65535 pixel slots", r0, e0);
+  }
+  gran.resize((size_t)n_k * kMmadGran, kMmadEmpty);
+  std::vector<uint2> terms;
+  double bfac[kMmaN] = {0}, bdk[kMmaN] = {0};
+  float blw[kMmaN] = {0};
+  for (int i = 0; i < nr; ++i)
+    for (int j = 0; j < nc; ++j) {
+      const int64_t b = (int64_t)(r0 + i) * m.n_eta + e0 + j;
+      const uint32_t n = (uint32_t)(i * kMmaCols + j);
+      bfac[n] = fac[b];
+      blw[n] = lw[b];
+      const double wm = wmax[b];
+      for (int64_t t = csr.row_ptr[b]; t < csr.row_ptr[b + 1]; ++t) {
+        double qd = wm > 0.0 ? std::llround(csr.w[t] / wm * kMmadQMax) : 0.0;
+        qd = std::min(std::max(qd, 0.0), kMmadQMax);
+        terms.push_back(make_uint2((uint32_t)qd, (uint32_t)lut[csr.col[t]] | (n << 16)));
+      }
+    }
+  std::stable_sort(terms.begin(), terms.end(),
+                   [](const uint2 &x, const uint2 &y) { return (x.y & 0xFFFFu) < (y.y & 0xFFFFu); });
+  std::vector<uint32_t> sp(n_k + 1, 0);
+  for (const uint2 &t : terms) ++sp[(t.y & 0xFFFFu) / kMmaKStep + 1];
+  for (int s2 = 0; s2 < n_k; ++s2) sp[s2 + 1] += sp[s2];
+  for (int32_t q : pix) lut[q] = -1;
+  const MmadBlob L = mmad_blob_layout(n_k, (int)terms.size());
+  blob.assign(L.bytes, 0);
+  MmaHdr h{nr, nc, r0, e0, n_k, (int32_t)terms.size(), box_rows, 0};
+  memcpy(blob.data(), &h, sizeof(h));
+  memcpy(blob.data() + kMmaBinsOff, bfac, sizeof(bfac));
+  memcpy(blob.data() + kMmaBinsOff + sizeof(bfac), bdk, sizeof(bdk));
+  memcpy(blob.data() + kMmaBinsOff + sizeof(bfac) + sizeof(bdk), blw, sizeof(blw));
+  memcpy(blob.data() + L.gran, gran.data(), gran.size() * 4);
+  memcpy(blob.data() + L.step_ptr, sp.data(), sp.size() * 4);
+  if (!terms.empty()) memcpy(blob.data() + L.terms, terms.data(), terms.size() * 8);
+  *nnz_out = (int)terms.size();
+  *nu_out = (int)pix.size();
+  return MI_OK;
+}
+
 static int build_mma_tiles(const HostCSR &csr, const mi_map_desc &m, Plan *p, const std::vector<int32_t> &span_lo,
-                           const std::vector<int32_t> &row_off, int *n_slots_out, std::vector<TileRef> *tiles_out,
-                           std::vector<WorkItem> *items_out, std::vector<uint8_t> *blobs_out) {
+                           const std::vector<int32_t> &row_off, bool direct, int *n_slots_out,
+                           std::vector<TileRef> *tiles_out, std::vector<WorkItem> *items_out,
+                           std::vector<uint8_t> *blobs_out) {
+  const double qmax = direct ? kMmadQMax : 4294967295.0;
   const int64_t n_bins = (int64_t)m.n_r * m.n_eta, n_pix = (int64_t)m.ny * m.nz;
   std::vector<double> wmax(n_bins, 0.0), fac(n_bins, 0.0);
   std::vector<float> lw(n_bins, 0.0f);
@@ -735,7 +810,7 @@ static int build_mma_tiles(const HostCSR &csr, const mi_map_desc &m, Plan *p, co
     float sc32;
     double sc;
     bin_scale(csr, p, b, &sc32, &lw[b], &sc);
-    fac[b] = wm / 4294967295.0 * sc;
+    fac[b] = wm / qmax * sc;
   }
   // items of about 12 per band, on 8-column (32-byte) cake boundaries when there are enough
   // columns, always on kMmaCols boundaries
@@ -775,8 +850,11 @@ static int build_mma_tiles(const HostCSR &csr, const mi_map_desc &m, Plan *p, co
             for (int e0 = sl * item_cols; e0 < e_end; e0 += kMmaCols) {
               bo.blobs.emplace_back();
               int nnz = 0, nu = 0;
-              const int e = mma_tile_blob(csr, m, span_lo, row_off, wmax, fac, lw, r0, nr, h, e0,
-                                          std::min(kMmaCols, e_end - e0), lut, bo.blobs.back(), &nnz, &nu);
+              const int e =
+                  direct ? mmad_tile_blob(csr, m, wmax, fac, lw, r0, nr, h, e0, std::min(kMmaCols, e_end - e0), lut,
+                                          bo.blobs.back(), &nnz, &nu)
+                         : mma_tile_blob(csr, m, span_lo, row_off, wmax, fac, lw, r0, nr, h, e0,
+                                         std::min(kMmaCols, e_end - e0), lut, bo.blobs.back(), &nnz, &nu);
               if (e) {
 #pragma omp critical
                 err = e;
@@ -894,8 +972,11 @@ static int build_plan(const mi_map_desc &m, const mi_plan_opts &o, Plan *p, Host
   p->oob = csr.oob;
 
   // ---- encoding and limits
-  const int enc = (o.encoding == MI_ENC_CSR) ? MI_ENC_CSR : (o.encoding == MI_ENC_MMA ? MI_ENC_MMA : MI_ENC_RUNS);
-  if (o.encoding < 0 || o.encoding > 3) return set_error(MI_E_ARG, "unknown encoding %d", o.encoding);
+  const int enc = (o.encoding == MI_ENC_CSR || o.encoding == MI_ENC_MMA || o.encoding == MI_ENC_MMAD) ? o.encoding
+                                                                                                    : MI_ENC_RUNS;
+  if (o.encoding < 0 || o.encoding > 4) return set_error(MI_E_ARG, "unknown encoding %d", o.encoding);
+  if (enc == MI_ENC_MMAD && (m.ny > 65535 || m.nz > 65535))
+    return set_error(MI_E_UNSUPPORTED, "the direct MMA encoding takes detectors up to 65535 x 65535 pixels");
   p->encoding = enc;
   int fpl = o.frames_per_lane > 0 ? o.frames_per_lane : 1;
   if (fpl != 1 && fpl != 2 && fpl != 4) return set_error(MI_E_ARG, "frames_per_lane must be 1, 2 or 4");
@@ -990,8 +1071,9 @@ static int build_plan(const mi_map_desc &m, const mi_plan_opts &o, Plan *p, Host
   std::vector<TileRef> tiles;
   std::vector<WorkItem> items;
   std::vector<uint8_t> blobs;
-  if (enc == MI_ENC_MMA) {
-    if ((rc = build_mma_tiles(csr, m, p, span_lo, row_off, &n_slots, &tiles, &items, &blobs))) return rc;
+  if (enc == MI_ENC_MMA || enc == MI_ENC_MMAD) {
+    if ((rc = build_mma_tiles(csr, m, p, span_lo, row_off, enc == MI_ENC_MMAD, &n_slots, &tiles, &items, &blobs)))
+      return rc;
     n_items = (int)items.size();
   } else {
     // ---- items and tiles; shrink the tile limits until the kernel's shared memory fits
@@ -1285,7 +1367,7 @@ int mi_plan_create_panels(const mi_map_desc *maps, int n_panels, const mi_plan_o
   if (o.mode < 0 || o.mode > 2 || o.semantics < 0 || o.semantics > 2 ||
       (o.semantics == MI_SEM_IC && o.mode == MI_MODE_FLOOR))
     return set_error(MI_E_ARG, "mi_plan_create_panels: bad mode %d / semantics %d", o.mode, o.semantics);
-  if (o.encoding == MI_ENC_CSR || (o.encoding != MI_ENC_MMA && o.tile_rows > 16))
+  if (o.encoding == MI_ENC_CSR || o.encoding == MI_ENC_MMAD || (o.encoding != MI_ENC_MMA && o.tile_rows > 16))
     return set_error(MI_E_UNSUPPORTED,
                      "mi_plan_create_panels: panel plans use the run encoding with tile_rows <= 16 or the MMA encoding");
   int ndev = 0;
@@ -1384,10 +1466,10 @@ int mi_plan_set_dark(mi_plan *p, const float *dark) {
   else MI_CUDA(cudaMemset(p->d_dark, 0, n * sizeof(float)));
   p->has_dark = dark ? 1 : 0;
   int rc = MI_OK;
-  if (p->encoding == MI_ENC_MMA) {
+  if (p->encoding == MI_ENC_MMA || p->encoding == MI_ENC_MMAD) {
     // the per-bin dark terms, computed once per dark on the legacy stream; waiting for that
     // stream alone leaves other threads' streams running
-    rc = launch_mma_dark(p, nullptr);
+    rc = p->encoding == MI_ENC_MMA ? launch_mma_dark(p, nullptr) : launch_mmad_dark(p, nullptr);
     if (rc == MI_OK) MI_CUDA(cudaStreamSynchronize(nullptr));
   }
   cudaSetDevice(prev);
@@ -1467,7 +1549,7 @@ int mi_integrate_batch(mi_plan *p, const void *frames, int dtype, int n_frames, 
     rc = launch_cake(p, (const uint8_t *)frames + (size_t)f0 * stride * es, dtype, nf, stride,
                      cake ? cake + (size_t)f0 * p->n_bins : nullptr,
                      lo_aw ? lo_aw + (size_t)f0 * p->n_r : nullptr,
-                     lo_sm ? lo_sm + (size_t)f0 * p->n_r : nullptr, (cudaStream_t)stream);
+                     lo_sm ? lo_sm + (size_t)f0 * p->n_r : nullptr, p->d_partial, (cudaStream_t)stream);
   }
   if (prev != p->device) cudaSetDevice(prev);
   return rc;
@@ -1515,7 +1597,7 @@ int mi_integrate_panels(mi_plan *p, const void *const *frames, const int *dtypes
                                 p->d_partial + (size_t)f0 * p->n_r * p->n_slots * 2, want_lo, s);
     }
     if (rc == MI_OK && want_lo)
-      rc = launch_lineout(p, ng, lo_aw ? lo_aw + (size_t)g0 * p->n_r : nullptr,
+      rc = launch_lineout(p, p->d_partial, ng, lo_aw ? lo_aw + (size_t)g0 * p->n_r : nullptr,
                           lo_sm ? lo_sm + (size_t)g0 * p->n_r : nullptr, s);
   }
   if (prev != p->device) cudaSetDevice(prev);

@@ -558,15 +558,16 @@ int launch_runs_staged(Plan *p, bool as_f32, int F, float *cake, double *partial
   return as_f32 ? launch_runs_xc<float>(p, a, s) : launch_runs_xc<uint16_t>(p, a, s);
 }
 
-int launch_runs(Plan *p, const void *frames, int dtype, int n_frames, int64_t stride, float *cake, bool want_lo,
-                cudaStream_t s) {
+int launch_runs(Plan *p, const void *frames, int dtype, int n_frames, int64_t stride, float *cake, double *partial,
+                bool want_lo, cudaStream_t s) {
   RunArgs a = run_args(p, cake, want_lo);
+  a.partial = partial;
   a.frames = frames;
   a.stride = stride;
   a.F = n_frames;
   if (runs_uses_xc(p, dtype)) {
     // kernel (a) transposes a chunk of frames into the pixel-major buffer, kernel (b) stages
-    // from it; the partial sums of frame f live at row f of the plan's scratch
+    // from it; the partial sums of frame f live at row f of the scratch
     const bool as_f32 = !(dtype == MI_DT_U16 || dtype == MI_DT_U8);
     const size_t es = dtype_size(dtype);
     const int chunk = as_f32 ? kXcFramesF * kXcGroupsF : kXcFrames * kXcGroups;
@@ -575,7 +576,7 @@ int launch_runs(Plan *p, const void *frames, int dtype, int n_frames, int64_t st
       int rc = launch_xc(p, 0, (const uint8_t *)frames + (size_t)f0 * stride * es, dtype, nf, stride, as_f32, s);
       if (rc) return rc;
       rc = launch_runs_staged(p, as_f32, nf, cake ? cake + (size_t)f0 * p->n_bins : nullptr,
-                              p->d_partial + (size_t)f0 * p->n_r * p->n_slots * 2, want_lo, s);
+                              partial + (size_t)f0 * p->n_r * p->n_slots * 2, want_lo, s);
       if (rc) return rc;
     }
     return MI_OK;

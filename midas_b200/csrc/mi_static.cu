@@ -2,9 +2,7 @@
 //
 // Some callers cannot have device memory allocated on their behalf once they are
 // running: a detector front-end that reserves the device's whole memory budget at
-// start-up and hands the library only its own buffers, or a host that records its
-// per-batch work while a stream is being captured into a CUDA graph (cudaMalloc is
-// not allowed there).  This entry point runs the same kernels as mi_integrate_batch
+// start-up and hands the library only its own buffers.  This entry point runs the same kernels as mi_integrate_batch
 // (batched caking + lineout reduction) but keeps their only scratch -- the per-row
 // lineout partial sums -- in a fixed array compiled into the library, so a call
 // touches nothing but the plan, the caller's frames and outputs, and that array.
@@ -14,9 +12,16 @@
 // batches are processed in chunks that fit, and a plan whose single frame does not
 // fit is rejected with MI_E_RANGE.  The first call on a device looks up the array's
 // device address (cudaGetSymbolAddress) -- make that first call before any stream
-// capture.  All calls share the array: calls that overlap on the GPU (other streams,
-// other threads) race on it.  Nothing in it must start at zero: every launch writes
-// every partial it later reads.
+// capture.  The address is kept for the life of the process, so a device reset
+// (cudaDeviceReset, or a reset of the primary context) while the library is loaded is not
+// supported: the module reloads and the kept address goes stale.  All calls share the
+// array: calls that overlap on the GPU (other streams, other threads) race on it.  Nothing
+// in it must start at zero: every launch writes every partial it later reads.  A call
+// copies nothing of the plan; it passes the array to the same launchers as
+// mi_integrate_batch.  On a tensor-core (MMA) plan the chunk is at most what the array
+// holds (a 3960 x 360 bin plan with 12 partial slots per row: 11 frames per launch), and
+// that encoding's cost is per pass over the map, so such a plan runs slower per frame here
+// than through mi_integrate_batch.
 #include <mutex>
 
 #include "mi_internal.h"
@@ -72,15 +77,14 @@ extern "C" int mi_integrate_batch_static(mi_plan *p, const void *frames, int dty
   double *scratch = nullptr;
   int rc = static_scratch(p->device, &scratch);
   if (rc == MI_OK) {
-    mi::Plan view = *p;                 // same plan, lineout partials redirected to the fixed array
-    view.d_partial = scratch;
+    // the same launches as mi_integrate_batch, with the lineout partials in the fixed array
     const int chunk = (int)std::min<size_t>((size_t)kMaxFramesPerLaunch, kStaticScratchDoubles / per_frame);
     const size_t es = dtype_size(dtype);
     for (int f0 = 0; f0 < n_frames && rc == MI_OK; f0 += chunk) {
       const int nf = std::min(chunk, n_frames - f0);
-      rc = launch_cake(&view, (const uint8_t *)frames + (size_t)f0 * stride * es, dtype, nf, stride,
+      rc = launch_cake(p, (const uint8_t *)frames + (size_t)f0 * stride * es, dtype, nf, stride,
                        cake ? cake + (size_t)f0 * p->n_bins : nullptr, lo_aw ? lo_aw + (size_t)f0 * p->n_r : nullptr,
-                       lo_sm ? lo_sm + (size_t)f0 * p->n_r : nullptr, (cudaStream_t)stream);
+                       lo_sm ? lo_sm + (size_t)f0 * p->n_r : nullptr, scratch, (cudaStream_t)stream);
     }
   }
   if (prev != p->device) cudaSetDevice(prev);

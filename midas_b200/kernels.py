@@ -63,7 +63,8 @@ class CakePlan:
         tile_rows, tile_pixels, frames_per_lane: tiling knobs (0 = default).
         encoding: 'auto' (= 'runs') | 'runs' (register-blocked radial runs) | 'csr'
             (per-bin term lists) | 'mma' (tensor cores, exact int8 products; 8/16-bit
-            frames only); run_len: rows per run record (2, 4, 8; 0 = auto).
+            frames only) | 'mmad' (tensor cores reading the frames in place, 8/16-bit
+            frames); run_len: rows per run record (2, 4, 8; 0 = auto).
         variance: a variance plan (integrate_with_variance, kernels.py:474-536): frames
             are per-pixel variance maps, caked with the squared coalesced weights and
             divided by the squared bin area; its lineouts are the propagated variances of
@@ -95,7 +96,7 @@ class CakePlan:
                            nmap.ctypes.data, self.n_r, self.n_eta, self.ny, self.nz,
                            self.bc_y, self.bc_z)
         if encoding not in L.ENC:
-            raise ValueError(f"unknown encoding {encoding!r}; expected 'auto' | 'csr' | 'runs' | 'mma'")
+            raise ValueError(f"unknown encoding {encoding!r}; expected 'auto' | 'csr' | 'runs' | 'mma' | 'mmad'")
         opts = L.MiPlanOpts(L.MODE[mode], int(self.normalize), L.SEM[semantics],
                             int(tile_rows), int(tile_pixels), int(frames_per_lane),
                             L.ENC[encoding], int(run_len), int(self.variance), int(host_threads))

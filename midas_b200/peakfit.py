@@ -55,15 +55,117 @@ def fit_batch(x: torch.Tensor, lineouts: torch.Tensor, peaks: torch.Tensor, *, m
     return FitResult(out, it)
 
 
+class FitPlan:
+    """The reference's fit jobs for one (x axis, peak list, options), fit on the device.
+
+    kind "peaks": fitPeaks / fit_peaks (FF_HEDM/src/PeakFit.c:275-545;
+    packages/midas_integrate/midas_integrate/peakfit.py:334) -- nearest bin per peak, ROI
+    +- half_window bins, overlapping ROIs merged into one joint TCH fit.
+    kind "eta": the per-eta-bin fits of FF_HEDM/src/IntegratorZarrOMP.c:1902-2030 -- height-
+    normalised pseudo-Voigt singlets, doublets for adjacent peaks closer than doublet_sep,
+    on every eta column of a cake with at least 5 nonzero samples.
+    device="cpu" builds the job table only (``jobs``, ``info``); it cannot run.
+    """
+
+    def __init__(self, x, peaks, *, kind: str = "peaks", half_window: int = 20, x_bin: float = 1.0,
+                 max_iter: int = 200, doublet_sep: float = 0.0, px_um: float = 0.0, lsd_um: float = 0.0,
+                 device="cuda"):
+        self.device = torch.device(device)
+        xs = np.ascontiguousarray(np.asarray(x, np.float64))
+        pk = np.ascontiguousarray(np.asarray(peaks, np.float64).reshape(-1))
+        self.n_x, self.n_peaks = xs.size, pk.size
+        k = {"peaks": L.FIT_KIND_PEAKS, "eta": L.FIT_KIND_ETA}[kind]
+        self.kind = kind
+        opts = L.MiFitJobOpts(k, int(half_window), int(max_iter), 0, float(x_bin), float(doublet_sep),
+                              float(px_um), float(lsd_um))
+        h = C.c_void_p()
+        dev = -1 if self.device.type == "cpu" else (self.device.index or 0)
+        L.check(L.lib().mi_fit_plan_create(xs.ctypes.data, xs.size, pk.ctypes.data, pk.size, C.byref(opts),
+                                           dev, C.byref(h)), "mi_fit_plan_create")
+        self._h = h
+
+    def jobs(self):
+        """The job table: (jobs [n_jobs, 4] = first sample, last sample, peaks, first entry;
+        peak ids [n_valid] = the caller's index of each entry)."""
+        inf = self.info()
+        jb = np.zeros((inf["n_jobs"], 4), np.int32)
+        ids = np.zeros(inf["n_valid"], np.int32)
+        L.check(L.lib().mi_fit_plan_jobs(self._h, jb.ctypes.data, ids.ctypes.data), "mi_fit_plan_jobs")
+        return jb, ids
+
+    def info(self):
+        nj, nv, mx = C.c_int(), C.c_int(), C.c_int()
+        L.check(L.lib().mi_fit_plan_info(self._h, C.byref(nj), C.byref(nv), C.byref(mx)), "mi_fit_plan_info")
+        return {"n_jobs": nj.value, "n_valid": nv.value, "max_job_peaks": mx.value}
+
+    def run(self, series: torch.Tensor, *, n_sub: int = 1, ld_series=None, ld_sub: int = 0, ld_x: int = 1,
+            stream=None) -> FitResult:
+        """Fit the series of a device tensor (float32 or float64).  A [F, n_x] tensor is F
+        lineouts; see ``fit_cake_eta`` for the eta columns of a cake."""
+        if series.device.type != "cuda":
+            raise RuntimeError("FitPlan.run takes a CUDA tensor")
+        if series.dtype not in (torch.float32, torch.float64):
+            series = series.to(torch.float64)
+        series = series.contiguous()
+        n_series = series.shape[0] if series.dim() > 1 else 1
+        if ld_series is None:
+            ld_series = series.stride(0) if series.dim() > 1 else 0
+        dt = L.DT_F64 if series.dtype == torch.float64 else L.DT_F32
+        tot = n_series * n_sub
+        out = torch.zeros((tot, self.n_peaks, L.FIT_NOUT), dtype=torch.float64, device=series.device)
+        it = torch.zeros((tot, self.n_peaks), dtype=torch.int32, device=series.device)
+        with torch.cuda.device(series.device):
+            L.check(L.lib().mi_fit_plan_run(self._h, series.data_ptr(), dt, n_series, n_sub, int(ld_series),
+                                            int(ld_sub), int(ld_x), out.data_ptr(), it.data_ptr(),
+                                            L.stream_ptr(stream)), "mi_fit_plan_run")
+        return FitResult(out, it)
+
+    def fit_cake_eta(self, cake: torch.Tensor, stream=None) -> FitResult:
+        """Per-eta fits of a [F, n_r, n_eta] cake: params [F * n_eta, n_peaks, 11] (series
+        f * n_eta + e)."""
+        F, n_r, n_eta = cake.shape
+        if n_r != self.n_x:
+            raise ValueError("cake rows and the plan's x axis disagree")
+        cake = cake.contiguous()
+        return self.run(cake.reshape(F, -1), n_sub=n_eta, ld_series=n_r * n_eta, ld_sub=1, ld_x=n_eta,
+                        stream=stream)
+
+    def close(self):
+        if getattr(self, "_h", None):
+            L.lib().mi_fit_plan_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
 def fit_peaks(x, intensity, peak_locations, *, x_bin_size: float, fit_roi_padding: int = 20,
-              model="tch", device="cuda") -> np.ndarray:
-    """Single-lineout API (peakfit.py:fit_peaks): returns (n_peaks, 7) rows
-    [area, center, sig, gam, FWHM, eta, chi2/dof]; rejected peaks are zero rows."""
-    xt = torch.as_tensor(np.asarray(x, np.float64), device=device)
-    yt = torch.as_tensor(np.asarray(intensity, np.float64), device=device).reshape(1, -1)
-    pt = torch.as_tensor(np.asarray(peak_locations, np.float64), device=device)
-    r = fit_batch(xt, yt, pt, model=model, half_window=fit_roi_padding, x_bin=x_bin_size)
-    return r.params[0, :, :7].cpu().numpy()
+              device="cuda") -> np.ndarray:
+    """Single-lineout API of peakfit.py:fit_peaks (the reference's fitPeaks): rows
+    [area, center, sig, gam, FWHM, eta, chi2/dof] of the peaks within 2 bins of the grid, in
+    ascending bin order (overlapping windows fit jointly); (n_peaks, 7) zeros when none is."""
+    xs = np.asarray(x, np.float64)
+    locs = np.asarray(peak_locations, np.float64).reshape(-1)
+    if locs.size == 0 or xs.size == 0:
+        return np.zeros((0, 7), np.float64)
+    plan = FitPlan(xs, locs, kind="peaks", half_window=fit_roi_padding, x_bin=x_bin_size, device=device)
+    try:
+        y = torch.as_tensor(np.asarray(intensity, np.float64), device=device).reshape(1, -1)
+        r = plan.run(y)
+        p, it = r.params[0].cpu().numpy(), r.iters[0].cpu().numpy()
+    finally:
+        plan.close()
+    idx = np.array([int(np.argmin(np.abs(xs - c))) for c in locs])
+    valid = np.abs(xs[idx] - locs) < 2.0 * x_bin_size
+    if not valid.any():
+        return np.zeros((locs.size, 7), np.float64)
+    order = [k for k in np.argsort(idx, kind="stable") if valid[k]]
+    rows = p[order, :7].copy()
+    rows[it[order] < 0] = 0.0
+    return rows
 
 
 PEAK_ROW_DTYPE = np.dtype([("frame_idx", "<i4"), ("eta_idx", "<i4"), ("peak_nr", "<i4"), ("eta_deg", "<f8"),

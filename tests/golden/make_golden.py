@@ -1,9 +1,8 @@
 """Generate the golden fixtures in tests/golden/ from the reference implementation.
 
-Run in a container that has the MIDAS sources (read-only) at $MIDAS_REF
-(default /root/reference):
+Run where the MIDAS sources are checked out (read-only), naming the checkout:
 
-    python tests/golden/make_golden.py
+    MIDAS_REF=<MIDAS checkout> python tests/golden/make_golden.py
 
 It imports the reference's own Python package (packages/midas_integrate) --
 without executing its __init__, which pulls in optional I/O dependencies -- and
@@ -41,7 +40,9 @@ import numpy as np
 
 OUT = Path(__file__).resolve().parent
 REPO = OUT.parents[1]
-REF = Path(os.environ.get("MIDAS_REF", "/root/reference"))
+if "MIDAS_REF" not in os.environ:
+    sys.exit("make_golden.py: set MIDAS_REF to the MIDAS checkout whose outputs the fixtures record")
+REF = Path(os.environ["MIDAS_REF"])
 PKG = REF / "packages" / "midas_integrate" / "midas_integrate"
 
 

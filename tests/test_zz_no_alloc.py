@@ -1,7 +1,8 @@
 """mi_integrate_batch_static: the batched integration for callers that cannot have device
-memory allocated for them (a front-end owning the whole device memory budget, or a host
-recording its work into a CUDA graph).  It keeps its lineout scratch in a fixed array in
-the library; its results must equal those of mi_integrate_batch, call after call.
+memory allocated for them once running (a detector front-end that reserves the device's
+whole memory budget at start-up and hands the library only its own buffers).  It keeps its
+lineout scratch in a fixed array in the library; its results must equal those of
+mi_integrate_batch, call after call.
 
 Collected last (file name) so a run that stops at the first failure has run everything
 else first; it also passes alone in a fresh process."""
@@ -13,8 +14,10 @@ import torch
 
 from conftest import load_mapper_case, rel_err
 from midas_b200 import _lib as L
+from midas_b200 import synth
 from midas_b200.bin_io import from_arrays
 from midas_b200.kernels import CakePlan
+from midas_b200.mapper import build_map
 
 pytestmark = pytest.mark.gpu
 
@@ -46,6 +49,31 @@ def test_static_scratch_entry_point_matches_batched(cuda, enc):
         assert rel_err(aw.cpu().numpy(), ref_aw.cpu().numpy())[0] <= 1e-6
         assert rel_err(sm.cpu().numpy(), ref_sm.cpu().numpy())[0] <= 1e-6
     assert plan.status() == 0
+
+
+def test_static_scratch_tensor_core_plan_in_chunks(cuda):
+    """The tensor-core (MMA) encoding through the fixed array: 990 x 360 bins need
+    990 x 12 x 2 doubles of scratch per frame, so 100 frames run as chunks of 44, 44 and 12
+    launches, against one 100-frame launch of mi_integrate_batch."""
+    w = synth.scaled(synth.sweep_2880(), 4)
+    pm, _ = build_map(w.mapper, device=0)
+    plan = CakePlan(pm, n_r=w.n_r, n_eta=w.n_eta, n_pixels_y=w.mapper.NrPixelsY, n_pixels_z=w.mapper.NrPixelsZ,
+                    mode=w.mode, bc_y=w.mapper.BC_y, bc_z=w.mapper.BC_z, device=cuda, encoding="mma")
+    assert (1 << 20) // (w.n_r * 12 * 2) < 100
+    plan.set_dark(w.dark(device=cuda).cpu().numpy())
+    frames = w.frames(0, 100, device=cuda)
+    ref_ck, ref_aw, ref_sm = plan.integrate(frames)
+    for call in range(2):
+        ck = torch.full_like(ref_ck, float("nan"))
+        aw = torch.full_like(ref_aw, float("nan"))
+        sm = torch.full_like(ref_sm, float("nan"))
+        L.check(_static_call(plan, frames, ck, aw, sm), "mi_integrate_batch_static")
+        torch.cuda.synchronize()
+        assert rel_err(ck.cpu().numpy(), ref_ck.cpu().numpy())[0] <= 1e-6
+        assert rel_err(aw.cpu().numpy(), ref_aw.cpu().numpy())[0] <= 1e-6
+        assert rel_err(sm.cpu().numpy(), ref_sm.cpu().numpy())[0] <= 1e-6
+    assert plan.status() == 0
+    plan.close()
 
 
 def test_static_scratch_rejects_plans_beyond_the_array(cuda):
