@@ -67,6 +67,15 @@ extern "C" {
                                 then over; normaliser = sum of ALL areaWeight (<= 1e-9 ->
                                 0). It has no floor mode: MI_MODE_FLOOR is rejected, and
                                 mi_integrate_plain does not take this semantics.          */
+#define MI_SEM_OMP 3         /* IntegratorZarrOMP.c:1709-1778 (the OpenMP integrator): the
+                                sums of MI_SEM_IC; a nonzero sum is divided by the sum of
+                                ALL areaWeight of the bin (no validity threshold; a bin with
+                                a nonzero sum and zero area gives 0 here, +-inf there); bins
+                                flagged by mi_plan_set_bin_mask are NaN; lineout_sm is the
+                                mean of the row's nonzero, non-NaN bins (:1829-1843) and
+                                lineout_aw the area-weighted mean over its valid, non-NaN
+                                bins, both computed from the cake, which must be requested
+                                with them.  No floor mode; single-detector plans only.    */
 
 /* ---- frame dtype codes: the socket protocol's codes (MI/image.py:24-30) -- */
 #define MI_DT_U8 0
@@ -185,6 +194,11 @@ int mi_plan_set_dark_panels(mi_plan *plan, const float *const *darks_host);
 int mi_integrate_panels(mi_plan *plan, const void *const *frames, const int *dtypes,
                         const int64_t *strides, int n_frames, float *cake, double *lineout_aw,
                         double *lineout_sm, void *stream);
+/* Per-bin mask of a MI_SEM_OMP plan (host, n_bins bytes, nonzero = the bin holds a masked
+ * pixel, DetectorMapper's bin mask): those bins of every cake are NaN, as the OpenMP
+ * integrator writes them (IntegratorZarrOMP.c:1766-1767).  NULL clears it. */
+int mi_plan_set_bin_mask(mi_plan *plan, const uint8_t *bin_mask);
+
 /* Device-side status of the plan's launches so far: the plan's error word (MI_E_TIMEOUT
  * when a bounded in-kernel wait expired, else 0), which is then cleared.  Synchronises
  * the plan's device. */

@@ -23,7 +23,7 @@ MI_E_UNSUPPORTED = -6
 MI_E_RANGE = -7
 
 MODE = {"floor": 0, "bilinear": 1, "gradient": 2}
-SEM = {"py": 0, "gpustream": 1, "ic": 2}
+SEM = {"py": 0, "gpustream": 1, "ic": 2, "omp": 3}
 DT_U8, DT_U16, DT_U32, DT_I64, DT_F32, DT_F64, DT_I32 = 0, 1, 2, 3, 4, 5, 7
 FIT_PV, FIT_TCH = 0, 1
 FIT_NOUT = 11
@@ -111,6 +111,7 @@ SIGNATURES = [
                                       C.POINTER(C.c_int64), C.c_int, C.c_void_p, C.c_void_p, C.c_void_p,
                                       C.c_void_p]),
     ("mi_plan_get_info", C.c_int, [C.c_void_p, C.POINTER(MiPlanInfo)]),
+    ("mi_plan_set_bin_mask", C.c_int, [C.c_void_p, C.c_void_p]),
     ("mi_plan_bytes", C.c_int, [C.c_void_p, C.POINTER(C.c_size_t)]),
     ("mi_plan_status", C.c_int, [C.c_void_p, C.POINTER(C.c_int)]),
     ("mi_plan_destroy", None, [C.c_void_p]),

@@ -350,6 +350,13 @@ int launch_cake(Plan *p, const void *frames, int dtype, int n_frames, int64_t st
   a.n_bins = p->n_bins;
   a.want_cake = cake != nullptr;
   a.want_lo = (lo_aw != nullptr) || (lo_sm != nullptr);
+  // MI_SEM_OMP: masked bins are NaN and the lineouts come from the cake (mean of nonzero,
+  // non-NaN bins), not from the kernels' partial sums
+  const bool omp = p->semantics == MI_SEM_OMP;
+  const bool want_lo_omp = omp && a.want_lo;
+  if (want_lo_omp && !cake)
+    return set_error(MI_E_ARG, "OpenMP-integrator semantics computes the lineouts from the cake: pass a cake");
+  if (omp) a.want_lo = false;
   a.rows_max = p->lim.rows;
   a.blob_cap = (p->max_blob + 15u) & ~15u;
   a.u_cap = std::max(p->max_u, 1);
@@ -393,6 +400,11 @@ int launch_cake(Plan *p, const void *frames, int dtype, int n_frames, int64_t st
     default: return set_error(MI_E_ARG, "unknown dtype %d", dtype);
   }
   if (rc) return rc;
+  if (omp) {
+    rc = launch_nan_bins(p, cake, n_frames, s);
+    if (rc == MI_OK && want_lo_omp) rc = launch_profile(p, cake, MI_DT_F32, n_frames, lo_aw, lo_sm, s);
+    return rc;
+  }
   return a.want_lo ? launch_lineout(p, partial, n_frames, lo_aw, lo_sm, s) : MI_OK;
 }
 

@@ -346,6 +346,8 @@ struct Plan {
   double *d_den_aw = nullptr;    // per R row: sum of valid in-bounds area
   double *d_cnt = nullptr;       // per R row: number of valid bins
   double *d_partial = nullptr;   // [kMaxFramesPerLaunch][n_r][n_slots][2]
+  int32_t *d_nan_bins = nullptr; // MI_SEM_OMP: bins written as NaN (the plan's bin mask)
+  int n_nan_bins = 0;
   float *d_dark = nullptr;       // ny*nz (zeros when no dark is set)
   int has_dark = 0;
   int *d_err = nullptr;          // device error word (bounded waits)
@@ -415,6 +417,8 @@ int launch_cast(const void *frames, int dtype, int64_t n_pixels, int n_frames,
                 const float *dark, float *out, cudaStream_t s);
 int launch_profile(Plan *p, const void *cake, int cake_dtype, int n_frames, double *lo_aw,
                    double *lo_sm, cudaStream_t s);
+// MI_SEM_OMP plans: NaN into the masked bins of F cakes
+int launch_nan_bins(Plan *p, float *cake, int n_frames, cudaStream_t s);
 
 size_t dtype_size(int dtype);
 

@@ -188,7 +188,7 @@ __global__ void k_plain_integrate(PlainArgs a) {
 // sum(V) / N^2
 template <typename T>
 __global__ void k_profile(const T *cake, const double *area_in, int n_r, int n_eta, double *lo_aw,
-                          double *lo_sm, int variance) {
+                          double *lo_sm, int variance, int omp) {
   const int r = blockIdx.x;
   const int64_t f = blockIdx.y;
   if (r >= n_r) return;
@@ -198,8 +198,21 @@ __global__ void k_profile(const T *cake, const double *area_in, int n_r, int n_e
   for (int e = threadIdx.x; e < n_eta; e += blockDim.x) {
     const int64_t b = (int64_t)r * n_eta + e;
     const double A = area_in[b];
-    if (A > kAreaThreshold) {
-      const double I = (double)ck[b];
+    const double I = (double)ck[b];
+    if (omp) {
+      // IntegratorZarrOMP.c:1829-1843: the mean of the row's nonzero, non-NaN bins; the
+      // area-weighted mean over its valid, non-NaN bins
+      if (!isnan(I)) {
+        if (A > kAreaThreshold) {
+          s_ia += I * A;
+          s_a += A;
+        }
+        if (I != 0.0) {
+          s_i += I;
+          ++n;
+        }
+      }
+    } else if (A > kAreaThreshold) {
       s_ia += variance ? I * A * A : I * A;
       s_a += A;
       s_i += I;
@@ -236,12 +249,27 @@ int launch_profile(Plan *p, const void *cake, int cake_dtype, int n_frames, doub
   const dim3 grid((unsigned)p->n_r, (unsigned)n_frames);
   if (cake_dtype == MI_DT_F32)
     k_profile<float><<<grid, 256, 0, s>>>((const float *)cake, p->d_area_in, p->n_r, p->n_eta, lo_aw, lo_sm,
-                                                  p->variance);
+                                          p->variance, p->semantics == MI_SEM_OMP);
   else if (cake_dtype == MI_DT_F64)
     k_profile<double><<<grid, 256, 0, s>>>((const double *)cake, p->d_area_in, p->n_r, p->n_eta, lo_aw, lo_sm,
-                                                  p->variance);
+                                           p->variance, p->semantics == MI_SEM_OMP);
   else
     return set_error(MI_E_ARG, "mi_profile_batch: cake dtype must be MI_DT_F32 or MI_DT_F64");
+  MI_CUDA(cudaGetLastError());
+  return MI_OK;
+}
+
+__global__ void k_nan_bins(float *cake, int64_t n_bins, const int32_t *bins, int n, int F) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= (int64_t)n * F) return;
+  const int64_t f = i / n;
+  cake[f * n_bins + bins[i % n]] = __int_as_float(0x7fc00000);
+}
+
+int launch_nan_bins(Plan *p, float *cake, int n_frames, cudaStream_t s) {
+  if (!cake || p->n_nan_bins == 0 || n_frames <= 0) return MI_OK;
+  const int64_t n = (int64_t)p->n_nan_bins * n_frames;
+  k_nan_bins<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(cake, p->n_bins, p->d_nan_bins, p->n_nan_bins, n_frames);
   MI_CUDA(cudaGetLastError());
   return MI_OK;
 }

@@ -142,7 +142,7 @@ static void bin_terms(const mi_map_desc &m, int64_t b, int mode, int sem,
       } else if (inb) {
         t.push_back({(int32_t)(tz * ny + ty), r.frac});
       }
-    } else if (sem == MI_SEM_IC) {
+    } else if (sem == MI_SEM_IC || sem == MI_SEM_OMP) {
       // IntegrationCore.c:38-50: FP64 shift, only for records with deltaR != 0 and R > 1
       double sy = y, sz = z;
       if (mode == MI_MODE_GRADIENT && r.deltaR != 0.0f) {
@@ -362,7 +362,10 @@ static inline void bin_scale(const HostCSR &csr, const Plan *p, int64_t b, float
                              double *scale64 = nullptr) {
   const double an = csr.area_norm[b], ai = csr.area_in[b];
   double sc;
-  if (p->semantics != MI_SEM_PY)
+  if (p->semantics == MI_SEM_OMP)
+    // IntegratorZarrOMP.c:1749-1753: a nonzero sum is divided by the area, whatever its size
+    sc = p->normalize ? (an > 0.0 ? 1.0 / an : 0.0) : 1.0;
+  else if (p->semantics != MI_SEM_PY)
     sc = an > kAreaThreshold ? (p->normalize ? 1.0 / an : 1.0) : 0.0;
   else
     sc = p->normalize ? (ai > kAreaThreshold ? 1.0 / ai : 0.0) : 1.0;
@@ -565,7 +568,7 @@ static int free_plan_mem(Plan *p) {
                   p->d_dark, p->d_err, p->d_nmap, p->d_sorted, p->d_off, p->d_w, p->d_aw,
                   p->d_dr, p->d_py, p->d_pz, p->d_area_in, p->d_area_all, p->d_plain_img,
                   p->d_ctr, p->d_span_lo, p->d_row_off, p->d_xchunks, p->d_xc,
-                  p->d_xc_pix};
+                  p->d_xc_pix, p->d_nan_bins};
   for (void *q : ptrs)
     if (q) cudaFree(q);
   return MI_OK;
@@ -1313,9 +1316,9 @@ int mi_plan_create(const mi_map_desc *map, const mi_plan_opts *opts, int device,
   if (opts) o = *opts;
   else { o.mode = MI_MODE_FLOOR; o.normalize = 1; o.semantics = MI_SEM_PY; }
   if (o.mode < 0 || o.mode > 2) return set_error(MI_E_ARG, "mi_plan_create: unknown mode %d", o.mode);
-  if (o.semantics < 0 || o.semantics > 2)
+  if (o.semantics < 0 || o.semantics > 3)
     return set_error(MI_E_ARG, "mi_plan_create: unknown semantics %d", o.semantics);
-  if (o.semantics == MI_SEM_IC && o.mode == MI_MODE_FLOOR)
+  if ((o.semantics == MI_SEM_IC || o.semantics == MI_SEM_OMP) && o.mode == MI_MODE_FLOOR)
     return set_error(MI_E_ARG, "mi_plan_create: IntegrationCore semantics has no floor mode "
                                "(integration_apply_map always interpolates)");
   int ndev = 0;
@@ -1471,6 +1474,31 @@ int mi_plan_set_dark(mi_plan *p, const float *dark) {
     // stream alone leaves other threads' streams running
     rc = p->encoding == MI_ENC_MMA ? launch_mma_dark(p, nullptr) : launch_mmad_dark(p, nullptr);
     if (rc == MI_OK) MI_CUDA(cudaStreamSynchronize(nullptr));
+  }
+  cudaSetDevice(prev);
+  return rc;
+}
+
+int mi_plan_set_bin_mask(mi_plan *p, const uint8_t *mask) {
+  if (!p) return set_error(MI_E_ARG, "mi_plan_set_bin_mask: null plan");
+  if (p->semantics != MI_SEM_OMP)
+    return set_error(MI_E_ARG, "mi_plan_set_bin_mask: only MI_SEM_OMP plans write masked bins as NaN");
+  std::vector<int32_t> bins;
+  if (mask)
+    for (int64_t b = 0; b < p->n_bins; ++b)
+      if (mask[b]) bins.push_back((int32_t)b);
+  int prev = 0;
+  cudaGetDevice(&prev);
+  MI_CUDA(cudaSetDevice(p->device));
+  MI_CUDA(cudaDeviceSynchronize());
+  cudaFree(p->d_nan_bins);
+  p->d_nan_bins = nullptr;
+  p->n_nan_bins = 0;
+  int rc = MI_OK;
+  if (!bins.empty()) {
+    size_t acct = 0;
+    rc = upload(&p->d_nan_bins, bins.data(), bins.size(), &acct);
+    if (rc == MI_OK) p->n_nan_bins = (int)bins.size();
   }
   cudaSetDevice(prev);
   return rc;
@@ -1665,7 +1693,7 @@ int mi_integrate_plain(mi_plan *p, const void *frame, int dtype, double *cake, d
   if (p->panels.size() > 1 || !p->d_plain_img)
     return set_error(MI_E_UNSUPPORTED, "mi_integrate_plain: a panel plan has no one-frame path");
   if (dtype_size(dtype) == 0) return set_error(MI_E_ARG, "mi_integrate_plain: unknown dtype code %d", dtype);
-  if (p->semantics == MI_SEM_IC)
+  if (p->semantics == MI_SEM_IC || p->semantics == MI_SEM_OMP)
     return set_error(MI_E_UNSUPPORTED, "mi_integrate_plain: the one-frame GPU kernel follows the GPU stream "
                                        "or midas_integrate semantics, not IntegrationCore's");
   if (p->variance)

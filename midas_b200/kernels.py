@@ -56,8 +56,11 @@ class CakePlan:
         mode: 'floor' | 'bilinear' | 'gradient'.
         normalize: divide by the bin area (Normalize key).
         semantics: 'py' (midas_integrate kernels.py), 'gpustream'
-            (IntegratorFitPeaksGPUStream normaliser and fp32 resampling) or 'ic'
-            (IntegrationCore.c integration_apply_map: bilinear/gradient only).
+            (IntegratorFitPeaksGPUStream normaliser and fp32 resampling), 'ic'
+            (IntegrationCore.c integration_apply_map: bilinear/gradient only) or 'omp'
+            (IntegratorZarrOMP.c: the 'ic' sums, a nonzero sum divided by the bin's whole
+            area, masked bins NaN (``set_bin_mask``), the lineouts computed from the cake:
+            lineout_sm = mean of the row's nonzero, non-NaN bins).
         bc_y, bc_z: beam centre (px), used by gradient mode.
         device: CUDA device.
         tile_rows, tile_pixels, frames_per_lane: tiling knobs (0 = default).
@@ -146,6 +149,18 @@ class CakePlan:
             raise ValueError(f"dark has {d.size} pixels, expected {self.ny * self.nz}")
         L.check(L.lib().mi_plan_set_dark(self._h, d.ctypes.data), "mi_plan_set_dark")
         self._dark = d
+
+    def set_bin_mask(self, bin_mask) -> None:
+        """Semantics 'omp' only: bins flagged in ``bin_mask`` (n_bins, nonzero = the bin holds
+        a masked pixel; DetectorMapper's bin mask) are NaN in every cake, as the OpenMP
+        integrator writes them (IntegratorZarrOMP.c:1766-1767).  None clears it."""
+        if bin_mask is None:
+            L.check(L.lib().mi_plan_set_bin_mask(self._h, None), "mi_plan_set_bin_mask")
+            return
+        m = np.ascontiguousarray(np.asarray(bin_mask).reshape(-1) != 0, dtype=np.uint8)
+        if m.size != self.n_r * self.n_eta:
+            raise ValueError(f"bin mask has {m.size} entries, expected {self.n_r * self.n_eta}")
+        L.check(L.lib().mi_plan_set_bin_mask(self._h, m.ctypes.data), "mi_plan_set_bin_mask")
 
     # -- work ---------------------------------------------------------------
     def _frames(self, frames: torch.Tensor) -> Tuple[torch.Tensor, int, int]:

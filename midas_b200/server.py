@@ -118,6 +118,9 @@ class StreamConfig:
     want_cake: bool = False
     tile_rows: int = 0
     max_batch: int = 0             # frames per launch at most (0 = the backend's default)
+    output_dir: Optional[str] = None   # write the reference's per-frame files there (writers.py):
+                                       # lineout.bin, lineout_simple_mean.bin, fit.bin (peaks
+                                       # set), Int2D.bin (want_cake)
 
 
 @dataclass
@@ -156,6 +159,8 @@ class _Stream:
     inflight: collections.deque = field(default_factory=collections.deque)   # (handle, reqs)
     seq: itertools.count = field(default_factory=itertools.count)
     closing: bool = False
+    writer: object = None          # writers.StreamOutputs when cfg.output_dir is set
+    fit_valid: Optional[np.ndarray] = None
 
 
 class DeviceBackend:
@@ -365,6 +370,14 @@ class DeviceBackend:
             self.pool.release(tok)
 
 
+def _fit_file_rows(s: "_Stream", fit: np.ndarray) -> np.ndarray:
+    """fit.bin rows of one frame: the peaks within 2 bins of the grid, ascending by bin
+    (IntegratorFitPeaksGPUStream.cu:2632-2688), first seven outputs."""
+    if s.fit_valid is None:
+        return np.zeros((0, 7))
+    return np.ascontiguousarray(np.asarray(fit, np.float64)[s.fit_valid, :7])
+
+
 class CakeServer:
     """Continuous-batching scheduler over admitted detector streams.
 
@@ -417,10 +430,21 @@ class CakeServer:
             with self._lock:
                 self.used -= est
             raise
+        writer, valid = None, None
+        if cfg.output_dir:
+            from .writers import StreamOutputs
+            r_axis = cfg.r_axis if cfg.r_axis is not None else np.arange(cfg.n_r, dtype=np.float64)
+            writer = StreamOutputs(cfg.output_dir, r_axis, write_2d=cfg.want_cake, write_fit=cfg.peaks is not None)
+            if cfg.peaks is not None and cfg.r_axis is not None:
+                xs = np.asarray(cfg.r_axis, np.float64)
+                pk = np.asarray(cfg.peaks, np.float64).reshape(-1)
+                bins = np.array([int(np.argmin(np.abs(xs - c))) for c in pk])
+                ok = np.abs(xs[bins] - pk) < 2.0 * cfg.x_bin
+                valid = np.array([k for k in np.argsort(bins, kind="stable") if ok[k]], dtype=np.int64)
         with self._lock:
             self.used += fp - est
             sid = next(self._ids)
-            self.streams[sid] = _Stream(sid, cfg, state, fp)
+            self.streams[sid] = _Stream(sid, cfg, state, fp, writer=writer, fit_valid=valid)
         return sid
 
     def remove(self, sid: int, *, drain: bool = True, timeout: float = 30.0) -> None:
@@ -449,6 +473,8 @@ class CakeServer:
             del self.streams[sid]
             self.used -= s.footprint
         self.backend.close(s.state)
+        if s.writer is not None:
+            s.writer.close()
 
     # -- requests ---------------------------------------------------------------
     def submit(self, sid: int, frame: np.ndarray, t_arrival: Optional[float] = None) -> Future:
@@ -489,6 +515,8 @@ class CakeServer:
                 now = clock()
                 ps["max_collect_ms"] = max(ps["max_collect_ms"], (now - t1) * 1e3)
                 for r, (aw, sm, fit, cake) in zip(reqs, res):
+                    if s.writer is not None:
+                        s.writer.write_frame(aw, sm, cake, None if fit is None else _fit_file_rows(s, fit))
                     lat = now - r.t_arrival
                     self.latencies.append(lat)
                     r.fut.set_result(FrameResult(s.cfg.name, r.seq, aw, sm, fit, cake, lat, len(reqs),

@@ -25,7 +25,7 @@ REF_LIB = HERE / "_ref" / "libmidas_ref.so"
 REC_DTYPE = np.dtype([("y", "<f4"), ("z", "<f4"), ("frac", "<f8"), ("deltaR", "<f4"),
                       ("areaWeight", "<f4")])
 MODES = {"floor": 0, "bilinear": 1, "gradient": 2}
-SEMS = {"py": 0, "gpustream": 1, "ic": 2}
+SEMS = {"py": 0, "gpustream": 1, "ic": 2, "omp": 3}
 
 _lib = None
 _ref = None
@@ -51,6 +51,8 @@ def lib() -> C.CDLL:
         L.or_integrate_var.restype = i
         L.or_profile.argtypes = [vp, vp, i, i, vp, vp]
         L.or_profile.restype = None
+        L.or_profile_omp.argtypes = [vp, vp, i, i, vp, vp]
+        L.or_profile_omp.restype = None
         L.or_fit.argtypes = [vp, vp, i, d, i, i, i, d, d, d, vp]
         L.or_fit.restype = i
         _lib = L
@@ -182,6 +184,17 @@ def area_in(records, nmap, n_bins, ny, nz):
     out = np.zeros(n_bins)
     lib().or_area_in(rec.ctypes.data if rec.size else None, nm.ctypes.data, n_bins, ny, nz, out.ctypes.data)
     return out
+
+
+def profile_omp(cake, area, n_r, n_eta):
+    """The OpenMP integrator's lineout (IntegratorZarrOMP.c:1829-1843): per row the mean of
+    the nonzero, non-NaN bins (second) and the area-weighted mean over valid, non-NaN bins."""
+    ck = _c(cake, np.float64).reshape(-1)
+    ar = _c(area, np.float64).reshape(-1)
+    aw = np.zeros(n_r)
+    sm = np.zeros(n_r)
+    lib().or_profile_omp(ck.ctypes.data, ar.ctypes.data, n_r, n_eta, aw.ctypes.data, sm.ctypes.data)
+    return aw, sm
 
 
 def profile(cake, area, n_r, n_eta):

@@ -1,7 +1,8 @@
 /*
  * oracle.c -- FP64 CPU restatement of the MIDAS caking hot path (test infrastructure).
  *
- * or_integrate follows, per semantics:
+ * or_integrate follows, per semantics (3 = IntegratorZarrOMP.c:1709-1778: the IntegrationCore
+ * sums, a nonzero sum divided by the bin's whole area):
  *   0: integrate() of packages/midas_integrate/midas_integrate/kernels.py:416-473 with the
  *      CSR of build_csr (kernels.py:242-375) written as the explicit per-record loops of
  *      packages/midas_integrate/tests/test_kernels.py:55-114 (floor: truncated (y,z),
@@ -71,7 +72,7 @@ void or_area_in(const or_record *rec, const int32_t *nmap, int64_t n_bins, int n
 int or_integrate(const or_record *rec, const int32_t *nmap, int64_t n_bins, int ny, int nz, double bc_y,
                  double bc_z, const double *image, int mode, int sem, int normalize, double *cake, double *area_out) {
   const long npix = (long)ny * nz;
-  if (sem == 2 && mode == 0) return -3; /* IntegrationCore has no floor mode */
+  if ((sem == 2 || sem == 3) && mode == 0) return -3; /* IntegrationCore / OMP: no floor mode */
   for (int64_t b = 0; b < n_bins; ++b) {
     double I = 0.0, A_in = 0.0, A_all = 0.0;
     const int cnt = nmap[2 * b], off = nmap[2 * b + 1];
@@ -92,8 +93,8 @@ int or_integrate(const or_record *rec, const int32_t *nmap, int64_t n_bins, int 
         } else if (inb) {
           I += image[tz * ny + ty] * e->frac;
         }
-      } else if (sem == 2) {
-        /* IntegrationCore.c:38-50 */
+      } else if (sem == 2 || sem == 3) {
+        /* IntegrationCore.c:38-50; IntegratorZarrOMP.c:1722-1745 samples the same way */
         double sy = y, sz = z;
         if (mode == 2 && e->deltaR != 0.0f) {
           double dy = y - bc_y, dz = z - bc_z;
@@ -129,7 +130,11 @@ int or_integrate(const or_record *rec, const int32_t *nmap, int64_t n_bins, int 
       }
     }
     double out;
-    if (sem == 1 || sem == 2) {
+    if (sem == 3) {
+      /* IntegratorZarrOMP.c:1749-1753: a nonzero sum is divided by the area, whatever it is */
+      out = (I != 0.0 && normalize) ? I / A_all : I;
+      if (area_out) area_out[b] = A_all;
+    } else if (sem == 1 || sem == 2) {
       out = A_all > AREA_THRESHOLD ? (normalize ? I / A_all : I) : 0.0;
       if (area_out) area_out[b] = A_all;
     } else {
@@ -275,6 +280,30 @@ void or_profile(const double *cake, const double *area_in, int n_r, int n_eta, d
         sia += cake[b] * A;
         sa += A;
         si += cake[b];
+        ++n;
+      }
+    }
+    if (lo_aw) lo_aw[r] = sa > AREA_THRESHOLD ? sia / sa : 0.0;
+    if (lo_sm) lo_sm[r] = n > 0 ? si / n : 0.0;
+  }
+}
+
+/* IntegratorZarrOMP.c:1829-1843: per R row the mean of the nonzero, non-NaN bins, and the
+ * area-weighted mean over the valid (in-bounds area > 1e-9), non-NaN bins */
+void or_profile_omp(const double *cake, const double *area_in, int n_r, int n_eta, double *lo_aw, double *lo_sm) {
+  for (int r = 0; r < n_r; ++r) {
+    double sia = 0, sa = 0, si = 0;
+    int n = 0;
+    for (int e = 0; e < n_eta; ++e) {
+      const long b = (long)r * n_eta + e;
+      const double I = cake[b], A = area_in[b];
+      if (isnan(I)) continue;
+      if (A > AREA_THRESHOLD) {
+        sia += I * A;
+        sa += A;
+      }
+      if (I != 0.0) {
+        si += I;
         ++n;
       }
     }

@@ -20,7 +20,8 @@ typedef struct {
   float deltaR, areaWeight;
 } or_record;
 
-/* semantics: 0 = midas_integrate kernels.py, 1 = IntegratorFitPeaksGPUStream.cu, 2 = IntegrationCore.c
+/* semantics: 0 = midas_integrate kernels.py, 1 = IntegratorFitPeaksGPUStream.cu, 2 = IntegrationCore.c,
+ * 3 = IntegratorZarrOMP.c (the sums of 2, a nonzero sum divided by the whole area)
  * mode: 0 floor, 1 bilinear, 2 gradient
  * image: dark-subtracted frame, double, nz*ny (flat index z*ny + y)
  * cake_out: n_bins, area_out (may be NULL): normaliser per bin */
@@ -41,6 +42,11 @@ int or_integrate_var(const or_record *rec, const int32_t *nmap, int64_t n_bins, 
 /* profile_1d: area-weighted (lo_aw) and simple-mean (lo_sm) eta reductions */
 void or_profile(const double *cake, const double *area_in, int n_r, int n_eta, double *lo_aw,
                 double *lo_sm);
+
+/* the OpenMP integrator's lineout: mean of the nonzero, non-NaN bins of each row (lo_sm),
+ * and the area-weighted mean over its valid, non-NaN bins (lo_aw) */
+void or_profile_omp(const double *cake, const double *area_in, int n_r, int n_eta, double *lo_aw,
+                    double *lo_sm);
 
 /* one LM fit (same algorithm as the device fitter, in FP64).  model 0 = PV, 1 = TCH.
  * out: 11 doubles (layout of MI_FIT_NOUT).  Returns iterations, or <0 if rejected. */

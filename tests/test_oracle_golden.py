@@ -172,3 +172,28 @@ def test_oracle_bin_table_columns():
     np.testing.assert_allclose(t[:, 3], g["area_per_bin"], rtol=1e-12)
     q = 4 * np.pi / 0.172979 * np.sin(np.arctan(rm * 200.0 / 1e6) / 2)
     np.testing.assert_allclose(t[:, 4], q, rtol=1e-14)
+
+
+@pytest.mark.parametrize("tag", MAPPER_CASES)
+@pytest.mark.parametrize("mode", ["bilinear", "gradient"])
+def test_oracle_omp_semantics_from_integration_core_sums(tag, mode):
+    """Semantics 'omp' (IntegratorZarrOMP.c:1709-1778) applies the OpenMP loop's rules to the
+    IntegrationCore sums: a nonzero sum divided by the whole area.  Pinned on the compiled
+    reference integrator's sums and norms recorded in the fixture; the lineout is the mean
+    of the nonzero, non-NaN bins of each row (:1829-1843) after the bin mask's NaNs."""
+    g = load_mapper_case(tag)
+    nb = g["nmap"].shape[0]
+    n_r, n_eta = g["r_lo"].size, g["eta_lo"].size
+    ck, area = oracle.integrate(g["records"], g["nmap"], nb, g["ny"], g["nz"], g["image"] - g["dark"],
+                                mode=mode, semantics="omp", normalize=True, bc_y=g["bc_y"], bc_z=g["bc_z"])
+    sums, norms = g[f"ic_sums_{mode}"], g[f"ic_norms_{mode}"]
+    want = np.where(sums != 0, sums / np.where(norms != 0, norms, 1.0), 0.0)
+    np.testing.assert_allclose(ck, want, rtol=1e-10, atol=1e-12)
+    mask = np.random.default_rng(3).random(nb) < 0.05      # bins holding a masked pixel
+    ck = np.where(mask, np.nan, ck)
+    a_in = oracle.area_in(g["records"], g["nmap"], nb, g["ny"], g["nz"])
+    aw, sm = oracle.profile_omp(ck, a_in, n_r, n_eta)
+    v = ck.reshape(n_r, n_eta)
+    ok = (v != 0) & ~np.isnan(v)
+    want_sm = np.where(ok.sum(1) > 0, np.where(ok, v, 0).sum(1) / np.maximum(ok.sum(1), 1), 0.0)
+    np.testing.assert_allclose(sm, want_sm, rtol=1e-12, atol=1e-12)
