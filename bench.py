@@ -62,6 +62,10 @@ def parse():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-check", action="store_true")
     ap.add_argument("--no-fit", action="store_true")
+    ap.add_argument("--no-sweep", action="store_true", help="skip the F = 1, 8, 32, 128 launch sweep")
+    ap.add_argument("--no-eta-fits", action="store_true", help="skip the per-eta ring fits of the timed cake")
+    ap.add_argument("--no-published", action="store_true",
+                    help="skip the reference's published PILATUS3 2M configuration")
     ap.add_argument("--no-panels", action="store_true")
     ap.add_argument("--no-graph", action="store_true", help="skip the CUDA-graph replay of the batched step")
     ap.add_argument("--autotune", action="store_true", help="time candidate tile shapes / run lengths first")
@@ -407,6 +411,14 @@ def main_ours(args):
         out["autotune"] = {"best": tuned.best, "best_ms": tuned.best_ms, "candidates": tuned.table,
                            "seconds": round(tuned_s, 1)}
 
+    # ---- per-eta ring fits of the timed batch's cake (IntegratorZarrOMP.c:1902-2030)
+    if not args.no_eta_fits:
+        out["eta_fits"] = eta_fit_bench(bufs["cake"], w, dev)
+
+    # ---- frames per launch F = 1, 8, 32, 128: one launch per step, new frames every step
+    if not args.no_sweep:
+        out["f_sweep"] = f_sweep(plan, frames, bufs, F, info, w, args, world, peak)
+
     # ---- the same steps replayed from CUDA graphs (one graph per resident batch)
     if not args.no_graph:
         graphs = [plan.capture(frames[b * F:(b + 1) * F], bufs) for b in range(n_batches)]
@@ -449,6 +461,10 @@ def main_ours(args):
     fit_sample = None
     if not args.no_fit:
         out["fits"], fit_sample = fit_bench(plan, frames, w, F, dev)
+
+    # ---- the reference's published configuration (PILATUS3 2M), beside its H100 numbers
+    if rank == 0 and world == 1 and not args.no_published:
+        out["published_config"] = published_bench(args, dev)
 
     # ---- uneven multi-panel batch: five panels, one merged Q x eta cake (rank 0, N = 1)
     panel_sample = None
@@ -781,6 +797,129 @@ def fit_bench(plan, frames, w, F, dev, reps=5):
         params[model] = r.params[:16].cpu().numpy()
     sample = (synth.r_centres(w), lo[:16].cpu().numpy(), peaks.cpu().numpy(), w, params)
     return res, sample
+
+
+def eta_fit_bench(cake, w, dev, reps=3):
+    """Every ring in every eta column of one F-frame cake, in one launch of the fit-plan
+    kernel: the per-eta pseudo-Voigt fits of the OpenMP integrator (singlets; SNR > 1
+    kept)."""
+    import numpy as np
+    import torch
+
+    from midas_b200 import synth
+    from midas_b200.peakfit import FitPlan
+
+    x = synth.r_centres(w)
+    peaks = synth.ring_peaks(w, FIT_HALF_WINDOW)
+    fp = FitPlan(x, peaks, kind="eta", half_window=FIT_HALF_WINDOW, x_bin=w.mapper.RBinSize, px_um=w.mapper.px,
+                 lsd_um=w.mapper.Lsd, device=dev)
+    r = fp.fit_cake_eta(cake)
+    torch.cuda.synchronize()
+    stream = torch.cuda.current_stream()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(reps):
+        r = fp.fit_cake_eta(cake)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / reps
+    it = r.iters.cpu().numpy()
+    kept = int((r.params[..., 6] > 1.0).sum().item())
+    fp.close()
+    return {"frames": int(cake.shape[0]), "eta_bins": int(cake.shape[2]), "rings": int(len(peaks)),
+            "windows_per_launch": int(it.size), "ms_per_launch": round(ms, 4),
+            "fits_per_s": round(it.size / (ms / 1e3), 1), "fits_kept_snr_gt_1": kept,
+            "iterations_mean": round(float(it[it >= 0].mean()), 2) if (it >= 0).any() else None}
+
+
+def f_sweep(plan, frames, bufs, F_max, info, w, args, world, peak, steps=10):
+    """Frames per launch F in {1, 8, 32, 128}: frames/s and the HBM roofline of one launch,
+    A(F) = map bytes + F * frame bytes over the launch time (CUDA events, consecutive
+    batches of the resident sweep, so no launch re-reads its frames from L2)."""
+    import torch
+    ny, nz = w.mapper.NrPixelsY, w.mapper.NrPixelsZ
+    stream = torch.cuda.current_stream()
+    out = {}
+    n = frames.shape[0]
+    for F in (1, 8, 32, 128):
+        if F > F_max:
+            continue
+        ob = {k: v[:F] for k, v in bufs.items()}
+        nb = n // F
+        for i in range(3):
+            plan.integrate(frames[(i % nb) * F:(i % nb + 1) * F], out=ob)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for i in range(steps):
+            b = (3 + i) % nb
+            plan.integrate(frames[b * F:(b + 1) * F], out=ob)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms = dist_max(e0.elapsed_time(e1), world) / steps
+        alg = info["map_bytes"] + F * ny * nz * 2
+        out[str(F)] = {"frames_per_s": round(world * F / (ms / 1e3), 1), "ms_per_launch": round(ms, 4),
+                       "roofline_frac": round(alg / (ms / 1e3) / 1e9 / peak, 4),
+                       "alg_bytes_per_launch": alg}
+    return out
+
+
+def published_bench(args, dev, F=128, reps=10):
+    """The reference's published benchmark configuration (PILATUS3 2M 1475x1679 u16, 172 um,
+    Lsd 500 mm, beam centre at the detector centre, no tilt, RBin 1 px over 10..1117.4 px,
+    eta 5 deg: packages/midas_integrate/tests/benchmarks/run_benchmarks.py:83-86, README
+    'Performance') caked F frames per launch, on the device and end to end from host frames,
+    beside the reference's H100 figures (C GPU stream ~1,600 frames/s; torch CSR FP32
+    ~3,250 frames/s; packages/midas_integrate/README.md:75-80)."""
+    import torch
+
+    from midas_b200 import synth
+    from midas_b200.kernels import CakePlan
+    from midas_b200.mapper import build_map
+
+    w = synth.pilatus3_2m_published()
+    m = w.mapper
+    ny, nz = m.NrPixelsY, m.NrPixelsZ
+    pm, _ = build_map(m, device=dev.index)
+    res = {"workload": w.name, "n_bins": w.n_r * w.n_eta, "mode": w.mode,
+           "reference_h100_frames_per_s": {"c_gpu_stream": 1600, "torch_csr_fp32": 3250}}
+    frames = w.frames(0, 4 * F, device=dev)
+    stream = torch.cuda.current_stream()
+    for enc in ("mma", "runs"):
+        plan = CakePlan(pm, n_r=w.n_r, n_eta=w.n_eta, n_pixels_y=ny, n_pixels_z=nz, mode=w.mode, bc_y=m.BC_y,
+                        bc_z=m.BC_z, device=dev, encoding=enc)
+        plan.set_dark(w.dark(device=dev).cpu().numpy())
+        ob = {"cake": torch.empty((F, w.n_r, w.n_eta), dtype=torch.float32, device=dev),
+              "lineout_aw": torch.empty((F, w.n_r), dtype=torch.float64, device=dev),
+              "lineout_sm": torch.empty((F, w.n_r), dtype=torch.float64, device=dev)}
+        for i in range(3):
+            plan.integrate(frames[(i % 4) * F:(i % 4 + 1) * F], out=ob)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for i in range(reps):
+            plan.integrate(frames[(i % 4) * F:(i % 4 + 1) * F], out=ob)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / reps
+        r = {"frames_per_s": round(F / (ms / 1e3), 1), "ms_per_launch_of_128": round(ms, 4)}
+        e2 = e2e_rate(plan, frames, F, argparse.Namespace(warmup=3, steps=reps), w, dev, 1)
+        r["e2e_frames_per_s"] = e2["value"]
+        r["e2e_h2d_bytes_per_step"] = e2["h2d_bytes_per_step"]
+        res[enc] = r
+        if enc == "mma":
+            P = 16
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            plan.integrate_plain(frames[0])
+            torch.cuda.synchronize()
+            a.record(stream)
+            for k in range(P):
+                plan.integrate_plain(frames[k])
+            b.record(stream)
+            torch.cuda.synchronize()
+            res["plain_frames_per_s"] = round(P / (a.elapsed_time(b) / 1e3), 1)
+        plan.close()
+    return res
 
 
 def fit_accuracy(sample):

@@ -194,6 +194,13 @@ int mi_plan_set_dark_panels(mi_plan *plan, const float *const *darks_host);
 int mi_integrate_panels(mi_plan *plan, const void *const *frames, const int *dtypes,
                         const int64_t *strides, int n_frames, float *cake, double *lineout_aw,
                         double *lineout_sm, void *stream);
+/* Failure-detection self test (no counterpart in the reference, which aborts on errors):
+ * one mbarrier wait bounded to `polls` polls, as every wait in this library's kernels is,
+ * on a barrier that nothing completes (arrive = 0) or that its thread completed first
+ * (arrive = 1).  *status receives MI_E_TIMEOUT when the limit ran out, MI_OK when the wait
+ * succeeded; the device context stays usable either way. */
+int mi_selftest_wait(uint32_t polls, int arrive, int device, int *status);
+
 /* Per-bin mask of a MI_SEM_OMP plan (host, n_bins bytes, nonzero = the bin holds a masked
  * pixel, DetectorMapper's bin mask): those bins of every cake are NaN, as the OpenMP
  * integrator writes them (IntegratorZarrOMP.c:1766-1767).  NULL clears it. */

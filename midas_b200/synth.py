@@ -169,6 +169,15 @@ def pilatus_1679() -> Workload:
                     module_gaps=(487, 7, 195, 17), tile_rows=8)
 
 
+def pilatus3_2m_published() -> Workload:
+    """The reference's published benchmark detector (run_benchmarks.py 'pilatus3_2m'): 1475x1679
+    u16, 172 um pixels, Lsd 500 mm, beam centre (737.5, 839.5) px, no tilt, RMin 10 .. RMax
+    1117.4 px at 1 px, eta -180 .. 180 at 5 deg (1108 x 72 bins), floor mode."""
+    m = MapperParams(NrPixelsY=1475, NrPixelsZ=1679, px=172.0, Lsd=5.0e5, BC_y=737.5, BC_z=839.5, RMin=10.0,
+                     RMax=1117.4, RBinSize=1.0, EtaMin=-180.0, EtaMax=180.0, EtaBinSize=5.0)
+    return Workload("pilatus3_2m_1475x1679_u16_1108x72_floor", m, "floor", n_frames=512, tile_rows=8)
+
+
 def detector_1024(variant: int = 0) -> Workload:
     """1024x1024 u16 panels of the serving mix: variant 0 = RBin 1 px, eta 8 deg (495x45 bins,
     floor); variant 1 = tilted, RBin 0.5 px, eta 5 deg (990x72 bins, bilinear)."""
@@ -294,4 +303,5 @@ def host_frames(w: Workload, first: int, n: int, device: int = 0) -> np.ndarray:
 
 
 WORKLOADS = {"powder_2048": powder_2048, "sweep_2880": sweep_2880, "pilatus_1679": pilatus_1679,
-             "detector_1024": detector_1024, "powder_2048_fine": powder_2048_fine}
+             "detector_1024": detector_1024, "powder_2048_fine": powder_2048_fine,
+             "pilatus3_2m_published": pilatus3_2m_published}
