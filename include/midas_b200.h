@@ -403,6 +403,19 @@ int mi_fit_plan_run(const mi_fit_plan *plan, const void *src, int src_dtype, int
                     void *stream);
 void mi_fit_plan_destroy(mi_fit_plan *plan);
 
+/* Automatic peak detection and fit of each lineout: fitPeaksAutoDetect (FF_HEDM/src/
+ * PeakFit.c:549-877; the GPU stream's AutoDetectPeaks mode, IntegratorFitPeaksGPUStream.cu:
+ * 2606-2629).  SNIP background (snip_iter passes; 0 = none), Savitzky-Golay-smoothed
+ * negative second difference, the most prominent candidates at least max(3, 3 x_bin / bin
+ * width) bins apart (up to 3 max_peaks), fitPeaks jobs on the background-subtracted profile
+ * (TCH, +-roi_padding bins, overlapping ROIs joint), then the reference's quality filter.
+ * x: device [n_x] bin centres; lineouts: device [F][n_x]; out: device [F][max_peaks]
+ * [MI_FIT_NOUT] (first n_found[f] rows filled, in position order, the rest zero);
+ * n_found: device [F] int32.  One block per lineout. */
+int mi_fit_autodetect(const double *x, const double *lineouts, int n_frames, int n_x, int max_peaks,
+                      double x_bin, int roi_padding, int snip_iter, double px_um, double lsd_um,
+                      double *out, int32_t *n_found, void *stream);
+
 /* ---- map building (DetectorMapper on the device) -------------------------- */
 typedef struct {
   int32_t ny, nz;

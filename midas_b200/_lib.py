@@ -145,6 +145,8 @@ SIGNATURES = [
     ("mi_fit_plan_run", C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int64, C.c_int64,
                                   C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p]),
     ("mi_fit_plan_destroy", None, [C.c_void_p]),
+    ("mi_fit_autodetect", C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_double, C.c_int, C.c_int,
+                                    C.c_double, C.c_double, C.c_void_p, C.c_void_p, C.c_void_p]),
     ("mi_map_build", C.c_int, [C.POINTER(MiGeometry), C.POINTER(MiBinning), C.c_int,
                                C.POINTER(C.c_void_p)]),
     ("mi_map_sizes", C.c_int, [C.c_void_p, C.POINTER(C.c_int64), C.POINTER(C.c_int64)]),

@@ -169,9 +169,8 @@ __device__ inline float job_model(int kind, int n_p, const float *p, const float
 
 // every lane: evaluate the job at parameters q over the window; chi^2 (all lanes) and,
 // with jac, J rows, residuals, J^T r and the lower triangle of J^T J in shared memory
-__device__ double job_eval(const FitPlanArgs &a, const JobSmem &S, int n, int np, int n_p, const float *q, bool jac,
-                           int lane) {
-  if (a.kind == MI_FIT_KIND_PEAKS) {
+__device__ double job_eval(int kind, const JobSmem &S, int n, int np, int n_p, const float *q, bool jac, int lane) {
+  if (kind == MI_FIT_KIND_PEAKS) {
     if (lane < n_p) {
       float F, et, t0, t1, t2, t3;
       tch(q[4 * lane + 2], q[4 * lane + 3], &F, &et, &t0, &t1, &t2, &t3);
@@ -183,7 +182,7 @@ __device__ double job_eval(const FitPlanArgs &a, const JobSmem &S, int n, int np
   double c2 = 0.0;
   float g[4 * MI_FIT_JOB_MAX_PEAKS + 2];
   for (int i = lane; i < n; i += 32) {
-    const float m = job_model(a.kind, n_p, q, S.pk, S.xl[i], S.xn[i], g);
+    const float m = job_model(kind, n_p, q, S.pk, S.xl[i], S.xn[i], g);
     const double r = S.y[i] - (double)m;
     c2 += r * r;
     if (jac) {
@@ -246,6 +245,200 @@ __device__ bool job_solve(const JobSmem &S, int np, double lam) {
   return true;
 }
 
+// fitting parameters shared by every job of a launch
+struct JobParams {
+  int kind, max_iter;
+  double x_bin, px, lsd;
+  const double *x;   // the axis [n_x]
+};
+
+// One job of one series, by one warp: window, initial values and bounds, projected LM,
+// outputs.  sample(i) is sample i of the series; rows go to out + id * MI_FIT_NOUT and
+// iteration counts to its[id], id = pk_id[entry] (or the entry itself when pk_id is null).
+template <typename Sample>
+__device__ void fit_one_job(const JobParams &c, const JobSmem &S, const FitJobDev jd, const double *pk_x,
+                            const int32_t *pk_bin, const int32_t *pk_id, Sample sample, double *out, int32_t *its,
+                            int lane) {
+  const int n = jd.s1 - jd.s0 + 1, n_p = jd.n_p;
+  const int np = c.kind == MI_FIT_KIND_PEAKS ? 4 * n_p + 2 : 3 * n_p + 2;
+  if (n <= np) {
+    // fewer samples than parameters: the job's peaks are not fit
+    for (int k = lane; k < n_p; k += 32) its[pk_id ? pk_id[jd.p0 + k] : jd.p0 + k] = -2;
+    __syncwarp();
+    return;
+  }
+  // window samples: x relative to the window's centre bin, normalised x, values
+  const int cb = (jd.s0 + jd.s1) / 2;
+  const double xref = c.x[cb], xlo = c.x[jd.s0], xhi = c.x[jd.s1];
+  const double xr = fmax(xhi - xlo, 1e-12);
+  for (int i = lane; i < n; i += 32) {
+    const double xi = c.x[jd.s0 + i];
+    S.xl[i] = (float)(xi - xref);
+    S.xn[i] = (float)(2.0 * (xi - xlo) / xr - 1.0);
+    S.y[i] = sample(jd.s0 + i);
+  }
+  __syncwarp();
+  // initial values and bounds (lane 0)
+  if (lane == 0) {
+    if (c.kind == MI_FIT_KIND_PEAKS) {
+      double rmax = -1e30, rmin = 1e30;
+      for (int i = 0; i < n; ++i) { rmax = fmax(rmax, S.y[i]); rmin = fmin(rmin, S.y[i]); }
+      const double range = fmax(rmax - rmin, 1.0);
+      const int bgw = max(1, min(5, n / 4));
+      double bgs = 0.0;
+      for (int i = 0; i < bgw; ++i) bgs += S.y[i] + S.y[n - 1 - i];
+      const double bg = bgs / (2.0 * bgw);   // pf_estimate_initial_params: same for every peak
+      for (int k = 0; k < n_p; ++k) {
+        const int loc = pk_bin[jd.p0 + k] - jd.s0;
+        double amp = S.y[loc] - bg;
+        if (amp <= 0) amp = S.y[loc];
+        const double hm = bg + 0.5 * amp;
+        int li = loc, ri = loc;
+        while (li > 0 && S.y[li] > hm) --li;
+        while (ri < n - 1 && S.y[ri] > hm) ++ri;
+        double fwb = (double)(ri - li);
+        if (!(fwb > 1.0)) fwb = 2.0;
+        const double fwx = fwb * c.x_bin;
+        const double fg0 = 0.5 * fwx;
+        double sg = (fg0 * 100.0) * (fg0 * 100.0) / 5.545177444479562;
+        if (sg < 1e-6) sg = 1.0;
+        double gm = fwx * 0.5 * 100.0;
+        if (gm < 0.01) gm = 1.0;
+        double ar = amp * fwx * 1.5;
+        if (ar <= 0) ar = range * c.x_bin;
+        const double c0 = pk_x[jd.p0 + k] - xref;
+        const double crange = fmax(fwx, (double)n * c.x_bin * 0.5);
+        double ahi = range * (double)n * c.x_bin * 2.0;
+        if (ahi < 1.0) ahi = 1.0;
+        const double shi = (c.x_bin * 2e4) * (c.x_bin * 2e4) / 5.545177444479562;
+        const double ghi = c.x_bin * 2e4;
+        const double lo4[4] = {0.0, c0 - crange, 1e-6, 0.01}, hi4[4] = {ahi, c0 + crange, shi, ghi};
+        double v4[4] = {fmax(fmin(ar, ahi * 0.9), 0.01), c0, fmax(fmin(sg, shi * 0.5), 2e-6),
+                        fmax(fmin(gm, ghi * 0.5), 0.02)};
+        for (int u = 0; u < 4; ++u) {
+          if (v4[u] <= lo4[u]) v4[u] = lo4[u] + (hi4[u] - lo4[u]) * 0.01;
+          if (v4[u] >= hi4[u]) v4[u] = hi4[u] - (hi4[u] - lo4[u]) * 0.01;
+          S.p[4 * k + u] = (float)v4[u];
+          S.lb[4 * k + u] = (float)lo4[u];
+          S.ub[4 * k + u] = (float)hi4[u];
+        }
+      }
+      double b0 = bg, b0lo = fmin(rmin - range * 0.5, -1.0), b0hi = rmax + range;
+      if (b0 <= b0lo) b0 = b0lo + 0.01;
+      if (b0 >= b0hi) b0 = b0hi - 0.01;
+      S.p[4 * n_p] = (float)b0;
+      S.lb[4 * n_p] = (float)b0lo;
+      S.ub[4 * n_p] = (float)b0hi;
+      S.p[4 * n_p + 1] = 0.0f;
+      S.lb[4 * n_p + 1] = (float)-range;
+      S.ub[4 * n_p + 1] = (float)range;
+    } else {
+      double bg0 = 0.5 * (S.y[0] + S.y[n - 1]);
+      if (bg0 < 0) bg0 = 0;
+      double mx = -1e20;
+      for (int i = 0; i < n; ++i) mx = fmax(mx, S.y[i]);
+      const double step = c.x_bin, gam0 = 3.0 * step;
+      const double xfirst = xlo - xref, xlast = xhi - xref;
+      if (n_p == 1) {
+        const double c0 = pk_x[jd.p0] - xref;
+        S.p[0] = (float)c0;  S.lb[0] = (float)xfirst;  S.ub[0] = (float)xlast;
+        S.p[1] = (float)gam0;  S.lb[1] = (float)(step / 2);  S.ub[1] = (float)(step * n / 2);
+        S.p[2] = (float)(mx - bg0);  S.lb[2] = (float)((mx - bg0) / 100);  S.ub[2] = (float)(mx * 1.5);
+      } else {
+        double ig = mx - bg0;
+        if (ig < 1e-6) ig = 1e-6;
+        const double c1 = pk_x[jd.p0] - xref, c2 = pk_x[jd.p0 + 1] - xref, cm = 0.5 * (c1 + c2);
+        S.p[0] = (float)c1;  S.lb[0] = (float)xfirst;  S.ub[0] = (float)cm;
+        S.p[3] = (float)c2;  S.lb[3] = (float)cm;  S.ub[3] = (float)xlast;
+        for (int k = 0; k < 2; ++k) {
+          S.p[3 * k + 1] = (float)gam0;  S.lb[3 * k + 1] = (float)(step / 2);  S.ub[3 * k + 1] = (float)(step * n / 2);
+          S.p[3 * k + 2] = (float)(ig / 2);  S.lb[3 * k + 2] = (float)(ig / 100);  S.ub[3 * k + 2] = (float)(mx * 1.5);
+        }
+      }
+      S.p[3 * n_p] = 0.5f;  S.lb[3 * n_p] = 0.0f;  S.ub[3 * n_p] = 1.0f;
+      S.p[3 * n_p + 1] = (float)bg0;  S.lb[3 * n_p + 1] = 0.0f;
+      S.ub[3 * n_p + 1] = (float)(bg0 > 0 ? bg0 * 1.5 : mx * 0.5);
+    }
+  }
+  __syncwarp();
+  // ---- LM with the step projected onto the bounds
+  double chi2 = job_eval(c.kind, S, n, np, n_p, S.p, true, lane);
+  double lam = 1e-3;
+  int it = 0, stall = 0;
+  for (; it < c.max_iter; ++it) {
+    int ok = 0;
+    if (lane == 0) {
+      ok = job_solve(S, np, lam) ? 1 : 0;
+      for (int u = 0; u < np; ++u) {
+        float v = ok ? (float)((double)S.p[u] + S.d[u]) : S.p[u];
+        S.pn[u] = fminf(fmaxf(v, S.lb[u]), S.ub[u]);
+      }
+    }
+    ok = __shfl_sync(0xffffffffu, ok, 0);
+    __syncwarp();
+    const double c2n = job_eval(c.kind, S, n, np, n_p, S.pn, false, lane);
+    if (ok && c2n <= chi2) {
+      double rel = 0.0;
+      for (int u = 0; u < np; ++u)
+        rel = fmax(rel, fabs((double)S.pn[u] - (double)S.p[u]) / fmax(fabs((double)S.p[u]), 1e-3));
+      const double dec = chi2 - c2n;
+      __syncwarp();
+      for (int u = lane; u < np; u += 32) S.p[u] = S.pn[u];
+      __syncwarp();
+      chi2 = job_eval(c.kind, S, n, np, n_p, S.p, true, lane);
+      lam = fmax(lam * 0.1, 1e-12);
+      if (rel < 1e-6 || dec <= 1e-9 * chi2) {
+        if (++stall >= 2) { ++it; break; }
+      } else {
+        stall = 0;
+      }
+    } else {
+      lam *= 10.0;
+      if (lam > 1e12) { ++it; break; }
+    }
+  }
+  // ---- outputs, FP64 (centres back to absolute x)
+  if (lane < n_p) {
+    const int k = lane, id = pk_id ? pk_id[jd.p0 + k] : jd.p0 + k;
+    double *o = out + (int64_t)id * MI_FIT_NOUT;
+    double center;
+    if (c.kind == MI_FIT_KIND_PEAKS) {
+      float F, et, t0, t1, t2, t3;
+      tch(S.p[4 * k + 2], S.p[4 * k + 3], &F, &et, &t0, &t1, &t2, &t3);
+      const double area = S.p[4 * k];
+      center = xref + (double)S.p[4 * k + 1];
+      const double sgm = (double)F * 0.42466090014400953;
+      o[0] = area;
+      o[1] = center;
+      o[2] = S.p[4 * k + 2];
+      o[3] = S.p[4 * k + 3];
+      o[4] = F;
+      o[5] = et;
+      o[6] = chi2 / fmax((double)(n - np), 1.0);
+      o[7] = area * (et * (2.0 / (3.141592653589793 * (double)F)) + (1.0 - et) * 0.3989422804014327 / sgm);
+      o[8] = S.p[4 * n_p];
+      o[9] = S.p[4 * n_p + 1];
+    } else {
+      center = xref + (double)S.p[3 * k];
+      const double rms = sqrt(chi2 / (double)n);
+      const double snr = rms > 0 ? (double)S.p[3 * k + 2] / rms : 1.0;
+      // the reference keeps a fit only when SNR > 1; area, sig, gam, FWHM, eta stay 0
+      if (snr > 1.0) {
+        o[1] = center;
+        o[6] = snr;
+        o[7] = S.p[3 * k + 2];
+        o[8] = S.p[3 * n_p + 1];
+        o[9] = 0.0;
+      } else {
+        center = 0.0;
+      }
+    }
+    o[10] = (center != 0.0 && c.px > 0 && c.lsd > 0) ? atan(center * c.px / c.lsd) * 57.29577951308232 : 0.0;
+    its[id] = it;
+  }
+  __syncwarp();
+}
+
 __global__ void __launch_bounds__(32 * kJobWarps) k_fit_job(const FitPlanArgs a) {
   extern __shared__ __align__(16) uint8_t fsm[];
   const int lane = threadIdx.x & 31, wl = threadIdx.x >> 5;
@@ -275,187 +468,250 @@ __global__ void __launch_bounds__(32 * kJobWarps) k_fit_job(const FitPlanArgs a)
       return;
     }
   }
-  for (int jb = 0; jb < a.n_jobs; ++jb) {
-    const FitJobDev jd = a.jobs[jb];
-    const int n = jd.s1 - jd.s0 + 1, n_p = jd.n_p;
-    const int np = a.kind == MI_FIT_KIND_PEAKS ? 4 * n_p + 2 : 3 * n_p + 2;
-    if (n <= np) {
-      // fewer samples than parameters: the job's peaks are not fit
-      for (int k = lane; k < n_p; k += 32) its[a.pk_id[jd.p0 + k]] = -2;
-      __syncwarp();
-      continue;
-    }
-    // window samples: x relative to the window's centre bin, normalised x, values
-    const int cb = (jd.s0 + jd.s1) / 2;
-    const double xref = a.x[cb], xlo = a.x[jd.s0], xhi = a.x[jd.s1];
-    const double xr = fmax(xhi - xlo, 1e-12);
-    for (int i = lane; i < n; i += 32) {
-      const double xi = a.x[jd.s0 + i];
-      S.xl[i] = (float)(xi - xref);
-      S.xn[i] = (float)(2.0 * (xi - xlo) / xr - 1.0);
-      S.y[i] = sample(jd.s0 + i);
-    }
-    __syncwarp();
-    // initial values and bounds (lane 0)
-    if (lane == 0) {
-      if (a.kind == MI_FIT_KIND_PEAKS) {
-        double rmax = -1e30, rmin = 1e30;
-        for (int i = 0; i < n; ++i) { rmax = fmax(rmax, S.y[i]); rmin = fmin(rmin, S.y[i]); }
-        const double range = fmax(rmax - rmin, 1.0);
-        const int bgw = max(1, min(5, n / 4));
-        double bgs = 0.0;
-        for (int i = 0; i < bgw; ++i) bgs += S.y[i] + S.y[n - 1 - i];
-        const double bg = bgs / (2.0 * bgw);   // pf_estimate_initial_params: same for every peak
-        for (int k = 0; k < n_p; ++k) {
-          const int loc = a.pk_bin[jd.p0 + k] - jd.s0;
-          double amp = S.y[loc] - bg;
-          if (amp <= 0) amp = S.y[loc];
-          const double hm = bg + 0.5 * amp;
-          int li = loc, ri = loc;
-          while (li > 0 && S.y[li] > hm) --li;
-          while (ri < n - 1 && S.y[ri] > hm) ++ri;
-          double fwb = (double)(ri - li);
-          if (!(fwb > 1.0)) fwb = 2.0;
-          const double fwx = fwb * a.x_bin;
-          const double fg0 = 0.5 * fwx;
-          double sg = (fg0 * 100.0) * (fg0 * 100.0) / 5.545177444479562;
-          if (sg < 1e-6) sg = 1.0;
-          double gm = fwx * 0.5 * 100.0;
-          if (gm < 0.01) gm = 1.0;
-          double ar = amp * fwx * 1.5;
-          if (ar <= 0) ar = range * a.x_bin;
-          const double c0 = a.pk_x[jd.p0 + k] - xref;
-          const double crange = fmax(fwx, (double)n * a.x_bin * 0.5);
-          double ahi = range * (double)n * a.x_bin * 2.0;
-          if (ahi < 1.0) ahi = 1.0;
-          const double shi = (a.x_bin * 2e4) * (a.x_bin * 2e4) / 5.545177444479562;
-          const double ghi = a.x_bin * 2e4;
-          const double lo4[4] = {0.0, c0 - crange, 1e-6, 0.01}, hi4[4] = {ahi, c0 + crange, shi, ghi};
-          double v4[4] = {fmax(fmin(ar, ahi * 0.9), 0.01), c0, fmax(fmin(sg, shi * 0.5), 2e-6),
-                          fmax(fmin(gm, ghi * 0.5), 0.02)};
-          for (int u = 0; u < 4; ++u) {
-            if (v4[u] <= lo4[u]) v4[u] = lo4[u] + (hi4[u] - lo4[u]) * 0.01;
-            if (v4[u] >= hi4[u]) v4[u] = hi4[u] - (hi4[u] - lo4[u]) * 0.01;
-            S.p[4 * k + u] = (float)v4[u];
-            S.lb[4 * k + u] = (float)lo4[u];
-            S.ub[4 * k + u] = (float)hi4[u];
-          }
-        }
-        double b0 = bg, b0lo = fmin(rmin - range * 0.5, -1.0), b0hi = rmax + range;
-        if (b0 <= b0lo) b0 = b0lo + 0.01;
-        if (b0 >= b0hi) b0 = b0hi - 0.01;
-        S.p[4 * n_p] = (float)b0;
-        S.lb[4 * n_p] = (float)b0lo;
-        S.ub[4 * n_p] = (float)b0hi;
-        S.p[4 * n_p + 1] = 0.0f;
-        S.lb[4 * n_p + 1] = (float)-range;
-        S.ub[4 * n_p + 1] = (float)range;
-      } else {
-        double bg0 = 0.5 * (S.y[0] + S.y[n - 1]);
-        if (bg0 < 0) bg0 = 0;
-        double mx = -1e20;
-        for (int i = 0; i < n; ++i) mx = fmax(mx, S.y[i]);
-        const double step = a.x_bin, gam0 = 3.0 * step;
-        const double xfirst = xlo - xref, xlast = xhi - xref;
-        if (n_p == 1) {
-          const double c0 = a.pk_x[jd.p0] - xref;
-          S.p[0] = (float)c0;  S.lb[0] = (float)xfirst;  S.ub[0] = (float)xlast;
-          S.p[1] = (float)gam0;  S.lb[1] = (float)(step / 2);  S.ub[1] = (float)(step * n / 2);
-          S.p[2] = (float)(mx - bg0);  S.lb[2] = (float)((mx - bg0) / 100);  S.ub[2] = (float)(mx * 1.5);
-        } else {
-          double ig = mx - bg0;
-          if (ig < 1e-6) ig = 1e-6;
-          const double c1 = a.pk_x[jd.p0] - xref, c2 = a.pk_x[jd.p0 + 1] - xref, cm = 0.5 * (c1 + c2);
-          S.p[0] = (float)c1;  S.lb[0] = (float)xfirst;  S.ub[0] = (float)cm;
-          S.p[3] = (float)c2;  S.lb[3] = (float)cm;  S.ub[3] = (float)xlast;
-          for (int k = 0; k < 2; ++k) {
-            S.p[3 * k + 1] = (float)gam0;  S.lb[3 * k + 1] = (float)(step / 2);  S.ub[3 * k + 1] = (float)(step * n / 2);
-            S.p[3 * k + 2] = (float)(ig / 2);  S.lb[3 * k + 2] = (float)(ig / 100);  S.ub[3 * k + 2] = (float)(mx * 1.5);
-          }
-        }
-        S.p[3 * n_p] = 0.5f;  S.lb[3 * n_p] = 0.0f;  S.ub[3 * n_p] = 1.0f;
-        S.p[3 * n_p + 1] = (float)bg0;  S.lb[3 * n_p + 1] = 0.0f;
-        S.ub[3 * n_p + 1] = (float)(bg0 > 0 ? bg0 * 1.5 : mx * 0.5);
+  const JobParams c{a.kind, a.max_iter, a.x_bin, a.px, a.lsd, a.x};
+  for (int jb = 0; jb < a.n_jobs; ++jb)
+    fit_one_job(c, S, a.jobs[jb], a.pk_x, a.pk_bin, a.pk_id, sample, out, its, lane);
+}
+
+// ---- automatic peak detection + fit of each lineout (fitPeaksAutoDetect, PeakFit.c:720-877)
+//
+// One block per lineout.  SNIP background (Morhac's LLS-transformed iterative clipping,
+// pf_snip_background, PeakFit.c:549-590), background-subtracted profile clipped at 0;
+// Savitzky-Golay smoothing (quadratic, 7 points) and its negative second difference;
+// candidates = positive local maxima of that curve on a positive profile, with the
+// prominence over +-minSep bins (minSep = max(3, 3 x_bin / bin width)); the most prominent
+// candidates taken greedily at least minSep bins apart, up to min(3 max_peaks, n / 2); their
+// fitPeaks jobs (overlapping ROIs merged) fit on the corrected profile; then the quality
+// filter: area and FWHM > 0, FWHM <= max(5 x median, 2 x_bin) when more than two remain,
+// the max_peaks largest areas, in position order.
+constexpr int kAutoThreads = 128;
+
+struct AutoArgs {
+  const double *x, *lineouts;
+  int F, n_x, max_peaks, over, pad, snip, max_iter, fit_warps, n_max, np_max;
+  double x_bin, px, lsd;
+  double *out;
+  int32_t *found;
+  uint32_t warp_bytes, off_job;
+};
+
+__host__ __device__ inline uint32_t auto_smem(int n, int over, uint32_t warp_bytes, int fit_warps, uint32_t *off_job) {
+  auto a16 = [](uint32_t x) { return (x + 15u) & ~15u; };
+  uint32_t o = 0;
+  o = a16(o + 8u * n);                          // corrected profile
+  o = a16(o + 8u * n);                          // SNIP v / negative second difference
+  o = a16(o + 8u * n);                          // copy / smoothed / prominence
+  o = a16(o + 4u * (uint32_t)(n / 2 + 1));      // candidates: bins
+  o = a16(o + 8u * (uint32_t)(n / 2 + 1));      //   prominences
+  o = a16(o + 4u * (uint32_t)over);             // selected bins
+  o = a16(o + 16u * (uint32_t)over);            // jobs
+  o = a16(o + 8u * (uint32_t)over);             // peak x
+  o = a16(o + 8u * MI_FIT_NOUT * (uint32_t)over);  // fits of the detected peaks
+  o = a16(o + 4u * (uint32_t)over);             // their iteration counts
+  o = a16(o + 16u * (uint32_t)over);            // filter entries
+  o = a16(o + 64u);                             // counters
+  *off_job = o;
+  return o + warp_bytes * (uint32_t)fit_warps;
+}
+
+__global__ void __launch_bounds__(kAutoThreads) k_fit_autodetect(const AutoArgs a) {
+  extern __shared__ __align__(16) uint8_t sm[];
+  auto a16 = [](uint32_t x) { return (x + 15u) & ~15u; };
+  const int n = a.n_x, over = a.over, tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+  const int64_t f = blockIdx.x;
+  uint32_t o = 0;
+  double *corr = (double *)(sm + o);  o = a16(o + 8u * n);
+  double *v = (double *)(sm + o);     o = a16(o + 8u * n);
+  double *t = (double *)(sm + o);     o = a16(o + 8u * n);
+  int32_t *cbin = (int32_t *)(sm + o);  o = a16(o + 4u * (uint32_t)(n / 2 + 1));
+  double *cprom = (double *)(sm + o);   o = a16(o + 8u * (uint32_t)(n / 2 + 1));
+  int32_t *sel = (int32_t *)(sm + o);   o = a16(o + 4u * (uint32_t)over);
+  FitJobDev *jobs = (FitJobDev *)(sm + o);  o = a16(o + 16u * (uint32_t)over);
+  double *pkx = (double *)(sm + o);     o = a16(o + 8u * (uint32_t)over);
+  double *raw = (double *)(sm + o);     o = a16(o + 8u * MI_FIT_NOUT * (uint32_t)over);
+  int32_t *rit = (int32_t *)(sm + o);   o = a16(o + 4u * (uint32_t)over);
+  double2 *ent = (double2 *)(sm + o);   o = a16(o + 16u * (uint32_t)over);   // (area, fwhm) per kept entry
+  int32_t *cnt = (int32_t *)(sm + o);   // [0] candidates, [1] selected, [2] jobs, [3] kept, [4] argmax bin
+  const double *y = a.lineouts + f * (int64_t)n;
+  double *out = a.out + f * (int64_t)a.max_peaks * MI_FIT_NOUT;
+  for (int i = tid; i < a.max_peaks * MI_FIT_NOUT; i += kAutoThreads) out[i] = 0.0;
+  // ---- SNIP background
+  if (a.snip > 0) {
+    for (int i = tid; i < n; i += kAutoThreads) v[i] = log(log(sqrt(fmax(y[i], 0.0) + 1.0) + 1.0) + 1.0);
+    __syncthreads();
+    for (int p = a.snip; p >= 1; --p) {
+      for (int i = tid; i < n; i += kAutoThreads) t[i] = v[i];
+      __syncthreads();
+      for (int i = p + tid; i < n - p; i += kAutoThreads) {
+        const double avg = (t[i - p] + t[i + p]) / 2.0;
+        if (v[i] > avg) v[i] = avg;
       }
+      __syncthreads();
     }
-    __syncwarp();
-    // ---- LM with the step projected onto the bounds
-    double chi2 = job_eval(a, S, n, np, n_p, S.p, true, lane);
-    double lam = 1e-3;
-    int it = 0, stall = 0;
-    for (; it < a.max_iter; ++it) {
-      int ok = 0;
-      if (lane == 0) {
-        ok = job_solve(S, np, lam) ? 1 : 0;
-        for (int u = 0; u < np; ++u) {
-          float v = ok ? (float)((double)S.p[u] + S.d[u]) : S.p[u];
-          S.pn[u] = fminf(fmaxf(v, S.lb[u]), S.ub[u]);
-        }
-      }
-      ok = __shfl_sync(0xffffffffu, ok, 0);
-      __syncwarp();
-      const double c2n = job_eval(a, S, n, np, n_p, S.pn, false, lane);
-      if (ok && c2n <= chi2) {
-        double rel = 0.0;
-        for (int u = 0; u < np; ++u)
-          rel = fmax(rel, fabs((double)S.pn[u] - (double)S.p[u]) / fmax(fabs((double)S.p[u]), 1e-3));
-        const double dec = chi2 - c2n;
-        __syncwarp();
-        for (int u = lane; u < np; u += 32) S.p[u] = S.pn[u];
-        __syncwarp();
-        chi2 = job_eval(a, S, n, np, n_p, S.p, true, lane);
-        lam = fmax(lam * 0.1, 1e-12);
-        if (rel < 1e-6 || dec <= 1e-9 * chi2) {
-          if (++stall >= 2) { ++it; break; }
-        } else {
-          stall = 0;
-        }
-      } else {
-        lam *= 10.0;
-        if (lam > 1e12) { ++it; break; }
-      }
+    for (int i = tid; i < n; i += kAutoThreads) {
+      const double w = exp(exp(v[i]) - 1.0) - 1.0;
+      corr[i] = fmax(y[i] - fmax(w * w - 1.0, 0.0), 0.0);
     }
-    // ---- outputs, FP64 (centres back to absolute x)
-    if (lane < n_p) {
-      const int k = lane, id = a.pk_id[jd.p0 + k];
-      double *o = out + (int64_t)id * MI_FIT_NOUT;
-      double center;
-      if (a.kind == MI_FIT_KIND_PEAKS) {
-        float F, et, t0, t1, t2, t3;
-        tch(S.p[4 * k + 2], S.p[4 * k + 3], &F, &et, &t0, &t1, &t2, &t3);
-        const double area = S.p[4 * k];
-        center = xref + (double)S.p[4 * k + 1];
-        const double sgm = (double)F * 0.42466090014400953;
-        o[0] = area;
-        o[1] = center;
-        o[2] = S.p[4 * k + 2];
-        o[3] = S.p[4 * k + 3];
-        o[4] = F;
-        o[5] = et;
-        o[6] = chi2 / fmax((double)(n - np), 1.0);
-        o[7] = area * (et * (2.0 / (3.141592653589793 * (double)F)) + (1.0 - et) * 0.3989422804014327 / sgm);
-        o[8] = S.p[4 * n_p];
-        o[9] = S.p[4 * n_p + 1];
-      } else {
-        center = xref + (double)S.p[3 * k];
-        const double rms = sqrt(chi2 / (double)n);
-        const double snr = rms > 0 ? (double)S.p[3 * k + 2] / rms : 1.0;
-        // the reference keeps a fit only when SNR > 1; area, sig, gam, FWHM, eta stay 0
-        if (snr > 1.0) {
-          o[1] = center;
-          o[6] = snr;
-          o[7] = S.p[3 * k + 2];
-          o[8] = S.p[3 * n_p + 1];
-          o[9] = 0.0;
-        } else {
-          center = 0.0;
-        }
-      }
-      o[10] = (center != 0.0 && a.px > 0 && a.lsd > 0) ? atan(center * a.px / a.lsd) * 57.29577951308232 : 0.0;
-      its[id] = it;
-    }
-    __syncwarp();
+  } else {
+    for (int i = tid; i < n; i += kAutoThreads) corr[i] = fmax(y[i], 0.0);
   }
+  if (tid < 8) cnt[tid] = 0;
+  __syncthreads();
+  const bool detect = n >= 10 && a.max_peaks > 0;
+  // ---- smoothing (Savitzky-Golay, quadratic, window 7) and its negative second difference
+  if (detect) {
+    for (int i = tid; i < n; i += kAutoThreads) {
+      if (i < 3 || i >= n - 3) {
+        t[i] = corr[i];
+      } else {
+        t[i] = (-2.0 * corr[i - 3] + 3.0 * corr[i - 2] + 6.0 * corr[i - 1] + 7.0 * corr[i] + 6.0 * corr[i + 1] +
+                3.0 * corr[i + 2] - 2.0 * corr[i + 3]) / 21.0;
+      }
+    }
+    __syncthreads();
+    for (int i = tid; i < n; i += kAutoThreads)
+      v[i] = (i >= 1 && i < n - 1) ? -(t[i + 1] - 2.0 * t[i] + t[i - 1]) : 0.0;
+    __syncthreads();
+  }
+  const double bw = n > 1 ? fabs(a.x[1] - a.x[0]) : 1.0;
+  const int msep = (int)fmax(3.0, (a.x_bin * 3.0) / bw);
+  // ---- candidates and their prominence (NaN: not a candidate)
+  if (detect) {
+    for (int i = tid; i < n; i += kAutoThreads) {
+      double pr = __longlong_as_double(0x7ff8000000000000ll);
+      if (i >= 2 && i < n - 2 && v[i] > 0 && v[i] >= v[i - 1] && v[i] >= v[i + 1] && corr[i] > 0) {
+        double lm = v[i], rm = v[i];
+        for (int j = i - 1; j >= 0 && j >= i - msep; --j) lm = fmin(lm, v[j]);
+        for (int j = i + 1; j < n && j <= i + msep; ++j) rm = fmin(rm, v[j]);
+        pr = v[i] - fmax(lm, rm);
+        if (pr < 0) pr = v[i];
+      }
+      t[i] = pr;
+    }
+    __syncthreads();
+    if (tid == 0) {
+      // in bin order, at most n / 2 (the reference's candidate buffer)
+      int nc = 0;
+      for (int i = 0; i < n && nc < n / 2; ++i)
+        if (!isnan(t[i])) { cbin[nc] = i; cprom[nc] = t[i]; ++nc; }
+      cnt[0] = nc;
+    }
+    __syncthreads();
+  }
+  // ---- greedy selection by prominence, at least msep bins apart
+  const int nc = cnt[0];
+  for (;;) {
+    if (!detect || cnt[1] >= over) break;
+    // the most prominent remaining candidate (lowest bin on ties)
+    double best = -1e300;
+    int bi = -1;
+    for (int c = tid; c < nc; c += kAutoThreads)
+      if (cbin[c] >= 0 && (bi < 0 || cprom[c] > best || (cprom[c] == best && cbin[c] < cbin[bi]))) {
+        best = cprom[c];
+        bi = c;
+      }
+    for (int off = 16; off > 0; off >>= 1) {
+      const double ob = __shfl_xor_sync(0xffffffffu, best, off);
+      const int oi = __shfl_xor_sync(0xffffffffu, bi, off);
+      if (oi >= 0 && (bi < 0 || ob > best || (ob == best && cbin[oi] < cbin[bi]))) { best = ob; bi = oi; }
+    }
+    __shared__ double s_best[kAutoThreads / 32];
+    __shared__ int s_bi[kAutoThreads / 32];
+    if (lane == 0) { s_best[wid] = best; s_bi[wid] = bi; }
+    __syncthreads();
+    if (tid == 0) {
+      int b2 = -1;
+      double bb = -1e300;
+      for (int w = 0; w < kAutoThreads / 32; ++w) {
+        const int oi = s_bi[w];
+        if (oi >= 0 && (b2 < 0 || s_best[w] > bb || (s_best[w] == bb && cbin[oi] < cbin[b2]))) { bb = s_best[w]; b2 = oi; }
+      }
+      cnt[4] = b2;
+      if (b2 >= 0) {
+        const int bin = cbin[b2];
+        bool close = false;
+        for (int k = 0; k < cnt[1]; ++k) close = close || abs(bin - sel[k]) < msep;
+        if (!close) sel[cnt[1]++] = bin;
+        cbin[b2] = -1;   // taken or discarded
+      }
+    }
+    __syncthreads();
+    if (cnt[4] < 0) break;
+  }
+  // ---- sort the selected by position; fitPeaks jobs on the corrected profile
+  if (tid == 0) {
+    const int ns = cnt[1];
+    for (int i = 1; i < ns; ++i)
+      for (int j = i; j > 0 && sel[j] < sel[j - 1]; --j) { const int q = sel[j]; sel[j] = sel[j - 1]; sel[j - 1] = q; }
+    int nj = 0;
+    for (int k = 0; k < ns; ++k) {
+      const int b = sel[k], s0 = max(0, b - a.pad), s1 = min(n - 1, b + a.pad);
+      pkx[k] = a.x[b];
+      if (nj > 0 && s0 <= jobs[nj - 1].s1 && jobs[nj - 1].n_p < MI_FIT_JOB_MAX_PEAKS) {
+        jobs[nj - 1].s1 = s1;
+        jobs[nj - 1].n_p++;
+      } else {
+        jobs[nj++] = FitJobDev{s0, s1, 1, k};
+      }
+    }
+    cnt[2] = nj;
+  }
+  __syncthreads();
+  const int ns = cnt[1];
+  for (int i = tid; i < ns * MI_FIT_NOUT; i += kAutoThreads) raw[i] = 0.0;
+  for (int i = tid; i < ns; i += kAutoThreads) rit[i] = -1;
+  __syncthreads();
+  if (wid < a.fit_warps) {
+    JobSmem S;
+    job_warp_bytes(a.n_max, a.np_max, &S, sm + a.off_job + (size_t)wid * a.warp_bytes);
+    const JobParams c{MI_FIT_KIND_PEAKS, a.max_iter, a.x_bin, a.px, a.lsd, a.x};
+    auto sample = [&](int i) -> double { return corr[i]; };
+    for (int jb = wid; jb < cnt[2]; jb += a.fit_warps)
+      fit_one_job(c, S, jobs[jb], pkx, sel, nullptr, sample, raw, rit, lane);
+  }
+  __syncthreads();
+  // ---- quality filter and output (thread 0; a few dozen entries)
+  if (tid == 0) {
+    int nv = 0;
+    for (int i = 0; i < ns; ++i) {
+      const double ar = fabs(raw[i * MI_FIT_NOUT]), fw = raw[i * MI_FIT_NOUT + 4];
+      if (ar > 0 && fw > 0) {
+        sel[nv] = i;                  // the entry's index among the detected peaks
+        ent[nv] = make_double2(ar, fw);
+        ++nv;
+      }
+    }
+    if (nv > 2) {
+      // median FWHM: the middle of the sorted FWHMs (index nv / 2)
+      for (int i = 0; i < nv; ++i) t[i] = ent[i].y;
+      for (int i = 1; i < nv; ++i)
+        for (int j = i; j > 0 && t[j] < t[j - 1]; --j) { const double q = t[j]; t[j] = t[j - 1]; t[j - 1] = q; }
+      const double cap = fmax(5.0 * t[nv / 2], a.x_bin * 2.0);
+      int d = 0;
+      for (int i = 0; i < nv; ++i)
+        if (ent[i].y <= cap) { sel[d] = sel[i]; ent[d] = ent[i]; ++d; }
+      nv = d;
+    }
+    if (nv > a.max_peaks) {
+      // the largest areas first (exchange sort, as the reference orders them), keep max_peaks
+      for (int i = 0; i < nv - 1; ++i)
+        for (int j = i + 1; j < nv; ++j)
+          if (ent[j].x > ent[i].x) {
+            const double2 q = ent[i]; ent[i] = ent[j]; ent[j] = q;
+            const int qi = sel[i]; sel[i] = sel[j]; sel[j] = qi;
+          }
+      nv = a.max_peaks;
+    }
+    for (int i = 1; i < nv; ++i)
+      for (int j = i; j > 0 && sel[j] < sel[j - 1]; --j) {
+        const int qi = sel[j]; sel[j] = sel[j - 1]; sel[j - 1] = qi;
+      }
+    cnt[3] = nv;
+    a.found[f] = nv;
+  }
+  __syncthreads();
+  for (int i = tid; i < cnt[3] * MI_FIT_NOUT; i += kAutoThreads)
+    out[i] = raw[sel[i / MI_FIT_NOUT] * MI_FIT_NOUT + i % MI_FIT_NOUT];
 }
 
 }  // namespace mi
@@ -711,4 +967,46 @@ extern "C" void mi_fit_plan_destroy(mi_fit_plan *fp) {
   fit_plan_free(fp);
   cudaSetDevice(prev);
   delete fp;
+}
+
+extern "C" int mi_fit_autodetect(const double *x, const double *lineouts, int n_frames, int n_x, int max_peaks,
+                                 double x_bin, int roi_padding, int snip_iter, double px_um, double lsd_um,
+                                 double *out, int32_t *n_found, void *stream) {
+  if (!x || !lineouts || !out || !n_found) return set_error(MI_E_ARG, "mi_fit_autodetect: null argument");
+  if (n_frames < 0 || n_x < 0 || max_peaks < 0 || roi_padding < 1 || !(x_bin > 0))
+    return set_error(MI_E_ARG, "mi_fit_autodetect: bad sizes or bin width");
+  if (n_frames == 0 || n_x == 0 || max_peaks == 0) return MI_OK;
+  AutoArgs a;
+  a.x = x;
+  a.lineouts = lineouts;
+  a.F = n_frames;
+  a.n_x = n_x;
+  a.max_peaks = max_peaks;
+  a.over = std::max(1, std::min(max_peaks * 3, n_x / 2));
+  a.pad = roi_padding;
+  a.snip = snip_iter;
+  a.max_iter = 200;
+  a.x_bin = x_bin;
+  a.px = px_um;
+  a.lsd = lsd_um;
+  a.out = out;
+  a.found = n_found;
+  a.n_max = std::min(n_x, MI_FIT_JOB_MAX_PEAKS * (2 * roi_padding + 1));
+  a.np_max = 4 * MI_FIT_JOB_MAX_PEAKS + 2;
+  a.warp_bytes = job_warp_bytes(a.n_max, a.np_max, nullptr, nullptr);
+  int dev = 0, dev_smem = 0;
+  MI_CUDA(cudaGetDevice(&dev));
+  MI_CUDA(cudaDeviceGetAttribute(&dev_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+  uint32_t total = 0;
+  for (a.fit_warps = kAutoThreads / 32; a.fit_warps >= 1; --a.fit_warps) {
+    total = auto_smem(n_x, a.over, a.warp_bytes, a.fit_warps, &a.off_job);
+    if (total <= (uint32_t)dev_smem) break;
+  }
+  if (a.fit_warps < 1)
+    return set_error(MI_E_RANGE, "mi_fit_autodetect: %d samples with +-%d-bin windows need %u B of shared memory",
+                     n_x, roi_padding, total);
+  MI_CUDA(cudaFuncSetAttribute(k_fit_autodetect, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)total));
+  k_fit_autodetect<<<(unsigned)n_frames, kAutoThreads, total, (cudaStream_t)stream>>>(a);
+  MI_CUDA(cudaGetLastError());
+  return MI_OK;
 }

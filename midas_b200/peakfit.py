@@ -168,6 +168,38 @@ def fit_peaks(x, intensity, peak_locations, *, x_bin_size: float, fit_roi_paddin
     return rows
 
 
+@dataclass
+class AutoResult:
+    params: torch.Tensor   # [F, max_peaks, 11] float64, first n_found[f] rows filled
+    n_found: torch.Tensor  # [F] int32
+
+
+def fit_autodetect(x: torch.Tensor, lineouts: torch.Tensor, *, max_peaks: int, x_bin: float,
+                   roi_padding: int = 20, snip_iter: int = 50, px_um: float = 0.0, lsd_um: float = 0.0,
+                   stream=None) -> AutoResult:
+    """fitPeaksAutoDetect (FF_HEDM/src/PeakFit.c:720-877) of every lineout on the device:
+    SNIP background, peak detection, joint TCH fits on the background-subtracted profile,
+    the reference's quality filter; rows in position order."""
+    dev = lineouts.device
+    if dev.type != "cuda":
+        raise RuntimeError("fit_autodetect runs on a CUDA device")
+    lo = lineouts.to(torch.float64).contiguous()
+    if lo.dim() == 1:
+        lo = lo.unsqueeze(0)
+    xs = x.to(dev, torch.float64).contiguous()
+    F, n_x = lo.shape
+    if xs.numel() != n_x:
+        raise ValueError("x and lineouts disagree in length")
+    out = torch.zeros((F, max(max_peaks, 0), L.FIT_NOUT), dtype=torch.float64, device=dev)
+    found = torch.zeros(F, dtype=torch.int32, device=dev)
+    with torch.cuda.device(dev):
+        L.check(L.lib().mi_fit_autodetect(xs.data_ptr(), lo.data_ptr(), F, n_x, int(max_peaks), float(x_bin),
+                                          int(roi_padding), int(snip_iter), float(px_um), float(lsd_um),
+                                          out.data_ptr(), found.data_ptr(), L.stream_ptr(stream)),
+                "mi_fit_autodetect")
+    return AutoResult(out, found)
+
+
 PEAK_ROW_DTYPE = np.dtype([("frame_idx", "<i4"), ("eta_idx", "<i4"), ("peak_nr", "<i4"), ("eta_deg", "<f8"),
                            ("area", "<f8"), ("sig", "<f8"), ("gam", "<f8"), ("FWHM_deg", "<f8"),
                            ("eta_mix", "<f8"), ("chi_sq", "<f8"), ("center_2theta", "<f8"),

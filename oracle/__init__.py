@@ -53,6 +53,8 @@ def lib() -> C.CDLL:
         L.or_profile.restype = None
         L.or_profile_omp.argtypes = [vp, vp, i, i, vp, vp]
         L.or_profile_omp.restype = None
+        L.or_snip_detect.argtypes = [vp, vp, i, i, d, i, vp, vp]
+        L.or_snip_detect.restype = i
         L.or_fit.argtypes = [vp, vp, i, d, i, i, i, d, d, d, vp]
         L.or_fit.restype = i
         _lib = L
@@ -184,6 +186,17 @@ def area_in(records, nmap, n_bins, ny, nz):
     out = np.zeros(n_bins)
     lib().or_area_in(rec.ctypes.data if rec.size else None, nm.ctypes.data, n_bins, ny, nz, out.ctypes.data)
     return out
+
+
+def snip_detect(x, y, *, n_iter=50, x_bin=1.0, max_sel=30):
+    """fitPeaksAutoDetect's SNIP background and detection: (corrected profile, selected bins)."""
+    xs = _c(x, np.float64)
+    ys = _c(y, np.float64)
+    corr = np.zeros(ys.size)
+    sel = np.zeros(max(max_sel, 1), np.int32)
+    k = lib().or_snip_detect(xs.ctypes.data, ys.ctypes.data, ys.size, int(n_iter), float(x_bin), int(max_sel),
+                             corr.ctypes.data, sel.ctypes.data)
+    return corr, sel[:k].copy()
 
 
 def profile_omp(cake, area, n_r, n_eta):

@@ -555,3 +555,79 @@ int or_fit(const double *x, const double *y, int n_x, double loc, int half, int 
   out[10] = (px > 0 && lsd > 0) ? atan(center * px / lsd) * 57.29577951308232 : 0.0;
   return it;
 }
+
+/* ------------------------------------------------------------------ peak detection
+ * or_snip_detect restates fitPeaksAutoDetect's detection (FF_HEDM/src/PeakFit.c:549-755):
+ * SNIP background on the log-log-sqrt transformed profile (Morhac's LLS clipping with
+ * windows n_iter .. 1), the background-subtracted profile clipped at 0 (corrected), a
+ * 7-point quadratic Savitzky-Golay smoothing, its negative second difference, candidates
+ * at its positive local maxima where the corrected profile is positive, prominence over
+ * +-min_sep bins, greedy selection by prominence (ties: lower bin) at least min_sep bins
+ * apart, up to max_sel, returned in bin order.  Returns the number selected. */
+int or_snip_detect(const double *x, const double *y, int n, int n_iter, double x_bin, int max_sel, double *corrected,
+                   int *sel) {
+  double *v = (double *)malloc(sizeof(double) * (n > 0 ? n : 1));
+  double *t = (double *)malloc(sizeof(double) * (n > 0 ? n : 1));
+  for (int i = 0; i < n; ++i) v[i] = log(log(sqrt(fmax(y[i], 0.0) + 1.0) + 1.0) + 1.0);
+  for (int p = n_iter; p >= 1; --p) {
+    memcpy(t, v, sizeof(double) * n);
+    for (int i = p; i < n - p; ++i) {
+      const double avg = (t[i - p] + t[i + p]) / 2.0;
+      if (v[i] > avg) v[i] = avg;
+    }
+  }
+  for (int i = 0; i < n; ++i) {
+    double bg = 0.0;
+    if (n_iter > 0) {
+      const double w = exp(exp(v[i]) - 1.0) - 1.0;
+      bg = fmax(w * w - 1.0, 0.0);
+    }
+    corrected[i] = fmax(y[i] - bg, 0.0);
+  }
+  int ns = 0;
+  if (n >= 10 && max_sel > 0) {
+    static const double c7[7] = {-2, 3, 6, 7, 6, 3, -2};
+    for (int i = 0; i < n; ++i) {
+      if (i < 3 || i >= n - 3) t[i] = corrected[i];
+      else {
+        double s = 0;
+        for (int j = 0; j < 7; ++j) s += c7[j] * corrected[i - 3 + j];
+        t[i] = s / 21.0;
+      }
+    }
+    for (int i = 0; i < n; ++i) v[i] = (i >= 1 && i < n - 1) ? -(t[i + 1] - 2.0 * t[i] + t[i - 1]) : 0.0;
+    const double bw = n > 1 ? fabs(x[1] - x[0]) : 1.0;
+    const int msep = (int)fmax(3.0, x_bin * 3.0 / bw);
+    int *cb = (int *)malloc(sizeof(int) * (n / 2 + 1));
+    double *cp = (double *)malloc(sizeof(double) * (n / 2 + 1));
+    int nc = 0;
+    for (int i = 2; i < n - 2 && nc < n / 2; ++i)
+      if (v[i] > 0 && v[i] >= v[i - 1] && v[i] >= v[i + 1] && corrected[i] > 0) {
+        double lm = v[i], rm = v[i];
+        for (int j = i - 1; j >= 0 && j >= i - msep; --j) lm = fmin(lm, v[j]);
+        for (int j = i + 1; j < n && j <= i + msep; ++j) rm = fmin(rm, v[j]);
+        double pr = v[i] - fmax(lm, rm);
+        if (pr < 0) pr = v[i];
+        cb[nc] = i;
+        cp[nc] = pr;
+        ++nc;
+      }
+    while (ns < max_sel) {
+      int bi = -1;
+      for (int c = 0; c < nc; ++c)
+        if (cb[c] >= 0 && (bi < 0 || cp[c] > cp[bi] || (cp[c] == cp[bi] && cb[c] < cb[bi]))) bi = c;
+      if (bi < 0) break;
+      int close = 0;
+      for (int k = 0; k < ns; ++k) close |= abs(cb[bi] - sel[k]) < msep;
+      if (!close) sel[ns++] = cb[bi];
+      cb[bi] = -1;
+    }
+    for (int i = 1; i < ns; ++i)
+      for (int j = i; j > 0 && sel[j] < sel[j - 1]; --j) { const int q = sel[j]; sel[j] = sel[j - 1]; sel[j - 1] = q; }
+    free(cb);
+    free(cp);
+  }
+  free(v);
+  free(t);
+  return ns;
+}

@@ -53,4 +53,10 @@ void or_profile_omp(const double *cake, const double *area_in, int n_r, int n_et
 int or_fit(const double *x, const double *y, int n_x, double peak, int half_window, int model,
            int max_iter, double x_bin, double px_um, double lsd_um, double *out);
 
+/* fitPeaksAutoDetect's background subtraction and peak detection (SNIP, Savitzky-Golay,
+ * prominence, greedy separation): corrected [n] and up to max_sel selected bins; returns
+ * their number */
+int or_snip_detect(const double *x, const double *y, int n, int n_iter, double x_bin, int max_sel,
+                   double *corrected, int *sel);
+
 #endif

@@ -120,3 +120,43 @@ def test_eta_fits_match_bounded_least_squares(cuda):
                     assert abs(out[s, k, 6] - snr) <= 1e-4 * snr, (f, e, k, out[s, k, 6], snr)
                     assert abs(out[s, k, 10] - np.degrees(np.arctan(c * 200.0 / 1e6))) <= 1e-7
     fp.close()
+
+
+def test_autodetect_matches_oracle_detection_and_fit_plan(cuda):
+    """fitPeaksAutoDetect on the device: the peaks it keeps are the oracle's detected bins
+    (SNIP + detection restated in FP64 on the CPU), fit jointly on the background-
+    subtracted profile exactly as a fit plan fits them, after the reference's filter."""
+    import oracle
+    rng = np.random.default_rng(9)
+    n, F, max_peaks = 800, 5, 4
+    x = 20.0 + 0.25 * (np.arange(n) + 0.5)
+    Y = []
+    for f in range(F):
+        y = 300.0 + 40.0 * np.sin(x / 60.0) + 0.1 * (x - x[0])
+        for k, c in enumerate((40.2, 75.9, 78.4, 110.3, 180.6)):
+            w = 0.8 + 0.2 * k
+            y = y + (400.0 + 150 * k + 30 * f) * np.exp(-0.5 * ((x - c - 0.05 * f) / w) ** 2)
+        Y.append(y + rng.normal(0, 0.5, n))
+    Y = np.array(Y)
+    r = peakfit.fit_autodetect(torch.from_numpy(x).to(cuda), torch.from_numpy(Y).to(cuda), max_peaks=max_peaks,
+                               x_bin=0.25, roi_padding=20, snip_iter=50)
+    out, found = r.params.cpu().numpy(), r.n_found.cpu().numpy()
+    for f in range(F):
+        corr, sel = oracle.snip_detect(x, Y[f], n_iter=50, x_bin=0.25, max_sel=min(3 * max_peaks, n // 2))
+        fp = FitPlan(x, x[sel], kind="peaks", half_window=20, x_bin=0.25, device=cuda)
+        ref = fp.run(torch.from_numpy(corr[None]).to(cuda)).params[0].cpu().numpy()
+        fp.close()
+        # the reference's filter, restated: |area| > 0 and FWHM > 0, FWHM <= max(5 median, 2 bins),
+        # the largest areas, position order
+        keep = [i for i in range(len(sel)) if abs(ref[i, 0]) > 0 and ref[i, 4] > 0]
+        if len(keep) > 2:
+            med = np.sort(ref[keep, 4])[len(keep) // 2]
+            keep = [i for i in keep if ref[i, 4] <= max(5 * med, 0.5)]
+        if len(keep) > max_peaks:
+            keep = sorted(keep, key=lambda i: -abs(ref[i, 0]))[:max_peaks]
+        keep = sorted(keep)
+        assert found[f] == len(keep), (f, found[f], keep)
+        for j, i in enumerate(keep):
+            assert abs(out[f, j, 1] - ref[i, 1]) <= 1e-4, (f, j, out[f, j, 1], ref[i, 1])
+            assert abs(out[f, j, 4] - ref[i, 4]) <= 1e-4 * ref[i, 4]
+        assert not out[f, found[f]:].any()
