@@ -302,6 +302,7 @@ def main_ours(args):
         del sample
         args.tile_rows, args.run_len, args.tile_pixels = (tuned.best["tile_rows"], tuned.best["run_len"],
                                                           tuned.best["tile_pixels"])
+        args.encoding = tuned.best["encoding"]
     t1 = time.time()
     plan = CakePlan(pm, n_r=w.n_r, n_eta=w.n_eta, n_pixels_y=ny, n_pixels_z=nz, mode=w.mode,
                     bc_y=w.mapper.BC_y, bc_z=w.mapper.BC_z, device=dev,

@@ -1,7 +1,11 @@
-"""Autotuner of the batched caking plan: picks the tile shape and register-run length for a
-map by timing candidate plans on the device.
+"""Autotuner of the batched caking plan: picks the encoding, tile shape and register-run
+length for a map by timing candidate plans on the device.
 
 The knobs (all plan options of ``CakePlan``):
+  encoding     'mmad' (tensor cores, frames read in place), 'mma' (tensor cores, frames
+               transposed into byte planes first), 'runs' (CUDA cores); the tensor-core
+               encodings are candidates for 8/16-bit frames only, and their tiles (12 R rows x
+               4 eta columns, 128 frames a pass) are fixed by the kernels;
   tile_rows    R rows per strip (8 or 16): the register block of a consumer warp (bins per
                warp along R) and, with the pixel cap, the tile shape;
   run_len      rows per run record (2, 4, 8; 0 = the plan's own choice from the map's run
@@ -28,6 +32,10 @@ import torch
 from . import _lib as L
 from .kernels import CakePlan
 
+TENSOR_CANDIDATES = [
+    {"encoding": "mmad", "tile_rows": 0, "run_len": 0, "tile_pixels": 0},
+    {"encoding": "mma", "tile_rows": 0, "run_len": 0, "tile_pixels": 0},
+]
 DEFAULT_CANDIDATES = [
     {"tile_rows": 16, "run_len": 0, "tile_pixels": 0},
     {"tile_rows": 16, "run_len": 4, "tile_pixels": 0},
@@ -74,7 +82,11 @@ def tune(pixmap, frames: torch.Tensor, *, n_r: int, n_eta: int, n_pixels_y: int,
             return _CACHE[key]
     table = []
     stream = torch.cuda.current_stream()
-    for cand in (candidates or DEFAULT_CANDIDATES):
+    if candidates is None:
+        candidates = list(DEFAULT_CANDIDATES)
+        if frames.dtype in (torch.uint8, torch.uint16):
+            candidates = TENSOR_CANDIDATES + candidates
+    for cand in candidates:
         row = dict(cand)
         try:
             plan = CakePlan(pixmap, n_r=n_r, n_eta=n_eta, n_pixels_y=n_pixels_y, n_pixels_z=n_pixels_z, mode=mode,
@@ -104,7 +116,8 @@ def tune(pixmap, frames: torch.Tensor, *, n_r: int, n_eta: int, n_pixels_y: int,
     if not ok:
         raise RuntimeError(f"no candidate plan could be built: {table}")
     best = min(ok, key=lambda r: r["ms"])
-    res = TuneResult({k: best[k] for k in ("tile_rows", "run_len", "tile_pixels")}, best["ms"], table, key)
+    res = TuneResult({k: best.get(k, "runs" if k == "encoding" else 0)
+                      for k in ("encoding", "tile_rows", "run_len", "tile_pixels")}, best["ms"], table, key)
     _CACHE[key] = res
     if cache_path:
         p = Path(cache_path)

@@ -43,8 +43,12 @@ def test_static_scratch_entry_point_matches_batched(cuda, enc):
         ck = torch.full_like(ref_ck, float("nan"))
         aw = torch.full_like(ref_aw, float("nan"))
         sm = torch.full_like(ref_sm, float("nan"))
+        torch.cuda.synchronize()
+        free0 = torch.cuda.mem_get_info()[0]
         L.check(_static_call(plan, frames, ck, aw, sm), "mi_integrate_batch_static")
         torch.cuda.synchronize()
+        if call == 1:                        # after the first call's set-up: no device memory taken
+            assert torch.cuda.mem_get_info()[0] == free0
         assert rel_err(ck.cpu().numpy(), ref_ck.cpu().numpy())[0] <= 1e-6
         assert rel_err(aw.cpu().numpy(), ref_aw.cpu().numpy())[0] <= 1e-6
         assert rel_err(sm.cpu().numpy(), ref_sm.cpu().numpy())[0] <= 1e-6
