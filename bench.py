@@ -38,7 +38,8 @@ TRAFFIC = {"runs": {"bytes_per_step": int(0.840295e9 + 0.761555e9 + 1.830098e9 +
            "mma": {"bytes_per_step": int(0.839712e9 + 0.764601e9 + 1.282986e9 + 0.862686e9),
                    "kernels": "k_xc + k_mma"}}
 SCOPE = {"runs": "whole batch: k_xc + k_runs + k_lineout (k_runs 88 %)",
-         "mma": "whole batch: k_xc + k_mma + k_lineout"}
+         "mma": "whole batch: k_xc + k_mma + k_lineout",
+         "mmad": "whole batch: k_mmad + k_lineout"}
 UNIT = "frames/s"
 
 

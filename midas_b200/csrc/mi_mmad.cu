@@ -431,8 +431,8 @@ __global__ void __launch_bounds__(kDThreads, 1) k_mmad(const __grid_constant__ M
         if (ji >= 0) {
           __syncwarp();
           if (lane == 0) m_arrive(&bempty[ji % NB]);
-          ++ji;
         }
+        ++ji;
         const int sl = ji % NB;
         bool got = true;
         if (lane == 0) got = m_wait(&bfull[sl], (uint32_t)(ji / NB) & 1u);
