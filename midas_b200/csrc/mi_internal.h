@@ -108,7 +108,7 @@ constexpr uint32_t kRunUnitsBytes = kRunWarps * 8 + kRunWarps * 4;
 //                                    and split the strip's records evenly
 //   uint16 strips[kRunWarps][2]      {first unit, number of units} of each strip
 //   uint16 rs_ptr[n_cols][G-L+2]
-//   float  scale[nb], lw[nb]         nb = n_rows * n_cols, row-major
+//   double scale[nb]; float lw[nb]   nb = n_rows * n_cols, row-major
 //   uint32 upix[n_u]
 //   uint16 lcol[n_rec]
 //   float  w[n_rec][L]
@@ -119,7 +119,7 @@ __host__ __device__ inline uint32_t runs_blob_layout(int nb, int n_cols, int n_r
   auto a16 = [](uint32_t x) { return (x + 15u) & ~15u; };
   uint32_t o = kRunUnitsOff + kRunUnitsBytes;
   *o_rsp = o; o = a16(o + 2u * (uint32_t)n_cols * (uint32_t)(G - L + 2));
-  *o_sc = o;  o = a16(o + 4u * (uint32_t)nb);
+  *o_sc = o;  o = a16(o + 8u * (uint32_t)nb);
   *o_lw = o;  o = a16(o + 4u * (uint32_t)nb);
   *o_up = o;  o = a16(o + 4u * (uint32_t)n_u);
   *o_lc = o;  o = a16(o + 2u * (uint32_t)n_rec);

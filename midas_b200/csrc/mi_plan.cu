@@ -510,11 +510,14 @@ static void runs_blob(const HostCSR &csr, const mi_map_desc &m, const Plan *p, c
     }
   }
   memcpy(blob + o_rsp, rsp.data(), rsp.size() * sizeof(uint16_t));
-  float *scale = (float *)(blob + o_sc);
+  double *scale = (double *)(blob + o_sc);
   float *lw = (float *)(blob + o_lw);
   for (int r = 0; r < t.n_rows; ++r)
-    for (int c = 0; c < t.n_cols; ++c)
-      bin_scale(csr, p, (int64_t)(t.r0 + r) * m.n_eta + t.e0 + c, scale + r * t.n_cols + c, lw + r * t.n_cols + c);
+    for (int c = 0; c < t.n_cols; ++c) {
+      float sc32;
+      bin_scale(csr, p, (int64_t)(t.r0 + r) * m.n_eta + t.e0 + c, &sc32, lw + r * t.n_cols + c,
+                scale + r * t.n_cols + c);
+    }
   uint32_t *upix = (uint32_t *)(blob + o_up);
   for (size_t i = 0; i < u.size(); ++i) upix[i] = (uint32_t)u[i];
   uint16_t *lcol = (uint16_t *)(blob + o_lc);

@@ -137,6 +137,12 @@ __device__ __forceinline__ float u16hi_to_f(uint32_t w) {
 }
 
 // The FPL frame values of one staged pixel for this lane, dark subtracted.
+#ifdef MI_RUNS_ACC32
+using Acc = float;
+#else
+using Acc = double;
+#endif
+
 template <bool kU16, int FPL, int FG>
 __device__ __forceinline__ void staged_values(const uint8_t *s_val, uint32_t u, int lane, float *v) {
   const uint8_t *row = s_val + u * (uint32_t)kRunPitch;
@@ -333,7 +339,7 @@ __global__ void __launch_bounds__((kRunWarps + NP) * 32, kRunCtasPerSm) k_runs(R
     uint32_t o_rsp, o_sc, o_lw, o_up, o_lc, o_w;
     runs_blob_layout(h.nb, h.n_cols, h.nnz, h.n_u, G, L, &o_rsp, &o_sc, &o_lw, &o_up, &o_lc, &o_w);
     const uint16_t *rsp = (const uint16_t *)(blob + o_rsp);
-    const float *scale = (const float *)(blob + o_sc);
+    const double *scale = (const double *)(blob + o_sc);
     const float *lw = (const float *)(blob + o_lw);
     const uint16_t *lcol = (const uint16_t *)(blob + o_lc);
     const float *wts = (const float *)(blob + o_w);
@@ -341,11 +347,13 @@ __global__ void __launch_bounds__((kRunWarps + NP) * 32, kRunCtasPerSm) k_runs(R
     const uint32_t *strips = (const uint32_t *)(units + 4 * kRunWarps);   // {first unit | count << 16}
 
     const int ns = h.n_cols;
-    float acc[G][FPL];
+    // FP64 accumulation of the exact FP64 products of the FP32 weights and staged values
+    // (compensates the FP32 rounding of long sums); built with MI_RUNS_ACC32: FP32
+    Acc acc[G][FPL];
 #pragma unroll
     for (int i = 0; i < G; ++i)
 #pragma unroll
-      for (int p = 0; p < FPL; ++p) acc[i][p] = 0.0f;
+      for (int p = 0; p < FPL; ++p) acc[i][p] = (Acc)0;
     {
       // this warp's unit: records [j0, j1) of strip s, walked rs by rs
       const uint2 ud = *(const uint2 *)(units + 4 * warp);
@@ -372,7 +380,7 @@ __global__ void __launch_bounds__((kRunWarps + NP) * 32, kRunCtasPerSm) k_runs(R
 #pragma unroll
             for (int q = 0; q < L; ++q)
 #pragma unroll
-              for (int p = 0; p < FPL; ++p) acc[rs + q][p] = fmaf(ww[r][q], vv[r][p], acc[rs + q][p]);
+              for (int p = 0; p < FPL; ++p) acc[rs + q][p] = fma((Acc)ww[r][q], (Acc)vv[r][p], acc[rs + q][p]);
         }
         for (; j < je; ++j) {
           float v0[FPL], w0[L];
@@ -381,15 +389,15 @@ __global__ void __launch_bounds__((kRunWarps + NP) * 32, kRunCtasPerSm) k_runs(R
 #pragma unroll
           for (int q = 0; q < L; ++q)
 #pragma unroll
-            for (int p = 0; p < FPL; ++p) acc[rs + q][p] = fmaf(w0[q], v0[p], acc[rs + q][p]);
+            for (int p = 0; p < FPL; ++p) acc[rs + q][p] = fma((Acc)w0[q], (Acc)v0[p], acc[rs + q][p]);
         }
       }
       // unit partials
 #pragma unroll
       for (int i = 0; i < G; ++i) {
         float *d = s_part + ((size_t)warp * G + i) * FG + lane * FPL;
-        if constexpr (FPL == 2) *(float2 *)d = make_float2(acc[i][0], acc[i][1]);
-        else d[0] = acc[i][0];
+        if constexpr (FPL == 2) *(float2 *)d = make_float2((float)acc[i][0], (float)acc[i][1]);
+        else d[0] = (float)acc[i][0];
       }
     }
     nb_sync(1, NCT);                     // unit partials written; staging of slot b consumed
@@ -404,27 +412,28 @@ __global__ void __launch_bounds__((kRunWarps + NP) * 32, kRunCtasPerSm) k_runs(R
       for (int s = 0; s < ns; ++s) {
         const uint32_t st = strips[s];
         const int u0 = st & 0xFFFF, nu = st >> 16;
-        float v[FPL];
+        double v[FPL];
 #pragma unroll
-        for (int p = 0; p < FPL; ++p) v[p] = 0.0f;
+        for (int p = 0; p < FPL; ++p) v[p] = 0.0;
         for (int kk = 0; kk < nu; ++kk) {
           const float *src = s_part + ((size_t)(u0 + kk) * G + i) * FG + lane * FPL;
           if constexpr (FPL == 2) {
             const float2 t2 = *(const float2 *)src;
-            v[0] += t2.x;
-            v[1] += t2.y;
+            v[0] += (double)t2.x;
+            v[1] += (double)t2.y;
           } else {
-            v[0] += src[0];
+            v[0] += (double)src[0];
           }
         }
         const int bb = i * ns + s;
-        const float sc = scale[bb], l = lw[bb];
+        const double sc = scale[bb];
+        const float l = lw[bb];
 #pragma unroll
         for (int p = 0; p < FPL; ++p) {
-          const float o = v[p] * sc;
-          s_out[(lane * FPL + p) * nbp + bb] = o;
-          saw[p] += (double)o * (double)l;
-          ssm[p] += (l > 0.0f) ? (double)o : 0.0;
+          const double o = v[p] * sc;
+          s_out[(lane * FPL + p) * nbp + bb] = (float)o;
+          saw[p] += o * (double)l;
+          ssm[p] += (l > 0.0f) ? o : 0.0;
         }
       }
       if (a.want_lo) {
