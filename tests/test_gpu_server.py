@@ -38,12 +38,14 @@ def _alone(cfg, frame):
     return out
 
 
-def test_results_are_the_same_alone_and_in_the_mix(cuda):
+@pytest.mark.parametrize("graphs", [8, 0])
+def test_results_are_the_same_alone_and_in_the_mix(cuda, graphs):
+    """graphs: batches up to this size replay a recorded CUDA graph (0: direct calls)."""
     work = _mix()
     cfgs = [synth.serving_stream(w) for w in work]
     frames = [synth.host_frames(w, 0, N_FRAMES) for w in work]
     assert frames[2].dtype == np.int32
-    srv = CakeServer(backend=DeviceBackend(max_batch=5, max_inflight=2)).start()
+    srv = CakeServer(backend=DeviceBackend(max_batch=5, max_inflight=2, graph_batches=graphs)).start()
     try:
         ids = [srv.admit(c) for c in cfgs]
         results = {}
