@@ -55,7 +55,7 @@ def parse():
     ap.add_argument("--tile-rows", type=int, default=0)
     ap.add_argument("--tile-pixels", type=int, default=0)
     ap.add_argument("--fpl", type=int, default=0)
-    ap.add_argument("--encoding", default="mma", choices=["auto", "runs", "csr", "mma"],
+    ap.add_argument("--encoding", default="mma", choices=["auto", "runs", "csr", "mma", "mmad"],
                     help="tile encoding of the batched plan (mma: tensor cores, the default for these u16 sweeps)")
     ap.add_argument("--run-len", type=int, default=0)
     ap.add_argument("--no-e2e", action="store_true")
@@ -355,11 +355,10 @@ def main_ours(args):
     barrier(world)
     torch.cuda.synchronize()
     clk = clocks.stop()
-    lane_idx = torch.tensor(lanes, device=dev)
-    checked = {"frames": frames[b_last * F + lane_idx].cpu().numpy(),
-               "cake": bufs["cake"][lane_idx].reshape(len(lanes), -1).cpu().numpy().astype(np.float64),
-               "lineout_aw": bufs["lineout_aw"][lane_idx].cpu().numpy(),
-               "lineout_sm": bufs["lineout_sm"][lane_idx].cpu().numpy(),
+    checked = {"frames": np.stack([frames[b_last * F + k].cpu().numpy() for k in lanes]),
+               "cake": np.stack([bufs["cake"][k].reshape(-1).cpu().numpy() for k in lanes]).astype(np.float64),
+               "lineout_aw": np.stack([bufs["lineout_aw"][k].cpu().numpy() for k in lanes]),
+               "lineout_sm": np.stack([bufs["lineout_sm"][k].cpu().numpy() for k in lanes]),
                "lanes": lanes, "batch": b_last}
     frame0 = checked["frames"][0]
     elapsed_ms = dist_max(e0.elapsed_time(e1), world)

@@ -139,7 +139,7 @@ typedef struct {
                               tiles of MI_ENC_MMA, pixels in 8-pixel row granules loaded per
                               frame into tensor memory (one vector load per granule when rows
                               are a multiple of 8 pixels and frames and strides 16-byte
-                              aligned), 24-bit fixed-point weights, four int32 accumulators;
+                              aligned), 32-bit fixed-point weights, five int32 accumulators;
                               no pixel-major staging pass                                 */
 
 typedef struct {

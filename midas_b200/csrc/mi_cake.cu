@@ -177,7 +177,7 @@ __global__ void __launch_bounds__(kCakeThreads) k_cake(CakeArgs a) {
     uint32_t o_rp, o_sc, o_lw, o_up, o_lc, o_w, bytes;
     blob_layout(h.nb, h.nnz, h.n_u, &o_rp, &o_sc, &o_lw, &o_up, &o_lc, &o_w, &bytes);
     const uint32_t *rowp = (const uint32_t *)(s_blob + o_rp);
-    const float *scale = (const float *)(s_blob + o_sc);
+    const double *scale = (const double *)(s_blob + o_sc);
     const float *lw = (const float *)(s_blob + o_lw);
     const uint32_t *upix = (const uint32_t *)(s_blob + o_up);
     const uint16_t *lcol = (const uint16_t *)(s_blob + o_lc);
@@ -207,9 +207,10 @@ __global__ void __launch_bounds__(kCakeThreads) k_cake(CakeArgs a) {
     // ---- compute: warp per bin, lane = frame(s)
     for (int b = warp; b < h.nb; b += NW) {
       const uint32_t j0 = rowp[b], j1 = rowp[b + 1];
-      float acc[FPL];
+      // FP64 sums of the exact FP64 products (no error growth with the bin's term count)
+      double acc[FPL];
 #pragma unroll
-      for (int q = 0; q < FPL; ++q) acc[q] = 0.0f;
+      for (int q = 0; q < FPL; ++q) acc[q] = 0.0;
       uint32_t j = j0;
       for (; j + 4 <= j1; j += 4) {
         uint32_t c[4];
@@ -224,18 +225,18 @@ __global__ void __launch_bounds__(kCakeThreads) k_cake(CakeArgs a) {
 #pragma unroll
         for (int q = 0; q < 4; ++q)
 #pragma unroll
-          for (int r = 0; r < FPL; ++r) acc[r] = fmaf(w[q], v[q][r], acc[r]);
+          for (int r = 0; r < FPL; ++r) acc[r] = fma((double)w[q], (double)v[q][r], acc[r]);
       }
       for (; j < j1; ++j) {
         float v[FPL];
         FVec<FPL>::ld(s_val + (uint32_t)lcol[j] * SROW + lane * FPL, v);
         const float w = wt[j];
 #pragma unroll
-        for (int r = 0; r < FPL; ++r) acc[r] = fmaf(w, v[r], acc[r]);
+        for (int r = 0; r < FPL; ++r) acc[r] = fma((double)w, (double)v[r], acc[r]);
       }
-      const float sc = scale[b];
+      const double sc = scale[b];
 #pragma unroll
-      for (int r = 0; r < FPL; ++r) s_out[(lane * FPL + r) * nbp + b] = acc[r] * sc;
+      for (int r = 0; r < FPL; ++r) s_out[(lane * FPL + r) * nbp + b] = (float)(acc[r] * sc);
     }
     __syncthreads();
 

@@ -43,7 +43,7 @@ int cuda_error(cudaError_t e, const char *what, const char *file, int line);
 //
 //   TileHdr                        32 B
 //   uint32 row_ptr[nb + 1]         term offsets per bin (bins row-major in tile)
-//   float  scale[nb]               result = sum * scale (1/area, 1 or 0)
+//   double scale[nb]               result = sum * scale (1/area, 1 or 0)
 //   float  lw[nb]                  lineout weight: in-bounds area if > 1e-9 else 0
 //   uint32 upix[n_u]               staged pixels (flat detector index), ascending
 //   uint16 lcol[nnz]               term -> index into upix
@@ -81,7 +81,7 @@ __host__ __device__ inline void blob_layout(int nb, int nnz, int n_u, uint32_t *
   auto a16 = [](uint32_t x) { return (x + 15u) & ~15u; };
   uint32_t o = 32;
   *o_rowptr = o; o = a16(o + 4u * (uint32_t)(nb + 1));
-  *o_scale = o;  o = a16(o + 4u * (uint32_t)nb);
+  *o_scale = o;  o = a16(o + 8u * (uint32_t)nb);
   *o_lw = o;     o = a16(o + 4u * (uint32_t)nb);
   *o_upix = o;   o = a16(o + 4u * (uint32_t)n_u);
   *o_lcol = o;   o = a16(o + 2u * (uint32_t)nnz);
@@ -285,10 +285,10 @@ __host__ __device__ inline MmaBlob mma_blob_layout(int n_k, int n_runs, int n_te
 // step of 32 slots is four granules, slot k holding pixel k % 8 of granule k / 8.  The
 // producer warps load a frame's granule with one 16-byte load per frame (u16 frames), split
 // it into its low and high byte planes and store both into tensor memory, where they are
-// the A operand of the MMAs.  Weights are 24-bit fixed point, q = round(w / w_max(bin) x
-// (2^24 - 1)), in three byte planes (the B operand, N = 144), so four int32 accumulators
-// (byte shifts 0..3) hold the exact products:
-//   cake = fac * sum_k 2^(8k) acc_k - dk,  fac = w_max / (2^24 - 1) * scale.
+// the A operand of the MMAs.  Weights are 32-bit fixed point, q = round(w / w_max(bin) x
+// (2^32 - 1)), in four byte planes (the B operand, N = 192), so five int32 accumulators
+// (byte shifts 0..4) hold the exact products:
+//   cake = fac * sum_k 2^(8k) acc_k - dk,  fac = w_max / (2^32 - 1) * scale.
 // Blob of a tile (16-byte aligned arrays):
 //   MmaHdr                       32 B (n_runs: 0)
 //   double fac[48], dk[48]; float lw[48]
@@ -298,7 +298,7 @@ __host__ __device__ inline MmaBlob mma_blob_layout(int n_k, int n_runs, int n_te
 constexpr int kMmadGran = 4;           // granules per K step
 constexpr int kMmadGranPx = 8;         // pixels per granule
 constexpr uint32_t kMmadEmpty = 0xFFFFFFFFu;
-constexpr double kMmadQMax = 16777215.0;  // 2^24 - 1
+constexpr double kMmadQMax = 4294967295.0;  // 2^32 - 1
 
 struct MmadBlob {
   uint32_t gran, step_ptr, terms, bytes;

@@ -10,11 +10,11 @@
 //   D[frame][bin] (int32, TMEM) += A[frame][slot] (a byte plane of the frames, in TMEM)
 //                                  x B[slot][bin]  (a byte plane of the weights, in SMEM)
 // K = 32 slots per step = four 8-pixel granules (8 consecutive pixels of one detector row).
-// Per K step two tcgen05.mma of N = 144 (the three weight planes side by side): the frames'
-// low byte plane into accumulators 0-2, the high plane, one byte up, into accumulators 1-3.
+// Per K step two tcgen05.mma of N = 192 (the four weight planes side by side): the frames'
+// low byte plane into accumulators 0-3, the high plane, one byte up, into accumulators 1-4.
 // Every product and sum is exact; the epilogue forms sum_k 2^(8k) acc_k in FP64, subtracts
-// the bin's dark term and scales: cake = fac * value - dk.  The approximation is the 24-bit
-// fixed-point weight (2^-25 of the bin's largest weight) and the final rounding to float.
+// the bin's dark term and scales: cake = fac * value - dk.  The approximation is the 32-bit
+// fixed-point weight (2^-33 of the bin's largest weight) and the final rounding to float.
 //
 // Operands:
 //   A (frames): in tensor memory, a ring of kDASlots K steps of 16 columns each (8 columns
@@ -22,13 +22,13 @@
 //     Producer warp q (TMEM lanes 32q..32q+31) loads, per frame, each granule with one
 //     16-byte load from the frame's own rows, splits the eight u16 pixels into their two
 //     byte planes with byte permutes and stores both planes with one tcgen05.st.
-//   B (weights): K-major without swizzle in shared memory, the three byte planes as rows
+//   B (weights): K-major without swizzle in shared memory, the four byte planes as rows
 //     n' = 48 j + n; byte (n', k) at (n' % 8) * 16 + (n' / 8) * 256 + (k % 16) + (k / 16) * 128,
 //     zeroed and scattered per stage from the stage's terms.
 //
 // Roles (one persistent CTA per SM, 16 warps, 128 registers a thread):
-//   warp 0             TMEM allocation (512 columns: two accumulator sets of 4 x 48 and the
-//                      A ring) and, on one lane, the MMA issue
+//   warp 0             TMEM allocation (512 columns: two accumulator sets of 5 x 48 and the
+//                      two-slot A ring) and, on one lane, the MMA issue
 //   warp 1             loader: claims work items (heaviest first), bulk-copies each tile's
 //                      blob into a blob slot and its bins' factors into the epilogue's ring
 //   warps 2,3,12-15    B producers: stage g (over the CTA's tiles) built by producer g % 6
@@ -58,13 +58,13 @@ constexpr int kDEpiWarps = 4;
 constexpr int kDAWarps = 4;
 constexpr int kDWarps = 2 + kDProducers + kDEpiWarps + kDAWarps;
 constexpr int kDThreads = kDWarps * 32;
-constexpr int kDPlanes = 3;                              // weight byte planes
-constexpr int kDAcc = 4;                                 // accumulators (byte shifts 0..3)
+constexpr int kDPlanes = 4;                              // weight byte planes
+constexpr int kDAcc = 5;                                 // accumulators (byte shifts 0..4)
 constexpr uint32_t kDBPlane = 1536u;                     // 48 rows x 32 bytes
-constexpr uint32_t kDStageBytes = kDPlanes * kDBPlane;   // 4608
-constexpr int kDAccCols = kDAcc * kMmaN;                 // 192 columns per accumulator set
-constexpr int kDASlots = 8;                              // A ring: K steps in tensor memory
-constexpr int kDACol0 = 2 * kDAccCols;                   // 384: first column of the ring
+constexpr uint32_t kDStageBytes = kDPlanes * kDBPlane;   // 6144
+constexpr int kDAccCols = kDAcc * kMmaN;                 // 240 columns per accumulator set
+constexpr int kDASlots = 2;                              // A ring: K steps in tensor memory
+constexpr int kDACol0 = 2 * kDAccCols;                   // 480: first column of the ring
 constexpr int kDAhead = 4;                               // K steps loaded ahead of their store
 constexpr int kDTmemCols = 512;
 static_assert(kDACol0 + 16 * kDASlots <= kDTmemCols, "TMEM budget");
@@ -268,11 +268,11 @@ __global__ void __launch_bounds__(kDThreads, 1) k_mmad(const __grid_constant__ M
           m_mma_ta(dbase + (uint32_t)kMmaN, a_hi, bd, mmad_idesc(kDPlanes * kMmaN), 1u);
         } else {
           // a tile's first step starts each accumulator from zero: the low plane's product
-          // starts 0-2, the high plane's adds onto 1-2 and starts 3
+          // starts 0-3, the high plane's adds onto 1-3 and starts 4
           m_mma_ta(dbase, a_lo, bd, mmad_idesc(kDPlanes * kMmaN), 0u);
           m_mma_ta(dbase + (uint32_t)kMmaN, a_hi, bd, mmad_idesc((kDPlanes - 1) * kMmaN), 1u);
-          m_mma_ta(dbase + (uint32_t)(kDPlanes * kMmaN), a_hi, m_desc(bsa + 2u * kDBPlane, 128u, 256u, 0u),
-                   mmad_idesc(kMmaN), 0u);
+          m_mma_ta(dbase + (uint32_t)(kDPlanes * kMmaN), a_hi,
+                   m_desc(bsa + (uint32_t)(kDPlanes - 1) * kDBPlane, 128u, 256u, 0u), mmad_idesc(kMmaN), 0u);
         }
         m_commit(&empty[q]);
         m_commit(&rempty[rs]);
@@ -389,6 +389,7 @@ __global__ void __launch_bounds__(kDThreads, 1) k_mmad(const __grid_constant__ M
             b0[0] = (uint8_t)(tm.x & 0xFFu);
             b0[kDBPlane] = (uint8_t)((tm.x >> 8) & 0xFFu);
             b0[2 * kDBPlane] = (uint8_t)((tm.x >> 16) & 0xFFu);
+            b0[3 * kDBPlane] = (uint8_t)(tm.x >> 24);
           }
         }
         if (lane == 0) {
@@ -560,9 +561,10 @@ __global__ void __launch_bounds__(kDThreads, 1) k_mmad(const __grid_constant__ M
 #pragma unroll
         for (int i = 0; i < 8; ++i) {
           const int lrow = (8 * c + i) / kMmaCols;
-          const double x3 = m_u2d(r[3][i]), x2 = m_u2d(r[2][i]), x1 = m_u2d(r[1][i]), x0 = m_u2d(r[0][i]);
-          // sum_k 2^(8k) x_k = ((x3 256 + x2) 256 + x1) 256 + x0
-          const double v = fma(fma(fma(x3, 256.0, x2), 256.0, x1), 256.0, x0);
+          const double x4 = m_u2d(r[4][i]), x3 = m_u2d(r[3][i]), x2 = m_u2d(r[2][i]), x1 = m_u2d(r[1][i]),
+                       x0 = m_u2d(r[0][i]);
+          // sum_k 2^(8k) x_k = (256 x4 + x3) 2^24 + (256 x2 + x1) 256 + x0
+          const double v = fma(fma(x4, 256.0, x3), 16777216.0, fma(fma(x2, 256.0, x1), 256.0, x0));
           const double res = fma(bfac[8 * c + i], v, -bdk[8 * c + i]);
           const float l = blw[8 * c + i];
           o[i] = (float)res;

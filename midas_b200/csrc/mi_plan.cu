@@ -403,7 +403,7 @@ static void csr_blob(const HostCSR &csr, const mi_map_desc &m, const Plan *p, co
   TileHdr *h = (TileHdr *)blob;
   *h = TileHdr{nb, t.nnz, t.n_u, t.n_rows, t.n_cols, t.r0, t.e0, row_in_band};
   uint32_t *rowp = (uint32_t *)(blob + o_rp);
-  float *scale = (float *)(blob + o_sc);
+  double *scale = (double *)(blob + o_sc);
   float *lw = (float *)(blob + o_lw);
   uint32_t *upix = (uint32_t *)(blob + o_up);
   uint16_t *lcol = (uint16_t *)(blob + o_lc);
@@ -421,7 +421,8 @@ static void csr_blob(const HostCSR &csr, const mi_map_desc &m, const Plan *p, co
         wt[nz_o] = (float)csr.w[j];
         ++nz_o;
       }
-      bin_scale(csr, p, b, scale + lb, lw + lb);
+      float sc32;
+      bin_scale(csr, p, b, &sc32, lw + lb, scale + lb);
     }
   rowp[nb] = nz_o;
   for (int32_t v : u) lut[v] = -1;
@@ -727,7 +728,7 @@ static int mma_tile_blob(const HostCSR &csr, const mi_map_desc &m, const std::ve
 
 // ---- Direct MMA encoding (see MmadBlob): the tile's pixels covered by 8-pixel row granules
 // in (row, column) order, four granules per K step; pixel (z, y) of granule g sits in slot
-// 8 g + (y - y0).  Weights in 24-bit fixed point relative to the bin's largest weight.
+// 8 g + (y - y0).  Weights in 32-bit fixed point relative to the bin's largest weight.
 static int mmad_tile_blob(const HostCSR &csr, const mi_map_desc &m, const std::vector<double> &wmax,
                           const std::vector<double> &fac, const std::vector<float> &lw, int r0, int nr, int box_rows,
                           int e0, int nc, std::vector<int32_t> &lut, std::vector<uint8_t> &blob, int *nnz_out,
