@@ -22,6 +22,7 @@
  *                           packages/midas_integrate/midas_integrate/peakfit.py:334
  *   mi_fit_plan_*        <- fitPeaks() job construction and joint fits, PeakFit.c:292-545, and the
  *                           per-eta fits of FF_HEDM/src/IntegratorZarrOMP.c:1902-2030
+ *   mi_plan_create_fused <- build_fused_geometry()     packages/midas_integrate/midas_integrate/fused_csr.py:139
  *   mi_map_build         <- mapper_build_map()         FF_HEDM/src/MapperCore.c:45 (DetectorMapper)
  *   mi_last_error        <- (new) the reference aborts the process on any CUDA error
  *                           (gpuAssert, IntegratorFitPeaksGPUStream.cu:299-308); this library
@@ -131,15 +132,16 @@ typedef struct {
 #define MI_ENC_CSR 1       /* per-bin term lists, one warp per bin, lane = frame         */
 #define MI_ENC_RUNS 2      /* per-pixel radial runs: one staged value feeds run_len bins */
 #define MI_ENC_MMA 3       /* tensor cores (8/16-bit frames only): 12 x 4-bin tiles as dense
-                              int8 MMAs, frames split into two byte planes and weights into
-                              32-bit fixed point (relative to the bin's largest weight), exact
-                              int32 accumulation, FP64 recombination; other frame types get
+                              int8 MMAs, frames split into two u8 byte planes and weights into
+                              signed fixed point (four s8 digits, relative to the bin's largest
+                              |weight|), exact int32 accumulation, FP64 recombination; other
+                              frame types get
                               MI_E_UNSUPPORTED                                            */
 #define MI_ENC_MMAD 4      /* tensor cores reading the frames in place (u16/u8 frames): the
                               tiles of MI_ENC_MMA, pixels in 8-pixel row granules loaded per
                               frame into tensor memory (one vector load per granule when rows
                               are a multiple of 8 pixels and frames and strides 16-byte
-                              aligned), 32-bit fixed-point weights, five int32 accumulators;
+                              aligned), the same signed weight digits, five int32 accumulators;
                               no pixel-major staging pass                                 */
 
 typedef struct {
@@ -194,6 +196,26 @@ int mi_plan_set_dark_panels(mi_plan *plan, const float *const *darks_host);
 int mi_integrate_panels(mi_plan *plan, const void *const *frames, const int *dtypes,
                         const int64_t *strides, int n_frames, float *cake, double *lineout_aw,
                         double *lineout_sm, void *stream);
+/* ---- fused multi-shift maps ------------------------------------------------------------
+ * Replaces build_fused_geometry (packages/midas_integrate/midas_integrate/fused_csr.py:139):
+ * n_shifts maps of one detector whose R edges are shifted by k / n_shifts of a bin
+ * (RMin + k/N x RBinSize), r_axes[k] the n_r of map k's R bin centres.  Each shift's
+ * bilinear or gradient weights (py semantics) are divided by the bin's in-bounds area
+ * (bins at or under 1e-9: 0), moved onto shift 0's R axis by linear interpolation in R
+ * (at most two source rows per row, fused_csr.py:63-104: clamped to the first / last pair
+ * outside the axis), summed over the shifts and divided by n_shifts.  The cake of the
+ * fused plan is the average of the shifts' normalised cakes, interpolated onto shift 0's
+ * axis, in one pass; every bin's area is 1, so `normalize` changes nothing and the
+ * lineouts weigh every bin of a row alike.  Shifts share n_eta and the detector shape;
+ * n_r may differ (at least 2).  opts: mode bilinear or gradient, semantics MI_SEM_PY, no
+ * variance; any encoding.                                                              */
+int mi_plan_create_fused(const mi_map_desc *maps, int n_shifts, const double *const *r_axes,
+                         const mi_plan_opts *opts, int device, mi_plan **out);
+/* The fused weights themselves, on the host (no device needed): row_ptr (n_bins + 1, or
+ * NULL), then col / w (both NULL to ask for *nnz only, else `capacity` entries). */
+int mi_fused_csr(const mi_map_desc *maps, int n_shifts, const double *const *r_axes, int mode,
+                 int64_t *row_ptr, int32_t *col, double *w, int64_t capacity, int64_t *nnz);
+
 /* Failure-detection self test (no counterpart in the reference, which aborts on errors):
  * one mbarrier wait bounded to `polls` polls, as every wait in this library's kernels is,
  * on a barrier that nothing completes (arrive = 0) or that its thread completed first
@@ -266,6 +288,12 @@ int mi_integrate_batch_static(mi_plan *plan, const void *frames, int dtype, int 
  * gradient mode, FP64 cake, then the two profile kernels.  This is the plain baseline. */
 int mi_integrate_plain(mi_plan *plan, const void *frame, int dtype, double *cake,
                        double *lineout_aw, double *lineout_sm, void *stream);
+
+/* SumImages (IntegratorFitPeaksGPUStream.cu:1043-1046, the running dSumMatrix of
+ * :2141-2144): sum[b] += cake[f][b] for the F frames of a float32 [F][n_r][n_eta] device
+ * cake, in FP64 and frame order; NaN bins add nothing.  sum: n_r*n_eta doubles on the
+ * device, zeroed by the caller before the first batch; stream-ordered like the caking. */
+int mi_sum_cake(mi_plan *plan, const float *cake, int n_frames, double *sum, void *stream);
 
 /* Kernel (c) on a cake the caller already holds: area-weighted and simple-mean eta
  * reductions of F frames of a [F][n_r][n_eta] cake (float32 with cake_dtype = MI_DT_F32,

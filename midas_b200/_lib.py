@@ -107,10 +107,15 @@ SIGNATURES = [
     ("mi_plan_create_panels", C.c_int, [C.POINTER(MiMapDesc), C.c_int, C.POINTER(MiPlanOpts), C.c_int,
                                         C.POINTER(C.c_void_p)]),
     ("mi_plan_set_dark_panels", C.c_int, [C.c_void_p, C.POINTER(C.c_void_p)]),
+    ("mi_plan_create_fused", C.c_int, [C.POINTER(MiMapDesc), C.c_int, C.POINTER(C.c_void_p),
+                                       C.POINTER(MiPlanOpts), C.c_int, C.POINTER(C.c_void_p)]),
+    ("mi_fused_csr", C.c_int, [C.POINTER(MiMapDesc), C.c_int, C.POINTER(C.c_void_p), C.c_int, C.c_void_p,
+                               C.c_void_p, C.c_void_p, C.c_int64, C.POINTER(C.c_int64)]),
     ("mi_integrate_panels", C.c_int, [C.c_void_p, C.POINTER(C.c_void_p), C.POINTER(C.c_int),
                                       C.POINTER(C.c_int64), C.c_int, C.c_void_p, C.c_void_p, C.c_void_p,
                                       C.c_void_p]),
     ("mi_plan_get_info", C.c_int, [C.c_void_p, C.POINTER(MiPlanInfo)]),
+    ("mi_sum_cake", C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p]),
     ("mi_plan_set_bin_mask", C.c_int, [C.c_void_p, C.c_void_p]),
     ("mi_selftest_wait", C.c_int, [C.c_uint32, C.c_int, C.c_int, C.POINTER(C.c_int)]),
     ("mi_plan_bytes", C.c_int, [C.c_void_p, C.POINTER(C.c_size_t)]),

@@ -226,11 +226,11 @@ struct XcChunk {
 // MMA encoding (MI_ENC_MMA, kernel k_mma of mi_mma.cu): caking of 8/16-bit frames on the
 // tensor cores with exact integer arithmetic.  A tile is kMmaRows x kMmaCols bins (bin
 // n = row * kMmaCols + col) and its staged pixels in K slots; a frame batch is the M = 128
-// rows of the MMA.  Frames are split into two byte planes (lo, hi), weights into four
-// byte planes of a 32-bit fixed-point value q = round(w / w_max(bin) * (2^32 - 1)); the
-// eight u8 x u8 products accumulate exactly in int32 (five accumulators, one per byte
-// shift 0..4), and the epilogue recombines them in FP64:
-//   cake = fac * sum_k 2^(8k) acc_k - dk,  fac = w_max / (2^32 - 1) * scale,
+// rows of the MMA.  Frames are split into two u8 byte planes (lo, hi), weights into four
+// s8 digit planes of a signed fixed-point value q = round(w / max|w|(bin) * kMmaQMax) (see
+// mma_digits); the eight u8 x s8 products accumulate exactly in int32 (five accumulators,
+// one per byte shift 0..4), and the epilogue recombines them in FP64:
+//   cake = fac * sum_k 2^(8k) acc_k - dk,  fac = max|w| / kMmaQMax * scale,
 //   dk = fac * sum q * dark (the dark term of the bin, set with the dark).
 // The pixel-major buffer of an MMA plan holds two byte planes, [lo: n_xc x 128][hi: n_xc x
 // 128]: row c of a plane is compact pixel c's byte of 128 frames, its 16-byte granule g
@@ -245,7 +245,7 @@ struct XcChunk {
 //                                       c % 8 == k % 8 (the swizzle phase of its row)
 //   uint32 run_ptr[n_k + 1]             runs of K step s: [run_ptr[s], run_ptr[s+1])
 //   uint32 step_ptr[n_k + 1]            terms of K step s
-//   uint2  terms[n_terms]               {q, k | n << 16}, sorted by k
+//   uint2  terms[n_terms]               {mma_digits(q), k | n << 16}, sorted by k
 struct MmaHdr {
   int32_t n_rows, n_cols, r0, e0, n_k, n_terms;
   int32_t box_rows;   // rows of the item's sub-band (12, 6, 3 or 1): the cake store's box height
@@ -258,7 +258,32 @@ constexpr int kMmaN = kMmaRows * kMmaCols;  // 48 bins: the N of every MMA
 constexpr int kMmaFrames = 128;        // frames per launch: the M of every MMA
 constexpr int kMmaKStep = 32;          // K slots (staged pixels) per MMA step
 constexpr uint32_t kMmaEmpty = 0xFFFFFFFFu;
-constexpr int kMmaMaxBinTerms = 16000; // int32 accumulators: 2 x 255 x 255 per term
+constexpr int kMmaMaxBinTerms = 16000; // int32 accumulators: 2 x 255 x 128 per term
+// Tensor-core weights: q = round(w / max|w|(bin) x kMmaQMax), |q| <= kMmaQMax, written as four
+// balanced base-256 digits d_k in [-128, 127] (q = sum_k 256^k d_k), one s8 byte plane each:
+// bilinear weights of the IntegrationCore semantics can be negative.  127 x (1 + 2^8 + 2^16 +
+// 2^24) is the largest magnitude the four digits hold either way.
+constexpr double kMmaQMax = 2139062143.0;
+// the digits packed one per byte (two's complement), plane k in byte k
+__host__ __device__ inline uint32_t mma_digits(int64_t q) {
+  uint32_t packed = 0;
+  for (int k = 0; k < 4; ++k) {
+    const int64_t d = ((q % 256) + 384) % 256 - 128;   // q - d divisible by 256, d in [-128, 127]
+    packed |= (uint32_t)(uint8_t)(int8_t)d << (8 * k);
+    q = (q - d) / 256;
+  }
+  return packed;
+}
+// Shared-memory bank of a term's byte in the B operand of one K step (byte (n, k) at
+// (n % 8) * 16 + (n / 8) * 256 + (k % 16) + (k / 16) * 128, the plane offsets multiples of 128)
+__host__ __device__ inline int mma_bank(uint32_t n, uint32_t kk) {
+  return (int)((n & 7u) * 4u + ((kk & 15u) >> 2));
+}
+__host__ __device__ inline int64_t mma_digits_value(uint32_t packed) {
+  int64_t q = 0;
+  for (int k = 3; k >= 0; --k) q = q * 256 + (int8_t)(uint8_t)(packed >> (8 * k));
+  return q;
+}
 constexpr uint32_t kMmaBlobCap = 24 * 1024;  // largest tile blob (blob slots in shared memory)
 constexpr uint32_t kMmaBinsOff = 32;   // fac, dk, lw after the header
 constexpr uint32_t kMmaBinsBytes = kMmaN * (8 + 8 + 4);
@@ -285,20 +310,19 @@ __host__ __device__ inline MmaBlob mma_blob_layout(int n_k, int n_runs, int n_te
 // step of 32 slots is four granules, slot k holding pixel k % 8 of granule k / 8.  The
 // producer warps load a frame's granule with one 16-byte load per frame (u16 frames), split
 // it into its low and high byte planes and store both into tensor memory, where they are
-// the A operand of the MMAs.  Weights are 32-bit fixed point, q = round(w / w_max(bin) x
-// (2^32 - 1)), in four byte planes (the B operand, N = 192), so five int32 accumulators
-// (byte shifts 0..4) hold the exact products:
-//   cake = fac * sum_k 2^(8k) acc_k - dk,  fac = w_max / (2^32 - 1) * scale.
+// the A operand of the MMAs.  Weights are the MMA encoding's signed fixed point (kMmaQMax),
+// four s8 digit planes (the B operand, N = 192), so five int32 accumulators (byte shifts
+// 0..4) hold the exact products:
+//   cake = fac * sum_k 2^(8k) acc_k - dk,  fac = max|w| / kMmaQMax * scale.
 // Blob of a tile (16-byte aligned arrays):
 //   MmaHdr                       32 B (n_runs: 0)
 //   double fac[48], dk[48]; float lw[48]
 //   uint32 gran[n_k][4]          granule z | y0 << 16 (kMmadEmpty: none)
 //   uint32 step_ptr[n_k + 1]     terms of K step s
-//   uint2  terms[n_terms]        {q, k | n << 16}, sorted by slot k (k / 32 = K step)
+//   uint2  terms[n_terms]        {mma_digits(q), k | n << 16}, sorted by slot k (k / 32 = K step)
 constexpr int kMmadGran = 4;           // granules per K step
 constexpr int kMmadGranPx = 8;         // pixels per granule
 constexpr uint32_t kMmadEmpty = 0xFFFFFFFFu;
-constexpr double kMmadQMax = 4294967295.0;  // 2^32 - 1
 
 struct MmadBlob {
   uint32_t gran, step_ptr, terms, bytes;
@@ -419,6 +443,7 @@ int launch_profile(Plan *p, const void *cake, int cake_dtype, int n_frames, doub
                    double *lo_sm, cudaStream_t s);
 // MI_SEM_OMP plans: NaN into the masked bins of F cakes
 int launch_nan_bins(Plan *p, float *cake, int n_frames, cudaStream_t s);
+int launch_sum_cake(Plan *p, const float *cake, int n_frames, double *sum, cudaStream_t s);
 
 size_t dtype_size(int dtype);
 

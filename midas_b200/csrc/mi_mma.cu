@@ -11,9 +11,9 @@
 // two frame planes x four weight planes, issued as two tcgen05.mma of N = 192 per K step of
 // 32 staged pixels, into five int32 accumulators (one per byte shift 0..4).  Every product and sum is exact;
 // the epilogue forms sum_k 2^(8k) acc_k in FP64, subtracts the bin's dark term and scales:
-// cake = fac * value - dk.  The only approximation is the 32-bit fixed-point weight
-// (2^-33 of the bin's largest weight); the reference's fp32 (raw - dark) and fp32 sums are
-// replaced by exact integer sums, so the result is closer to the FP64 one.
+// cake = fac * value - dk.  The only approximation is the signed fixed-point weight (four s8
+// digits, a step of 2^-31 of the bin's largest |w|); the reference's fp32 (raw - dark) and
+// fp32 sums are replaced by exact integer sums, so the result is closer to the FP64 one.
 //
 // Operands in shared memory, per pipeline stage (kMmaStepsPerStage K steps of 32 pixel slots):
 //   A (frames): MN-major, 128B swizzle; slot k of the stage is the 128-byte row
@@ -21,9 +21,10 @@
 //     at position g ^ (k % 8).  Kernel (a) writes each pixel-major row with its granules
 //     already in that order for phase c % 8, and the tiler puts pixel c in a slot with
 //     k % 8 == c % 8, so a slot is filled by one plain 128-byte bulk copy per plane.
-//   B (weights): K-major, no swizzle, the four byte planes as rows n' = 48 j + n; byte (n', k)
-//     at (n' % 8) * 16 + (n' / 8) * kMmaBSbo + (k % 16) + (k / 16) * 128, zeroed and then
-//     scattered from the stage's terms.
+//   B (weights): K-major, no swizzle, the four s8 digit planes as rows n' = 48 j + n; byte
+//     (n', k) at (n' % 8) * 16 + (n' / 8) * kMmaBSbo + (k % 16) + (k / 16) * 128, zeroed and
+//     then scattered from the stage's terms (the tiler orders a step's terms so that each
+//     32 consecutive ones fall in distinct banks where the step allows: mma_bank).
 //
 // Roles (one persistent CTA per SM, 16 warps):
 //   warp 0          TMEM allocation (512 columns: two accumulator sets of 5 x 48) and, on one
@@ -35,9 +36,9 @@
 //                   g % 6 into stage slot g % kMmaStages
 //   warps 4-11      epilogue: warp w reads TMEM lanes 32 (w % 4) + 0..31 (= frames) and half
 //                   of the tile's bins (8 bins x 5 accumulators at a time), recombines, puts the
-//                   cake values into a shared-memory tile holding two adjacent tiles of the item
-//                   (8 columns: 32-byte rows, whole sectors) that one TMA tensor store writes
-//                   to the [F][n_r][n_eta] cake, and accumulates the lineout
+//                   cake values into a shared-memory image holding two adjacent tiles of the
+//                   item (8 columns: 32-byte rows, whole sectors) that one TMA tensor store
+//                   writes to the [F][n_r][n_eta] cake, and accumulates the lineout
 //                   partial sums of the item's rows in registers (a frame's result does not
 //                   depend on the rest of its batch)
 // Every wait is an mbarrier poll with an iteration limit; on expiry the kernel sets the
@@ -82,10 +83,9 @@ constexpr int kMmaTmemCols = 512;
 constexpr int kMmaAccCols = 256;            // columns per accumulator set (5 x 48 used)
 constexpr uint32_t kMmaOutBytes = kMmaFrames * kMmaN * 4;   // one cake tile: [128][rows][4] floats
 // The epilogue stores two adjacent tiles of an item (8 columns) with one box: 32-byte rows
-constexpr int kMmaBoxes = 8;                // cake store boxes of 4 and 8 columns x 12, 6, 3, 1 rows
 
 struct MmaArgs {
-  CUtensorMap tmap[kMmaBoxes];  // the call's cake as (n_eta, n_r, F) floats, box w x h x 128
+  CUtensorMap tmap[kCakeBoxes];  // the call's cake as (n_eta, F, n_r) floats (encode_cake_boxes)
   const WorkItem *items;
   const TileRef *tiles;
   const uint8_t *blobs;
@@ -130,10 +130,10 @@ __host__ __device__ inline MmaSmem mma_smem_layout(uint32_t blob_cap, int n_blob
   return L;
 }
 
-// instruction descriptor, kind::i8: D s32, A u8 MN-major, B u8 K-major, M = 128, N = 48
+// instruction descriptor, kind::i8: D s32, A u8 MN-major, B s8 K-major, M = 128, N = 48
 // with N = 192 (the four weight planes, 48 bins each, side by side), 144 (planes 0-2) or 48
 __host__ __device__ constexpr uint32_t mma_idesc(int n) {
-  return (2u << 4) | (1u << 15) | ((uint32_t)(n >> 3) << 17) | ((uint32_t)(kMmaFrames >> 4) << 24);
+  return (2u << 4) | (1u << 10) | (1u << 15) | ((uint32_t)(n >> 3) << 17) | ((uint32_t)(kMmaFrames >> 4) << 24);
 }
 
 __device__ __forceinline__ void m_mma(uint32_t d_tmem, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
@@ -448,8 +448,8 @@ __global__ void __launch_bounds__(kMmaThreads, 1) k_mma(const __grid_constant__ 
 #pragma unroll
         for (int i = 0; i < kHalfRows; ++i) saw[i] = ssm[i] = 0.0;
       }
-      // cake tiles go out in pairs: the item's tiles 2i and 2i+1 share one [128][box][8] tile of
-      // shared memory and one 8-column store; an item's odd last tile goes alone, [128][box][4]
+      // cake tiles go out in pairs through one store box (cake_box_off); an item's odd last
+      // tile goes alone
       float *ot = (float *)(smem + L.off_out);
       const bool second = (tg.pos & 1) != 0;
       const int pitch = (second || !tg.last) ? 2 * kMmaCols : kMmaCols;
@@ -489,8 +489,8 @@ __global__ void __launch_bounds__(kMmaThreads, 1) k_mma(const __grid_constant__ 
 #pragma unroll
         for (int i = 0; i < 8; ++i) {
           const int lrow = (8 * c + i) / kMmaCols;
-          const double x4 = m_u2d(r[4][i]), x3 = m_u2d(r[3][i]), x2 = m_u2d(r[2][i]), x1 = m_u2d(r[1][i]),
-                       x0 = m_u2d(r[0][i]);
+          const double x4 = m_i2d(r[4][i]), x3 = m_i2d(r[3][i]), x2 = m_i2d(r[2][i]), x1 = m_i2d(r[1][i]),
+                       x0 = m_i2d(r[0][i]);
           // sum_k 2^(8k) x_k = (256 x4 + x3) 2^24 + (256 x2 + x1) 256 + x0
           const double v = fma(fma(x4, 256.0, x3), 16777216.0, fma(fma(x2, 256.0, x1), 256.0, x0));
           const double res = fma(bfac[8 * c + i], v, -bdk[8 * c + i]);
@@ -511,7 +511,7 @@ __global__ void __launch_bounds__(kMmaThreads, 1) k_mma(const __grid_constant__ 
 #pragma unroll
           for (int q = 0; q < 2; ++q) {
             const int row = kHalfRows * half + 2 * c + q;
-            if (row < tg.box) *(float4 *)(ot + ((size_t)m * tg.box + row) * pitch + coff) =
+            if (row < tg.box) *(float4 *)(ot + cake_box_off(row, m, pitch, coff)) =
                 make_float4(o[4 * q], o[4 * q + 1], o[4 * q + 2], o[4 * q + 3]);
           }
         }
@@ -520,10 +520,10 @@ __global__ void __launch_bounds__(kMmaThreads, 1) k_mma(const __grid_constant__ 
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
         asm volatile("bar.sync 1, %0;" ::"r"(kMmaEpiWarps * 32) : "memory");
         if (issuer) {
-          const int bi = (tg.box == kMmaRows ? 0 : (tg.box == 6 ? 1 : (tg.box == 3 ? 2 : 3))) + (second ? 4 : 0);
+          const int bi = cake_box_index(tg.box, second);
           asm volatile(
               "cp.async.bulk.tensor.3d.global.shared::cta.bulk_group [%0, {%1, %2, %3}], [%4];" ::"l"(&a.tmap[bi]),
-              "r"(tg.e0 - coff), "r"(tg.r0), "r"(0), "r"(m_smem(ot))
+              "r"(tg.e0 - coff), "r"(0), "r"(tg.r0), "r"(m_smem(ot))
               : "memory");
           asm volatile("cp.async.bulk.commit_group;" ::: "memory");
         }
@@ -580,7 +580,7 @@ __global__ void k_mma_dark(const TileRef *tiles, uint8_t *blobs, const int32_t *
         const uint32_t k0 = runs[r].y & 0xFFu, len = runs[r].y >> 8;
         if (kk >= k0 && kk < k0 + len) { c = runs[r].x + (kk - k0); break; }
       }
-      d += (double)tm.x * (double)dark[xc_pix[c]];
+      d += (double)mma_digits_value(tm.x) * (double)dark[xc_pix[c]];
     }
   dk[n] = fac[n] * d;
 }
@@ -612,20 +612,8 @@ int launch_mma(Plan *p, int F, float *cake, double *partial, bool want_lo, cudaS
   // (n_eta % 4 == 0) and the cake is 16-byte aligned; otherwise through plain stores
   a.use_tma = 0;
   if (cake && p->n_eta % kMmaCols == 0 && (uintptr_t)cake % 16 == 0) {
-    EncodeTiledFn enc = encode_tiled();
-    if (!enc) return set_error(MI_E_CUDA, "launch_mma: cuTensorMapEncodeTiled is not available");
-    const cuuint64_t dims[3] = {(cuuint64_t)p->n_eta, (cuuint64_t)p->n_r, (cuuint64_t)F};
-    const cuuint64_t strides[2] = {(cuuint64_t)p->n_eta * 4u, (cuuint64_t)p->n_bins * 4u};
-    const cuuint32_t estr[3] = {1, 1, 1};
-    const int rows[4] = {kMmaRows, 6, 3, 1};
-    for (int i = 0; i < kMmaBoxes; ++i) {
-      const cuuint32_t box[3] = {(cuuint32_t)(i < 4 ? kMmaCols : 2 * kMmaCols), (cuuint32_t)rows[i % 4],
-                                 (cuuint32_t)kMmaFrames};
-      const CUresult r = enc(&a.tmap[i], CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, cake, dims, strides, box, estr,
-                             CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
-                             CU_TENSOR_MAP_L2_PROMOTION_NONE, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
-      if (r != CUDA_SUCCESS) return set_error(MI_E_CUDA, "launch_mma: cuTensorMapEncodeTiled failed (%d)", (int)r);
-    }
+    const int rc = encode_cake_boxes(a.tmap, cake, p->n_eta, p->n_r, p->n_bins, F, "launch_mma");
+    if (rc != MI_OK) return rc;
     a.use_tma = 1;
   }
   // up to four blob slots, as shared memory allows (two suffice for progress: the epilogue

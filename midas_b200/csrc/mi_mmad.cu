@@ -72,10 +72,9 @@ constexpr int kDBlobSlotsMax = 4;
 constexpr int kDFacSlots = 6;
 constexpr uint32_t kDFacBytes = 1024;
 constexpr uint32_t kDOutBytes = kMmaFrames * kMmaN * 4;
-constexpr int kDBoxes = 8;
 
 struct MmadArgs {
-  CUtensorMap tmap[kDBoxes];
+  CUtensorMap tmap[kCakeBoxes];
   const WorkItem *items;
   const TileRef *tiles;
   const uint8_t *blobs;
@@ -123,9 +122,9 @@ __host__ __device__ inline MmadSmem mmad_smem_layout(uint32_t blob_cap, int n_bl
   return L;
 }
 
-// instruction descriptor, kind::i8: D s32, A u8 K-major (tensor memory), B u8 K-major, M = 128
+// instruction descriptor, kind::i8: D s32, A u8 K-major (tensor memory), B s8 K-major, M = 128
 __host__ __device__ constexpr uint32_t mmad_idesc(int n) {
-  return (2u << 4) | ((uint32_t)(n >> 3) << 17) | ((uint32_t)(kMmaFrames >> 4) << 24);
+  return (2u << 4) | (1u << 10) | ((uint32_t)(n >> 3) << 17) | ((uint32_t)(kMmaFrames >> 4) << 24);
 }
 
 __device__ __forceinline__ void m_mma_ta(uint32_t d_tmem, uint32_t a_tmem, uint64_t bdesc, uint32_t idesc,
@@ -561,8 +560,8 @@ __global__ void __launch_bounds__(kDThreads, 1) k_mmad(const __grid_constant__ M
 #pragma unroll
         for (int i = 0; i < 8; ++i) {
           const int lrow = (8 * c + i) / kMmaCols;
-          const double x4 = m_u2d(r[4][i]), x3 = m_u2d(r[3][i]), x2 = m_u2d(r[2][i]), x1 = m_u2d(r[1][i]),
-                       x0 = m_u2d(r[0][i]);
+          const double x4 = m_i2d(r[4][i]), x3 = m_i2d(r[3][i]), x2 = m_i2d(r[2][i]), x1 = m_i2d(r[1][i]),
+                       x0 = m_i2d(r[0][i]);
           // sum_k 2^(8k) x_k = (256 x4 + x3) 2^24 + (256 x2 + x1) 256 + x0
           const double v = fma(fma(x4, 256.0, x3), 16777216.0, fma(fma(x2, 256.0, x1), 256.0, x0));
           const double res = fma(bfac[8 * c + i], v, -bdk[8 * c + i]);
@@ -582,7 +581,7 @@ __global__ void __launch_bounds__(kDThreads, 1) k_mmad(const __grid_constant__ M
 #pragma unroll
           for (int q = 0; q < 2; ++q) {
             const int row = kHalfRows * half + 2 * c + q;
-            if (row < tg.box) *(float4 *)(ot + ((size_t)m * tg.box + row) * pitch + coff) =
+            if (row < tg.box) *(float4 *)(ot + cake_box_off(row, m, pitch, coff)) =
                 make_float4(o[4 * q], o[4 * q + 1], o[4 * q + 2], o[4 * q + 3]);
           }
         }
@@ -591,10 +590,10 @@ __global__ void __launch_bounds__(kDThreads, 1) k_mmad(const __grid_constant__ M
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
         asm volatile("bar.sync 1, %0;" ::"r"(kDEpiWarps * 32) : "memory");
         if (issuer) {
-          const int bi = (tg.box == kMmaRows ? 0 : (tg.box == 6 ? 1 : (tg.box == 3 ? 2 : 3))) + (second ? 4 : 0);
+          const int bi = cake_box_index(tg.box, second);
           asm volatile(
               "cp.async.bulk.tensor.3d.global.shared::cta.bulk_group [%0, {%1, %2, %3}], [%4];" ::"l"(&a.tmap[bi]),
-              "r"(tg.e0 - coff), "r"(tg.r0), "r"(0), "r"(m_smem(ot))
+              "r"(tg.e0 - coff), "r"(0), "r"(tg.r0), "r"(m_smem(ot))
               : "memory");
           asm volatile("cp.async.bulk.commit_group;" ::: "memory");
         }
@@ -643,7 +642,7 @@ __global__ void k_mmad_dark(const TileRef *tiles, uint8_t *blobs, int ny, const 
       if ((int)(tm.y >> 16) != n) continue;
       const uint32_t k = tm.y & 0xFFFFu, g = gran[k / kMmadGranPx];
       const size_t px = (size_t)(g & 0xFFFFu) * (size_t)ny + (g >> 16) + (k % kMmadGranPx);
-      d += (double)tm.x * (double)dark[px];
+      d += (double)mma_digits_value(tm.x) * (double)dark[px];
     }
   dk[n] = fac[n] * d;
 }
@@ -684,20 +683,8 @@ int launch_mmad(Plan *p, const void *frames, int dtype, int F, int64_t stride, f
   if (a.blob_cap > kMmaBlobCap) return set_error(MI_E_RANGE, "launch_mmad: tile blob of %u B", a.blob_cap);
   a.use_tma = 0;
   if (cake && p->n_eta % kMmaCols == 0 && (uintptr_t)cake % 16 == 0) {
-    EncodeTiledFn enc = encode_tiled();
-    if (!enc) return set_error(MI_E_CUDA, "launch_mmad: cuTensorMapEncodeTiled is not available");
-    const cuuint64_t dims[3] = {(cuuint64_t)p->n_eta, (cuuint64_t)p->n_r, (cuuint64_t)F};
-    const cuuint64_t strides[2] = {(cuuint64_t)p->n_eta * 4u, (cuuint64_t)p->n_bins * 4u};
-    const cuuint32_t estr[3] = {1, 1, 1};
-    const int rows[4] = {kMmaRows, 6, 3, 1};
-    for (int i = 0; i < kDBoxes; ++i) {
-      const cuuint32_t box[3] = {(cuuint32_t)(i < 4 ? kMmaCols : 2 * kMmaCols), (cuuint32_t)rows[i % 4],
-                                 (cuuint32_t)kMmaFrames};
-      const CUresult r = enc(&a.tmap[i], CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, cake, dims, strides, box, estr,
-                             CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
-                             CU_TENSOR_MAP_L2_PROMOTION_NONE, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
-      if (r != CUDA_SUCCESS) return set_error(MI_E_CUDA, "launch_mmad: cuTensorMapEncodeTiled failed (%d)", (int)r);
-    }
+    const int rc = encode_cake_boxes(a.tmap, cake, p->n_eta, p->n_r, p->n_bins, F, "launch_mmad");
+    if (rc != MI_OK) return rc;
     a.use_tma = 1;
   }
   int dev_smem = 0;

@@ -10,6 +10,8 @@
 // written here from the algorithm, not copied.
 #include <stdint.h>
 
+#include <algorithm>
+
 #include "mi_internal.h"
 
 namespace mi {
@@ -270,6 +272,38 @@ int launch_nan_bins(Plan *p, float *cake, int n_frames, cudaStream_t s) {
   if (!cake || p->n_nan_bins == 0 || n_frames <= 0) return MI_OK;
   const int64_t n = (int64_t)p->n_nan_bins * n_frames;
   k_nan_bins<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(cake, p->n_bins, p->d_nan_bins, p->n_nan_bins, n_frames);
+  MI_CUDA(cudaGetLastError());
+  return MI_OK;
+}
+
+// SumImages (IntegratorFitPeaksGPUStream.cu:1043-1046 into dSumMatrix, allocated at
+// :2141-2144): sum[b] += cake[f][b] over the batch's frames, in FP64, frames in order (the
+// reference adds per frame with atomics in any order); NaN bins (masked bins of the OpenMP
+// semantics) add nothing.  Thread per bin; eight frames' loads in flight before the adds.
+__global__ void k_sum_cake(const float *__restrict__ cake, int F, int64_t n_bins, double *__restrict__ sum) {
+  const int64_t step = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t b = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; b < n_bins; b += step) {
+    double s = sum[b];
+    int f = 0;
+    for (; f + 8 <= F; f += 8) {
+      float v[8];
+#pragma unroll
+      for (int u = 0; u < 8; ++u) v[u] = __ldcs(cake + (int64_t)(f + u) * n_bins + b);
+#pragma unroll
+      for (int u = 0; u < 8; ++u) s += isnan(v[u]) ? 0.0 : (double)v[u];
+    }
+    for (; f < F; ++f) {
+      const float v = __ldcs(cake + (int64_t)f * n_bins + b);
+      s += isnan(v) ? 0.0 : (double)v;
+    }
+    sum[b] = s;
+  }
+}
+
+int launch_sum_cake(Plan *p, const float *cake, int n_frames, double *sum, cudaStream_t s) {
+  if (n_frames <= 0 || p->n_bins == 0) return MI_OK;
+  const int64_t blocks = std::min<int64_t>((p->n_bins + 255) / 256, (int64_t)std::max(p->n_sms, 1) * 8);
+  k_sum_cake<<<(unsigned)blocks, 256, 0, s>>>(cake, n_frames, p->n_bins, sum);
   MI_CUDA(cudaGetLastError());
   return MI_OK;
 }

@@ -587,6 +587,40 @@ static int upload(T **dst, const T *src, size_t n, size_t *acct) {
   return MI_OK;
 }
 
+// A weight of a tensor-core tile: signed fixed point relative to the bin's largest |w|,
+// packed as four s8 digits (mma_digits).
+static uint32_t mma_weight(double w, double wm) {
+  double qd = wm > 0.0 ? (double)std::llround(w / wm * kMmaQMax) : 0.0;
+  qd = std::min(std::max(qd, -kMmaQMax), kMmaQMax);
+  return mma_digits((int64_t)qd);
+}
+
+// Within each K step, order the terms so that every 32 consecutive ones (the 32 lanes of one
+// store of the B operand builders, which start at the step's first term) fall in distinct
+// shared-memory banks as far as the step's terms allow: each group takes one term per bank,
+// fullest banks first, and repeats banks only when fewer than 32 are left to draw from.
+static void bank_order(std::vector<uint2> &terms, const std::vector<uint32_t> &sp, int n_k) {
+  std::vector<uint2> bucket[32];
+  int order[32];
+  for (int st = 0; st < n_k; ++st) {
+    for (auto &b : bucket) b.clear();
+    for (uint32_t t = sp[st]; t < sp[st + 1]; ++t)
+      bucket[mma_bank(terms[t].y >> 16, (terms[t].y & 0xFFFFu) % kMmaKStep)].push_back(terms[t]);
+    uint32_t pos = sp[st];
+    while (pos < sp[st + 1]) {
+      for (int b = 0; b < 32; ++b) order[b] = b;
+      std::stable_sort(order, order + 32, [&](int x, int y) { return bucket[x].size() > bucket[y].size(); });
+      const uint32_t g_end = std::min(pos + 32u, sp[st + 1]);
+      while (pos < g_end)
+        for (int i = 0; i < 32 && pos < g_end; ++i)
+          if (!bucket[order[i]].empty()) {
+            terms[pos++] = bucket[order[i]].back();
+            bucket[order[i]].pop_back();
+          }
+    }
+  }
+}
+
 // ---- MMA encoding: tiles of up to kMmaRows x kMmaCols bins (see MmaHdr).  Each band of
 // kMmaRows rows is cut into sub-bands of h rows (h = 12, 6, 3, 1: the largest whose tile
 // blobs all fit the kernel's blob slots); a work item is a sub-band x item_cols columns,
@@ -699,9 +733,7 @@ static int mma_tile_blob(const HostCSR &csr, const mi_map_desc &m, const std::ve
       blw[n] = lw[b];
       const double wm = wmax[b];
       for (int64_t t = csr.row_ptr[b]; t < csr.row_ptr[b + 1]; ++t) {
-        double qd = wm > 0.0 ? std::llround(csr.w[t] / wm * 4294967295.0) : 0.0;
-        qd = std::min(std::max(qd, 0.0), 4294967295.0);
-        terms.push_back(make_uint2((uint32_t)qd, (uint32_t)lut[csr.col[t]] | (n << 16)));
+        terms.push_back(make_uint2(mma_weight(csr.w[t], wm), (uint32_t)lut[csr.col[t]] | (n << 16)));
       }
     }
   std::stable_sort(terms.begin(), terms.end(),
@@ -709,6 +741,7 @@ static int mma_tile_blob(const HostCSR &csr, const mi_map_desc &m, const std::ve
   std::vector<uint32_t> sp(n_k + 1, 0);
   for (const uint2 &t : terms) ++sp[(t.y & 0xFFFFu) / kMmaKStep + 1];
   for (int s = 0; s < n_k; ++s) sp[s + 1] += sp[s];
+  bank_order(terms, sp, n_k);
   for (int32_t q : pix) lut[q] = -1;
   const MmaBlob L = mma_blob_layout(n_k, (int)runs.size(), (int)terms.size());
   blob.assign(L.bytes, 0);
@@ -728,7 +761,7 @@ static int mma_tile_blob(const HostCSR &csr, const mi_map_desc &m, const std::ve
 
 // ---- Direct MMA encoding (see MmadBlob): the tile's pixels covered by 8-pixel row granules
 // in (row, column) order, four granules per K step; pixel (z, y) of granule g sits in slot
-// 8 g + (y - y0).  Weights in 32-bit fixed point relative to the bin's largest weight.
+// 8 g + (y - y0).  Weights as in the MMA encoding (mma_weight).
 static int mmad_tile_blob(const HostCSR &csr, const mi_map_desc &m, const std::vector<double> &wmax,
                           const std::vector<double> &fac, const std::vector<float> &lw, int r0, int nr, int box_rows,
                           int e0, int nc, std::vector<int32_t> &lut, std::vector<uint8_t> &blob, int *nnz_out,
@@ -773,9 +806,7 @@ static int mmad_tile_blob(const HostCSR &csr, const mi_map_desc &m, const std::v
       blw[n] = lw[b];
       const double wm = wmax[b];
       for (int64_t t = csr.row_ptr[b]; t < csr.row_ptr[b + 1]; ++t) {
-        double qd = wm > 0.0 ? std::llround(csr.w[t] / wm * kMmadQMax) : 0.0;
-        qd = std::min(std::max(qd, 0.0), kMmadQMax);
-        terms.push_back(make_uint2((uint32_t)qd, (uint32_t)lut[csr.col[t]] | (n << 16)));
+        terms.push_back(make_uint2(mma_weight(csr.w[t], wm), (uint32_t)lut[csr.col[t]] | (n << 16)));
       }
     }
   std::stable_sort(terms.begin(), terms.end(),
@@ -783,6 +814,7 @@ static int mmad_tile_blob(const HostCSR &csr, const mi_map_desc &m, const std::v
   std::vector<uint32_t> sp(n_k + 1, 0);
   for (const uint2 &t : terms) ++sp[(t.y & 0xFFFFu) / kMmaKStep + 1];
   for (int s2 = 0; s2 < n_k; ++s2) sp[s2 + 1] += sp[s2];
+  bank_order(terms, sp, n_k);
   for (int32_t q : pix) lut[q] = -1;
   const MmadBlob L = mmad_blob_layout(n_k, (int)terms.size());
   blob.assign(L.bytes, 0);
@@ -803,7 +835,6 @@ static int build_mma_tiles(const HostCSR &csr, const mi_map_desc &m, Plan *p, co
                            const std::vector<int32_t> &row_off, bool direct, int *n_slots_out,
                            std::vector<TileRef> *tiles_out, std::vector<WorkItem> *items_out,
                            std::vector<uint8_t> *blobs_out) {
-  const double qmax = direct ? kMmadQMax : 4294967295.0;
   const int64_t n_bins = (int64_t)m.n_r * m.n_eta, n_pix = (int64_t)m.ny * m.nz;
   std::vector<double> wmax(n_bins, 0.0), fac(n_bins, 0.0);
   std::vector<float> lw(n_bins, 0.0f);
@@ -812,12 +843,12 @@ static int build_mma_tiles(const HostCSR &csr, const mi_map_desc &m, Plan *p, co
       return set_error(MI_E_RANGE, "bin %lld has more than %d terms: use the run encoding", (long long)b,
                        kMmaMaxBinTerms);
     double wm = 0.0;
-    for (int64_t t = csr.row_ptr[b]; t < csr.row_ptr[b + 1]; ++t) wm = std::max(wm, csr.w[t]);
+    for (int64_t t = csr.row_ptr[b]; t < csr.row_ptr[b + 1]; ++t) wm = std::max(wm, std::fabs(csr.w[t]));
     wmax[b] = wm;
     float sc32;
     double sc;
     bin_scale(csr, p, b, &sc32, &lw[b], &sc);
-    fac[b] = wm / qmax * sc;
+    fac[b] = wm / kMmaQMax * sc;
   }
   // items of about 12 per band, on 8-column (32-byte) cake boundaries when there are enough
   // columns, always on kMmaCols boundaries
@@ -1299,6 +1330,125 @@ static int build_plan(const mi_map_desc &m, const mi_plan_opts &o, Plan *p, Host
 
 using namespace mi;
 
+// ---------------------------------------------------------------------------
+// Fused multi-shift maps (build_fused_geometry, packages/midas_integrate/midas_integrate/
+// fused_csr.py:139-296): N maps whose R edges are shifted by k / N of a bin, each
+// area-normalised (1 / area_in where it exceeds the area threshold, else 0: D_k), moved
+// onto shift 0's R axis by linear interpolation in R (P_k, fused_csr.py:63-104: at most two
+// source rows per target row, identity in eta) and averaged:
+//   M = 1/N sum_k P_k D_k M_k,  every bin's area 1 (the normalisation is in the weights).
+// ---------------------------------------------------------------------------
+namespace mi {
+static void interp_row(const double *src, int n_src, double r, int *j, double *wl, double *wh) {
+  if (r <= src[0]) {
+    *j = 0; *wl = 1.0; *wh = 0.0;
+  } else if (r >= src[n_src - 1]) {
+    *j = n_src - 2; *wl = 0.0; *wh = 1.0;
+  } else {
+    int jj = (int)(std::upper_bound(src, src + n_src, r) - src) - 1;
+    jj = std::max(0, std::min(jj, n_src - 2));
+    const double den = src[jj + 1] - src[jj];
+    const double t = den > 0.0 ? (r - src[jj]) / den : 0.0;
+    *j = jj; *wl = 1.0 - t; *wh = t;
+  }
+}
+
+int build_fused_csr(const mi_map_desc *maps, int n_shifts, const double *const *r_axes, int mode, HostCSR *out) {
+  if (!maps || !r_axes || n_shifts < 1) return set_error(MI_E_ARG, "fused map: null argument or no shifts");
+  if (mode != MI_MODE_BILINEAR && mode != MI_MODE_GRADIENT)
+    return set_error(MI_E_ARG, "fused map: mode must be bilinear or gradient");
+  const mi_map_desc &m0 = maps[0];
+  for (int k = 0; k < n_shifts; ++k) {
+    const mi_map_desc &m = maps[k];
+    if (m.n_eta != m0.n_eta || m.ny != m0.ny || m.nz != m0.nz)
+      return set_error(MI_E_ARG, "fused map: shift %d has another eta binning or detector shape", k);
+    if (m.n_r < 2 || m.n_eta <= 0 || m.ny < 2 || m.nz < 2 || !m.nmap || (m.n_records > 0 && !m.records) ||
+        !r_axes[k])
+      return set_error(MI_E_ARG, "fused map: shift %d has a bad shape or null arrays (two R bins at least)", k);
+  }
+  const int n_eta = m0.n_eta, n_r0 = m0.n_r;
+  const int64_t n_bins = (int64_t)n_r0 * n_eta;
+  std::vector<HostCSR> part(n_shifts);
+  std::vector<std::vector<double>> inv_a(n_shifts);
+  std::vector<int> jlo((size_t)n_shifts * n_r0);
+  std::vector<double> wlo((size_t)n_shifts * n_r0), whi((size_t)n_shifts * n_r0);
+  int64_t oob = 0;
+  for (int k = 0; k < n_shifts; ++k) {
+    int rc = build_host_csr(maps[k], mode, MI_SEM_PY, &part[k]);
+    if (rc) return rc;
+    oob += part[k].oob;
+    inv_a[k].resize(part[k].area_in.size());
+    for (size_t b = 0; b < inv_a[k].size(); ++b) {
+      const double a = part[k].area_in[b];
+      inv_a[k][b] = a > kAreaThreshold ? 1.0 / std::max(a, kAreaThreshold) : 0.0;
+    }
+    for (int i = 0; i < n_r0; ++i)
+      interp_row(r_axes[k], maps[k].n_r, r_axes[0][i], &jlo[(size_t)k * n_r0 + i], &wlo[(size_t)k * n_r0 + i],
+                 &whi[(size_t)k * n_r0 + i]);
+  }
+  const double inv_n = 1.0 / n_shifts;
+  auto gather = [&](int64_t b, std::vector<Term> &t) {
+    t.clear();
+    const int i = (int)(b / n_eta), e = (int)(b % n_eta);
+    for (int k = 0; k < n_shifts; ++k) {
+      const size_t q = (size_t)k * n_r0 + i;
+      const int js[2] = {jlo[q], jlo[q] + 1};
+      const double ws[2] = {wlo[q], whi[q]};
+      for (int h = 0; h < 2; ++h) {
+        if (ws[h] == 0.0) continue;
+        const int64_t bs = (int64_t)js[h] * n_eta + e;
+        const double f = ws[h] * inv_a[k][bs] * inv_n;
+        if (f == 0.0) continue;
+        for (int64_t x = part[k].row_ptr[bs]; x < part[k].row_ptr[bs + 1]; ++x)
+          t.push_back({part[k].col[x], part[k].w[x] * f});
+      }
+    }
+    std::stable_sort(t.begin(), t.end(), [](const Term &a, const Term &c) { return a.col < c.col; });
+    size_t o = 0;
+    for (size_t x = 0; x < t.size();) {
+      size_t y = x;
+      double sum = 0.0;
+      while (y < t.size() && t[y].col == t[x].col) sum += t[y++].w;
+      if (sum != 0.0) t[o++] = {t[x].col, sum};
+      x = y;
+    }
+    t.resize(o);
+  };
+  std::vector<int64_t> counts(n_bins + 1, 0);
+#pragma omp parallel
+  {
+    std::vector<Term> t;
+#pragma omp for schedule(dynamic, 256)
+    for (int64_t b = 0; b < n_bins; ++b) {
+      gather(b, t);
+      counts[b + 1] = (int64_t)t.size();
+    }
+  }
+  out->row_ptr.assign(n_bins + 1, 0);
+  for (int64_t b = 0; b < n_bins; ++b) out->row_ptr[b + 1] = out->row_ptr[b] + counts[b + 1];
+  out->col.resize(out->row_ptr[n_bins]);
+  out->w.resize(out->row_ptr[n_bins]);
+#pragma omp parallel
+  {
+    std::vector<Term> t;
+#pragma omp for schedule(dynamic, 256)
+    for (int64_t b = 0; b < n_bins; ++b) {
+      gather(b, t);
+      int64_t o = out->row_ptr[b];
+      for (const Term &x : t) {
+        out->col[o] = x.col;
+        out->w[o++] = x.w;
+      }
+    }
+  }
+  out->area_in.assign(n_bins, 1.0);
+  out->area_norm.assign(n_bins, 1.0);
+  out->area_gs.assign(n_bins, 1.0);
+  out->oob = oob;
+  return MI_OK;
+}
+}  // namespace mi
+
 struct mi_plan : public mi::Plan {};
 
 extern "C" {
@@ -1442,6 +1592,69 @@ int mi_plan_create_panels(const mi_map_desc *maps, int n_panels, const mi_plan_o
   cudaSetDevice(prev);
   if (rc == MI_OK && p->n_xc == 0)
     rc = set_error(MI_E_UNSUPPORTED, "mi_plan_create_panels: the plan has no pixel-major staging");
+  if (rc) {
+    free_plan_mem(p);
+    delete p;
+    return rc;
+  }
+  *out = p;
+  return MI_OK;
+}
+
+int mi_fused_csr(const mi_map_desc *maps, int n_shifts, const double *const *r_axes, int mode, int64_t *row_ptr,
+                 int32_t *col, double *w, int64_t capacity, int64_t *nnz) {
+  if (!nnz) return set_error(MI_E_ARG, "mi_fused_csr: null nnz");
+  HostCSR csr;
+  int rc = build_fused_csr(maps, n_shifts, r_axes, mode, &csr);
+  if (rc) return rc;
+  const int64_t n = (int64_t)csr.col.size();
+  *nnz = n;
+  if (row_ptr) memcpy(row_ptr, csr.row_ptr.data(), csr.row_ptr.size() * sizeof(int64_t));
+  if (col || w) {
+    if (!col || !w) return set_error(MI_E_ARG, "mi_fused_csr: col and w go together");
+    if (capacity < n) return set_error(MI_E_RANGE, "mi_fused_csr: %lld terms, capacity %lld", (long long)n,
+                                       (long long)capacity);
+    if (n) {
+      memcpy(col, csr.col.data(), n * sizeof(int32_t));
+      memcpy(w, csr.w.data(), n * sizeof(double));
+    }
+  }
+  return MI_OK;
+}
+
+int mi_plan_create_fused(const mi_map_desc *maps, int n_shifts, const double *const *r_axes, const mi_plan_opts *opts,
+                         int device, mi_plan **out) {
+  if (!out) return set_error(MI_E_ARG, "mi_plan_create_fused: null argument");
+  *out = nullptr;
+  mi_plan_opts o{};
+  if (opts) o = *opts;
+  else { o.mode = MI_MODE_GRADIENT; o.normalize = 1; o.semantics = MI_SEM_PY; }
+  if (o.semantics != MI_SEM_PY || o.variance)
+    return set_error(MI_E_UNSUPPORTED, "mi_plan_create_fused: fused maps are midas_integrate CSR geometries "
+                                       "(py semantics, no variance plan)");
+  if (!maps || n_shifts < 1) return set_error(MI_E_ARG, "mi_plan_create_fused: null argument or no shifts");
+  if ((int64_t)maps[0].ny * maps[0].nz > (int64_t)INT32_MAX)
+    return set_error(MI_E_RANGE, "mi_plan_create_fused: detector larger than 2^31 pixels");
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
+    return set_error(MI_E_CUDA, "mi_plan_create_fused: no CUDA device available");
+  if (device < 0 || device >= ndev) return set_error(MI_E_ARG, "mi_plan_create_fused: bad device %d", device);
+  HostThreads ht(o.host_threads);
+  HostCSR csr;
+  int rc = build_fused_csr(maps, n_shifts, r_axes, o.mode, &csr);
+  if (rc) return rc;
+  mi_map_desc vm = maps[0];
+  vm.records = nullptr;
+  vm.nmap = nullptr;
+  vm.n_records = 0;
+  for (int k = 0; k < n_shifts; ++k) vm.n_records += maps[k].n_records;
+  mi_plan *p = new (std::nothrow) mi_plan();
+  if (!p) return set_error(MI_E_OOM, "mi_plan_create_fused: host allocation failed");
+  p->device = device;
+  int prev = 0;
+  cudaGetDevice(&prev);
+  rc = build_plan(vm, o, p, &csr);
+  cudaSetDevice(prev);
   if (rc) {
     free_plan_mem(p);
     delete p;
@@ -1718,6 +1931,17 @@ int mi_profile_batch(mi_plan *p, const void *cake, int cake_dtype, int n_frames,
   cudaGetDevice(&prev);
   if (prev != p->device) MI_CUDA(cudaSetDevice(p->device));
   int rc = launch_profile(p, cake, cake_dtype, n_frames, lo_aw, lo_sm, (cudaStream_t)stream);
+  if (prev != p->device) cudaSetDevice(prev);
+  return rc;
+}
+
+int mi_sum_cake(mi_plan *p, const float *cake, int n_frames, double *sum, void *stream) {
+  if (!p || !sum || (n_frames > 0 && !cake)) return set_error(MI_E_ARG, "mi_sum_cake: null argument");
+  if (n_frames < 0) return set_error(MI_E_ARG, "mi_sum_cake: n_frames < 0");
+  int prev = 0;
+  cudaGetDevice(&prev);
+  if (prev != p->device) MI_CUDA(cudaSetDevice(p->device));
+  int rc = launch_sum_cake(p, cake, n_frames, sum, (cudaStream_t)stream);
   if (prev != p->device) cudaSetDevice(prev);
   return rc;
 }

@@ -7,6 +7,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include "mi_internal.h"
+
 namespace mi {
 
 constexpr uint32_t kMmaWaitLimit = 1u << 26;   // mbarrier polls before a wait is declared lost
@@ -73,8 +75,11 @@ __device__ __forceinline__ void m_ld8(uint32_t taddr, uint32_t *r) {
 }
 __device__ __forceinline__ void m_ld_wait() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
 
-// non-negative int32 -> double exactly, on the FP64 pipe: 2^52 + x has x in its low bits
-__device__ __forceinline__ double m_u2d(uint32_t x) { return __hiloint2double(0x43300000, (int)x) - 4503599627370496.0; }
+// int32 -> double exactly, on the FP64 pipe: 2^52 + (x + 2^31) has x + 2^31 (the sign bit
+// flipped) in its low bits
+__device__ __forceinline__ double m_i2d(uint32_t x) {
+  return __hiloint2double(0x43300000, (int)(x ^ 0x80000000u)) - 4503601774854144.0;
+}
 
 typedef CUresult (*EncodeTiledFn)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
                                   const cuuint64_t *, const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave,
@@ -93,6 +98,43 @@ inline EncodeTiledFn encode_tiled() {
       fn = (EncodeTiledFn)f;
   }
   return fn;
+}
+
+// ---- cake store boxes of the tensor-core kernels.  An item's tiles leave in pairs: tiles 2i
+// and 2i+1 (8 adjacent columns) share one shared-memory image and one TMA tensor store; an
+// item's odd last tile goes alone (4 columns).  The tensor map views the [F][n_r][n_eta]
+// cake as (n_eta, F, n_r), so a box's image is [rows][128 frames][columns]: the epilogue
+// lane of frame m writes float4s 32 (pair) or 16 bytes apart from its neighbours'.  Pair
+// images use the 32-byte swizzle (the 16-byte half of a row flipped when bit 7 of its
+// address, here bit 2 of the frame, is set), so every 8 lanes of a warp cover the 32 banks
+// once: 4 wavefronts per warp store, the minimum for 512 bytes.
+constexpr int kCakeBoxes = 8;   // 4 and 8 columns x 12, 6, 3, 1 rows
+__device__ __forceinline__ int cake_box_off(int row, int m, int pitch, int coff) {
+  return (row * kMmaFrames + m) * pitch + (pitch == 2 * kMmaCols ? (coff ^ ((m & 4) ? kMmaCols : 0)) : coff);
+}
+__device__ __forceinline__ int cake_box_index(int box_rows, bool pair) {
+  return (box_rows == kMmaRows ? 0 : (box_rows == 6 ? 1 : (box_rows == 3 ? 2 : 3))) + (pair ? 4 : 0);
+}
+// the eight maps of a call's cake (F frames); the caller has checked n_eta % 4 == 0 and a
+// 16-byte aligned cake
+inline int encode_cake_boxes(CUtensorMap *maps, float *cake, int n_eta, int n_r, int64_t n_bins, int F,
+                             const char *who) {
+  EncodeTiledFn enc = encode_tiled();
+  if (!enc) return set_error(MI_E_CUDA, "%s: cuTensorMapEncodeTiled is not available", who);
+  const cuuint64_t dims[3] = {(cuuint64_t)n_eta, (cuuint64_t)F, (cuuint64_t)n_r};
+  const cuuint64_t strides[2] = {(cuuint64_t)n_bins * 4u, (cuuint64_t)n_eta * 4u};
+  const cuuint32_t estr[3] = {1, 1, 1};
+  const int rows[4] = {kMmaRows, 6, 3, 1};
+  for (int i = 0; i < kCakeBoxes; ++i) {
+    const bool pair = i >= 4;
+    const cuuint32_t box[3] = {(cuuint32_t)(pair ? 2 * kMmaCols : kMmaCols), (cuuint32_t)kMmaFrames,
+                               (cuuint32_t)rows[i % 4]};
+    const CUresult r = enc(&maps[i], CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, cake, dims, strides, box, estr,
+                           CU_TENSOR_MAP_INTERLEAVE_NONE, pair ? CU_TENSOR_MAP_SWIZZLE_32B : CU_TENSOR_MAP_SWIZZLE_NONE,
+                           CU_TENSOR_MAP_L2_PROMOTION_NONE, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) return set_error(MI_E_CUDA, "%s: cuTensorMapEncodeTiled failed (%d)", who, (int)r);
+  }
+  return MI_OK;
 }
 
 }  // namespace mi

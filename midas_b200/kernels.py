@@ -180,11 +180,21 @@ class CakePlan:
         return flat, F, flat.stride(0) if F else per
 
     def integrate(self, frames: torch.Tensor, *, cake: bool = True, lineouts: bool = True,
-                  out: Optional[Dict[str, torch.Tensor]] = None, stream=None):
+                  out: Optional[Dict[str, torch.Tensor]] = None, stream=None,
+                  sum_into: Optional[torch.Tensor] = None):
         """Cake a batch of frames (device tensor, any supported dtype).
+
+        sum_into: a float64 [n_r, n_eta] device tensor that the batch's cakes are added to
+        (the SumImages running sum, IntegratorFitPeaksGPUStream.cu:1043-1046; needs cake).
 
         Returns (cake [F, n_r, n_eta] float32 or None, lineout_aw [F, n_r] float64 or None,
         lineout_sm [F, n_r] float64 or None)."""
+        if sum_into is not None:
+            if not cake:
+                raise ValueError("sum_into adds the cakes: cake must be on")
+            if (sum_into.dtype != torch.float64 or sum_into.device != self.device or not sum_into.is_contiguous()
+                    or sum_into.numel() != self.n_bins):
+                raise ValueError("sum_into is a contiguous float64 tensor of n_r x n_eta on the plan's device")
         flat, F, stride = self._frames(frames)
         out = out or {}
         ck = out.get("cake") if cake else None
@@ -202,6 +212,9 @@ class CakePlan:
             L.check(L.lib().mi_integrate_batch(self._h, flat.data_ptr(), dtype_code(flat.dtype), F,
                                                stride, L.ptr(ck), L.ptr(aw), L.ptr(sm),
                                                L.stream_ptr(stream)), "mi_integrate_batch")
+            if sum_into is not None:
+                L.check(L.lib().mi_sum_cake(self._h, ck.data_ptr(), F, sum_into.data_ptr(), L.stream_ptr(stream)),
+                        "mi_sum_cake")
         return ck, aw, sm
 
     def capture(self, frames: torch.Tensor, out: Dict[str, torch.Tensor], *, cake: bool = True,

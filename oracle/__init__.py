@@ -199,6 +199,42 @@ def snip_detect(x, y, *, n_iter=50, x_bin=1.0, max_sel=30):
     return corr, sel[:k].copy()
 
 
+def r_interp(r_src, r_tgt):
+    """Linear interpolation in R of a cake on r_src onto r_tgt, per target row (j, w_lo,
+    w_hi) over source rows j, j + 1: clamped to the first / last pair outside the axis
+    (packages/midas_integrate/midas_integrate/fused_csr.py:63-104)."""
+    src = np.asarray(r_src, np.float64)
+    n = src.size
+    out = []
+    for r in np.asarray(r_tgt, np.float64):
+        if r <= src[0]:
+            out.append((0, 1.0, 0.0))
+        elif r >= src[-1]:
+            out.append((n - 2, 0.0, 1.0))
+        else:
+            j = min(max(int(np.searchsorted(src, r, side="right")) - 1, 0), n - 2)
+            den = src[j + 1] - src[j]
+            t = (r - src[j]) / den if den > 0 else 0.0
+            out.append((j, 1.0 - t, t))
+    return out
+
+
+def fused_average(maps, r_axes, n_eta, ny, nz, image, *, mode="gradient", bc_y=0.0, bc_z=0.0):
+    """Naive multi-map averaging, which the fused geometry folds into one matrix
+    (fused_csr.py:1-37, 212-250): each shift's normalised py-semantics cake, interpolated
+    in R onto shift 0's axis, averaged over the shifts.  maps: (records, nmap) per shift."""
+    r0 = np.asarray(r_axes[0], np.float64)
+    out = np.zeros((r0.size, n_eta))
+    for (rec, nm), ax in zip(maps, r_axes):
+        n_r = np.asarray(ax).size
+        ck, _ = integrate(rec, nm, n_r * n_eta, ny, nz, image, mode=mode, semantics="py", normalize=True,
+                          bc_y=bc_y, bc_z=bc_z)
+        ck = ck.reshape(n_r, n_eta)
+        for i, (j, wl, wh) in enumerate(r_interp(ax, r0)):
+            out[i] += wl * ck[j] + wh * ck[j + 1]
+    return (out / len(maps)).reshape(-1)
+
+
 def profile_omp(cake, area, n_r, n_eta):
     """The OpenMP integrator's lineout (IntegratorZarrOMP.c:1829-1843): per row the mean of
     the nonzero, non-NaN bins (second) and the area-weighted mean over valid, non-NaN bins."""

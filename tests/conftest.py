@@ -70,6 +70,24 @@ def load_mapper_case(tag):
     return g
 
 
+def load_fused_case():
+    """fused.npz: the reference's shifted maps (PixelMaps), R axes, image and fused cakes."""
+    from midas_b200.bin_io import from_arrays
+    g = dict(np.load(GOLDEN / "fused.npz"))
+    for k in ("ny", "nz", "n_eta", "n_shifts"):
+        g[k] = int(g[k])
+    for k in ("bc_y", "bc_z", "rbin"):
+        g[k] = float(g[k])
+    g["maps"], g["nmaps"], g["r_axes"] = [], [], []
+    for k in range(g["n_shifts"]):
+        rec = g[f"records_{k}"].view(REC_DTYPE)
+        nm = np.stack([g[f"counts_{k}"], g[f"offsets_{k}"]], 1).astype(np.int32)
+        g["maps"].append(from_arrays(rec, nm))
+        g["nmaps"].append((rec, nm))
+        g["r_axes"].append(g[f"r_axis_{k}"])
+    return g
+
+
 KERNEL_CASES = ["a", "b", "c", "d"]
 MAPPER_CASES = ["m1", "m2", "m3"]
 VARIANCE_CASES = ["a", "b", "d"]

@@ -23,6 +23,8 @@ the reference's C mapper and integrator compiled into oracle/_ref, and writes:
                   every mode, normalize on/off
   image.npz       hybrid (dtype 6) payloads decoded by decode_hybrid_payload and a
                   multi-frame int64 dark averaged by average_dark_frames
+  fused.npz       build_fused_geometry (4 R shifts) of a small tilted detector: the
+                  shifted maps, their R axes, an image and the fused cakes
 
 Selected groups only: python tests/golden/make_golden.py variance image
 
@@ -266,11 +268,53 @@ def header_case(M):
     print("wrote", OUT / "header.npz")
 
 
+def fused_case(M):
+    """build_fused_geometry (fused_csr.py) of a small tilted detector, 4 shifts: the shifted
+    maps its own build_map made (captured as it runs), their R axes, an image and the
+    integrate() cakes of the fused geometry for bilinear and gradient, FP64."""
+    import importlib
+    import torch
+    kernels = M["kernels"]
+    fc = importlib.import_module("midas_integrate.fused_csr")
+    params_mod = importlib.import_module("midas_integrate.params")
+    p = params_mod.IntegrationParams(NrPixelsY=56, NrPixelsZ=48, pxY=200.0, pxZ=200.0, Lsd=250000.0, BC_y=27.3,
+                                     BC_z=23.8, RhoD=2.0e5, ty=0.1, tz=-0.05, RMin=3.0, RMax=27.0, RBinSize=1.5,
+                                     EtaMin=-180.0, EtaMax=180.0, EtaBinSize=15.0)
+    captured = []
+    orig = fc.build_map
+
+    def capture(pk, **kw):
+        res = orig(pk, **kw)
+        captured.append((float(pk.RMin), res.as_pixel_map()))
+        return res
+
+    fc.build_map = capture
+    rng = np.random.default_rng(21)
+    image = rng.uniform(20, 900, size=(p.NrPixelsZ, p.NrPixelsY))
+    out = dict(image=image, ny=p.NrPixelsY, nz=p.NrPixelsZ, bc_y=p.BC_y, bc_z=p.BC_z, n_eta=p.n_eta_bins,
+               rbin=p.RBinSize, n_shifts=4)
+    for mode in ("bilinear", "gradient"):
+        captured.clear()
+        geom = fc.build_fused_geometry(p, n_shifts=4, mode=mode, dtype=torch.float64)
+        cake = kernels.integrate(torch.from_numpy(image), geom, mode=mode, normalize=False)
+        out[f"cake_{mode}"] = cake.numpy().reshape(-1)
+        if mode == "gradient":
+            for k, (rmin, pm) in enumerate(captured):
+                out[f"records_{k}"] = np.ascontiguousarray(pm.pxList).view(np.uint8).copy()
+                out[f"counts_{k}"] = np.asarray(pm.counts, np.int32)
+                out[f"offsets_{k}"] = np.asarray(pm.offsets, np.int32)
+                n_r = pm.counts.size // p.n_eta_bins
+                out[f"r_axis_{k}"] = kernels.r_axis(n_r=n_r, RMin=rmin, RBinSize=p.RBinSize)
+    fc.build_map = orig
+    np.savez_compressed(OUT / "fused.npz", **out)
+    print("wrote", OUT / "fused.npz", [out[f"records_{k}"].size // 24 for k in range(4)], "records")
+
+
 def main():
     M = ref_modules()
     groups = {"kernels": lambda: kernels_cases(M), "mapper": mapper_cases, "peakfit": lambda: peakfit_case(M),
               "header": lambda: header_case(M), "variance": lambda: variance_cases(M),
-              "image": lambda: image_case(M)}
+              "image": lambda: image_case(M), "fused": lambda: fused_case(M)}
     for name in (sys.argv[1:] or list(groups)):
         groups[name]()
 

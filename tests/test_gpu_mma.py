@@ -149,6 +149,26 @@ def test_mma_matches_run_encoding_at_detector_scale(cuda):
     _check((cm[[0, 19]], am[[0, 19]], sm_[[0, 19]]), ref)
 
 
+@pytest.mark.parametrize("encoding", ["mma", "mmad"])
+def test_tensor_core_ic_semantics_at_detector_scale(cuda, encoding):
+    """IntegrationCore semantics on a 1440x1440 detector (gradient mode): its bilinear bin
+    weights include negative ones, which the signed weight digits carry; the cake matches
+    the oracle to the same bar as the other semantics."""
+    from midas_b200 import synth
+    from midas_b200.mapper import build_map
+    w = synth.scaled(synth.sweep_2880(), 2)
+    m = w.mapper
+    pm, _ = build_map(m, device=0)
+    plan = CakePlan(pm, n_r=w.n_r, n_eta=w.n_eta, n_pixels_y=m.NrPixelsY, n_pixels_z=m.NrPixelsZ, mode="gradient",
+                    semantics="ic", bc_y=m.BC_y, bc_z=m.BC_z, device=cuda, encoding=encoding)
+    frames = w.frames(0, 3)
+    res = plan.integrate(frames)
+    assert plan.status() == 0
+    g = dict(records=pm.pxList, nmap=pm.nmap_pairs(), ny=m.NrPixelsY, nz=m.NrPixelsZ, bc_y=m.BC_y, bc_z=m.BC_z)
+    ref = _oracle(g, frames.cpu().numpy().astype(np.float64), "gradient", True, "ic", w.n_r)
+    _check(res, ref)
+
+
 def test_mma_panels(cuda):
     """Four u16 panels of a scaled panel set, one merged cake through the MMA plan, against
     the run-encoded panel plan."""

@@ -1,5 +1,5 @@
 """Parity of the direct tensor-core caking path (MI_ENC_MMAD: frames read in place into
-tensor memory as byte planes, 24-bit fixed-point weights, exact int8 tcgen05 products, FP64
+tensor memory as byte planes, signed fixed-point weights in four digit planes, exact int8 tcgen05 products, FP64
 recombination) with the FP64 oracle, through the C ABI: every mode x semantics x
 normalisation on random maps (rows of 8k and of other widths: vector and pixel-by-pixel
 granule loads), DetectorMapper maps with a dark over batches crossing the 128-frame launch,
