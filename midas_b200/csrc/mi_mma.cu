@@ -489,10 +489,8 @@ __global__ void __launch_bounds__(kMmaThreads, 1) k_mma(const __grid_constant__ 
 #pragma unroll
         for (int i = 0; i < 8; ++i) {
           const int lrow = (8 * c + i) / kMmaCols;
-          const double x4 = m_i2d(r[4][i]), x3 = m_i2d(r[3][i]), x2 = m_i2d(r[2][i]), x1 = m_i2d(r[1][i]),
-                       x0 = m_i2d(r[0][i]);
-          // sum_k 2^(8k) x_k = (256 x4 + x3) 2^24 + (256 x2 + x1) 256 + x0
-          const double v = fma(fma(x4, 256.0, x3), 16777216.0, fma(fma(x2, 256.0, x1), 256.0, x0));
+          // sum_k 2^(8k) acc_k exactly in int64 (|sum| < 2^63), one rounding to FP64
+          const double v = m_acc5(r[0][i], r[1][i], r[2][i], r[3][i], r[4][i]);
           const double res = fma(bfac[8 * c + i], v, -bdk[8 * c + i]);
           const float l = blw[8 * c + i];
           o[i] = (float)res;

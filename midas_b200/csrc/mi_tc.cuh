@@ -75,10 +75,13 @@ __device__ __forceinline__ void m_ld8(uint32_t taddr, uint32_t *r) {
 }
 __device__ __forceinline__ void m_ld_wait() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
 
-// int32 -> double exactly, on the FP64 pipe: 2^52 + (x + 2^31) has x + 2^31 (the sign bit
-// flipped) in its low bits
-__device__ __forceinline__ double m_i2d(uint32_t x) {
-  return __hiloint2double(0x43300000, (int)(x ^ 0x80000000u)) - 4503601774854144.0;
+// The five int32 accumulators of a bin (byte shifts 0..4) as one value: sum_k 2^(8k) acc_k
+// summed exactly in int64 on the integer pipe, then rounded once to FP64.  |acc_k| < 2^31,
+// so |sum| < 2^31 (1 + 2^8 + 2^16 + 2^24 + 2^32) < 2^63.
+__device__ __forceinline__ double m_acc5(uint32_t a0, uint32_t a1, uint32_t a2, uint32_t a3, uint32_t a4) {
+  const long long s = (long long)(int)a0 + (long long)(int)a1 * 256LL + (long long)(int)a2 * 65536LL +
+                      (long long)(int)a3 * 16777216LL + (long long)(int)a4 * 4294967296LL;
+  return __ll2double_rn(s);
 }
 
 typedef CUresult (*EncodeTiledFn)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
