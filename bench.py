@@ -595,11 +595,16 @@ def serving_load(args, dev, plain=False, n_distinct=8):
                          plan_s=round(t2 - t1, 3), name=c.name, window=(t0, t2))
         producer(c.name, sid, late_rate, late_frames, 99, stop_at[0])
 
-    # the host loop is Python: keep the cyclic garbage collector's pauses out of the window
+    # the host loop is Python: keep the cyclic garbage collector's pauses out of the window,
+    # and let the scheduler thread take the interpreter lock back within 0.5 ms of a
+    # producer or writer thread holding it (the default switch interval is 5 ms)
     import gc
+    import sys
     gc.collect()
     gc.freeze()
     gc.disable()
+    switch = sys.getswitchinterval()
+    sys.setswitchinterval(5e-4)
     t_start = time.perf_counter()
     stop_at[0] = t_start + T
     th = [threading.Thread(target=producer, args=(c.name, sid, rate, fr, k, stop_at[0]))
@@ -611,6 +616,7 @@ def serving_load(args, dev, plain=False, n_distinct=8):
         t.join()
     results = {name: [f.result(timeout=600) for f in futs] for name, futs in per_stream.items()}
     t_done = time.perf_counter()
+    sys.setswitchinterval(switch)
     gc.enable()
     gc.unfreeze()
     srv.stop()

@@ -116,7 +116,9 @@ class StreamConfig:
     fit_half_window: int = 12
     x_bin: float = 1.0
     want_cake: bool = False
-    tile_rows: int = 0
+    tile_rows: int = 0             # run encoding only
+    encoding: Optional[str] = None  # batched kernel (kernels.CakePlan encodings); None = the
+                                    # backend's choice (DeviceBackend.encoding_for)
     max_batch: int = 0             # frames per launch at most (0 = the backend's default)
     output_dir: Optional[str] = None   # write the reference's per-frame files there (writers.py):
                                        # lineout.bin, lineout_simple_mean.bin, fit.bin (peaks
@@ -147,6 +149,8 @@ class _Req:
     fut: Future
     t_submit: float = 0.0
     t_dispatch: float = 0.0
+    ring: int = -1                 # staging-ring entry holding the frame (backends that stage)
+    staged: bool = True            # the frame is in its ring entry
 
 
 @dataclass
@@ -161,38 +165,51 @@ class _Stream:
     closing: bool = False
     writer: object = None          # writers.StreamOutputs when cfg.output_dir is set
     fit_valid: Optional[np.ndarray] = None
+    submit_lock: threading.Lock = field(default_factory=threading.Lock)
 
 
 class DeviceBackend:
     """Runs a stream's batches through libmidas_b200 on one CUDA device.
 
-    Each admitted stream gets its plan (map, dark), its own CUDA stream and
-    ``max_inflight`` slots of pinned host staging + device buffers sized for its batch
-    limit; a batch is H2D -> ``mi_integrate_batch`` -> ``mi_fit_batch`` -> D2H, all on the
-    stream's CUDA stream, and a slot is reused only after its event has fired.
+    Each admitted stream gets its plan (map, dark), its own CUDA stream, a ring of
+    ``(max_inflight + 1) x batch limit`` pinned host frames and ``max_inflight`` slots of
+    device buffers and pinned results; a batch is H2D -> ``mi_integrate_batch`` ->
+    ``mi_fit_batch`` -> D2H, all on the stream's CUDA stream, and a slot is reused only after
+    its event has fired.  A frame is copied into its ring entry by the thread that submits
+    it (``reserve`` + ``stage``: the pixels the upload sends, in C without the interpreter
+    lock), so the scheduler thread only uploads and launches; an entry is reused once the
+    batch that uploaded it has finished.
 
     ``plain=True`` serves the same requests with the reference's algorithm, one frame
     per launch (``mi_integrate_plain`` and a one-frame fit per frame): the comparison
     arm of the serving benchmark.
 
-    ``graph_batches``: for batches of up to this many frames, the device part of a
-    dispatch (upload, caking, fits, result copies) is one CUDA graph per (slot, batch size),
-    recorded when the stream is admitted and replayed with one launch, so a small batch
-    costs the scheduler thread one call instead of one per step.
+    ``small_batch``: batches of at most this many frames go through that one-frame kernel
+    too (the batched kernels' cost per launch hardly depends on the frame count, and for
+    one frame the one-frame kernel is 1.5 to 4 times faster); larger batches use the
+    stream's batched encoding.  A frame's result then depends on which path served it,
+    never on the other frames of its batch.
+
+    ``graph_batches``: for batches of up to this many frames (by default every batch size up
+    to 32), the device part of a dispatch after the upload (caking, fits, result copies) is
+    one CUDA graph per (slot, batch size), recorded when the stream is admitted and replayed
+    with one launch, so a batch costs the scheduler thread the upload calls and one launch.
     """
 
     def __init__(self, device: int = 0, max_batch: int = 32, max_inflight: int = 2, plain: bool = False,
-                 pinned_bytes: int = 2 << 30, build_threads: int = 0, graph_batches: int = 8):
+                 pinned_bytes: int = 2 << 30, build_threads: int = 0, graph_batches: int = 32,
+                 small_batch: int = 1):
         import torch
         self.torch = torch
         self.device = torch.device("cuda", device)
         # host threads building an admitted stream's plan: a quarter of the cores (at most 4)
         self.build_threads = build_threads or max(1, min(4, (os.cpu_count() or 4) // 4))
-        self._dmax = dict.fromkeys(("stage_ms", "upload_ms", "integrate_ms", "fit_ms", "results_ms"), 0.0)
+        self._dmax = dict.fromkeys(("stage_ms", "upload_ms", "integrate_ms"), 0.0)
         self.max_batch = max_batch
         self.max_inflight = max_inflight
         self.plain = plain
         self.graph_batches = 0 if plain else int(graph_batches)
+        self.small_batch = int(small_batch)
         self.pool = PinnedPool(pinned_bytes)
         self.alg_bytes = 0          # map bytes per launch + frame bytes, summed over dispatches
         self.launches = 0           # libmidas_b200 entry-point calls that launch kernels
@@ -200,6 +217,18 @@ class DeviceBackend:
     def free_bytes(self) -> int:
         free, _ = self.torch.cuda.mem_get_info(self.device)
         return int(free)
+
+    @staticmethod
+    def encoding_for(cfg: StreamConfig) -> str:
+        """The stream's batched encoding: its own, else the tensor cores for 8/16-bit frames
+        and the per-bin CSR kernel otherwise (both cost less per launch than the run
+        encoding at serving batch sizes)."""
+        if cfg.encoding:
+            return cfg.encoding
+        return "mma" if cfg.frame_dtype in ("uint8", "uint16") else "csr"
+
+    def _one_frame(self, n: int) -> bool:
+        return self.plain or n <= self.small_batch
 
     def batch_limit(self, st) -> int:
         return st["B"]
@@ -220,11 +249,12 @@ class DeviceBackend:
             tokens.append(tok)
             return t
 
+        R = B * (self.max_inflight + 1)
         try:
+            ring = pinned((R, nz, ny), tdt)
             host = []
             for _ in range(self.max_inflight):
-                h = {"h_frames": pinned((B, nz, ny), tdt), "h_aw": pinned((B, cfg.n_r), torch.float64),
-                     "h_sm": pinned((B, cfg.n_r), torch.float64)}
+                h = {"h_aw": pinned((B, cfg.n_r), torch.float64), "h_sm": pinned((B, cfg.n_r), torch.float64)}
                 if cfg.want_cake:
                     h["h_cake"] = pinned((B, cfg.n_r, cfg.n_eta), ck_dt)
                 if fit:
@@ -236,9 +266,11 @@ class DeviceBackend:
             raise
         # a stream admitted while others are served builds its plan on a few host cores, so
         # the scheduler thread and the callers submitting frames keep theirs
+        enc = self.encoding_for(cfg)
         plan = CakePlan(cfg.pixmap, n_r=cfg.n_r, n_eta=cfg.n_eta, n_pixels_y=cfg.n_pixels_y,
                         n_pixels_z=cfg.n_pixels_z, mode=cfg.mode, bc_y=cfg.bc_y, bc_z=cfg.bc_z,
-                        device=self.device, tile_rows=cfg.tile_rows, host_threads=self.build_threads)
+                        device=self.device, tile_rows=cfg.tile_rows if enc == "runs" else 0, encoding=enc,
+                        host_threads=self.build_threads)
         if cfg.dark is not None:
             plan.set_dark(cfg.dark)
         slots = []
@@ -252,6 +284,10 @@ class DeviceBackend:
             })
             if cfg.want_cake or self.plain:
                 s["d_cake"] = torch.empty((B, cfg.n_r, cfg.n_eta), dtype=ck_dt, device=self.device)
+            if not self.plain and self.small_batch > 0:
+                # the one-frame kernel's FP64 cake of a small batch
+                s["d_cake64"] = torch.empty((min(B, self.small_batch), cfg.n_r, cfg.n_eta), dtype=torch.float64,
+                                            device=self.device)
             if fit:
                 npk = len(cfg.peaks)
                 s["d_fit"] = torch.empty((B, npk, L.FIT_NOUT), dtype=torch.float64, device=self.device)
@@ -259,7 +295,8 @@ class DeviceBackend:
             slots.append(s)
         st = {"plan": plan, "slots": slots, "free": list(range(self.max_inflight)), "B": B,
               "stream": torch.cuda.Stream(self.device), "map_bytes": int(plan.info["map_bytes"]),
-              "frame_bytes": nz * ny * np.dtype(cfg.frame_dtype).itemsize, "tokens": tokens}
+              "frame_bytes": nz * ny * np.dtype(cfg.frame_dtype).itemsize, "tokens": tokens,
+              "ring": ring, "R": R, "head": 0, "tail": 0, "ring_cv": threading.Condition()}
         if fit:
             st["x"] = torch.as_tensor(np.asarray(cfg.r_axis, np.float64), device=self.device)
             st["peaks"] = torch.as_tensor(np.asarray(cfg.peaks, np.float64), device=self.device)
@@ -274,15 +311,39 @@ class DeviceBackend:
                 s["graphs"][n] = self._record(st, cfg, s, n)
         return st, int(fp)
 
+    def _upload(self, st, s, r0, n, strm):
+        """H2D of ring entries r0 .. r0 + n - 1 (mod R) into the slot's first n device frames:
+        the referenced pixels only, one call per contiguous piece of the ring."""
+        R, ring, plan = st["R"], st["ring"], st["plan"]
+        a = min(n, R - r0)
+        plan.upload(ring[r0:r0 + a], s["d_frames"], stream=strm)
+        if a < n:
+            plan.upload(ring[:n - a], s["d_frames"][a:], stream=strm)
+
     def _device_work(self, st, cfg, s, n, strm):
-        """Upload, caking, fits and result copies of the slot's first n frames on strm."""
-        st["plan"].upload(s["h_frames"][:n], s["d_frames"], stream=strm)
-        out = {"lineout_aw": s["d_aw"][:n], "lineout_sm": s["d_sm"][:n]}
-        if cfg.want_cake:
-            out["cake"] = s["d_cake"][:n]
-        st["plan"].integrate(s["d_frames"][:n], cake=cfg.want_cake, out=out, stream=strm)
-        if "d_fit" in s:
-            self._fit(st, cfg, s, 0, n, strm)
+        """Caking, fits and result copies of the slot's first n device frames on strm: the
+        one-frame kernel per frame for small batches (and in plain mode), else one launch of
+        the batched plan."""
+        fit = "d_fit" in s
+        if self._one_frame(n):
+            code = dtype_code(s["d_frames"].dtype)
+            ck = s["d_cake"] if self.plain else s["d_cake64"]
+            for i in range(n):
+                L.check(L.lib().mi_integrate_plain(st["plan"]._h, s["d_frames"][i].data_ptr(), code,
+                                                   ck[i].data_ptr(), s["d_aw"][i].data_ptr(), s["d_sm"][i].data_ptr(),
+                                                   L.stream_ptr(strm)), "mi_integrate_plain")
+                if fit:
+                    self._fit(st, cfg, s, i, 1, strm)
+            if cfg.want_cake and not self.plain:
+                s["d_cake"][:n].copy_(ck[:n])
+        else:
+            out = {"lineout_aw": s["d_aw"][:n], "lineout_sm": s["d_sm"][:n]}
+            if cfg.want_cake:
+                out["cake"] = s["d_cake"][:n]
+            st["plan"].integrate(s["d_frames"][:n], cake=cfg.want_cake, out=out, stream=strm)
+            if fit:
+                self._fit(st, cfg, s, 0, n, strm)
+        if fit:
             s["h_fit"][:n].copy_(s["d_fit"][:n], non_blocking=True)
         s["h_aw"][:n].copy_(s["d_aw"][:n], non_blocking=True)
         s["h_sm"][:n].copy_(s["d_sm"][:n], non_blocking=True)
@@ -290,12 +351,14 @@ class DeviceBackend:
             s["h_cake"][:n].copy_(s["d_cake"][:n], non_blocking=True)
 
     def _record(self, st, cfg, s, n):
-        """The slot's device work for n frames as a CUDA graph, recorded on the stream's own
-        CUDA stream (capture errors local to this thread: other threads keep their calls)."""
+        """The slot's device work for n frames (after their upload) as a CUDA graph, recorded
+        on the stream's own CUDA stream (capture errors local to this thread: other threads
+        keep their calls)."""
         torch = self.torch
         strm = st["stream"]
         launches = self.launches
         with torch.cuda.stream(strm):
+            self._upload(st, s, 0, n, strm)
             self._device_work(st, cfg, s, n, strm)       # warm-up: kernels loaded, attributes set
         strm.synchronize()
         g = torch.cuda.CUDAGraph()
@@ -315,6 +378,32 @@ class DeviceBackend:
         plan = recs * 60 + 256 * cfg.n_r * 12 * 16 + cfg.n_pixels_y * cfg.n_pixels_z * 8
         return int(plan + self.max_inflight * per_slot)
 
+    # -- staging at submission ------------------------------------------------------
+    def reserve(self, st, timeout: float = 60.0) -> int:
+        """The next ring entry, in submission order; waits while every entry holds a frame
+        not yet uploaded (a fast producer is held back)."""
+        cv = st["ring_cv"]
+        with cv:
+            if not cv.wait_for(lambda: st["head"] - st["tail"] < st["R"], timeout):
+                raise TimeoutError("staging ring full: no batch of the stream finished in time")
+            i = st["head"] % st["R"]
+            st["head"] += 1
+            return i
+
+    def stage(self, st, idx: int, frame: np.ndarray, cfg: StreamConfig) -> None:
+        """Copy a frame into its ring entry (caller's thread)."""
+        dst = st["ring"][idx]
+        if frame.dtype == dst.numpy().dtype and frame.flags.c_contiguous:
+            st["plan"].stage_host(frame, dst)      # the pixels the upload sends, without the GIL
+        else:
+            dst.numpy()[...] = frame.reshape(cfg.n_pixels_z, cfg.n_pixels_y)
+
+    def _release(self, st, n: int) -> None:
+        cv = st["ring_cv"]
+        with cv:
+            st["tail"] += n
+            cv.notify_all()
+
     def can_dispatch(self, st) -> bool:
         return bool(st["free"])
 
@@ -323,80 +412,48 @@ class DeviceBackend:
                                      st["peaks"].data_ptr(), st["peaks"].numel(), C.byref(st["fit_opts"]),
                                      s["d_fit"][first].data_ptr(), s["d_iters"][first].data_ptr(),
                                      L.stream_ptr(strm)), "mi_fit_batch")
-        self.launches += 1
 
     def dispatch_stats(self, reset: bool = False) -> Dict[str, float]:
-        """Slowest step of dispatch() so far, per step (ms): the host staging copy, the
-        upload, the caking launch, the fit launch, the result copies and event record."""
+        """Slowest step of dispatch() so far, per step (ms): the host staging copy (frames
+        not staged at submission), the upload, and the device work (graph replay, or the
+        caking and fit launches and result copies) with the event record."""
         out = dict(self._dmax)
         if reset:
             self._dmax = dict.fromkeys(self._dmax, 0.0)
         return out
 
-    def dispatch(self, st, cfg: StreamConfig, frames: List[np.ndarray]):
+    def dispatch(self, st, cfg: StreamConfig, frames: List[np.ndarray], ring: Optional[List[int]] = None):
+        """Launch a batch: ``ring`` = the ring entries its frames were staged into (consecutive,
+        in order); without it the frames are staged here first."""
         torch = self.torch
         clock, dm = time.perf_counter, self._dmax
         t0 = clock()
         k = st["free"].pop()
         s = st["slots"][k]
         n = len(frames)
-        hf = s["h_frames"]
-        hdt = hf.numpy().dtype
-        for i, f in enumerate(frames):
-            if f.dtype == hdt and f.flags.c_contiguous:
-                st["plan"].stage_host(f, hf[i])   # the pixels the upload sends, without the GIL
-            else:
-                hf[i].numpy()[...] = f.reshape(cfg.n_pixels_z, cfg.n_pixels_y)
+        if ring is None:
+            ring = [self.reserve(st) for _ in range(n)]
+            for i, f in zip(ring, frames):
+                self.stage(st, i, f, cfg)
+        r0 = ring[0]
         strm = st["stream"]
         fit = "d_fit" in s
         t1 = clock()
         dm["stage_ms"] = max(dm["stage_ms"], (t1 - t0) * 1e3)
         g = s.get("graphs", {}).get(n)
-        if g is not None:
-            # the recorded upload + caking + fits + result copies, one launch
-            with torch.cuda.stream(strm):
-                g.replay()
-                s["event"].record(strm)
-            self.launches += 2 if fit else 1
-            self.alg_bytes += st["map_bytes"] + n * st["frame_bytes"]
-            dm["integrate_ms"] = max(dm["integrate_ms"], (clock() - t1) * 1e3)
-            return (k, n)
         with torch.cuda.stream(strm):
-            st["plan"].upload(hf[:n], s["d_frames"], stream=strm)   # referenced pixels only
+            self._upload(st, s, r0, n, strm)             # referenced pixels only
             t2 = clock()
             dm["upload_ms"] = max(dm["upload_ms"], (t2 - t1) * 1e3)
-            if self.plain:
-                code = dtype_code(s["d_frames"].dtype)
-                for i in range(n):
-                    L.check(L.lib().mi_integrate_plain(st["plan"]._h, s["d_frames"][i].data_ptr(), code,
-                                                       s["d_cake"][i].data_ptr(), s["d_aw"][i].data_ptr(),
-                                                       s["d_sm"][i].data_ptr(), L.stream_ptr(strm)),
-                            "mi_integrate_plain")
-                    self.launches += 1
-                    if fit:
-                        self._fit(st, cfg, s, i, 1, strm)
-                self.alg_bytes += n * (st["map_bytes"] + st["frame_bytes"])
+            if g is not None:
+                g.replay()                               # the recorded caking + fits + result copies
             else:
-                out = {"lineout_aw": s["d_aw"][:n], "lineout_sm": s["d_sm"][:n]}
-                if cfg.want_cake:
-                    out["cake"] = s["d_cake"][:n]
-                st["plan"].integrate(s["d_frames"][:n], cake=cfg.want_cake, out=out, stream=strm)
-                t3 = clock()
-                dm["integrate_ms"] = max(dm["integrate_ms"], (t3 - t2) * 1e3)
-                self.launches += 1
-                self.alg_bytes += st["map_bytes"] + n * st["frame_bytes"]
-                if fit:
-                    self._fit(st, cfg, s, 0, n, strm)
-                    dm["fit_ms"] = max(dm["fit_ms"], (clock() - t3) * 1e3)
-            t4 = clock()
-            if fit:
-                s["h_fit"][:n].copy_(s["d_fit"][:n], non_blocking=True)
-            s["h_aw"][:n].copy_(s["d_aw"][:n], non_blocking=True)
-            s["h_sm"][:n].copy_(s["d_sm"][:n], non_blocking=True)
-            if cfg.want_cake:
-                s["h_cake"][:n].copy_(s["d_cake"][:n], non_blocking=True)
+                self._device_work(st, cfg, s, n, strm)
             s["event"].record(strm)
-        dm["results_ms"] = max(dm["results_ms"], (clock() - t4) * 1e3)
+        dm["integrate_ms"] = max(dm["integrate_ms"], (clock() - t2) * 1e3)
+        one = self._one_frame(n)
+        self.launches += (n if one else 1) * (2 if fit else 1)
+        self.alg_bytes += (n * st["map_bytes"] if one else st["map_bytes"]) + n * st["frame_bytes"]
         return (k, n)
 
     def ready(self, st, handle) -> bool:
@@ -411,6 +468,7 @@ class DeviceBackend:
                         s["h_fit"][i].numpy().copy() if "h_fit" in s else None,
                         s["h_cake"][i].numpy().copy() if cfg.want_cake else None))
         st["free"].append(k)
+        self._release(st, n)
         return res
 
     def close(self, st):
@@ -529,6 +587,9 @@ class CakeServer:
 
     # -- requests ---------------------------------------------------------------
     def submit(self, sid: int, frame: np.ndarray, t_arrival: Optional[float] = None) -> Future:
+        """Queue one frame of a stream.  With a backend that stages (``reserve``/``stage``),
+        the frame is copied into the stream's staging ring here, in the caller's thread, so
+        the scheduler thread never copies frames; a full ring holds the caller back."""
         fut: Future = Future()
         with self._lock:
             s = self.streams.get(sid)
@@ -540,9 +601,27 @@ class CakeServer:
                 fut.set_exception(ValueError(f"frame has {frame.size} pixels, stream {cfg.name!r} expects "
                                              f"{cfg.n_pixels_y * cfg.n_pixels_z}"))
                 return fut
-            now = time.perf_counter()
-            s.pending.append(_Req(next(s.seq), frame, t_arrival if t_arrival is not None else now, fut, now))
-        self._wake.set()
+        now = time.perf_counter()
+        t_arr = t_arrival if t_arrival is not None else now
+        if not hasattr(self.backend, "reserve"):
+            with self._lock:
+                s.pending.append(_Req(next(s.seq), frame, t_arr, fut, now))
+            self._wake.set()
+            return fut
+        with s.submit_lock:          # ring entries in the order the frames enter the queue
+            try:
+                idx = self.backend.reserve(s.state)
+            except Exception as e:
+                fut.set_exception(e)
+                return fut
+            req = _Req(next(s.seq), frame, t_arr, fut, now, ring=idx, staged=False)
+            with self._lock:
+                s.pending.append(req)
+        try:
+            self.backend.stage(s.state, idx, frame, cfg)
+        finally:
+            req.staged = True
+            self._wake.set()
         return fut
 
     # -- scheduling ---------------------------------------------------------------
@@ -576,12 +655,21 @@ class CakeServer:
                 did = True
             while s.pending and self.backend.can_dispatch(s.state):
                 with self._lock:
-                    n = min(len(s.pending), self.backend.batch_limit(s.state))
+                    # the longest staged prefix of the queue, up to the batch limit
+                    lim = min(len(s.pending), self.backend.batch_limit(s.state))
+                    n = 0
+                    while n < lim and s.pending[n].staged:
+                        n += 1
                     reqs = [s.pending.popleft() for _ in range(n)]
+                if not reqs:
+                    break
                 t_disp = time.perf_counter()
                 for r in reqs:
                     r.t_dispatch = t_disp
-                handle = self.backend.dispatch(s.state, s.cfg, [r.frame for r in reqs])
+                if reqs[0].ring >= 0:
+                    handle = self.backend.dispatch(s.state, s.cfg, [r.frame for r in reqs], ring=[r.ring for r in reqs])
+                else:
+                    handle = self.backend.dispatch(s.state, s.cfg, [r.frame for r in reqs])
                 ps["max_dispatch_ms"] = max(ps["max_dispatch_ms"], (clock() - t_disp) * 1e3)
                 s.inflight.append((handle, reqs))
                 self.batches += 1

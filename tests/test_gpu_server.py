@@ -1,6 +1,8 @@
 """The continuous-batching server on the device: streams with different maps, detector
 shapes and frame types served concurrently must give every frame the result it gets
-alone (a one-frame launch on its own), and that result must match the FP64 oracle."""
+alone through the same path (the one-frame kernel for a batch of one frame, a one-frame
+launch of the stream's batched encoding otherwise), and that result must match the FP64
+oracle."""
 import threading
 import time
 
@@ -24,13 +26,19 @@ def _mix():
             synth.scaled(synth.pilatus_1679(), 5), synth.scaled(synth.detector_1024(1), 4)]
 
 
-def _alone(cfg, frame):
-    """One frame, one launch, on a plan of its own; fits on that frame's lineout alone."""
+def _alone(cfg, frame, batch_size, small_batch=1):
+    """One frame, one launch, on a plan of its own, through the path the server takes for
+    a batch of ``batch_size`` frames; fits on that frame's lineout alone."""
+    enc = DeviceBackend.encoding_for(cfg)
     plan = CakePlan(cfg.pixmap, n_r=cfg.n_r, n_eta=cfg.n_eta, n_pixels_y=cfg.n_pixels_y,
                     n_pixels_z=cfg.n_pixels_z, mode=cfg.mode, bc_y=cfg.bc_y, bc_z=cfg.bc_z,
-                    tile_rows=cfg.tile_rows, device="cuda")
+                    tile_rows=cfg.tile_rows if enc == "runs" else 0, encoding=enc, device="cuda")
     plan.set_dark(cfg.dark)
-    _, aw, sm = plan.integrate(torch.from_numpy(frame[None]).cuda(), cake=False)
+    if batch_size <= small_batch:
+        _, aw, sm = plan.integrate_plain(torch.from_numpy(frame).cuda())
+        aw, sm = aw[None], sm[None]
+    else:
+        _, aw, sm = plan.integrate(torch.from_numpy(frame[None]).cuda(), cake=False)
     fit = peakfit.fit_batch(torch.from_numpy(cfg.r_axis).cuda(), aw, torch.from_numpy(cfg.peaks).cuda(),
                             model=cfg.fit_model, half_window=cfg.fit_half_window, x_bin=cfg.x_bin)
     out = aw[0].cpu().numpy(), sm[0].cpu().numpy(), fit.params[0].cpu().numpy()
@@ -53,9 +61,10 @@ def test_results_are_the_same_alone_and_in_the_mix(cuda, graphs):
         def producer(k):
             rng = np.random.default_rng(k)
             futs = []
-            for f in frames[k]:
+            for i, f in enumerate(frames[k]):
                 futs.append(srv.submit(ids[k], f))
-                time.sleep(rng.exponential(1e-3))
+                if i % 4 == 3:                          # bursts of four: one-frame and batched paths
+                    time.sleep(rng.exponential(2e-3))
             results[k] = [fu.result(timeout=120) for fu in futs]
 
         th = [threading.Thread(target=producer, args=(k,)) for k in range(len(work))]
@@ -67,11 +76,13 @@ def test_results_are_the_same_alone_and_in_the_mix(cuda, graphs):
         srv.stop()
     assert srv.completed == N_FRAMES * len(work)
     assert srv.batches < srv.completed                  # some launches carried several frames
+    sizes = {r.batch_size for res in results.values() for r in res}
+    assert 1 in sizes and max(sizes) > 1                # both the one-frame and the batched path
     for k, cfg in enumerate(cfgs):
         res = results[k]
         assert [r.seq for r in res] == list(range(N_FRAMES))
         for i, r in enumerate(res):
-            aw, sm, fit = _alone(cfg, frames[k][i])
+            aw, sm, fit = _alone(cfg, frames[k][i], r.batch_size)
             np.testing.assert_array_equal(r.lineout_aw, aw)     # bitwise: batch composition is invisible
             np.testing.assert_array_equal(r.lineout_sm, sm)
             np.testing.assert_array_equal(r.fits, fit)
@@ -104,5 +115,5 @@ def test_stream_admitted_and_removed_while_others_run(cuda):
         ra = [f.result(timeout=60) for f in futs_a]
         rb = [f.result(timeout=60) for f in futs_b]
     for i in range(6):
-        np.testing.assert_array_equal(ra[i].lineout_aw, _alone(ca, fa[i])[0])
-        np.testing.assert_array_equal(rb[i].lineout_aw, _alone(cb, fb[i])[0])
+        np.testing.assert_array_equal(ra[i].lineout_aw, _alone(ca, fa[i], ra[i].batch_size)[0])
+        np.testing.assert_array_equal(rb[i].lineout_aw, _alone(cb, fb[i], rb[i].batch_size)[0])

@@ -221,3 +221,106 @@ def test_peak_rows_two_theta_and_d_spacing():
         assert r["d_spacing_A"] == (0.172979 / (2.0 * math.sin(th)) if th > 1e-10 else 0.0)
     assert rows["d_spacing_A"][2] == 0.0 and rows["d_spacing_A"][5] == 0.0
     assert np.all(rows["area"] == 5.0) and np.all(rows["FWHM_deg"] == 0.01)
+
+
+class HostRingBackend(HostTestBackend):
+    """HostTestBackend with the staging protocol of DeviceBackend: frames are copied into a
+    ring of ``R`` entries by the submitting thread (``reserve`` + ``stage``), batches name
+    their entries, and a batch's entries are released when it is collected."""
+
+    def __init__(self, R=6, slow=None, **kw):
+        super().__init__(**kw)
+        self.R, self.slow = R, slow or {}
+        self.rings = []
+
+    def open(self, cfg):
+        st, fp = super().open(cfg)
+        st.update(ring=[None] * self.R, R=self.R, head=0, tail=0, cv=threading.Condition(), n_staged=0)
+        return st, fp
+
+    def reserve(self, st, timeout=10.0):
+        with st["cv"]:
+            if not st["cv"].wait_for(lambda: st["head"] - st["tail"] < st["R"], timeout):
+                raise TimeoutError("ring full")
+            i = st["head"] % st["R"]
+            st["head"] += 1
+            return i
+
+    def stage(self, st, idx, frame, cfg):
+        k = st["n_staged"]
+        st["n_staged"] += 1
+        if k in self.slow:
+            time.sleep(self.slow[k])
+        st["ring"][idx] = np.array(frame, copy=True)
+
+    def dispatch(self, st, cfg, frames, ring=None):
+        assert ring is not None
+        assert all((b - a) % st["R"] == 1 for a, b in zip(ring, ring[1:])), ring
+        self.rings.append(list(ring))
+        return super().dispatch(st, cfg, [st["ring"][i] for i in ring])
+
+    def collect(self, st, cfg, handle):
+        res = super().collect(st, cfg, handle)
+        with st["cv"]:
+            st["tail"] += len(res)
+            st["cv"].notify_all()
+        return res
+
+
+def test_frames_staged_at_submission_in_ring_order_with_wraparound():
+    be = HostRingBackend(R=6, max_batch=4, max_inflight=1)
+    srv = CakeServer(backend=be, hbm_budget=10**8)
+    a = srv.admit(_cfg("a"))
+    rng = np.random.default_rng(1)
+    frames = [rng.integers(0, 100, (3, 4)) for _ in range(6)]
+    futs = [srv.submit(a, f) for f in frames[:4]]
+    _drive(srv, futs)                       # ring entries 0-3
+    futs += [srv.submit(a, f) for f in frames[4:]]
+    _drive(srv, futs)                       # entries 4, 5
+    more = [rng.integers(0, 100, (3, 4)) for _ in range(3)]
+    futs2 = [srv.submit(a, f) for f in more]
+    _drive(srv, futs2)                      # entries 0, 1, 2 again
+    for f, fut in zip(frames + more, futs + futs2):
+        np.testing.assert_array_equal(fut.result().lineout_aw, np.arange(1, 6) * f.sum())
+    assert be.rings == [[0, 1, 2, 3], [4, 5], [0, 1, 2]]
+
+
+def test_full_ring_holds_the_submitter_back_until_a_batch_finishes():
+    be = HostRingBackend(R=4, max_batch=4, max_inflight=1, delay_passes=2)
+    srv = CakeServer(backend=be, hbm_budget=10**8)
+    a = srv.admit(_cfg("a"))
+    futs = [srv.submit(a, np.full((3, 4), i)) for i in range(4)]
+    done = threading.Event()
+    extra = []
+
+    def late():
+        extra.append(srv.submit(a, np.full((3, 4), 9)))
+        done.set()
+
+    t = threading.Thread(target=late)
+    t.start()
+    assert not done.wait(0.2)               # all four entries hold frames not yet uploaded
+    _drive(srv, futs)
+    assert done.wait(5.0)
+    t.join()
+    _drive(srv, extra)
+    assert extra[0].result().lineout_sm[0] == 9 and be.rings == [[0, 1, 2, 3], [0]]
+
+
+def test_a_frame_still_being_staged_holds_back_the_frames_behind_it():
+    be = HostRingBackend(R=8, max_batch=8, max_inflight=1, slow={1: 0.3})
+    srv = CakeServer(backend=be, hbm_budget=10**8)
+    a = srv.admit(_cfg("a"))
+    first = srv.submit(a, np.full((3, 4), 1))
+    box = []
+    t = threading.Thread(target=lambda: box.append(srv.submit(a, np.full((3, 4), 2))))
+    t.start()
+    while not srv.streams[a].pending or len(srv.streams[a].pending) < 2:
+        time.sleep(0.01)
+    third = srv.submit(a, np.full((3, 4), 3))
+    srv._pass()                             # only the first frame is staged ahead of the slow one
+    assert be.dispatched == [("a", 1)]
+    t.join()
+    _drive(srv, [first, box[0], third])
+    assert be.dispatched == [("a", 1), ("a", 2)]
+    assert [f.result().lineout_sm[0] for f in (first, box[0], third)] == [1, 2, 3]
