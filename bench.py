@@ -31,12 +31,14 @@ REPO = Path(__file__).resolve().parent
 sys.path.insert(0, str(REPO))
 
 METRIC = "caked_frames_per_s"
-# DRAM bytes (read + write) per 128-frame batch of the sweep_2880 workload, from the committed
-# ncu captures (profiles/): the transpose kernel k_xc plus the caking kernel of the encoding
+# DRAM bytes (read + write) per 128-frame batch of the sweep_2880 workload: ncu
+# dram__bytes_read.sum + dram__bytes_write.sum of one launch of each kernel of the batch (the
+# transpose kernel k_xc plus the caking kernel of the encoding), summarised under profiles/; the
+# mma figures are of the kernels of commit fc01dae
 TRAFFIC = {"runs": {"bytes_per_step": int(0.840295e9 + 0.761555e9 + 1.830098e9 + 1.170938e9),
                     "kernels": "k_xc + k_runs"},
-           "mma": {"bytes_per_step": int(0.839712e9 + 0.764601e9 + 1.282986e9 + 0.862686e9),
-                   "kernels": "k_xc + k_mma"}}
+           "mma": {"bytes_per_step": int(0.839755e9 + 0.763452e9 + 1.285888e9 + 0.860974e9),
+                   "kernels": "k_xc + k_mma", "commit": "fc01dae"}}
 SCOPE = {"runs": "whole batch: k_xc + k_runs + k_lineout (k_runs 88 %)",
          "mma": "whole batch: k_xc + k_mma + k_lineout",
          "mmad": "whole batch: k_mmad + k_lineout"}
@@ -380,8 +382,8 @@ def main_ours(args):
     mean_step_s = sum(step_ms) / len(step_ms) / 1e3
     achieved = alg / mean_step_s / 1e9
     ref_bytes = map_bytes + F * (info["ref_pixels"] * 2 + w.n_r * w.n_eta * 4)
-    # DRAM bytes (read + write) of the batch's kernels from the committed ncu capture of this
-    # workload at F = 128 (profiles/k_runs_xc_sweep2880_f128.md); other shapes: not captured
+    # DRAM bytes (read + write) of the batch's kernels from the ncu captures of this workload at
+    # F = 128 (TRAFFIC); other shapes: not captured
     enc = args.encoding if args.encoding != "auto" else "runs"
     traffic = None
     if w.name.startswith("sweep_2880") and F == 128 and info["xc_pixels"] > 0 and enc in TRAFFIC:
