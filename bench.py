@@ -72,6 +72,7 @@ def parse():
     ap.add_argument("--no-panels", action="store_true")
     ap.add_argument("--no-graph", action="store_true", help="skip the CUDA-graph replay of the batched step")
     ap.add_argument("--autotune", action="store_true", help="time candidate tile shapes / run lengths first")
+    ap.add_argument("--mma-pipeline", default="", help="stages,producers of the tensor-core kernel (e.g. 6,6)")
     ap.add_argument("--panel-frames", type=int, default=256)
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--serve-seconds", type=float, default=10.0,
@@ -312,6 +313,13 @@ def main_ours(args):
                     tile_rows=args.tile_rows or w.tile_rows, tile_pixels=args.tile_pixels,
                     frames_per_lane=args.fpl, encoding=args.encoding, run_len=args.run_len)
     t_plan = time.time() - t1
+    pipeline = None
+    if tuned is not None and tuned.best.get("pipeline"):
+        pipeline = tuple(tuned.best["pipeline"])
+    elif args.mma_pipeline:
+        pipeline = tuple(int(x) for x in args.mma_pipeline.split(","))
+    if pipeline is not None:
+        plan.set_mma_pipeline(*pipeline)
     info = plan.info
     dark = w.dark(device=dev)
     dark_np = dark.cpu().numpy()
@@ -402,6 +410,7 @@ def main_ours(args):
                       "tile_rows": info["tile_rows"], "tile_pixels": info["tile_pixels"],
                       "frames_per_lane": info["frames_per_lane"],
                       "encoding": enc,
+                      "mma_pipeline": list(pipeline) if pipeline else ([7, 6] if enc == "mma" else None),
                       "run_len": info["run_len"], "staged_pixels_per_frame": info["staged_pixels"],
                       "referenced_pixels": info["ref_pixels"], "map_bytes": info["map_bytes"],
                       "l2": "inputs larger than L2: each step reads a new %.1f GB batch" % (F * frame_bytes / 1e9),

@@ -227,6 +227,11 @@ int mi_selftest_wait(uint32_t polls, int arrive, int device, int *status);
  * pixel, DetectorMapper's bin mask): those bins of every cake are NaN, as the OpenMP
  * integrator writes them (IntegratorZarrOMP.c:1766-1767).  NULL clears it. */
 int mi_plan_set_bin_mask(mi_plan *plan, const uint8_t *bin_mask);
+/* Pipeline depth of the MMA encoding's kernel (no counterpart in the reference): stage
+ * slots and producer warps, one of the compiled pairs 7/6 (the default), 6/6, 5/5, 7/7,
+ * 4/4; MI_E_UNSUPPORTED for other pairs or plans of other encodings.  Results are the same
+ * bit for bit; only the time differs (the autotuner times them per map). */
+int mi_plan_set_mma_pipeline(mi_plan *plan, int stages, int producers);
 
 /* Device-side status of the plan's launches so far: the plan's error word (MI_E_TIMEOUT
  * when a bounded in-kernel wait expired, else 0), which is then cleared.  Synchronises

@@ -117,6 +117,7 @@ SIGNATURES = [
     ("mi_plan_get_info", C.c_int, [C.c_void_p, C.POINTER(MiPlanInfo)]),
     ("mi_sum_cake", C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p]),
     ("mi_plan_set_bin_mask", C.c_int, [C.c_void_p, C.c_void_p]),
+    ("mi_plan_set_mma_pipeline", C.c_int, [C.c_void_p, C.c_int, C.c_int]),
     ("mi_selftest_wait", C.c_int, [C.c_uint32, C.c_int, C.c_int, C.POINTER(C.c_int)]),
     ("mi_plan_bytes", C.c_int, [C.c_void_p, C.POINTER(C.c_size_t)]),
     ("mi_plan_status", C.c_int, [C.c_void_p, C.POINTER(C.c_int)]),

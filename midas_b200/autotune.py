@@ -5,7 +5,10 @@ The knobs (all plan options of ``CakePlan``):
   encoding     'mmad' (tensor cores, frames read in place), 'mma' (tensor cores, frames
                transposed into byte planes first), 'runs' (CUDA cores); the tensor-core
                encodings are candidates for 8/16-bit frames only, and their tiles (12 R rows x
-               4 eta columns, 128 frames a pass) are fixed by the kernels;
+               4 eta columns, 128 frames a pass) are fixed by the kernels (24 x 2 tiles, which
+               stage fewer pixels twice, measured slower);
+  pipeline     'mma' only: the kernel's stage slots and producer warps (CakePlan.MMA_PIPELINES),
+               timed on the one plan without rebuilding it;
   tile_rows    R rows per strip (8 or 16): the register block of a consumer warp (bins per
                warp along R) and, with the pixel cap, the tile shape;
   run_len      rows per run record (2, 4, 8; 0 = the plan's own choice from the map's run
@@ -99,17 +102,24 @@ def tune(pixmap, frames: torch.Tensor, *, n_r: int, n_eta: int, n_pixels_y: int,
             plan.set_dark(dark)
         ck, aw, sm = plan.integrate(frames)           # warm-up, buffers
         bufs = {"cake": ck, "lineout_aw": aw, "lineout_sm": sm}
-        torch.cuda.synchronize()
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record(stream)
-        for _ in range(reps):
-            plan.integrate(frames, out=bufs)
-        e1.record(stream)
-        torch.cuda.synchronize()
         info = plan.info
-        row.update(ms=round(e0.elapsed_time(e1) / reps, 4), tiles=info["n_tiles"], run_len_used=info["run_len"],
-                   tile_pixels_used=info["tile_pixels"], map_bytes=info["map_bytes"])
-        table.append(row)
+        pipes = CakePlan.MMA_PIPELINES if cand.get("encoding") == "mma" and "pipeline" not in cand else [None]
+        for pipe in pipes:
+            r2 = dict(row)
+            if pipe is not None:
+                plan.set_mma_pipeline(*pipe)
+                plan.integrate(frames, out=bufs)       # the variant's first launch
+                r2["pipeline"] = list(pipe)
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            for _ in range(reps):
+                plan.integrate(frames, out=bufs)
+            e1.record(stream)
+            torch.cuda.synchronize()
+            r2.update(ms=round(e0.elapsed_time(e1) / reps, 4), tiles=info["n_tiles"], run_len_used=info["run_len"],
+                      tile_pixels_used=info["tile_pixels"], map_bytes=info["map_bytes"])
+            table.append(r2)
         plan.close()
         del ck, aw, sm, bufs
     ok = [r for r in table if "ms" in r]
@@ -117,7 +127,7 @@ def tune(pixmap, frames: torch.Tensor, *, n_r: int, n_eta: int, n_pixels_y: int,
         raise RuntimeError(f"no candidate plan could be built: {table}")
     best = min(ok, key=lambda r: r["ms"])
     res = TuneResult({k: best.get(k, "runs" if k == "encoding" else 0)
-                      for k in ("encoding", "tile_rows", "run_len", "tile_pixels")}, best["ms"], table, key)
+                      for k in ("encoding", "tile_rows", "run_len", "tile_pixels", "pipeline")}, best["ms"], table, key)
     _CACHE[key] = res
     if cache_path:
         p = Path(cache_path)

@@ -377,6 +377,7 @@ struct Plan {
   int *d_err = nullptr;          // device error word (bounded waits)
   int *d_ctr = nullptr;          // work-item counter of the persistent run kernel
   int n_sms = 0;
+  int mma_stages = 7, mma_producers = 6;   // pipeline of the MMA kernel (mi_plan_set_mma_pipeline)
 
   // pixel-major staging (run encoding with 64-frame groups)
   int64_t n_xc = 0;              // compact pixels (0: not built)
@@ -427,6 +428,7 @@ int launch_runs_staged(Plan *p, bool as_f32, int F, float *cake, double *partial
 // MMA encoding (mi_mma.cu): caking of frames [0, F) (F <= 128) staged as byte planes, and
 // the per-bin dark terms (after a dark is set)
 int launch_mma(Plan *p, int F, float *cake, double *partial, bool want_lo, cudaStream_t s);
+bool mma_pipeline_supported(int stages, int producers);
 int launch_mma_dark(Plan *p, cudaStream_t s);
 // Direct MMA encoding (mi_mmad.cu): caking of frames [0, F) (F <= 128, u16 or u8) read in
 // place at frames + f * stride, and the per-bin dark terms

@@ -26,14 +26,14 @@
 //     then scattered from the stage's terms (the tiler orders a step's terms so that each
 //     32 consecutive ones fall in distinct banks where the step allows: mma_bank).
 //
-// Roles (one persistent CTA per SM, 16 warps):
+// Roles (one persistent CTA per SM, 16 warps with the default 6 producers):
 //   warp 0          TMEM allocation (512 columns: two accumulator sets of 5 x 48) and, on one
 //                   lane, the MMA issue: 2 MMAs per K step, a commit that frees the stage, and
 //                   at a tile's last step a commit that hands the accumulators to the epilogue
 //   warp 1          loader: claims work items (heaviest first) and brings each tile's blob
 //                   into one of its blob slots with one bulk copy
-//   warps 2,3,12-15 producers: stage g (counted over the CTA's tiles) is built by producer
-//                   g % 6 into stage slot g % kMmaStages
+//   warps 2,3,12.. producers: stage g (counted over the CTA's tiles) is built by producer
+//                   g % producers into stage slot g % stages
 //   warps 4-11      epilogue: warp w reads TMEM lanes 32 (w % 4) + 0..31 (= frames) and half
 //                   of the tile's bins (8 bins x 5 accumulators at a time), recombines, puts the
 //                   cake values into a shared-memory image holding two adjacent tiles of the
@@ -54,23 +54,15 @@
 
 namespace mi {
 
-#ifndef MI_MMA_STAGES
-#define MI_MMA_STAGES 7
-#define MI_MMA_STEPS 1
-#endif
-constexpr int kMmaStages = MI_MMA_STAGES;
-constexpr int kMmaStepsPerStage = MI_MMA_STEPS;   // K steps (32 pixel slots each) per stage
-#ifndef MI_MMA_PRODUCERS
-#define MI_MMA_PRODUCERS 6
-#endif
-constexpr int kMmaProducers = MI_MMA_PRODUCERS;
-// A producer waits for its stage slot by the parity of the slot's empty barrier, which is sound
-// only while the barrier is at most one phase behind the waiter.  The producer of stage g has
-// seen stage g - producers - stages consumed; stage g - 2 stages must be: producers <= stages.
-static_assert(MI_MMA_PRODUCERS <= MI_MMA_STAGES, "more producers than stage slots aliases barrier phases");
+// Pipeline depth: the kernel is compiled for a few (stages, producer warps) pairs, chosen per
+// plan at launch (mi_plan_set_mma_pipeline; the autotuner times them); 7 stages and 6
+// producers by default.  A producer waits for its stage slot by the parity of the slot's
+// empty barrier, which is sound only while the barrier is at most one phase behind the
+// waiter.  The producer of stage g has seen stage g - producers - stages consumed; stage
+// g - 2 stages must be: producers <= stages.
+constexpr int kMmaStepsPerStage = 1;   // K steps (32 pixel slots each) per stage
 constexpr int kMmaEpiWarps = 8;
-constexpr int kMmaWarps = 2 + kMmaProducers + 8;   // MMA/TMEM, loader, producers, epilogue
-constexpr int kMmaThreads = kMmaWarps * 32;
+__host__ __device__ constexpr int mma_threads(int producers) { return (2 + producers + kMmaEpiWarps) * 32; }
 // per stage: A lo 4096 | A hi 4096 | B 6144 per K step
 constexpr uint32_t kMmaStageBytes = 14336u * kMmaStepsPerStage;
 constexpr uint32_t kMmaAHi = 4096u * kMmaStepsPerStage, kMmaB = 8192u * kMmaStepsPerStage;
@@ -115,16 +107,16 @@ struct MmaSmem {
   uint32_t off_out, off_blob, off_fac, off_shdr, off_btag, off_atag, off_bar, off_tmem, total;
 };
 
-__host__ __device__ inline MmaSmem mma_smem_layout(uint32_t blob_cap, int n_blob) {
+__host__ __device__ inline MmaSmem mma_smem_layout(uint32_t blob_cap, int n_blob, int stages) {
   MmaSmem L;
-  uint32_t o = (uint32_t)kMmaStages * kMmaStageBytes;
+  uint32_t o = (uint32_t)stages * kMmaStageBytes;
   L.off_out = o;   o += 2u * kMmaOutBytes;
   L.off_blob = o;  o += (uint32_t)n_blob * blob_cap;
   L.off_fac = o;   o += (uint32_t)kMmaFacSlots * kMmaFacBytes;
-  L.off_shdr = o;  o += (uint32_t)kMmaStages * sizeof(MmaTag);
+  L.off_shdr = o;  o += (uint32_t)stages * sizeof(MmaTag);
   L.off_btag = o;  o += (uint32_t)kMmaBlobSlotsMax * sizeof(MmaTag);
   L.off_atag = o;  o += 2u * sizeof(MmaTag);
-  L.off_bar = o;   o += 8u * (2u * kMmaStages + 2u * kMmaBlobSlotsMax + 2u * kMmaFacSlots + 4u);
+  L.off_bar = o;   o += 8u * (2u * stages + 2u * kMmaBlobSlotsMax + 2u * kMmaFacSlots + 4u);
   L.off_tmem = o;  o += 16u;
   L.total = o + 1024u;   // the base is rounded up to 1024 bytes inside the kernel
   return L;
@@ -143,12 +135,14 @@ __device__ __forceinline__ void m_mma(uint32_t d_tmem, uint64_t adesc, uint64_t 
       "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n" ::"r"(d_tmem),
       "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate), "r"(0u), "r"(0u), "r"(0u), "r"(0u));
 }
-__global__ void __launch_bounds__(kMmaThreads, 1) k_mma(const __grid_constant__ MmaArgs a) {
+template <int kMmaStages, int kMmaProducers>
+__global__ void __launch_bounds__(mma_threads(kMmaProducers), 1) k_mma(const __grid_constant__ MmaArgs a) {
+  static_assert(kMmaProducers <= kMmaStages, "more producers than stage slots aliases barrier phases");
   extern __shared__ uint8_t smem_raw[];
   // 1024-byte aligned base: the swizzled A operand's atoms start on 1024-byte boundaries
   const uint32_t raw = m_smem(smem_raw);
   uint8_t *smem = smem_raw + (((raw + 1023u) & ~1023u) - raw);
-  const MmaSmem L = mma_smem_layout(a.blob_cap, a.n_blob);
+  const MmaSmem L = mma_smem_layout(a.blob_cap, a.n_blob, kMmaStages);
   const int NB = a.n_blob;
   MmaTag *s_shdr = (MmaTag *)(smem + L.off_shdr);
   MmaTag *s_btag = (MmaTag *)(smem + L.off_btag);
@@ -583,6 +577,26 @@ __global__ void k_mma_dark(const TileRef *tiles, uint8_t *blobs, const int32_t *
   dk[n] = fac[n] * d;
 }
 
+// the compiled (stages, producers) pairs
+static constexpr int kMmaPipelines[][2] = {{7, 6}, {6, 6}, {5, 5}, {7, 7}, {4, 4}};
+
+template <int S, int P>
+static int launch_mma_t(int grid, uint32_t smem, const MmaArgs &a, cudaStream_t s) {
+  MI_CUDA(cudaFuncSetAttribute(k_mma<S, P>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  k_mma<S, P><<<grid, mma_threads(P), smem, s>>>(a);
+  MI_CUDA(cudaGetLastError());
+  return MI_OK;
+}
+
+static int launch_mma_variant(int S, int P, int grid, uint32_t smem, const MmaArgs &a, cudaStream_t s) {
+  if (S == 7 && P == 6) return launch_mma_t<7, 6>(grid, smem, a, s);
+  if (S == 6 && P == 6) return launch_mma_t<6, 6>(grid, smem, a, s);
+  if (S == 5 && P == 5) return launch_mma_t<5, 5>(grid, smem, a, s);
+  if (S == 7 && P == 7) return launch_mma_t<7, 7>(grid, smem, a, s);
+  if (S == 4 && P == 4) return launch_mma_t<4, 4>(grid, smem, a, s);
+  return set_error(MI_E_UNSUPPORTED, "launch_mma: no kernel for %d stages and %d producers", S, P);
+}
+
 int launch_mma(Plan *p, int F, float *cake, double *partial, bool want_lo, cudaStream_t s) {
   if (F <= 0 || F > kMmaFrames) return set_error(MI_E_ARG, "launch_mma: %d frames (1..%d)", F, kMmaFrames);
   MmaArgs a;
@@ -618,17 +632,21 @@ int launch_mma(Plan *p, int F, float *cake, double *partial, bool want_lo, cudaS
   // holds one, the producers use the next)
   int dev_smem = 0;
   MI_CUDA(cudaDeviceGetAttribute(&dev_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, p->device));
+  const int S = p->mma_stages;
   a.n_blob = kMmaBlobSlotsMax;
-  while (a.n_blob > 2 && mma_smem_layout(a.blob_cap, a.n_blob).total > (uint32_t)dev_smem) --a.n_blob;
-  const MmaSmem L = mma_smem_layout(a.blob_cap, a.n_blob);
+  while (a.n_blob > 2 && mma_smem_layout(a.blob_cap, a.n_blob, S).total > (uint32_t)dev_smem) --a.n_blob;
+  const MmaSmem L = mma_smem_layout(a.blob_cap, a.n_blob, S);
   if (L.total > (uint32_t)dev_smem)
     return set_error(MI_E_RANGE, "launch_mma: %u B of shared memory needed (device allows %d)", L.total, dev_smem);
-  MI_CUDA(cudaFuncSetAttribute(k_mma, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.total));
   MI_CUDA(cudaMemsetAsync(p->d_ctr, 0, sizeof(int), s));
   const int grid = std::max(1, std::min(p->n_items, p->n_sms));
-  k_mma<<<grid, kMmaThreads, L.total, s>>>(a);
-  MI_CUDA(cudaGetLastError());
-  return MI_OK;
+  return launch_mma_variant(p->mma_stages, p->mma_producers, grid, L.total, a, s);
+}
+
+bool mma_pipeline_supported(int stages, int producers) {
+  for (const auto &v : kMmaPipelines)
+    if (v[0] == stages && v[1] == producers) return true;
+  return false;
 }
 
 int launch_mma_dark(Plan *p, cudaStream_t s) {

@@ -1696,6 +1696,18 @@ int mi_plan_set_dark(mi_plan *p, const float *dark) {
   return rc;
 }
 
+int mi_plan_set_mma_pipeline(mi_plan *p, int stages, int producers) {
+  if (!p) return set_error(MI_E_ARG, "mi_plan_set_mma_pipeline: null plan");
+  if (p->encoding != MI_ENC_MMA)
+    return set_error(MI_E_UNSUPPORTED, "mi_plan_set_mma_pipeline: the plan does not use the MMA encoding");
+  if (!mma_pipeline_supported(stages, producers))
+    return set_error(MI_E_UNSUPPORTED, "mi_plan_set_mma_pipeline: no kernel for %d stages and %d producers "
+                                       "(7/6, 6/6, 5/5, 7/7, 4/4)", stages, producers);
+  p->mma_stages = stages;
+  p->mma_producers = producers;
+  return MI_OK;
+}
+
 int mi_plan_set_bin_mask(mi_plan *p, const uint8_t *mask) {
   if (!p) return set_error(MI_E_ARG, "mi_plan_set_bin_mask: null plan");
   if (p->semantics != MI_SEM_OMP)
