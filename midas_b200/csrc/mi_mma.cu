@@ -480,16 +480,32 @@ __global__ void __launch_bounds__(mma_threads(kMmaProducers), 1) k_mma(const __g
         }
         // bins outside the tile have fac = dk = lw = 0: no branches
         float o[8];
+        double fv[8], dv[8];
+        float lv[8];
+#pragma unroll
+        for (int i = 0; i < 8; i += 2) {
+          const double2 f2 = *(const double2 *)(bfac + 8 * c + i), d2 = *(const double2 *)(bdk + 8 * c + i);
+          fv[i] = f2.x; fv[i + 1] = f2.y; dv[i] = d2.x; dv[i + 1] = d2.y;
+        }
+#pragma unroll
+        for (int i = 0; i < 8; i += 4) {
+          const float4 l4 = *(const float4 *)(blw + 8 * c + i);
+          lv[i] = l4.x; lv[i + 1] = l4.y; lv[i + 2] = l4.z; lv[i + 3] = l4.w;
+        }
+        double rw[8], rs[8];
 #pragma unroll
         for (int i = 0; i < 8; ++i) {
-          const int lrow = (8 * c + i) / kMmaCols;
-          // sum_k 2^(8k) acc_k exactly in int64 (|sum| < 2^63), one rounding to FP64
           const double v = m_acc5(r[0][i], r[1][i], r[2][i], r[3][i], r[4][i]);
-          const double res = fma(bfac[8 * c + i], v, -bdk[8 * c + i]);
-          const float l = blw[8 * c + i];
+          const double res = fma(fv[i], v, -dv[i]);
           o[i] = (float)res;
-          saw[lrow] = fma(res, (double)l, saw[lrow]);
-          ssm[lrow] += (l > 0.0f) ? res : 0.0;
+          rw[i] = res * (double)lv[i];
+          rs[i] = (lv[i] > 0.0f) ? res : 0.0;
+        }
+#pragma unroll
+        for (int q = 0; q < 2; ++q) {
+          const int lrow = (8 * c) / kMmaCols + q;
+          saw[lrow] += (rw[4 * q] + rw[4 * q + 1]) + (rw[4 * q + 2] + rw[4 * q + 3]);
+          ssm[lrow] += (rs[4 * q] + rs[4 * q + 1]) + (rs[4 * q + 2] + rs[4 * q + 3]);
         }
         if (!a.use_tma && live && a.want_cake) {
 #pragma unroll
