@@ -73,6 +73,7 @@ def parse():
     ap.add_argument("--no-graph", action="store_true", help="skip the CUDA-graph replay of the batched step")
     ap.add_argument("--autotune", action="store_true", help="time candidate tile shapes / run lengths first")
     ap.add_argument("--mma-pipeline", default="", help="stages,producers of the tensor-core kernel (e.g. 6,6)")
+    ap.add_argument("--no-sum", action="store_true", help="skip the SumImages sweep and its all-reduce")
     ap.add_argument("--panel-frames", type=int, default=256)
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--serve-seconds", type=float, default=10.0,
@@ -448,6 +449,32 @@ def main_ours(args):
                         "ms_per_step": round(gms / args.steps, 4), "graphs": n_batches,
                         "nodes_per_graph": "memset + k_xc + caking kernel per 128 frames, k_lineout"}
         del graphs
+
+    # ---- SumImages over the sweep (midas_b200.sweep): every resident batch caked with its
+    # cakes added to an FP64 running sum, then the sum all-reduced over the ranks (the path's
+    # one collective; a no-op at N = 1)
+    if not args.no_sum:
+        from midas_b200.sweep import SweepSum
+        ssum = SweepSum(plan)
+        plan.integrate(frames[:F], out=bufs, sum_into=ssum.total)     # warm-up
+        ssum.total.zero_()
+        torch.cuda.synchronize()
+        s0, s1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s0.record(stream)
+        for b in range(n_batches):
+            ssum.add(plan, frames[b * F:(b + 1) * F], out=bufs)
+        s1.record(stream)
+        torch.cuda.synchronize()
+        sms = dist_max(s0.elapsed_time(s1), world)
+        barrier(world)
+        r0 = time.perf_counter()
+        total = ssum.reduce()
+        torch.cuda.synchronize()
+        red_ms = dist_max((time.perf_counter() - r0) * 1e3, world)
+        out["sum_images"] = {"frames_summed": world * ssum.frames, "ms_per_batch_with_sum": round(sms / n_batches, 4),
+                             "all_reduce_ms": round(red_ms, 3), "all_reduce_bytes": total.numel() * 8,
+                             "sum_of_sum": float(total.sum().item())}
+        del ssum, total
 
     # ---- plain one-frame-per-launch kernel (reference GPU algorithm) on the same frames
     if not args.no_plain:

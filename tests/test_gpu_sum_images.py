@@ -55,3 +55,25 @@ def test_sum_skips_nan_bins_and_checks_arguments(cuda):
         plan.integrate(img, sum_into=acc.float())
     with pytest.raises(ValueError):
         plan.integrate(img, cake=False, sum_into=acc)
+
+
+def test_sweep_sum_over_batches_matches_one_launch(cuda):
+    """SweepSum over batches of a sweep equals the sum of one launch's cakes (FP64), and its
+    reduce is a no-op without a process group."""
+    from midas_b200.sweep import SweepSum
+    g = load_mapper_case("m1")
+    n_r, n_eta = g["r_lo"].size, g["eta_lo"].size
+    pm = from_arrays(g["records"], g["nmap"])
+    plan = CakePlan(pm, n_r=n_r, n_eta=n_eta, n_pixels_y=g["ny"], n_pixels_z=g["nz"], mode="bilinear",
+                    bc_y=g["bc_y"], bc_z=g["bc_z"], device=cuda, encoding="mma")
+    rng = np.random.default_rng(8)
+    frames = torch.from_numpy(np.clip(np.rint(g["image"][None] * rng.uniform(1, 50, size=(9, 1, 1))), 0,
+                                      65535).astype(np.uint16)).to(cuda)
+    s = SweepSum(plan)
+    for a, b in ((0, 4), (4, 9)):
+        s.add(plan, frames[a:b])
+    ck, _, _ = plan.integrate(frames)
+    want = ck.double().sum(0).reshape(-1)
+    got = s.reduce()
+    assert s.frames == 9
+    torch.testing.assert_close(got, want, rtol=1e-12, atol=1e-9)
