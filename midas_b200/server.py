@@ -361,9 +361,16 @@ class DeviceBackend:
             self._upload(st, s, 0, n, strm)
             self._device_work(st, cfg, s, n, strm)       # warm-up: kernels loaded, attributes set
         strm.synchronize()
+        # capture_begin / capture_end directly: the torch.cuda.graph context would first
+        # synchronise the device and empty the device and pinned-host caches (frees, which
+        # stall every thread's CUDA calls) while the other streams are being served
         g = torch.cuda.CUDAGraph()
-        with torch.cuda.graph(g, stream=strm, capture_error_mode="thread_local"):
-            self._device_work(st, cfg, s, n, strm)
+        with torch.cuda.stream(strm):
+            g.capture_begin(capture_error_mode="thread_local")
+            try:
+                self._device_work(st, cfg, s, n, strm)
+            finally:
+                g.capture_end()
         strm.synchronize()
         self.launches = launches
         return g
