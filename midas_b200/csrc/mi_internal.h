@@ -258,6 +258,7 @@ constexpr int kMmaN = kMmaRows * kMmaCols;  // 48 bins: the N of every MMA
 constexpr int kMmaFrames = 128;        // frames per launch: the M of every MMA
 constexpr int kMmaKStep = 32;          // K slots (staged pixels) per MMA step
 constexpr uint32_t kMmaEmpty = 0xFFFFFFFFu;
+constexpr int kMmaDarkWarps = 8;       // warps of the dark-term kernels (48 bins: 6 per warp)
 constexpr int kMmaMaxBinTerms = 16000; // int32 accumulators: 2 x 255 x 128 per term
 // Tensor-core weights: q = round(w / max|w|(bin) x kMmaQMax), |q| <= kMmaQMax, written as four
 // balanced base-256 digits d_k in [-128, 127] (q = sum_k 256^k d_k), one s8 byte plane each:

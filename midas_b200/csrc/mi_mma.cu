@@ -561,8 +561,7 @@ __global__ void __launch_bounds__(mma_threads(kMmaProducers), 1) k_mma(const __g
 }
 
 // dark term of each bin: dk = fac * sum over the bin's terms of q * dark[pixel], written into
-// the tile's blob; one block per tile, thread n summing bin n's terms in blob order
-// (deterministic)
+// the tile's blob; one block per tile, one warp per six bins (deterministic order)
 __global__ void k_mma_dark(const TileRef *tiles, uint8_t *blobs, const int32_t *xc_pix, const float *dark,
                            int has_dark) {
   const TileRef tr = tiles[blockIdx.x];
@@ -572,15 +571,20 @@ __global__ void k_mma_dark(const TileRef *tiles, uint8_t *blobs, const int32_t *
   const uint2 *runs = (const uint2 *)(blob + BL.runs);
   const uint32_t *rptr = (const uint32_t *)(blob + BL.run_ptr);
   const uint2 *terms = (const uint2 *)(blob + BL.terms);
-  const int n = threadIdx.x;
-  if (n >= kMmaN) return;
+  // warp w sums the terms of bins w, w + 8, ..., its lanes striding over the tile's terms,
+  // then reduces over the lanes in a fixed order: the same dark gives the same dk bits
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  constexpr int kW = kMmaDarkWarps, kPer = kMmaN / kMmaDarkWarps;
   const double *fac = (const double *)(blob + kMmaBinsOff);
   double *dk = (double *)(blob + kMmaBinsOff) + kMmaN;
-  double d = 0.0;
+  double d[kPer];
+#pragma unroll
+  for (int i = 0; i < kPer; ++i) d[i] = 0.0;
   if (has_dark)
-    for (int t = 0; t < hd.n_terms; ++t) {
+    for (int t = lane; t < hd.n_terms; t += 32) {
       const uint2 tm = terms[t];
-      if ((int)(tm.y >> 16) != n) continue;
+      const int n = (int)(tm.y >> 16);
+      if (n % kW != w) continue;
       // the term's pixel: the run of its K step that covers its slot
       const uint32_t k = tm.y & 0xFFFFu, s = k / kMmaKStep, kk = k % kMmaKStep;
       uint32_t c = 0;
@@ -588,9 +592,17 @@ __global__ void k_mma_dark(const TileRef *tiles, uint8_t *blobs, const int32_t *
         const uint32_t k0 = runs[r].y & 0xFFu, len = runs[r].y >> 8;
         if (kk >= k0 && kk < k0 + len) { c = runs[r].x + (kk - k0); break; }
       }
-      d += (double)mma_digits_value(tm.x) * (double)dark[xc_pix[c]];
+      const double v = (double)mma_digits_value(tm.x) * (double)dark[xc_pix[c]];
+#pragma unroll
+      for (int i = 0; i < kPer; ++i)
+        if (n / kW == i) d[i] += v;
     }
-  dk[n] = fac[n] * d;
+#pragma unroll
+  for (int i = 0; i < kPer; ++i) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) d[i] += __shfl_xor_sync(0xffffffffu, d[i], o);
+    if (lane == 0) dk[w + kW * i] = fac[w + kW * i] * d[i];
+  }
 }
 
 // the compiled (stages, producers) pairs
@@ -667,7 +679,8 @@ bool mma_pipeline_supported(int stages, int producers) {
 
 int launch_mma_dark(Plan *p, cudaStream_t s) {
   if (p->n_tiles == 0) return MI_OK;
-  k_mma_dark<<<(unsigned)p->n_tiles, 64, 0, s>>>(p->d_tiles, p->d_blobs, p->d_xc_pix, p->d_dark, p->has_dark);
+  k_mma_dark<<<(unsigned)p->n_tiles, 32 * kMmaDarkWarps, 0, s>>>(p->d_tiles, p->d_blobs, p->d_xc_pix, p->d_dark,
+                                                                  p->has_dark);
   MI_CUDA(cudaGetLastError());
   return MI_OK;
 }

@@ -621,7 +621,7 @@ __global__ void __launch_bounds__(kDThreads, 1) k_mmad(const __grid_constant__ M
 }
 
 // dark term of each bin: dk = fac * sum over the bin's terms of q * dark[pixel], written into
-// the tile's blob; one block per tile, thread n summing bin n's terms in blob order
+// the tile's blob; one block per tile, one warp per six bins (deterministic order)
 __global__ void k_mmad_dark(const TileRef *tiles, uint8_t *blobs, int ny, const float *dark, int has_dark) {
   const TileRef tr = tiles[blockIdx.x];
   uint8_t *blob = blobs + tr.off;
@@ -629,20 +629,33 @@ __global__ void k_mmad_dark(const TileRef *tiles, uint8_t *blobs, int ny, const 
   const MmadBlob BL = mmad_blob_layout(hd.n_k, hd.n_terms);
   const uint32_t *gran = (const uint32_t *)(blob + BL.gran);
   const uint2 *terms = (const uint2 *)(blob + BL.terms);
-  const int n = threadIdx.x;
-  if (n >= kMmaN) return;
+  // warp w sums the terms of bins w, w + 8, ..., its lanes striding over the tile's terms,
+  // then reduces over the lanes in a fixed order: the same dark gives the same dk bits
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  constexpr int kW = kMmaDarkWarps, kPer = kMmaN / kMmaDarkWarps;
   const double *fac = (const double *)(blob + kMmaBinsOff);
   double *dk = (double *)(blob + kMmaBinsOff) + kMmaN;
-  double d = 0.0;
+  double d[kPer];
+#pragma unroll
+  for (int i = 0; i < kPer; ++i) d[i] = 0.0;
   if (has_dark)
-    for (int t = 0; t < hd.n_terms; ++t) {
+    for (int t = lane; t < hd.n_terms; t += 32) {
       const uint2 tm = terms[t];
-      if ((int)(tm.y >> 16) != n) continue;
+      const int n = (int)(tm.y >> 16);
+      if (n % kW != w) continue;
       const uint32_t k = tm.y & 0xFFFFu, g = gran[k / kMmadGranPx];
       const size_t px = (size_t)(g & 0xFFFFu) * (size_t)ny + (g >> 16) + (k % kMmadGranPx);
-      d += (double)mma_digits_value(tm.x) * (double)dark[px];
+      const double v = (double)mma_digits_value(tm.x) * (double)dark[px];
+#pragma unroll
+      for (int i = 0; i < kPer; ++i)
+        if (n / kW == i) d[i] += v;
     }
-  dk[n] = fac[n] * d;
+#pragma unroll
+  for (int i = 0; i < kPer; ++i) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) d[i] += __shfl_xor_sync(0xffffffffu, d[i], o);
+    if (lane == 0) dk[w + kW * i] = fac[w + kW * i] * d[i];
+  }
 }
 
 int launch_mmad(Plan *p, const void *frames, int dtype, int F, int64_t stride, float *cake, double *partial,
@@ -704,7 +717,8 @@ int launch_mmad(Plan *p, const void *frames, int dtype, int F, int64_t stride, f
 
 int launch_mmad_dark(Plan *p, cudaStream_t s) {
   if (p->n_tiles == 0) return MI_OK;
-  k_mmad_dark<<<(unsigned)p->n_tiles, 64, 0, s>>>(p->d_tiles, p->d_blobs, p->ny, p->d_dark, p->has_dark);
+  k_mmad_dark<<<(unsigned)p->n_tiles, 32 * kMmaDarkWarps, 0, s>>>(p->d_tiles, p->d_blobs, p->ny, p->d_dark,
+                                                                   p->has_dark);
   MI_CUDA(cudaGetLastError());
   return MI_OK;
 }
