@@ -144,6 +144,12 @@ def measured_peak():
 
 
 # ---------------------------------------------------------------------------
+def csr_map_bytes(info) -> int:
+    """The map's algorithmic bytes: its CSR of the mode's coalesced terms (4 B column + 4 B
+    weight each), n_bins + 1 row pointers and n_bins areas, 4 B each."""
+    return int(info["nnz"]) * 8 + (int(info["n_bins"]) + 1) * 4 + int(info["n_bins"]) * 4
+
+
 def dist_setup(args):
     import torch
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -383,10 +389,12 @@ def main_ours(args):
     else:
         launches = args.steps * 2 * len(groups)
 
-    # ---- roofline of the batched launch: A(F) = map bytes + F * frame bytes
+    # ---- roofline of the batched launch: A(F) = map bytes + F * frame bytes, the map counted as
+    # its CSR (nnz x (4 B column + 4 B weight) + (n_bins + 1) x 4 B row pointers + n_bins x 4 B
+    # area), whatever encoding the plan keeps it in
     peak, peak_kind = measured_peak()
     frame_bytes = ny * nz * 2
-    map_bytes = info["map_bytes"]
+    map_bytes = csr_map_bytes(info)
     alg = map_bytes + F * frame_bytes
     mean_step_s = sum(step_ms) / len(step_ms) / 1e3
     achieved = alg / mean_step_s / 1e9
@@ -413,7 +421,8 @@ def main_ours(args):
                       "encoding": enc,
                       "mma_pipeline": list(pipeline) if pipeline else ([7, 6] if enc == "mma" else None),
                       "run_len": info["run_len"], "staged_pixels_per_frame": info["staged_pixels"],
-                      "referenced_pixels": info["ref_pixels"], "map_bytes": info["map_bytes"],
+                      "referenced_pixels": info["ref_pixels"], "map_bytes": map_bytes,
+                      "plan_map_bytes_read": info["map_bytes"],
                       "l2": "inputs larger than L2: each step reads a new %.1f GB batch" % (F * frame_bytes / 1e9),
                       "parallelism": f"replicas{world}"},
            "roofline": roofline, "gpu_launches": launches,
@@ -761,7 +770,7 @@ def panel_bench(args, dev, reps=3):
            "map_records": [int(pm.n_entries) for pm in maps], "frames_per_panel": F,
            "ms_per_batch": round(ms, 3), "frame_sets_per_s": round(F / (ms / 1e3), 1),
            "panel_frames_per_s": round(len(ws) * F / (ms / 1e3), 1),
-           "alg_gb_s": round((info["map_bytes"] + F * frame_bytes) / (ms / 1e3) / 1e9, 1),
+           "alg_gb_s": round((csr_map_bytes(info) + F * frame_bytes) / (ms / 1e3) / 1e9, 1),
            "staging": "fp32 pixel-major (the int32 panel); one run-kernel launch per 64 frames for all panels",
            "setup_s": {"maps_gpu": round(t_map, 2), "plan_build": round(t_plan, 2)}}
     sample = (ws, maps, [f[0].cpu().numpy() for f in frames], darks, ck[0].cpu().numpy().reshape(-1),
@@ -902,7 +911,7 @@ def f_sweep(plan, frames, bufs, F_max, info, w, args, world, peak, steps=10):
         e1.record(stream)
         torch.cuda.synchronize()
         ms = dist_max(e0.elapsed_time(e1), world) / steps
-        alg = info["map_bytes"] + F * ny * nz * 2
+        alg = csr_map_bytes(info) + F * ny * nz * 2
         out[str(F)] = {"frames_per_s": round(world * F / (ms / 1e3), 1), "ms_per_launch": round(ms, 4),
                        "roofline_frac": round(alg / (ms / 1e3) / 1e9 / peak, 4),
                        "alg_bytes_per_launch": alg}
