@@ -244,8 +244,13 @@ struct XcChunk {
 //                                       per byte plane); slot k holds a pixel with
 //                                       c % 8 == k % 8 (the swizzle phase of its row)
 //   uint32 run_ptr[n_k + 1]             runs of K step s: [run_ptr[s], run_ptr[s+1])
-//   uint32 step_ptr[n_k + 1]            terms of K step s
-//   uint2  terms[n_terms]               {mma_digits(q), k | n << 16}, sorted by k
+//   uint32 step_ptr[n_k + 1]            words of K step s
+//   uint4  wpl[n_words]                 a bin's weights in four consecutive K slots 4w .. 4w+3
+//                                       of a step: one 32-bit word per digit plane (plane j
+//                                       in .x/.y/.z/.w, slot 4w + b in byte b; 0 where the bin
+//                                       has no term)
+//   uint16 widx[n_words]                w (0..7, within the step) | n << 3, words sorted by
+//                                       step (n_terms of the header counts the words)
 struct MmaHdr {
   int32_t n_rows, n_cols, r0, e0, n_k, n_terms;
   int32_t box_rows;   // rows of the item's sub-band (12, 6, 3 or 1): the cake store's box height
@@ -285,21 +290,22 @@ __host__ __device__ inline int64_t mma_digits_value(uint32_t packed) {
   for (int k = 3; k >= 0; --k) q = q * 256 + (int8_t)(uint8_t)(packed >> (8 * k));
   return q;
 }
-constexpr uint32_t kMmaBlobCap = 24 * 1024;  // largest tile blob (blob slots in shared memory)
+constexpr uint32_t kMmaBlobCap = 28 * 1024;  // largest tile blob (blob slots in shared memory)
 constexpr uint32_t kMmaBinsOff = 32;   // fac, dk, lw after the header
 constexpr uint32_t kMmaBinsBytes = kMmaN * (8 + 8 + 4);
 
 struct MmaBlob {
-  uint32_t runs, run_ptr, step_ptr, terms, bytes;
+  uint32_t runs, run_ptr, step_ptr, wpl, widx, bytes;
 };
-__host__ __device__ inline MmaBlob mma_blob_layout(int n_k, int n_runs, int n_terms) {
+__host__ __device__ inline MmaBlob mma_blob_layout(int n_k, int n_runs, int n_words) {
   auto a16 = [](uint32_t x) { return (x + 15u) & ~15u; };
   MmaBlob b;
   uint32_t o = a16(kMmaBinsOff + kMmaBinsBytes);
   b.runs = o;     o = a16(o + 8u * (uint32_t)n_runs);
   b.run_ptr = o;  o = a16(o + 4u * (uint32_t)(n_k + 1));
   b.step_ptr = o; o = a16(o + 4u * (uint32_t)(n_k + 1));
-  b.terms = o;    o = a16(o + 8u * (uint32_t)n_terms);
+  b.wpl = o;      o = a16(o + 16u * (uint32_t)n_words);
+  b.widx = o;     o = a16(o + 2u * (uint32_t)n_words);
   b.bytes = o;
   return b;
 }

@@ -337,7 +337,8 @@ __global__ void __launch_bounds__(mma_threads(kMmaProducers), 1) k_mma(const __g
       const uint2 *runs = (const uint2 *)(blob + BL.runs);
       const uint32_t *rptr = (const uint32_t *)(blob + BL.run_ptr);
       const uint32_t *sp = (const uint32_t *)(blob + BL.step_ptr);
-      const uint2 *terms = (const uint2 *)(blob + BL.terms);
+      const uint4 *wpl = (const uint4 *)(blob + BL.wpl);
+      const uint16_t *widx = (const uint16_t *)(blob + BL.widx);
       const int n_st = (hd.n_k + kMmaStepsPerStage - 1) / kMmaStepsPerStage;
       for (int s2 = 0; s2 < n_st; ++s2, ++g) {
         if ((int)(g % kMmaProducers) != pw) continue;
@@ -375,25 +376,30 @@ __global__ void __launch_bounds__(mma_threads(kMmaProducers), 1) k_mma(const __g
         uint4 *bz = (uint4 *)(st + kMmaB);
         for (int i = lane; i < (int)(4u * kMmaBPlane / 16u); i += 32) bz[i] = make_uint4(0u, 0u, 0u, 0u);
         __syncwarp();
+        static_assert(kMmaStepsPerStage == 1, "weight words are indexed within one K step");
         const int t0 = (int)sp[s0], t1 = (int)sp[s1];
-        const uint32_t kbase = (uint32_t)(kMmaKStep * s0);
-        // four terms per lane loaded before any store: the terms and the planes share shared
+        // four words per lane loaded before any store: the words and the planes share shared
         // memory, so the compiler cannot hoist the next loads above the stores by itself
         for (int t = t0 + lane; t < t1; t += 4 * 32) {
-          uint2 tmv[4];
+          uint4 wv[4];
+          uint32_t wi[4];
 #pragma unroll
-          for (int u = 0; u < 4; ++u) tmv[u] = t + 32 * u < t1 ? terms[t + 32 * u] : make_uint2(0u, 0u);
+          for (int u = 0; u < 4; ++u) {
+            const bool in = t + 32 * u < t1;
+            wv[u] = in ? wpl[t + 32 * u] : make_uint4(0u, 0u, 0u, 0u);
+            wi[u] = in ? widx[t + 32 * u] : 0u;
+          }
 #pragma unroll
           for (int u = 0; u < 4; ++u) {
             if (t + 32 * u >= t1) break;
-            const uint2 tm = tmv[u];
-            const uint32_t kk = (tm.y & 0xFFFFu) - kbase, n = tm.y >> 16;
-            const uint32_t off = (n & 7u) * 16u + (n >> 3) * kMmaBSbo + (kk & 15u) + (kk >> 4) * 128u;
-            uint8_t *b0 = st + kMmaB + off;
-            b0[0] = (uint8_t)(tm.x & 0xFFu);
-            b0[kMmaBPlane] = (uint8_t)((tm.x >> 8) & 0xFFu);
-            b0[2 * kMmaBPlane] = (uint8_t)((tm.x >> 16) & 0xFFu);
-            b0[3 * kMmaBPlane] = (uint8_t)(tm.x >> 24);
+            // word w of bin n: slots 4w .. 4w+3, bytes (k % 16) + (k / 16) * 128 of row n
+            const uint32_t w = wi[u] & 7u, n = wi[u] >> 3;
+            const uint32_t off = (n & 7u) * 16u + (n >> 3) * kMmaBSbo + (w & 3u) * 4u + (w >> 2) * 128u;
+            uint32_t *b0 = (uint32_t *)(st + kMmaB + off);
+            b0[0] = wv[u].x;
+            b0[kMmaBPlane / 4] = wv[u].y;
+            b0[2 * kMmaBPlane / 4] = wv[u].z;
+            b0[3 * kMmaBPlane / 4] = wv[u].w;
           }
         }
         if (lane == 0) {
@@ -570,7 +576,9 @@ __global__ void k_mma_dark(const TileRef *tiles, uint8_t *blobs, const int32_t *
   const MmaBlob BL = mma_blob_layout(hd.n_k, hd.n_runs, hd.n_terms);
   const uint2 *runs = (const uint2 *)(blob + BL.runs);
   const uint32_t *rptr = (const uint32_t *)(blob + BL.run_ptr);
-  const uint2 *terms = (const uint2 *)(blob + BL.terms);
+  const uint32_t *sp = (const uint32_t *)(blob + BL.step_ptr);
+  const uint4 *wpl = (const uint4 *)(blob + BL.wpl);
+  const uint16_t *widx = (const uint16_t *)(blob + BL.widx);
   // warp w sums the terms of bins w, w + 8, ..., its lanes striding over the tile's terms,
   // then reduces over the lanes in a fixed order: the same dark gives the same dk bits
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
@@ -582,20 +590,28 @@ __global__ void k_mma_dark(const TileRef *tiles, uint8_t *blobs, const int32_t *
   for (int i = 0; i < kPer; ++i) d[i] = 0.0;
   if (has_dark)
     for (int t = lane; t < hd.n_terms; t += 32) {
-      const uint2 tm = terms[t];
-      const int n = (int)(tm.y >> 16);
+      const int n = (int)(widx[t] >> 3);
       if (n % kW != w) continue;
-      // the term's pixel: the run of its K step that covers its slot
-      const uint32_t k = tm.y & 0xFFFFu, s = k / kMmaKStep, kk = k % kMmaKStep;
-      uint32_t c = 0;
-      for (uint32_t r = rptr[s]; r < rptr[s + 1]; ++r) {
-        const uint32_t k0 = runs[r].y & 0xFFu, len = runs[r].y >> 8;
-        if (kk >= k0 && kk < k0 + len) { c = runs[r].x + (kk - k0); break; }
-      }
-      const double v = (double)mma_digits_value(tm.x) * (double)dark[xc_pix[c]];
+      // the word's K step: the step whose word range holds it
+      uint32_t s = 0;
+      while (sp[s + 1] <= (uint32_t)t) ++s;
+      const uint4 wv = wpl[t];
+      for (int b = 0; b < 4; ++b) {
+        const uint32_t dg = ((wv.x >> (8 * b)) & 0xFFu) | (((wv.y >> (8 * b)) & 0xFFu) << 8) |
+                            (((wv.z >> (8 * b)) & 0xFFu) << 16) | (((wv.w >> (8 * b)) & 0xFFu) << 24);
+        if (dg == 0u) continue;
+        // the slot's pixel: the run of the step that covers the slot
+        const uint32_t kk = (widx[t] & 7u) * 4u + (uint32_t)b;
+        uint32_t c = 0;
+        for (uint32_t r = rptr[s]; r < rptr[s + 1]; ++r) {
+          const uint32_t k0 = runs[r].y & 0xFFu, len = runs[r].y >> 8;
+          if (kk >= k0 && kk < k0 + len) { c = runs[r].x + (kk - k0); break; }
+        }
+        const double v = (double)mma_digits_value(dg) * (double)dark[xc_pix[c]];
 #pragma unroll
-      for (int i = 0; i < kPer; ++i)
-        if (n / kW == i) d[i] += v;
+        for (int i = 0; i < kPer; ++i)
+          if (n / kW == i) d[i] += v;
+      }
     }
 #pragma unroll
   for (int i = 0; i < kPer; ++i) {

@@ -736,16 +736,46 @@ static int mma_tile_blob(const HostCSR &csr, const mi_map_desc &m, const std::ve
         terms.push_back(make_uint2(mma_weight(csr.w[t], wm), (uint32_t)lut[csr.col[t]] | (n << 16)));
       }
     }
-  std::stable_sort(terms.begin(), terms.end(),
-                   [](const uint2 &x, const uint2 &y) { return (x.y & 0xFFFFu) < (y.y & 0xFFFFu); });
+  // words: a bin's terms in four consecutive slots 4w .. 4w+3 of a step, one 32-bit word per
+  // digit plane (the B operand's K-major rows hold those four bytes side by side), so the
+  // stage builders store a word where they would store up to four bytes; words in step order
+  // (by slot), then bank-ordered within each step like the terms they replace
+  std::stable_sort(terms.begin(), terms.end(), [](const uint2 &x, const uint2 &y) {
+    const uint32_t kx = (x.y & 0xFFFFu) / 4, ky = (y.y & 0xFFFFu) / 4;
+    return kx != ky ? kx < ky : (x.y >> 16) < (y.y >> 16);
+  });
+  std::vector<uint4> wpl;
+  std::vector<uint2> wkey;   // {word index, (k / 4) | n << 16} for bank ordering
+  for (size_t t = 0; t < terms.size();) {
+    const uint32_t kq = (terms[t].y & 0xFFFFu) / 4, n = terms[t].y >> 16;
+    uint4 wv = make_uint4(0u, 0u, 0u, 0u);
+    size_t u = t;
+    for (; u < terms.size() && (terms[u].y & 0xFFFFu) / 4 == kq && (terms[u].y >> 16) == n; ++u) {
+      const uint32_t b = (terms[u].y & 0xFFFFu) % 4, d = terms[u].x;
+      wv.x |= (d & 0xFFu) << (8 * b);
+      wv.y |= ((d >> 8) & 0xFFu) << (8 * b);
+      wv.z |= ((d >> 16) & 0xFFu) << (8 * b);
+      wv.w |= (d >> 24) << (8 * b);
+    }
+    wkey.push_back(make_uint2((uint32_t)wpl.size(), (kq * 4) | (n << 16)));
+    wpl.push_back(wv);
+    t = u;
+  }
   std::vector<uint32_t> sp(n_k + 1, 0);
-  for (const uint2 &t : terms) ++sp[(t.y & 0xFFFFu) / kMmaKStep + 1];
+  for (const uint2 &k : wkey) ++sp[(k.y & 0xFFFFu) / kMmaKStep + 1];
   for (int s = 0; s < n_k; ++s) sp[s + 1] += sp[s];
-  bank_order(terms, sp, n_k);
+  bank_order(wkey, sp, n_k);
+  std::vector<uint4> wpl_o(wpl.size());
+  std::vector<uint16_t> widx(wpl.size());
+  for (size_t i = 0; i < wkey.size(); ++i) {
+    wpl_o[i] = wpl[wkey[i].x];
+    const uint32_t k = wkey[i].y & 0xFFFFu, n = wkey[i].y >> 16;
+    widx[i] = (uint16_t)(((k % kMmaKStep) / 4) | (n << 3));
+  }
   for (int32_t q : pix) lut[q] = -1;
-  const MmaBlob L = mma_blob_layout(n_k, (int)runs.size(), (int)terms.size());
+  const MmaBlob L = mma_blob_layout(n_k, (int)runs.size(), (int)wpl_o.size());
   blob.assign(L.bytes, 0);
-  MmaHdr h{nr, nc, r0, e0, n_k, (int32_t)terms.size(), box_rows, (int32_t)runs.size()};
+  MmaHdr h{nr, nc, r0, e0, n_k, (int32_t)wpl_o.size(), box_rows, (int32_t)runs.size()};
   memcpy(blob.data(), &h, sizeof(h));
   memcpy(blob.data() + kMmaBinsOff, bfac, sizeof(bfac));
   memcpy(blob.data() + kMmaBinsOff + sizeof(bfac), bdk, sizeof(bdk));
@@ -753,7 +783,10 @@ static int mma_tile_blob(const HostCSR &csr, const mi_map_desc &m, const std::ve
   if (!runs.empty()) memcpy(blob.data() + L.runs, runs.data(), runs.size() * 8);
   memcpy(blob.data() + L.run_ptr, rptr.data(), rptr.size() * 4);
   memcpy(blob.data() + L.step_ptr, sp.data(), sp.size() * 4);
-  if (!terms.empty()) memcpy(blob.data() + L.terms, terms.data(), terms.size() * 8);
+  if (!wpl_o.empty()) {
+    memcpy(blob.data() + L.wpl, wpl_o.data(), wpl_o.size() * 16);
+    memcpy(blob.data() + L.widx, widx.data(), widx.size() * 2);
+  }
   *nnz_out = (int)terms.size();
   *nu_out = (int)pix.size();
   return MI_OK;
