@@ -34,11 +34,11 @@ METRIC = "caked_frames_per_s"
 # DRAM bytes (read + write) per 128-frame batch of the sweep_2880 workload: ncu
 # dram__bytes_read.sum + dram__bytes_write.sum of one launch of each kernel of the batch (the
 # transpose kernel k_xc plus the caking kernel of the encoding), summarised under profiles/; the
-# mma figures are of the kernels of commit fc01dae
+# mma figures are of the kernels of commit 6d0d9e4
 TRAFFIC = {"runs": {"bytes_per_step": int(0.840295e9 + 0.761555e9 + 1.830098e9 + 1.170938e9),
                     "kernels": "k_xc + k_runs"},
-           "mma": {"bytes_per_step": int(0.839755e9 + 0.763452e9 + 1.285888e9 + 0.860974e9),
-                   "kernels": "k_xc + k_mma", "commit": "fc01dae"}}
+           "mma": {"bytes_per_step": int(0.839898e9 + 0.762710e9 + 1.313836e9 + 0.861997e9),
+                   "kernels": "k_xc + k_mma", "commit": "6d0d9e4"}}
 SCOPE = {"runs": "whole batch: k_xc + k_runs + k_lineout (k_runs 88 %)",
          "mma": "whole batch: k_xc + k_mma + k_lineout",
          "mmad": "whole batch: k_mmad + k_lineout"}
