@@ -61,6 +61,7 @@ def parse():
                     help="tile encoding of the batched plan (mma: tensor cores, the default for these u16 sweeps)")
     ap.add_argument("--run-len", type=int, default=0)
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-e2e-cake", action="store_true", help="skip the end-to-end run that returns the cakes")
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-check", action="store_true")
@@ -504,6 +505,9 @@ def main_ours(args):
     # ---- end to end through the public API: pinned host frames -> cake + lineouts -> host lineouts
     if not args.no_e2e:
         out["e2e"] = e2e_rate(plan, frames, F, args, w, dev, world)
+        # the same with the cakes returned to host memory (the reference's Write2D consumer)
+        if rank == 0 and world == 1 and not args.no_e2e_cake:
+            out["e2e_with_cake"] = e2e_rate(plan, frames, F, args, w, dev, 1, with_cake=True)
 
     # ---- ring fits of every resident frame: all rings in one launch, PV and TCH
     fit_sample = None
@@ -997,39 +1001,53 @@ def fit_accuracy(sample):
     return out
 
 
-def e2e_rate(plan, frames, F, args, w, dev, world):
+def e2e_rate(plan, frames, F, args, w, dev, world, with_cake=False):
     """Host (pinned) frames -> H2D of the referenced pixels (CakePlan.upload) -> batched
     caking -> D2H lineouts, double-buffered on two streams so the copy of batch i+1 overlaps
-    the caking of batch i."""
+    the caking of batch i.  with_cake: the float32 cakes come back too (the reference's
+    Write2D output), on a third stream from a double-buffered device cake."""
     import torch
     nz, ny = w.shape
     pool = min(frames.shape[0], 2 * F)
     host = torch.empty((pool, nz, ny), dtype=torch.uint16, pin_memory=True)
     host.copy_(frames[:pool].cpu())
     dbuf = [torch.empty((F, nz, ny), dtype=torch.uint16, device=dev) for _ in range(2)]
-    cake = torch.empty((F, w.n_r, w.n_eta), dtype=torch.float32, device=dev)
+    cakes = [torch.empty((F, w.n_r, w.n_eta), dtype=torch.float32, device=dev) for _ in range(2 if with_cake else 1)]
+    h_cake = [torch.empty((F, w.n_r, w.n_eta), dtype=torch.float32, pin_memory=True) for _ in range(2)] \
+        if with_cake else None
     aw = torch.empty((F, w.n_r), dtype=torch.float64, device=dev)
     sm = torch.empty((F, w.n_r), dtype=torch.float64, device=dev)
     h_aw = torch.empty((2, F, w.n_r), dtype=torch.float64, pin_memory=True)
     h_sm = torch.empty((2, F, w.n_r), dtype=torch.float64, pin_memory=True)
-    cs, ks = torch.cuda.Stream(dev), torch.cuda.Stream(dev)
+    cs, ks, ds = torch.cuda.Stream(dev), torch.cuda.Stream(dev), torch.cuda.Stream(dev)
     copied = [torch.cuda.Event() for _ in range(2)]
     done = [torch.cuda.Event() for _ in range(2)]
+    caked = [torch.cuda.Event() for _ in range(2)]
+    back = [torch.cuda.Event() for _ in range(2)]
     nb = pool // F
 
     def run(n):
         for i in range(n):
             s = i % 2
+            cake = cakes[s % len(cakes)]
             with torch.cuda.stream(cs):
                 cs.wait_event(done[s])
                 plan.upload(host[(i % nb) * F:(i % nb + 1) * F], dbuf[s], stream=cs)
                 copied[s].record(cs)
             with torch.cuda.stream(ks):
                 ks.wait_event(copied[s])
+                if with_cake:
+                    ks.wait_event(back[s])              # the cake buffer's previous copy is out
                 plan.integrate(dbuf[s], out={"cake": cake, "lineout_aw": aw, "lineout_sm": sm}, stream=ks)
                 h_aw[s].copy_(aw, non_blocking=True)
                 h_sm[s].copy_(sm, non_blocking=True)
                 done[s].record(ks)
+                caked[s].record(ks)
+            if with_cake:
+                with torch.cuda.stream(ds):
+                    ds.wait_event(caked[s])
+                    h_cake[s].copy_(cake, non_blocking=True)
+                    back[s].record(ds)
         torch.cuda.synchronize()
 
     run(max(2, args.warmup))
@@ -1038,7 +1056,7 @@ def e2e_rate(plan, frames, F, args, w, dev, world):
     a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     a.record(cs)
     run(args.steps)
-    b.record(ks)
+    b.record(ds if with_cake else ks)
     torch.cuda.synchronize()
     wall = time.perf_counter() - t0
     dev_ms = dist_max(a.elapsed_time(b), world)
@@ -1046,8 +1064,10 @@ def e2e_rate(plan, frames, F, args, w, dev, world):
     info = plan.info
     up = info["upload_pixels"]
     return {"value": round(rate, 1), "unit": UNIT, "h2d_bytes_per_step": F * up * 2,
-            "d2h_bytes_per_step": 2 * F * w.n_r * 8, "wall_s": round(wall, 3),
-            "pipeline": "2 streams, double-buffered H2D of the referenced columns of each 16-row "
+            "d2h_bytes_per_step": 2 * F * w.n_r * 8 + (F * w.n_r * w.n_eta * 4 if with_cake else 0),
+            "wall_s": round(wall, 3),
+            "pipeline": ("3 streams (cakes back on the third)" if with_cake else "2 streams")
+                        + ", double-buffered H2D of the referenced columns of each 16-row "
                         f"group of the referenced band ({info['ref_row_hi'] - info['ref_row_lo']} of {nz} "
                         f"rows, {up} of {nz * ny} pixels per frame)"}
 
