@@ -420,7 +420,7 @@ def main_ours(args):
                       "tile_rows": info["tile_rows"], "tile_pixels": info["tile_pixels"],
                       "frames_per_lane": info["frames_per_lane"],
                       "encoding": enc,
-                      "mma_pipeline": list(pipeline) if pipeline else ([7, 6] if enc == "mma" else None),
+                      "mma_pipeline": list(pipeline) if pipeline else ([8, 6] if enc == "mma" else None),
                       "run_len": info["run_len"], "staged_pixels_per_frame": info["staged_pixels"],
                       "referenced_pixels": info["ref_pixels"], "map_bytes": map_bytes,
                       "plan_map_bytes_read": info["map_bytes"],

@@ -228,8 +228,8 @@ int mi_selftest_wait(uint32_t polls, int arrive, int device, int *status);
  * integrator writes them (IntegratorZarrOMP.c:1766-1767).  NULL clears it. */
 int mi_plan_set_bin_mask(mi_plan *plan, const uint8_t *bin_mask);
 /* Pipeline depth of the MMA encoding's kernel (no counterpart in the reference): stage
- * slots and producer warps, one of the compiled pairs 7/6 (the default), 6/6, 5/5, 7/7,
- * 4/4; MI_E_UNSUPPORTED for other pairs or plans of other encodings.  Results are the same
+ * slots and producer warps, one of the compiled pairs 8/6 (the default), 7/6, 6/6, 5/5,
+ * 7/7, 4/4; MI_E_UNSUPPORTED for other pairs or plans of other encodings.  Results are the same
  * bit for bit; only the time differs (the autotuner times them per map). */
 int mi_plan_set_mma_pipeline(mi_plan *plan, int stages, int producers);
 

@@ -384,7 +384,7 @@ struct Plan {
   int *d_err = nullptr;          // device error word (bounded waits)
   int *d_ctr = nullptr;          // work-item counter of the persistent run kernel
   int n_sms = 0;
-  int mma_stages = 7, mma_producers = 6;   // pipeline of the MMA kernel (mi_plan_set_mma_pipeline)
+  int mma_stages = 8, mma_producers = 6;   // pipeline of the MMA kernel (mi_plan_set_mma_pipeline)
 
   // pixel-major staging (run encoding with 64-frame groups)
   int64_t n_xc = 0;              // compact pixels (0: not built)

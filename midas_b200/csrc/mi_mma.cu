@@ -55,7 +55,7 @@
 namespace mi {
 
 // Pipeline depth: the kernel is compiled for a few (stages, producer warps) pairs, chosen per
-// plan at launch (mi_plan_set_mma_pipeline; the autotuner times them); 7 stages and 6
+// plan at launch (mi_plan_set_mma_pipeline; the autotuner times them); 8 stages and 6
 // producers by default.  A producer waits for its stage slot by the parity of the slot's
 // empty barrier, which is sound only while the barrier is at most one phase behind the
 // waiter.  The producer of stage g has seen stage g - producers - stages consumed; stage
@@ -622,7 +622,7 @@ __global__ void k_mma_dark(const TileRef *tiles, uint8_t *blobs, const int32_t *
 }
 
 // the compiled (stages, producers) pairs
-static constexpr int kMmaPipelines[][2] = {{7, 6}, {6, 6}, {5, 5}, {7, 7}, {4, 4}};
+static constexpr int kMmaPipelines[][2] = {{8, 6}, {7, 6}, {6, 6}, {5, 5}, {7, 7}, {4, 4}};
 
 template <int S, int P>
 static int launch_mma_t(int grid, uint32_t smem, const MmaArgs &a, cudaStream_t s) {
@@ -638,6 +638,7 @@ static int launch_mma_variant(int S, int P, int grid, uint32_t smem, const MmaAr
   if (S == 5 && P == 5) return launch_mma_t<5, 5>(grid, smem, a, s);
   if (S == 7 && P == 7) return launch_mma_t<7, 7>(grid, smem, a, s);
   if (S == 4 && P == 4) return launch_mma_t<4, 4>(grid, smem, a, s);
+  if (S == 8 && P == 6) return launch_mma_t<8, 6>(grid, smem, a, s);
   return set_error(MI_E_UNSUPPORTED, "launch_mma: no kernel for %d stages and %d producers", S, P);
 }
 

@@ -1735,7 +1735,7 @@ int mi_plan_set_mma_pipeline(mi_plan *p, int stages, int producers) {
     return set_error(MI_E_UNSUPPORTED, "mi_plan_set_mma_pipeline: the plan does not use the MMA encoding");
   if (!mma_pipeline_supported(stages, producers))
     return set_error(MI_E_UNSUPPORTED, "mi_plan_set_mma_pipeline: no kernel for %d stages and %d producers "
-                                       "(7/6, 6/6, 5/5, 7/7, 4/4)", stages, producers);
+                                       "(8/6, 7/6, 6/6, 5/5, 7/7, 4/4)", stages, producers);
   p->mma_stages = stages;
   p->mma_producers = producers;
   return MI_OK;

@@ -162,11 +162,11 @@ class CakePlan:
             raise ValueError(f"bin mask has {m.size} entries, expected {self.n_r * self.n_eta}")
         L.check(L.lib().mi_plan_set_bin_mask(self._h, m.ctypes.data), "mi_plan_set_bin_mask")
 
-    MMA_PIPELINES = ((7, 6), (6, 6), (5, 5), (7, 7), (4, 4))
+    MMA_PIPELINES = ((8, 6), (7, 6), (6, 6), (5, 5), (7, 7), (4, 4))
 
     def set_mma_pipeline(self, stages: int, producers: int) -> None:
         """MMA encoding only: the tensor-core kernel's stage slots and producer warps, one of
-        ``MMA_PIPELINES`` (default 7 / 6).  Results are identical; only the time differs."""
+        ``MMA_PIPELINES`` (default 8 / 6).  Results are identical; only the time differs."""
         L.check(L.lib().mi_plan_set_mma_pipeline(self._h, int(stages), int(producers)), "mi_plan_set_mma_pipeline")
 
     # -- work ---------------------------------------------------------------
