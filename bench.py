@@ -38,7 +38,10 @@ METRIC = "caked_frames_per_s"
 TRAFFIC = {"runs": {"bytes_per_step": int(0.840295e9 + 0.761555e9 + 1.830098e9 + 1.170938e9),
                     "kernels": "k_xc + k_runs"},
            "mma": {"bytes_per_step": int(0.839898e9 + 0.762710e9 + 1.313836e9 + 0.861997e9),
-                   "kernels": "k_xc + k_mma", "commit": "6d0d9e4"}}
+                   "kernels": "k_xc + k_mma<7, 6>", "commit": "6d0d9e4",
+                   # the default 8-slot pipeline runs the same tiles, runs and blob reads; only
+                   # the number of stage slots in shared memory differs
+                   "pipeline_captured": [7, 6]}}
 SCOPE = {"runs": "whole batch: k_xc + k_runs + k_lineout (k_runs 88 %)",
          "mma": "whole batch: k_xc + k_mma + k_lineout",
          "mmad": "whole batch: k_mmad + k_lineout"}
